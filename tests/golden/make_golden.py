@@ -1,0 +1,264 @@
+"""Generate the golden fixtures in this folder from the reference implementation.
+
+Run in a container that has the reference checkout (path in
+CEEP_REFERENCE_ROOT, default /root/reference):
+
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py cfg1 ade   # a subset
+
+Every fixture is produced by the reference's own code through ``ref_shim``
+(NumPy array module, optional float32 forcing).  Nothing here is used at test
+time except the ``.npz`` files it writes.
+
+Fixtures
+--------
+ceep_results      brain / hemorrhage / empty series from the reference's
+                  ceep_results.json (CuPy GPU run, 64x64, 100 steps)
+fdtd2d_small_*    BatchedFDTD2D.run(), 48x40, CPML 6, 3 TX, 4 probes, 260 steps,
+                  lossy disk; probes + final fields + all eight psi arrays
+fdtd2d_cfg1_*     BatchedFDTD2D.run() at 200x200, 8 TX, 400 steps, CPML 15,
+                  disk r=40 eps 40 sigma 0.5 (the CPU-runnable headline case)
+fdtd2d_runcpu     BatchedFDTD2D.run_cpu() 40x36, 3 TX
+fdtd3d_small_*    BatchedFDTD3D.run(), 20^3, CPML 4, 3 TX (two inside the PML
+                  shell), region with sigma_m, sphere; probes, fields, psi, energy
+dft_cfg1          DFTMonitor over the cfg1 FP64 probe series, 101 frequencies
+das_small         DelayAndSumBeamformer DAS and DMAS on a 6-antenna S-matrix
+das_time_small    das_imaging (scripts/verify_dataset_with_das.py)
+ade2d_small       batched step composed with DispersiveManager (Debye pole 0,
+                  Lorentz pole 1), 44x40, CPML 5, 2 TX, 220 steps
+"""
+from __future__ import annotations
+
+import contextlib
+import io
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from ref_shim import REFERENCE_ROOT, import_reference  # noqa: E402
+
+CFG1 = dict(nx=200, ny=200, dx=0.5e-3, total_steps=400, cpml_thickness=15,
+            frequency=2e9)
+CFG1_POS = [(int(100 + 70 * np.cos(2 * np.pi * k / 8)), int(100 + 70 * np.sin(2 * np.pi * k / 8)))
+            for k in range(8)]
+SMALL = dict(nx=48, ny=40, dx=0.5e-3, total_steps=260, cpml_thickness=6, frequency=2e9)
+SMALL_SRC = [(20, 18), (8, 30), (40, 6)]
+SMALL_PRB = [(20, 18), (7, 7), (41, 33), (24, 2)]
+
+
+def _probes(out, B, P):
+    return np.array([[out[b][p] for p in range(P)] for b in range(B)])
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print("wrote", path, sum(a.nbytes for a in map(np.asarray, arrays.values())), "bytes raw")
+
+
+def gen_ceep_results():
+    with open(os.path.join(REFERENCE_ROOT, "ceep_results.json")) as f:
+        d = json.load(f)
+    p = d["parameters"]
+    sc = d["scenarios"]
+    _save("ceep_results",
+          empty=np.array(sc["empty"]["signal_real"]),
+          brain=np.array(sc["brain"]["signal_real"]),
+          hemorrhage=np.array(sc["hemorrhage"]["signal_real"]),
+          params=np.array([p["nx"], p["ny"], p["dx"], p["frequency"], p["total_steps"],
+                           p["cpml_thickness"], p["antenna_position"][0], p["antenna_position"][1],
+                           p["brain_eps_r"], p["brain_sigma"], p["blood_eps_r"], p["blood_sigma"]]))
+
+
+def gen_small(dtype):
+    import_reference(dtype)
+    from ceep.solvers.fdtd_2d_batched import BatchedFDTD2D
+    s = BatchedFDTD2D(source_positions=SMALL_SRC, probe_positions=SMALL_PRB, **SMALL)
+    s.set_material_circle(24, 20, 8, 12.0, 0.3)
+    out = s.run()
+    names = ["ez", "hx", "hy", "psi_hxy_lo", "psi_hxy_hi", "psi_ezx_lo", "psi_ezx_hi",
+             "psi_hyx_lo", "psi_hyx_hi", "psi_ezy_lo", "psi_ezy_hi"]
+    _save("fdtd2d_small_" + np.dtype(dtype).name,
+          probes=_probes(out, len(SMALL_SRC), len(SMALL_PRB)),
+          eps_r=s._eps_r, sigma_e=s._sigma_e, dt=np.float64(s.dt),
+          **{k: np.asarray(getattr(s, k)) for k in names})
+
+
+def gen_cfg1(dtype):
+    import_reference(dtype)
+    from ceep.solvers.fdtd_2d_batched import BatchedFDTD2D
+    s = BatchedFDTD2D(source_positions=CFG1_POS, probe_positions=CFG1_POS, **CFG1)
+    s.set_material_circle(100, 100, 40, 40.0, 0.5)
+    out = s.run()
+    _save("fdtd2d_cfg1_" + np.dtype(dtype).name, probes=_probes(out, 8, 8),
+          positions=np.array(CFG1_POS), dt=np.float64(s.dt))
+
+
+def gen_runcpu():
+    import_reference(np.float64)
+    from ceep.solvers.fdtd_2d_batched import BatchedFDTD2D
+    src = [(10, 12), (30, 20), (19, 30)]
+    prb = [(10, 12), (25, 25), (5, 31)]
+    s = BatchedFDTD2D(40, 36, 0.5e-3, 150, 5, src, prb, 2e9)
+    s.set_material_circle(20, 18, 6, 9.0, 0.2)
+    out = s.run_cpu()
+    _save("fdtd2d_runcpu", probes=_probes(out, 3, 3), eps_r=s._eps_r, sigma_e=s._sigma_e)
+
+
+def gen_3d(dtype):
+    import_reference(dtype)
+    from ceep.solvers.fdtd_3d_batched import BatchedFDTD3D
+    src = [(11, 10, 9), (2, 15, 3), (17, 2, 18)]
+    prb = [(11, 10, 9), (6, 6, 6), (15, 12, 10), (2, 3, 4)]
+    s = BatchedFDTD3D(20, 20, 20, 1e-3, 70, 4, src, prb, 2e9)
+    s.set_material_region(8, 14, 7, 13, 6, 12, eps_r=6.0, sigma_e=0.4, mu_r=1.5, sigma_m=200.0)
+    s.set_material_sphere(12, 10, 8, 3, eps_r=20.0, sigma_e=1.0)
+    out = s.run()
+    names = ["ex", "ey", "ez", "hx", "hy", "hz"] + [
+        f"psi_{a}_{side}" for a in ("hxy", "hzy", "hyx", "hzx", "hxz", "hyz") for side in ("lo", "hi")]
+    _save("fdtd3d_small_" + np.dtype(dtype).name,
+          probes=_probes(out, 3, 4), eps_r=s._eps_r, sigma_e=s._sigma_e, mu_r=s._mu_r,
+          sigma_m=s._sigma_m, energy=np.float64(s.compute_energy()), dt=np.float64(s.dt),
+          src=np.array(src), prb=np.array(prb),
+          **{k: np.asarray(getattr(s, k)) for k in names})
+
+
+def gen_dft():
+    import_reference(np.float64)
+    from ceep.solvers.dft import DFTMonitor
+    d = np.load(os.path.join(HERE, "fdtd2d_cfg1_float64.npz"))
+    series, dt = d["probes"], float(d["dt"])
+    freqs = np.linspace(0.5e9, 3.5e9, 101)
+    mon = DFTMonitor(freqs, (slice(None), slice(None)))
+    for step in range(series.shape[2]):
+        mon.update(series[:, :, step], step, dt)
+    S = mon.get_complex_field().transpose(0, 2, 1)   # (F, rx, tx)
+    _save("dft_cfg1", S=S, frequencies=freqs)
+
+
+def gen_das():
+    import_reference(np.float64)
+    from ceep.solvers.s_params import MultistaticSParameters
+    from ceep.imaging.beamforming import DelayAndSumBeamformer, ImagingRegion
+    rng = np.random.default_rng(7)
+    N, F = 6, 9
+    freqs = np.linspace(1.0e9, 3.0e9, F)
+    S = rng.standard_normal((F, N, N)) + 1j * rng.standard_normal((F, N, N))
+    ang = 2 * np.pi * np.arange(N) / N
+    pos = [(int(40 + 30 * np.cos(a)), int(40 + 30 * np.sin(a))) for a in ang]
+    sp = MultistaticSParameters(frequencies=freqs, s_matrix=S, antenna_positions=pos)
+    region = ImagingRegion(x_range=(30, 41), y_range=(28, 37), dx=1e-3, background_permittivity=4.0)
+    bf = DelayAndSumBeamformer(sp, pos, region, frequency_range=(1.2e9, 2.8e9))
+    with contextlib.redirect_stdout(io.StringIO()):
+        das = bf.reconstruct("das")
+        dmas = DelayAndSumBeamformer(sp, pos, region).reconstruct("dmas")
+    _save("das_small", S=S, frequencies=freqs, positions=np.array(pos), das=das, dmas=dmas,
+          x_range=np.array(region.x_range), y_range=np.array(region.y_range), dx=np.float64(1e-3),
+          eps_bg=np.float64(4.0), frange=np.array([1.2e9, 2.8e9]))
+
+
+def gen_das_time():
+    sys.modules.setdefault("matplotlib", types.ModuleType("matplotlib"))
+    sys.modules.setdefault("matplotlib.pyplot", types.ModuleType("matplotlib.pyplot"))
+    sys.path.insert(0, os.path.join(REFERENCE_ROOT, "scripts"))
+    import verify_dataset_with_das as v
+    rng = np.random.default_rng(11)
+    N, T, G, dx = 5, 48, 14, 2e-3
+    s = rng.standard_normal((N, N, T)) + 1j * rng.standard_normal((N, N, T))
+    ang = 2 * np.pi * np.arange(N) / N
+    pos = np.stack([0.014 + 0.012 * np.cos(ang), 0.014 + 0.012 * np.sin(ang)], 1)
+    img = v.das_imaging(s, pos, 2e9, G, dx)
+    _save("das_time_small", s=s, positions=pos, frequency=np.float64(2e9),
+          grid_size=np.int64(G), dx=np.float64(dx), image=img)
+
+
+def gen_ade():
+    """Batched step (reference methods) composed with DispersiveManager."""
+    import_reference(np.float64)
+    from ceep.solvers.fdtd_2d_batched import BatchedFDTD2D
+    from ceep.materials.dispersive import DispersiveManager, DebyePole, LorentzPole
+    from ceep.core.constants import EPS_0
+    nx, ny, n, T = 44, 40, 5, 220
+    src = [(14, 20), (30, 12)]
+    prb = [(14, 20), (30, 12), (22, 30)]
+    s = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9)
+    B = len(src)
+    x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    deb_mask = (x - 20) ** 2 + (y - 18) ** 2 <= 7 ** 2
+    lor_mask = (x - 27) ** 2 + (y - 24) ** 2 <= 4 ** 2
+    s._eps_r[deb_mask] = 8.0
+    s._sigma_e[deb_mask] = 0.4
+    s._eps_r[lor_mask] = 3.0
+    s._sigma_e[lor_mask] = 0.1
+    mgrs = []
+    for _ in range(B):
+        m = DispersiveManager(nx, ny, max_poles=2)
+        m.add_poles(deb_mask, [DebyePole(delta_eps=30.0, tau=9e-12)])
+        m.add_poles(lor_mask, [DebyePole(delta_eps=0.0, tau=0.0),
+                               LorentzPole(delta_eps=5.0, omega_0=2 * np.pi * 6e9, delta=2 * np.pi * 0.5e9)])
+        mgrs.append(m)
+    s._build()
+    dt = s.dt
+    eps_add = np.asarray(mgrs[0].compute_coefficients(dt))
+    for m in mgrs[1:]:
+        m.compute_coefficients(dt)
+    # Grid2D._precompute_coefficients (src/ceep/core/grid.py:174-189) with eps_inf = _eps_r
+    eps = s._eps_r * EPS_0 + eps_add
+    sd = s._sigma_e * dt / (2.0 * eps)
+    s.ca = ((1.0 - sd) / (1.0 + sd))[None]
+    s.cb = ((dt / eps) / (1.0 + sd))[None]
+    P = len(prb)
+    probes = np.zeros((B, P, T))
+    inv = s.inv_dx
+    for step in range(T):
+        # interior H and H-CPML: fdtd_2d_batched.py:471-486
+        s.hx[:, n:nx - n, n:ny - 1] = (s.da[:, n:nx - n, n:ny - 1] * s.hx[:, n:nx - n, n:ny - 1]
+                                       - s.db[:, n:nx - n, n:ny - 1] * inv * (s.ez[:, n:nx - n, n + 1:ny] - s.ez[:, n:nx - n, n:ny - 1]))
+        s.hy[:, n:nx - 1, n:ny - n] = (s.da[:, n:nx - 1, n:ny - n] * s.hy[:, n:nx - 1, n:ny - n]
+                                       + s.db[:, n:nx - 1, n:ny - n] * inv * (s.ez[:, n + 1:nx, n:ny - n] - s.ez[:, n:nx - 1, n:ny - n]))
+        s._apply_h_cpml()
+        I = (slice(None), slice(n + 1, nx - n), slice(n + 1, ny - n))
+        ez_old = s.ez.copy()
+        sum_gj = np.stack([np.asarray(m.get_sum_gamma_j("Ez")) for m in mgrs])
+        s.ez[I] = (s.ca[I[0:1] + I[1:]] * s.ez[I] + s.cb[(slice(None),) + I[1:]] * (
+            (s.hy[I] - s.hy[:, n:nx - n - 1, n + 1:ny - n]) * inv
+            - (s.hx[I] - s.hx[:, n + 1:nx - n, n:ny - n - 1]) * inv))
+        s.ez[I] -= s.cb[(slice(None),) + I[1:]] * sum_gj[I]
+        for b, m in enumerate(mgrs):
+            m.update_j_fields("Ez", s.ez[b], ez_old[b], dt)
+        s._apply_e_cpml()
+        s.ez[:, 0, :] = 0
+        s.ez[:, -1, :] = 0
+        s.ez[:, :, 0] = 0
+        s.ez[:, :, -1] = 0
+        w = float(s.waveform[step])
+        for b in range(B):
+            s.ez[b, src[b][0], src[b][1]] += w
+        for p, (px, py) in enumerate(prb):
+            probes[:, p, step] = s.ez[:, px, py]
+    _save("ade2d_small", probes=probes, eps_r=s._eps_r, sigma_e=s._sigma_e,
+          deb_mask=deb_mask, lor_mask=lor_mask, ez=s.ez,
+          j0=np.stack([np.asarray(m.j_ez[0]) for m in mgrs]),
+          j1=np.stack([np.asarray(m.j_ez[1]) for m in mgrs]))
+
+
+JOBS = {
+    "ceep_results": gen_ceep_results,
+    "small": lambda: (gen_small(np.float64), gen_small(np.float32)),
+    "cfg1": lambda: (gen_cfg1(np.float64), gen_cfg1(np.float32)),
+    "runcpu": gen_runcpu,
+    "3d": lambda: (gen_3d(np.float64), gen_3d(np.float32)),
+    "dft": gen_dft,
+    "das": gen_das,
+    "das_time": gen_das_time,
+    "ade": gen_ade,
+}
+
+if __name__ == "__main__":
+    for job in (sys.argv[1:] or list(JOBS)):
+        JOBS[job]()
