@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""Throughput of the batched multistatic FDTD path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload head600|disk200]
+
+A bench "step" is one complete head-imaging sample: the 800-step fused FDTD
+time loop for 16 transmit events with a one-pole Debye phantom, the DFT of
+all 16x16 probe series into S (301 frequencies) and a 64x64 DAS image.
+Metric: GCell-steps/s = nx * ny * time steps * TX / time.
+
+Multi-GPU: phantoms are independent, so each rank runs its own samples
+(weak scaling, no data-path collective); time is the max over ranks.
+
+The reference arm (--impl reference) times the CPU restatement of the
+reference algorithm (the oracle, NumPy FP64) on the host cores, spreading the
+transmit events over worker processes, on a bounded number of time steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # config 2 of the headline metric: 600x600, 0.5 mm, 800 steps, CPML 15, 16 TX/RX
+    # on r = 200 cells, Debye head phantom, 301 frequencies, 64x64 DAS
+    "head600": dict(nx=600, ny=600, dx=0.5e-3, steps=800, cpml=15, ntx=16, ring=200, nfreq=301, das=64,
+                    debye=True),
+    # config 1 (the reference's CPU-runnable case): 200x200, 400 steps, 8 TX, disk
+    "disk200": dict(nx=200, ny=200, dx=0.5e-3, steps=400, cpml=15, ntx=8, ring=70, nfreq=101, das=64,
+                    debye=False),
+}
+PUBLISHED_GCELLS = 1.40  # README.md:60 of the reference: 600x600x16 TX x 800 steps in 3.3 s (T4)
+
+
+def algorithmic_bytes_per_step(w, n_debye):
+    """Compulsory FP32 DRAM bytes of one fused step (read+write each state word
+    once, coefficients once per cell): 24 B per cell-TX for Ez/Hx/Hy, 8 B per
+    cell for (ca, cb), 16 B per strip cell-TX for the H and E psi of that
+    strip plus 4 B per strip cell for dt/eps, and per Debye pole 8 B per
+    interior cell-TX for J plus 12 B per interior cell for (k1, k2, gamma)."""
+    nx, ny, n, T = w["nx"], w["ny"], w["cpml"], w["ntx"]
+    cells = nx * ny
+    xstrip = 2 * n * ny
+    ystrip = 2 * n * nx
+    interior = (nx - 2 * n - 1) * (ny - 2 * n - 1)
+    b = cells * (24 * T + 8)
+    b += (xstrip + ystrip) * (16 * T + 4)
+    b += n_debye * interior * (8 * T + 12)
+    return b
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_inputs(w, nsamples, device, seed0=1000):
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
+    pos = ring_positions(w["ntx"], (w["nx"] // 2, w["ny"] // 2), w["ring"])
+    freqs = np.linspace(0.5e9, 3.5e9, w["nfreq"])
+    solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
+                           frequencies=freqs, device=str(device))
+    phantoms, mats = [], []
+    for k in range(nsamples):
+        if w["debye"]:
+            ph = HeadPhantom2D(w["nx"], w["ny"], w["dx"], seed=seed0 + k)
+            eps, sig = ph.get_eps_map()
+            d = ph.get_dispersion()
+            mats.append(solver.material_tensors(eps, sig, d["debye"], d["lorentz"]))
+        else:
+            x, y = np.meshgrid(np.arange(w["nx"]), np.arange(w["ny"]), indexing="ij")
+            m = (x - w["nx"] // 2) ** 2 + (y - w["ny"] // 2) ** 2 <= 40 ** 2
+            ph = None
+            mats.append(solver.material_tensors(np.where(m, 40.0, 1.0), np.where(m, 0.5, 0.0)))
+        phantoms.append(ph)
+    if w["debye"]:
+        solver.set_phantom(phantoms[0])
+    else:
+        solver.set_material_circle(w["nx"] // 2, w["ny"] // 2, 40, 40.0, 0.5)
+    return solver, pos, freqs, phantoms, mats
+
+
+def one_sample(solver, w, freqs, pos, das_ws, stream):
+    """Device-only sample: fresh state, the time loop, S, DAS image."""
+    import torch
+    from ceep_b200.spectral import das_image, dft
+    solver.reset()
+    solver.advance(0, w["steps"], stream=stream)
+    S = dft(solver.probe_data, freqs, solver.dt)
+    half = 0.09
+    img = das_image(S, freqs, np.asarray(pos, float) * w["dx"], w["das"], w["das"],
+                    (w["nx"] // 2) * w["dx"] - half, (w["ny"] // 2) * w["dx"] - half, 2 * half / w["das"],
+                    299_792_458.0, True, workspace=das_ws)
+    return S, img
+
+
+def run_ours(args, w):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    K, W = args.steps, args.warmup
+    solver, pos, freqs, phantoms, mats = build_inputs(w, K + W, device, seed0=1000 + 97 * rank)
+    solver._build()
+    stream = torch.cuda.current_stream(device)
+    das_ws = torch.empty(1 << 20, dtype=torch.uint8, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # > 126 MB L2
+    n_debye = 1 if w["debye"] else 0
+
+    for k in range(W):
+        solver.load_material_tensors(mats[K + k])
+        one_sample(solver, w, freqs, pos, das_ws, stream)
+    torch.cuda.synchronize()
+
+    # -- timed region: K samples, inputs resident in HBM, L2 flushed between samples
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(K):
+            flush.zero_()
+            solver.load_material_tensors(mats[k])
+            ev[k][0].record(stream)
+            one_sample(solver, w, freqs, pos, das_ws, stream)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(np.sum(ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    cell_steps = w["nx"] * w["ny"] * w["steps"] * w["ntx"]
+    value = world * K * cell_steps / (total_ms * 1e-3) / 1e9
+
+    # -- dominant kernel alone: the fused step, per-launch time over full loops
+    per_launch = []
+    for k in range(3):
+        flush.zero_()
+        solver.reset()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solver.advance(0, w["steps"], stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        per_launch.append(a.elapsed_time(b) / w["steps"])
+    launch_ms = float(np.median(per_launch))
+    bytes_step = algorithmic_bytes_per_step(w, n_debye)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = bytes_step / (launch_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "fdtd2d_step_head600_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("bytes_per_launch")
+
+    # -- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(w, phantoms[:min(K, 3)], pos, freqs, device)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w, sample_steps=args.cpu_steps)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "batched FDTD GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(total_ms / K, 3),
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": round(value / PUBLISHED_GCELLS, 2),
+        "dtype": "f32", "data": "synthetic (seeded phantoms)",
+        "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "time_steps": w["steps"],
+                   "tx": w["ntx"], "cpml": w["cpml"], "debye_poles": n_debye, "dft_freqs": w["nfreq"],
+                   "das": f"{w['das']}x{w['das']}", "parallelism": f"replicas{world}",
+                   "l2": "flushed (256 MB write) before every sample; per-step working set > L2",
+                   "sample": "fused time loop + DFT->S + DAS image"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "fdtd2d_step_kernel", "launch_ms": round(launch_ms, 5),
+                     "algorithmic_bytes_per_launch": bytes_step},
+        "gpu_launches": K * (w["steps"] + 3),
+        "clocks": clk.summary(),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(w, phantoms, pos, freqs, device):
+    """Public-API path per sample: host phantom maps -> set_phantom ->
+    update_materials (H2D) -> run() (D2H of every series) -> s_matrix() (D2H)
+    -> DAS image (D2H)."""
+    import torch
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.spectral import das_image
+    solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
+                           frequencies=freqs, device=str(device))
+    if phantoms[0] is not None:
+        solver.set_phantom(phantoms[0])
+    solver.run()  # builds and captures the graph once
+    torch.cuda.synchronize()
+    h2d = d2h = 0
+    times = []
+    for ph in phantoms:
+        t0 = time.perf_counter()
+        solver.reset()
+        if ph is not None:
+            solver.set_phantom(ph)
+        solver.update_materials()
+        out = solver.run()
+        S = solver.s_matrix()
+        img = das_image(torch.as_tensor(S, dtype=torch.complex64, device=device), freqs,
+                        np.asarray(pos, float) * w["dx"], w["das"], w["das"], w["nx"] // 2 * w["dx"] - 0.09,
+                        w["ny"] // 2 * w["dx"] - 0.09, 0.18 / w["das"], 299_792_458.0).cpu().numpy()
+        times.append(time.perf_counter() - t0)
+        h2d = (solver._coef.numel() + solver._dteps.numel() +
+               (solver._ade_coef.numel() if solver._ade_coef is not None else 0)) * 4 + S.size * 8
+        d2h = solver.probe_data.numel() * 4 + S.size * 8 + img.size * 4
+    cell_steps = w["nx"] * w["ny"] * w["steps"] * w["ntx"]
+    return {"value": round(len(times) * cell_steps / sum(times) / 1e9, 3), "unit": "GCell-steps/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "path": "BatchedFDTD2D.set_phantom/run/s_matrix + DAS, host arrays in and out"}
+
+
+def _oracle_worker_init(w, tx_list, seed):
+    global _ORACLE
+    from oracle.fdtd2d import Fdtd2DOracle
+    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
+    pos = ring_positions(w["ntx"], (w["nx"] // 2, w["ny"] // 2), w["ring"])
+    src = [pos[i] for i in tx_list]
+    if w["debye"]:
+        ph = HeadPhantom2D(w["nx"], w["ny"], w["dx"], seed=seed)
+        eps, sig = ph.get_eps_map()
+        disp = ph.get_dispersion()
+    else:
+        x, y = np.meshgrid(np.arange(w["nx"]), np.arange(w["ny"]), indexing="ij")
+        m = (x - w["nx"] // 2) ** 2 + (y - w["ny"] // 2) ** 2 <= 40 ** 2
+        eps, sig, disp = np.where(m, 40.0, 1.0), np.where(m, 0.5, 0.0), None
+    _ORACLE = Fdtd2DOracle(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], src, pos, 2e9,
+                           eps_r=eps, sigma_e=sig, dispersion=disp)
+
+
+def _oracle_worker_run(nsteps):
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        if _ORACLE.step_index >= _ORACLE.total_steps:
+            _ORACLE.step_index = 0
+        _ORACLE.step()
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(w, sample_steps=12):
+    """Oracle port, one process (NumPy elementwise is single-threaded), on a
+    bounded number of time steps of the same workload."""
+    _oracle_worker_init(w, list(range(w["ntx"])), 1000)
+    dt = _oracle_worker_run(sample_steps)
+    v = w["nx"] * w["ny"] * w["ntx"] * sample_steps / dt / 1e9
+    return {"value": round(v, 6), "unit": "GCell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{sample_steps} of {w['steps']} time steps, all {w['ntx']} TX, FP64 NumPy oracle, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args, w):
+    """Reference arm: the oracle port on all host cores (TX spread over spawn workers)."""
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    ncpu = os.cpu_count() or 1
+    nproc = max(1, min(ncpu, w["ntx"]))
+    groups = [list(range(w["ntx"]))[i::nproc] for i in range(nproc)]
+    ctx = mp.get_context("spawn")
+    per_step_steps = args.cpu_steps
+    pools = [ctx.Pool(1, initializer=_oracle_worker_init, initargs=(w, g, 1000)) for g in groups]
+    try:
+        for _ in range(args.warmup):
+            rs = [p.apply_async(_oracle_worker_run, (1,)) for p in pools]
+            [r.get() for r in rs]
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rs = [p.apply_async(_oracle_worker_run, (per_step_steps,)) for p in pools]
+            [r.get() for r in rs]
+            times.append(time.perf_counter() - t0)
+    finally:
+        for p in pools:
+            p.close()
+            p.join()
+    cell_steps = w["nx"] * w["ny"] * w["ntx"] * per_step_steps
+    value = len(times) * cell_steps / sum(times) / 1e9
+    line = {"impl": "reference", "metric": "batched FDTD GCell-steps/s", "value": round(value, 6),
+            "unit": "GCell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantoms)",
+            "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "tx": w["ntx"],
+                       "time_steps_per_bench_step": per_step_steps},
+            "cpu_baseline": {"value": round(value, 6), "unit": "GCell-steps/s", "cores": nproc, "kind": "port",
+                             "sample": f"{per_step_steps} time steps x {w['ntx']} TX per bench step, "
+                                       f"{nproc} spawn workers over TX, {ncpu} host cores"},
+            "e2e": {"value": round(value, 6), "unit": "GCell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_profile(args, w):
+    """A few fused steps of one sample, launched without a graph, then the DFT
+    and DAS once: the small command that ncu captures."""
+    import torch
+    device = torch.device("cuda", 0)
+    solver, pos, freqs, _, mats = build_inputs(w, 1, device)
+    solver.use_graph = False
+    solver.load_material_tensors(mats[0])
+    stream = torch.cuda.current_stream(device)
+    solver.advance(0, min(args.profile, w["steps"]), stream=stream)
+    das_ws = torch.empty(1 << 20, dtype=torch.uint8, device=device)
+    from ceep_b200.spectral import das_image, dft
+    S = dft(solver.probe_data, freqs, solver.dt)
+    das_image(S, freqs, np.asarray(pos, float) * w["dx"], w["das"], w["das"], 0.06, 0.06, 0.18 / w["das"],
+              299_792_458.0, True, workspace=das_ws)
+    torch.cuda.synchronize()
+    print("profile run done", flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=12)
+    ap.add_argument("--profile", type=int, default=0,
+                    help="run only N fused steps of one sample (for ncu), no timing, no JSON")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.profile:
+        run_profile(args, w)
+    elif args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_ours(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,13 @@
+"""ceep_b200 — B200-native batched multistatic FDTD (drop-in for ceep-v1's batched path).
+
+Public API:
+    BatchedFDTD2D                      2D TMz batched solver (fdtd_2d_batched.py)
+    MultistaticSParameters, ImagingRegion, DelayAndSumBeamformer, dft, das_time
+The compute runs in ``_lib/libceep_b200.so`` (sm_100a); there is no CPU path.
+"""
+from .solvers import BatchedFDTD2D
+from .spectral import (DelayAndSumBeamformer, ImagingRegion, MultistaticSParameters, das_image, das_time,
+                       dft)
+
+__all__ = ["BatchedFDTD2D", "MultistaticSParameters", "ImagingRegion", "DelayAndSumBeamformer", "dft",
+           "das_image", "das_time"]

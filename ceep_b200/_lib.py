@@ -1,0 +1,83 @@
+"""ctypes binding of include/ceep_b200.h (libceep_b200.so, built in-tree).
+
+There is no fallback: if the shared library is missing or lacks a symbol,
+importing the solvers raises.  ``build()`` compiles it with nvcc.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libceep_b200.so")
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+
+
+class Desc2D(C.Structure):
+    """Mirror of ``ceep2d_desc``."""
+    _fields_ = [
+        ("nx", I32), ("ny", I32), ("cpml", I32), ("ntx", I32), ("ntx_pad", I32),
+        ("nprobe", I32), ("nsteps", I32), ("n_debye", I32), ("n_lorentz", I32),
+        ("db", C.c_float), ("inv_dx", C.c_float), ("dt", C.c_float),
+        ("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hy", P * 2), ("psi_hx", P * 2),
+        ("psi_ezx", P), ("psi_ezy", P), ("j", P), ("j_prev", P),
+        ("coef", P), ("dteps", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
+        ("src_xy", P), ("prb_xy", P), ("row_flags", P), ("waveform", P), ("probes", P),
+        ("rows_per_block", I32),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "ceep_version": (C.c_int, []),
+    "ceep_last_error": (C.c_char_p, []),
+    "ceep2d_plan_create": (C.c_int, [C.POINTER(Desc2D), C.POINTER(P)]),
+    "ceep2d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
+    "ceep2d_plan_destroy": (C.c_int, [P]),
+    "ceep2d_launches_per_step": (C.c_int, [P]),
+    "ceep2d_plan_current_buffer": (C.c_int, [P]),
+    "ceep2d_plan_reset": (C.c_int, [P]),
+    "ceep2d_desc_size": (I64, []),
+    "ceep_dft": (C.c_int, [P, P, P, I32, I32, I32, I32, P]),
+    "ceep_das_workspace_bytes": (I64, [I32, I32, I32]),
+    "ceep_das": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),
+    "ceep_das_time": (C.c_int, [P, P, I32, I32, I32, C.c_double, C.c_double, P, P]),
+}
+
+_lib = None
+
+
+class CeepError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        msg = lib().ceep_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed (status {code}): {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libceep_b200.so once; raise if it is absent or incomplete."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with `python -m ceep_b200.csrc.build`")
+        h = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        if h.ceep2d_desc_size() != C.sizeof(Desc2D):
+            raise ImportError("ceep2d_desc layout mismatch between header and binding")
+        _lib = h
+    return _lib
+
+
+def check(code: int, where: str) -> None:
+    if code != 0:
+        raise CeepError(code, where)
+
+
+def exported_symbols():
+    return list(_SIGS)

@@ -1,0 +1,166 @@
+// extern "C" entry points declared in include/ceep_b200.h.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <new>
+#include <tuple>
+#include <utility>
+
+#include "../../include/ceep_b200.h"
+#include "capi_internal.h"
+#include "fdtd2d.cuh"
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+namespace ceep {
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(CEEP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+}  // namespace ceep
+
+using ceep::fail;
+
+extern "C" int ceep_version(void) { return 100; }
+extern "C" const char* ceep_last_error(void) { return g_err; }
+
+// --------------------------------------------------------------------------
+// 2D plan
+// --------------------------------------------------------------------------
+struct ceep2d_plan {
+  ceep::Fdtd2dParams p;
+  int cur = 0;  // ping-pong buffer holding the current state
+  // captured step loops keyed by (step0, nsteps, starting buffer)
+  std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
+};
+
+extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
+  if (!d || !out) return fail(CEEP_ERR_INVALID, "ceep2d_plan_create: null argument");
+  *out = nullptr;
+  const int n = d->cpml;
+  if (d->nx < 3 || d->ny < 3) return fail(CEEP_ERR_INVALID, "grid %dx%d too small", d->nx, d->ny);
+  if (n == 1 || n < 0) return fail(CEEP_ERR_INVALID, "cpml thickness must be 0 or >= 2 (got %d)", n);
+  if (d->nx < 2 * n + 2 || d->ny < 2 * n + 2)
+    return fail(CEEP_ERR_INVALID, "grid %dx%d must exceed twice the CPML (%d) by 2", d->nx, d->ny, n);
+  if (d->ntx < 1 || d->ntx_pad < d->ntx || d->ntx_pad % 4)
+    return fail(CEEP_ERR_INVALID, "ntx=%d ntx_pad=%d (pad must be a multiple of 4 and >= ntx)", d->ntx,
+                d->ntx_pad);
+  const int lanes = d->ntx_pad / 4;
+  const int group = lanes <= 8 ? lanes : 8;
+  if (lanes > 8 && lanes % 8)
+    return fail(CEEP_ERR_INVALID, "ntx_pad=%d above 32 must be a multiple of 32", d->ntx_pad);
+  if (group != 1 && group != 2 && group != 4 && group != 8)
+    return fail(CEEP_ERR_INVALID, "ntx_pad=%d: lanes per cell must be 1, 2, 4 or 8 (pad to 4, 8, 16, 32)",
+                d->ntx_pad);
+  if (d->n_debye < 0 || d->n_lorentz < 0 || d->n_debye + d->n_lorentz > 2)
+    return fail(CEEP_ERR_UNSUPPORTED, "ADE poles: at most 2 per cell (debye=%d lorentz=%d)", d->n_debye,
+                d->n_lorentz);
+  if (d->nsteps < 1 || d->nprobe < 0) return fail(CEEP_ERR_INVALID, "nsteps/nprobe");
+  for (int k = 0; k < 2; ++k)
+    if (!d->ez[k] || !d->hx[k] || !d->hy[k]) return fail(CEEP_ERR_INVALID, "null field buffer");
+  if (n > 0 && (!d->psi_hx[0] || !d->psi_hx[1] || !d->psi_hy[0] || !d->psi_hy[1] || !d->psi_ezx ||
+                !d->psi_ezy || !d->cpml_b || !d->cpml_c || !d->dteps))
+    return fail(CEEP_ERR_INVALID, "null CPML buffer");
+  if (d->n_debye + d->n_lorentz > 0 && (!d->j || !d->ade_coef || (d->n_lorentz && !d->j_prev)))
+    return fail(CEEP_ERR_INVALID, "null ADE buffer");
+  if (!d->coef || !d->src_xy || !d->row_flags || !d->waveform || (d->nprobe && (!d->prb_xy || !d->probes)))
+    return fail(CEEP_ERR_INVALID, "null coefficient/source/probe buffer");
+
+  ceep2d_plan* pl = new (std::nothrow) ceep2d_plan();
+  if (!pl) return fail(CEEP_ERR_INVALID, "host allocation failed");
+  ceep::Fdtd2dParams& p = pl->p;
+  p.nx = d->nx; p.ny = d->ny; p.n = n;
+  p.ntx = d->ntx; p.lanes = lanes; p.lanes_per_group = group;
+  p.nprobe = d->nprobe; p.nsteps = d->nsteps;
+  p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
+  p.rows = d->rows_per_block > 0 ? d->rows_per_block : 16;
+  p.db = d->db; p.db_dx = d->db * d->inv_dx; p.inv_dx = d->inv_dx; p.dt = d->dt;
+  for (int k = 0; k < 2; ++k) {
+    p.ez[k] = reinterpret_cast<float4*>(d->ez[k]);
+    p.hx[k] = reinterpret_cast<float4*>(d->hx[k]);
+    p.hy[k] = reinterpret_cast<float4*>(d->hy[k]);
+    p.psi_hy[k] = reinterpret_cast<float4*>(d->psi_hy[k]);
+    p.psi_hx[k] = reinterpret_cast<float4*>(d->psi_hx[k]);
+  }
+  p.psi_ezx = reinterpret_cast<float4*>(d->psi_ezx);
+  p.psi_ezy = reinterpret_cast<float4*>(d->psi_ezy);
+  p.j = reinterpret_cast<float4*>(d->j);
+  p.j_prev = reinterpret_cast<float4*>(d->j_prev);
+  p.coef = d->coef; p.dteps = d->dteps; p.ade_coef = d->ade_coef;
+  p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
+  p.src_xy = d->src_xy; p.prb_xy = d->prb_xy; p.row_flags = d->row_flags;
+  p.waveform = d->waveform; p.probes = d->probes;
+  *out = pl;
+  return CEEP_OK;
+}
+
+static int run_steps(ceep2d_plan* pl, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
+  for (int64_t k = 0; k < nsteps; ++k) {
+    cudaError_t e = ceep::fdtd2d_launch_step(pl->p, (int)(step0 + k), cur, s);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd2d step launch");
+    cur ^= 1;
+  }
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+  if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
+  if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
+    return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
+                (long long)(step0 + nsteps), pl->p.nsteps);
+  if (nsteps == 0) return CEEP_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int cur = pl->cur;
+  if (!use_graph || s == nullptr) {
+    int rc = run_steps(pl, step0, nsteps, cur, s);
+    if (rc == CEEP_OK) pl->cur = cur ^ (int)(nsteps & 1);
+    return rc;
+  }
+  auto key = std::make_tuple(step0, nsteps, cur);
+  auto it = pl->graphs.find(key);
+  if (it == pl->graphs.end()) {
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
+    int rc = run_steps(pl, step0, nsteps, cur, s);
+    e = cudaStreamEndCapture(s, &g);
+    if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphInstantiate");
+    it = pl->graphs.emplace(key, ex).first;
+  }
+  cudaError_t e = cudaGraphLaunch(it->second, s);
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
+  pl->cur = cur ^ (int)(nsteps & 1);
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_current_buffer(const ceep2d_plan* pl) { return pl ? pl->cur : -1; }
+extern "C" int ceep2d_plan_reset(ceep2d_plan* pl) {
+  if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
+  pl->cur = 0;
+  return CEEP_OK;
+}
+extern "C" int64_t ceep2d_desc_size(void) { return (int64_t)sizeof(ceep2d_desc); }
+
+extern "C" int ceep2d_plan_destroy(ceep2d_plan* pl) {
+  if (!pl) return CEEP_OK;
+  for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  delete pl;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_launches_per_step(const ceep2d_plan* pl) { return pl ? 1 : 0; }

@@ -1,0 +1,33 @@
+// Shared device helpers for the ceep_b200 kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CEEP_HD __host__ __device__ __forceinline__
+#define CEEP_D __device__ __forceinline__
+
+namespace ceep {
+
+// Lane-wise float4 arithmetic: one float4 carries four transmit events of
+// one cell, so every operator below is "the same update for 4 TX at once".
+CEEP_D float4 f4(float v) { return make_float4(v, v, v, v); }
+CEEP_D float4 operator+(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+CEEP_D float4 operator-(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+CEEP_D float4 operator*(float s, float4 a) { return make_float4(s * a.x, s * a.y, s * a.z, s * a.w); }
+CEEP_D float4 operator*(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+CEEP_D float4 operator/(float4 a, float s) { return make_float4(a.x / s, a.y / s, a.z / s, a.w / s); }
+CEEP_D float4 fma4(float s, float4 a, float4 b) {  // s*a + b
+  return make_float4(fmaf(s, a.x, b.x), fmaf(s, a.y, b.y), fmaf(s, a.z, b.z), fmaf(s, a.w, b.w));
+}
+CEEP_D float comp(const float4& v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+CEEP_D void add_comp(float4& v, int i, float s) {
+  if (i == 0) v.x += s; else if (i == 1) v.y += s; else if (i == 2) v.z += s; else v.w += s;
+}
+
+// Streaming loads/stores.  Field state is read once and written once per
+// step, so the read-only path with an L1 hint is used for neighbours that
+// other threads of the same block also read.
+CEEP_D float4 ld4(const float4* p) { return __ldg(p); }
+CEEP_D void st4(float4* p, float4 v) { *p = v; }
+
+}  // namespace ceep

@@ -1,0 +1,290 @@
+// On-device DFT into the S-matrix and delay-and-sum imaging (sm_100a).
+#include <cuda_runtime.h>
+
+#include "../../include/ceep_b200.h"
+#include "capi_internal.h"
+#include "common.cuh"
+
+namespace ceep {
+
+// --------------------------------------------------------------------------
+// DFT: S[f, rx, tx] = sum_n series[tx, rx, n] * tw[f, n]   (dft.py:55-90)
+// A (freq x pair) tile per block, the time axis staged through shared memory
+// in chunks of 32 samples; each thread owns a 2x2 block of outputs.  FP32
+// accumulation over <= a few thousand samples stays ~1e-6 relative.
+// --------------------------------------------------------------------------
+constexpr int kDftT = 32;   // tile edge (freqs and pairs)
+constexpr int kDftC = 32;   // samples per chunk
+
+__global__ void __launch_bounds__(256) dft_kernel(const float* __restrict__ series, const float2* __restrict__ tw,
+                                                  float2* __restrict__ out, int ntx, int nprobe, int nsteps,
+                                                  int nfreq) {
+  __shared__ float2 s_tw[kDftT][kDftC + 1];
+  __shared__ float s_x[kDftT][kDftC + 1];
+  const int npair = ntx * nprobe;
+  const int f0 = blockIdx.x * kDftT, k0 = blockIdx.y * kDftT;
+  const int tf = threadIdx.x / 16, tk = threadIdx.x % 16;
+  float2 acc[2][2] = {};
+  for (int c0 = 0; c0 < nsteps; c0 += kDftC) {
+    for (int i = threadIdx.x; i < kDftT * kDftC; i += blockDim.x) {
+      const int r = i / kDftC, c = i % kDftC, n = c0 + c;
+      const int f = f0 + r, k = k0 + r;
+      s_tw[r][c] = (f < nfreq && n < nsteps) ? tw[(size_t)f * nsteps + n] : make_float2(0.f, 0.f);
+      s_x[r][c] = (k < npair && n < nsteps) ? series[(size_t)k * nsteps + n] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int c = 0; c < kDftC; ++c) {
+      const float2 w0 = s_tw[tf][c], w1 = s_tw[tf + 16][c];
+      const float x0 = s_x[tk][c], x1 = s_x[tk + 16][c];
+      acc[0][0].x = fmaf(w0.x, x0, acc[0][0].x); acc[0][0].y = fmaf(w0.y, x0, acc[0][0].y);
+      acc[0][1].x = fmaf(w0.x, x1, acc[0][1].x); acc[0][1].y = fmaf(w0.y, x1, acc[0][1].y);
+      acc[1][0].x = fmaf(w1.x, x0, acc[1][0].x); acc[1][0].y = fmaf(w1.y, x0, acc[1][0].y);
+      acc[1][1].x = fmaf(w1.x, x1, acc[1][1].x); acc[1][1].y = fmaf(w1.y, x1, acc[1][1].y);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int f = f0 + tf + 16 * a, k = k0 + tk + 16 * b;
+      if (f < nfreq && k < npair) {
+        const int tx = k / nprobe, rx = k % nprobe;
+        out[((size_t)f * nprobe + rx) * ntx + tx] = acc[a][b];
+      }
+    }
+}
+
+// --------------------------------------------------------------------------
+// Frequency-domain DAS (beamforming.py:210-257).
+// The two-way phasor factorises: exp(-j k (d_tx + d_rx)) = a_tx * a_rx with
+// a_m = exp(-j k d_m), so per (pixel, f) the image term is
+//   sum_tx a_tx * sum_rx S[f, rx, tx] a_rx
+// i.e. N sincos + N^2 complex MACs instead of N^2 sincos.  Pixels map to
+// threads; frequencies are split into chunks across blockIdx.y so a small
+// image still fills all SMs; each chunk writes its partial complex sum to
+// the caller's workspace and a finishing kernel adds the chunks, takes |.|
+// and applies (I - min) / max.
+// --------------------------------------------------------------------------
+constexpr int kDasThreads = 128;
+constexpr int kDasMaxAnt = 32;
+
+static int das_chunks(int npix, int nfreq) {
+  const int pixblocks = (npix + kDasThreads - 1) / kDasThreads;
+  int chunks = (2 * 148 + pixblocks - 1) / pixblocks;
+  if (chunks > nfreq) chunks = nfreq;
+  if (chunks < 1) chunks = 1;
+  return chunks;
+}
+
+template <int MAXN>
+__global__ void __launch_bounds__(kDasThreads) das_partial_kernel(const float2* __restrict__ s,
+                                                                 const float* __restrict__ kfreq,
+                                                                 const float* __restrict__ ant, int nfreq, int nant,
+                                                                 int nxp, int nyp, float px0, float py0, float pix,
+                                                                 int chunks, float2* __restrict__ partial) {
+  extern __shared__ float2 s_s[];  // (fchunk, nant, nant)
+  const int npix = nxp * nyp;
+  const int fpc = (nfreq + chunks - 1) / chunks;
+  const int fa = blockIdx.y * fpc, fb = min(nfreq, fa + fpc);
+  const int nn = nant * nant;
+  for (int i = threadIdx.x; i < (fb - fa) * nn; i += blockDim.x) s_s[i] = s[(size_t)fa * nn + i];
+  __syncthreads();
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= npix) return;
+  const int i = pid / nyp, j = pid % nyp;
+  const float px = px0 + i * pix, py = py0 + j * pix;
+  float d[MAXN];
+#pragma unroll
+  for (int m = 0; m < MAXN; ++m) {
+    if (m < nant) {
+      const float dx = px - ant[2 * m], dy = py - ant[2 * m + 1];
+      d[m] = sqrtf(dx * dx + dy * dy);
+    }
+  }
+  float accx = 0.f, accy = 0.f;
+  for (int f = fa; f < fb; ++f) {
+    const float k = kfreq[f];
+    float ar[MAXN], ai[MAXN];
+#pragma unroll
+    for (int m = 0; m < MAXN; ++m) {
+      if (m < nant) {
+        float sn, cs;
+        sincosf(k * d[m], &sn, &cs);
+        ar[m] = cs;
+        ai[m] = -sn;
+      }
+    }
+    const float2* S = s_s + (size_t)(f - fa) * nn;
+#pragma unroll
+    for (int tx = 0; tx < MAXN; ++tx) {
+      if (tx < nant) {
+        float tr = 0.f, ti = 0.f;
+#pragma unroll
+        for (int rx = 0; rx < MAXN; ++rx) {
+          if (rx < nant) {
+            const float2 v = S[rx * nant + tx];
+            tr = fmaf(v.x, ar[rx], fmaf(-v.y, ai[rx], tr));
+            ti = fmaf(v.x, ai[rx], fmaf(v.y, ar[rx], ti));
+          }
+        }
+        accx = fmaf(tr, ar[tx], fmaf(-ti, ai[tx], accx));
+        accy = fmaf(tr, ai[tx], fmaf(ti, ar[tx], accy));
+      }
+    }
+  }
+  partial[(size_t)blockIdx.y * npix + pid] = make_float2(accx, accy);
+}
+
+// Single block: add the chunks, |.|, min/max with warp shuffles, normalise.
+__global__ void __launch_bounds__(1024) das_finish_kernel(const float2* __restrict__ partial, int chunks, int npix,
+                                                          int normalize, float* __restrict__ image) {
+  __shared__ float s_min[32], s_max[32];
+  float lo = 3.4e38f, hi = 0.f;
+  for (int p = threadIdx.x; p < npix; p += blockDim.x) {
+    float x = 0.f, y = 0.f;
+    for (int c = 0; c < chunks; ++c) {
+      const float2 v = partial[(size_t)c * npix + p];
+      x += v.x;
+      y += v.y;
+    }
+    const float m = hypotf(x, y);
+    image[p] = m;
+    lo = fminf(lo, m);
+    hi = fmaxf(hi, m);
+  }
+  if (!normalize) return;
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  const int w = threadIdx.x / 32, ln = threadIdx.x % 32;
+  if (ln == 0) { s_min[w] = lo; s_max[w] = hi; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) / 32;
+    lo = ln < nw ? s_min[ln] : 3.4e38f;
+    hi = ln < nw ? s_max[ln] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (ln == 0) { s_min[0] = lo; s_max[0] = hi; }
+  }
+  __syncthreads();
+  lo = s_min[0];
+  const float range = s_max[0] - lo;
+  for (int p = threadIdx.x; p < npix; p += blockDim.x) {
+    const float v = image[p] - lo;
+    image[p] = range > 0.f ? v / range : v;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Time-domain DAS (scripts/verify_dataset_with_das.py:37-103), one thread per
+// pixel.  FP64 without contraction for the delay index (int() truncation).
+// --------------------------------------------------------------------------
+__global__ void das_time_kernel(const float2* __restrict__ s, const double* __restrict__ ant, int nant, int ntime,
+                                int grid, double dx, double dt, float* __restrict__ image) {
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= grid * grid) return;
+  const int i = pid / grid, j = pid % grid;
+  const double px = __dmul_rn((double)i, dx), py = __dmul_rn((double)j, dx);
+  const double C = 3e8;
+  double acc = 0.0;
+  for (int tx = 0; tx < nant; ++tx) {
+    const double ax = __dsub_rn(ant[2 * tx], px), ay = __dsub_rn(ant[2 * tx + 1], py);
+    const double dtx = __dsqrt_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
+    for (int rx = 0; rx < nant; ++rx) {
+      if (rx == tx) continue;
+      const double bx = __dsub_rn(ant[2 * rx], px), by = __dsub_rn(ant[2 * rx + 1], py);
+      const double drx = __dsqrt_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)));
+      const double t = __ddiv_rn(__ddiv_rn(__dadd_rn(dtx, drx), C), dt);
+      const long long idx = (long long)t;  // truncation toward zero, as int()
+      if (idx >= 0 && idx < ntime) {
+        const float2 v = s[((size_t)tx * nant + rx) * ntime + idx];
+        acc += hypot((double)v.x, (double)v.y);
+      }
+    }
+  }
+  image[pid] = (float)acc;
+}
+
+}  // namespace ceep
+
+using ceep::fail;
+
+extern "C" int ceep_dft(const float* series, const float* twiddle, float* s_out, int32_t ntx, int32_t nprobe,
+                        int32_t nsteps, int32_t nfreq, void* stream) {
+  if (!series || !twiddle || !s_out) return fail(CEEP_ERR_INVALID, "ceep_dft: null pointer");
+  if (ntx < 1 || nprobe < 1 || nsteps < 1 || nfreq < 1)
+    return fail(CEEP_ERR_INVALID, "ceep_dft: sizes ntx=%d nprobe=%d nsteps=%d nfreq=%d", ntx, nprobe, nsteps,
+                nfreq);
+  dim3 grid((nfreq + ceep::kDftT - 1) / ceep::kDftT, (ntx * nprobe + ceep::kDftT - 1) / ceep::kDftT);
+  ceep::dft_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      series, reinterpret_cast<const float2*>(twiddle), reinterpret_cast<float2*>(s_out), ntx, nprobe, nsteps,
+      nfreq);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "dft_kernel launch");
+}
+
+extern "C" int64_t ceep_das_workspace_bytes(int32_t nx_pix, int32_t ny_pix, int32_t nfreq) {
+  if (nx_pix < 1 || ny_pix < 1 || nfreq < 1) return 0;
+  const int npix = nx_pix * ny_pix;
+  return (int64_t)ceep::das_chunks(npix, nfreq) * npix * (int64_t)sizeof(float2);
+}
+
+extern "C" int ceep_das(const float* s, const float* kfreq, const float* ant_xy, int32_t nfreq, int32_t nant,
+                        int32_t nx_pix, int32_t ny_pix, float px0, float py0, float pix, int normalize, void* work,
+                        float* image, void* stream) {
+  if (!s || !kfreq || !ant_xy || !work || !image) return fail(CEEP_ERR_INVALID, "ceep_das: null pointer");
+  if (nfreq < 1 || nant < 1 || nx_pix < 1 || ny_pix < 1)
+    return fail(CEEP_ERR_INVALID, "ceep_das: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix, ny_pix);
+  if (nant > ceep::kDasMaxAnt)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_das: %d antennas (at most %d)", nant, ceep::kDasMaxAnt);
+  const int npix = nx_pix * ny_pix;
+  const int chunks = ceep::das_chunks(npix, nfreq);
+  const int fpc = (nfreq + chunks - 1) / chunks;
+  const size_t smem = (size_t)fpc * nant * nant * sizeof(float2);
+  if (smem > 200 * 1024) return fail(CEEP_ERR_UNSUPPORTED, "ceep_das: S chunk of %zu bytes too large", smem);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  dim3 grid((npix + ceep::kDasThreads - 1) / ceep::kDasThreads, chunks);
+  float2* partial = static_cast<float2*>(work);
+  const float2* S = reinterpret_cast<const float2*>(s);
+  cudaError_t e;
+#define CEEP_DAS_LAUNCH(M)                                                                                 \
+  e = cudaFuncSetAttribute(ceep::das_partial_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                           (int)smem);                                                                     \
+  if (e == cudaSuccess) {                                                                                  \
+    ceep::das_partial_kernel<M><<<grid, ceep::kDasThreads, smem, st>>>(S, kfreq, ant_xy, nfreq, nant,      \
+                                                                      nx_pix, ny_pix, px0, py0, pix,       \
+                                                                      chunks, partial);                    \
+    e = cudaGetLastError();                                                                                \
+  }
+  if (nant <= 8) {
+    CEEP_DAS_LAUNCH(8)
+  } else if (nant <= 16) {
+    CEEP_DAS_LAUNCH(16)
+  } else {
+    CEEP_DAS_LAUNCH(32)
+  }
+#undef CEEP_DAS_LAUNCH
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "das_partial_kernel launch");
+  ceep::das_finish_kernel<<<1, 1024, 0, st>>>(partial, chunks, npix, normalize, image);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "das_finish_kernel launch");
+}
+
+extern "C" int ceep_das_time(const float* s, const double* ant_xy, int32_t nant, int32_t ntime, int32_t grid,
+                             double dx, double frequency, float* image, void* stream) {
+  if (!s || !ant_xy || !image) return fail(CEEP_ERR_INVALID, "ceep_das_time: null pointer");
+  if (nant < 1 || ntime < 1 || grid < 1 || !(frequency > 0))
+    return fail(CEEP_ERR_INVALID, "ceep_das_time: sizes nant=%d ntime=%d grid=%d", nant, ntime, grid);
+  const double dt = 1.0 / (4.0 * frequency);
+  const int npix = grid * grid;
+  ceep::das_time_kernel<<<(npix + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      reinterpret_cast<const float2*>(s), ant_xy, nant, ntime, grid, dx, dt, image);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "das_time_kernel launch");
+}

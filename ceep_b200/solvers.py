@@ -1,0 +1,337 @@
+"""Drop-in batched solvers backed by the sm_100a kernels.
+
+``BatchedFDTD2D`` keeps the constructor, attributes and methods of the
+reference class (src/ceep/solvers/fdtd_2d_batched.py:41-611) so callers such
+as dataset generators switch by changing the import.  Differences, all
+documented on the methods:
+
+* positions are validated up front (ValueError) instead of wrapping or
+  failing inside the loop;
+* arithmetic is FP32 on the device (the reference is FP64);
+* ``probe_data``, ``ez``, ``hx``, ``hy`` are torch CUDA tensors (the
+  reference exposes CuPy arrays); ``run()`` still returns host float64 series;
+* keyword-only extensions (defaults reproduce the reference): ``courant``,
+  ``cpml_R0``, ``cpml_order``, ``waveform``, ``frequencies`` (S-matrix),
+  ``set_dispersion`` (Debye/Lorentz ADE), ``device``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import physics
+from ._lib import Desc2D, check, lib
+from .constants import C_0, EPS_0, MU_0
+
+
+def _pad_tx(ntx: int) -> int:
+    if ntx <= 4:
+        return 4
+    if ntx <= 8:
+        return 8
+    if ntx <= 16:
+        return 16
+    return 32 * ((ntx + 31) // 32)
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+class BatchedFDTD2D:
+    """Batched 2D TMz FDTD, one transmit event per batch element, shared materials.
+
+    Parameters mirror fdtd_2d_batched.py:66-77.
+    """
+
+    def __init__(self, nx: int, ny: int, dx: float, total_steps: int, cpml_thickness: int,
+                 source_positions: List[Tuple[int, int]], probe_positions: List[Tuple[int, int]],
+                 frequency: float, delay_factor: float = 5.0, *, courant: Optional[float] = None,
+                 cpml_R0: float = 1e-8, cpml_order: int = 3, waveform: Optional[np.ndarray] = None,
+                 frequencies: Optional[Sequence[float]] = None, device: str = "cuda",
+                 rows_per_block: int = 0, use_graph: bool = True):
+        self.nx, self.ny = int(nx), int(ny)
+        self.dx = self.dy = float(dx)
+        self.total_steps = int(total_steps)
+        self.cpml_n = int(cpml_thickness)
+        self.source_positions = [tuple(int(v) for v in p) for p in source_positions]
+        self.probe_positions = [tuple(int(v) for v in p) for p in probe_positions]
+        self.frequency = float(frequency)
+        self.delay_factor = float(delay_factor)
+        self.batch = len(self.source_positions)
+        # CFL step of fdtd_2d_batched.py:92 unless a Courant number is given
+        self.dt = dx / (C_0 * np.sqrt(2.0)) * 0.99 if courant is None else float(courant) * dx / C_0
+        self._eps_r = np.ones((nx, ny), dtype=np.float64)
+        self._sigma_e = np.zeros((nx, ny), dtype=np.float64)
+        self._debye: list = []
+        self._lorentz: list = []
+        self.cpml_R0, self.cpml_order = float(cpml_R0), int(cpml_order)
+        self._waveform_override = None if waveform is None else np.asarray(waveform, np.float64)
+        self.frequencies = None if frequencies is None else np.asarray(frequencies, np.float64)
+        self.device = torch.device(device)
+        self.rows_per_block = int(rows_per_block)
+        self.use_graph = bool(use_graph)
+        self._built = False
+        self._plan = None
+        self._validate()
+
+    # -- validation (the reference silently wraps negative indices) ----------
+    def _validate(self):
+        n, nx, ny = self.cpml_n, self.nx, self.ny
+        if self.batch < 1:
+            raise ValueError("at least one source position is required")
+        if n < 0 or n == 1:
+            raise ValueError("cpml_thickness must be 0 or >= 2 (n = 1 divides by zero in the grading)")
+        if nx < 2 * n + 2 or ny < 2 * n + 2:
+            raise ValueError(f"grid {nx}x{ny} must exceed twice the CPML thickness ({n}) by 2")
+        if self.total_steps < 1:
+            raise ValueError("total_steps must be >= 1")
+        for kind, pts in (("source", self.source_positions), ("probe", self.probe_positions)):
+            for p in pts:
+                if len(p) != 2 or not (0 <= p[0] < nx and 0 <= p[1] < ny):
+                    raise ValueError(f"{kind} position {p} outside the {nx}x{ny} grid")
+        if self._waveform_override is not None and self._waveform_override.shape != (self.total_steps,):
+            raise ValueError("waveform must have total_steps samples")
+
+    # -- materials (fdtd_2d_batched.py:100-136) ------------------------------
+    def set_material_circle(self, center_x: int, center_y: int, radius: int, eps_r: float,
+                            sigma_e: float = 0.0) -> None:
+        x, y = np.meshgrid(np.arange(self.nx), np.arange(self.ny), indexing="ij")
+        mask = (x - center_x) ** 2 + (y - center_y) ** 2 <= radius ** 2
+        self._eps_r[mask] = eps_r
+        self._sigma_e[mask] = sigma_e
+
+    def set_phantom(self, phantom) -> None:
+        """Same duck typing as fdtd_2d_batched.py:112-136 (TypeError otherwise).
+        A phantom that also exposes ``get_dispersion()`` (Debye/Lorentz maps)
+        sets the ADE poles as well."""
+        if hasattr(phantom, "get_eps_map"):
+            eps_r, sigma_e = phantom.get_eps_map(self.frequency)
+            self._eps_r[:] = eps_r
+            self._sigma_e[:] = sigma_e
+        elif hasattr(phantom, "get_permittivity_map"):
+            eps_real, eps_imag = phantom.get_permittivity_map(self.frequency)
+            self._eps_r[:] = eps_real
+            self._sigma_e[:] = eps_imag * (2 * np.pi * self.frequency) * EPS_0
+        elif hasattr(phantom, "eps_r"):
+            self._eps_r[:] = phantom.eps_r
+            if hasattr(phantom, "sigma_e"):
+                self._sigma_e[:] = phantom.sigma_e
+        else:
+            raise TypeError("Phantom must have get_eps_map(), get_permittivity_map(), or eps_r attribute")
+        if hasattr(phantom, "get_dispersion"):
+            d = phantom.get_dispersion()
+            self.set_dispersion(debye=d.get("debye", ()), lorentz=d.get("lorentz", ()))
+
+    def set_dispersion(self, debye=(), lorentz=()) -> None:
+        """Debye poles ``(delta_eps, tau)`` and Lorentz poles ``(delta_eps, omega_0, delta)``
+        as per-cell (nx, ny) maps or scalars; ``_eps_r`` then holds eps_inf.
+        The ADE acts on the interior E region only, so every pole map must be zero
+        in the CPML strips (ValueError otherwise)."""
+        if self._built and (len(debye), len(lorentz)) != (len(self._debye), len(self._lorentz)):
+            raise RuntimeError("the number of Debye/Lorentz poles cannot change after the first run(); "
+                               "create a new solver")
+        if len(debye) + len(lorentz) > 2:
+            raise ValueError("at most two ADE poles per cell are compiled in")
+        shp = (self.nx, self.ny)
+        deb = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in debye]
+        lor = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in lorentz]
+        n = self.cpml_n
+        inner = np.zeros(shp, bool)
+        inner[n + 1:self.nx - n, n + 1:self.ny - n] = True
+        for p in deb:
+            if np.any((p[1] > 0) & (p[0] != 0) & ~inner):
+                raise ValueError("Debye pole present outside the interior E region")
+        for p in lor:
+            if np.any((p[1] > 0) & (p[0] != 0) & ~inner):
+                raise ValueError("Lorentz pole present outside the interior E region")
+        self._debye, self._lorentz = deb, lor
+
+    # -- build: host FP64 coefficients -> device FP32 (fdtd_2d_batched.py:138-270)
+    def _build(self):
+        dev = self.device
+        if dev.type != "cuda" or not torch.cuda.is_available():
+            raise RuntimeError("BatchedFDTD2D needs a CUDA device (B200); there is no CPU path")
+        lib()
+        nx, ny, n, B = self.nx, self.ny, self.cpml_n, self.batch
+        BP = _pad_tx(B)
+        self.ntx_pad = BP
+        dt = self.dt
+        f32 = dict(dtype=torch.float32, device=dev)
+        eps_add, ade = physics.ade_coefficients(dt, self._debye, self._lorentz, (nx, ny))
+        ca, cb = physics.update_coefficients(self._eps_r, self._sigma_e, dt, eps_add if ade.shape[0] else None)
+        to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
+        # (y, x) transposes of the reference's (x, y) maps
+        self._coef = to_dev(np.stack([ca.T, cb.T], axis=-1))
+        self._dteps = to_dev((dt / (self._eps_r * EPS_0)).T)
+        if ade.shape[0]:
+            self._ade_coef = to_dev(ade.transpose(0, 2, 1, 3))
+        else:
+            self._ade_coef = None
+        b, c = physics.cpml_profile(n, self.dx, dt, self.cpml_R0, self.cpml_order)
+        self._cpml_b, self._cpml_c = to_dev(b if n else np.zeros(1)), to_dev(c if n else np.zeros(1))
+        w = (self._waveform_override if self._waveform_override is not None
+             else physics.gaussian_derivative(self.total_steps, dt, self.frequency, self.delay_factor))
+        self.waveform = to_dev(w)
+        field = lambda: torch.zeros((ny, nx, BP), **f32)
+        self._ez = [field(), field()]
+        self._hx = [field(), field()]
+        self._hy = [field(), field()]
+        nn = max(n, 1)
+        self._psi_hy = [torch.zeros((ny, 2 * nn, BP), **f32) for _ in range(2)]
+        self._psi_hx = [torch.zeros((2 * nn, nx, BP), **f32) for _ in range(2)]
+        self._psi_ezx = torch.zeros((ny, 2 * nn, BP), **f32)
+        self._psi_ezy = torch.zeros((2 * nn, nx, BP), **f32)
+        nd, nl = len(self._debye), len(self._lorentz)
+        self._j = torch.zeros((nd + nl, ny, nx, BP), **f32) if nd + nl else None
+        self._j_prev = torch.zeros((nl, ny, nx, BP), **f32) if nl else None
+        P = len(self.probe_positions)
+        self._src = to_dev(np.array(self.source_positions, np.int32).reshape(-1, 2), torch.int32)
+        self._prb = to_dev(np.array(self.probe_positions, np.int32).reshape(-1, 2), torch.int32)
+        flags = np.zeros(ny, np.uint8)
+        for _, y in self.source_positions:
+            flags[y] |= 1
+        for _, y in self.probe_positions:
+            flags[y] |= 2
+        self._flags = to_dev(flags, torch.uint8)
+        self.probe_data = torch.zeros((B, max(P, 1), self.total_steps), **f32)
+
+        d = Desc2D()
+        d.nx, d.ny, d.cpml, d.ntx, d.ntx_pad = nx, ny, n, B, BP
+        d.nprobe, d.nsteps, d.n_debye, d.n_lorentz = P, self.total_steps, nd, nl
+        d.db, d.inv_dx, d.dt = dt / MU_0, 1.0 / self.dx, dt
+        for k in range(2):
+            d.ez[k], d.hx[k], d.hy[k] = _ptr(self._ez[k]), _ptr(self._hx[k]), _ptr(self._hy[k])
+            d.psi_hy[k], d.psi_hx[k] = _ptr(self._psi_hy[k]), _ptr(self._psi_hx[k])
+        d.psi_ezx, d.psi_ezy = _ptr(self._psi_ezx), _ptr(self._psi_ezy)
+        d.j, d.j_prev = _ptr(self._j), _ptr(self._j_prev)
+        d.coef, d.dteps, d.ade_coef = _ptr(self._coef), _ptr(self._dteps), _ptr(self._ade_coef)
+        d.cpml_b, d.cpml_c = _ptr(self._cpml_b), _ptr(self._cpml_c)
+        d.src_xy, d.prb_xy, d.row_flags = _ptr(self._src), _ptr(self._prb), _ptr(self._flags)
+        d.waveform, d.probes = _ptr(self.waveform), _ptr(self.probe_data)
+        d.rows_per_block = self.rows_per_block
+        self._desc = d
+        plan = C.c_void_p()
+        check(lib().ceep2d_plan_create(C.byref(d), C.byref(plan)), "ceep2d_plan_create")
+        self._plan = plan
+        self._built = True
+
+    def __del__(self):
+        if getattr(self, "_plan", None) is not None:
+            try:
+                lib().ceep2d_plan_destroy(self._plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    # -- time loop ------------------------------------------------------------
+    def advance(self, step0: int = 0, nsteps: Optional[int] = None, stream=None) -> None:
+        """Launch steps [step0, step0+nsteps) on ``stream`` without synchronising."""
+        if not self._built:
+            self._build()
+        nsteps = self.total_steps - step0 if nsteps is None else nsteps
+        s = torch.cuda.current_stream(self.device) if stream is None else stream
+        check(lib().ceep2d_plan_run(self._plan, step0, nsteps, C.c_void_p(s.cuda_stream),
+                                    int(self.use_graph)), "ceep2d_plan_run")
+
+    def run(self) -> Dict[int, Dict[int, np.ndarray]]:
+        """All time steps; returns ``{tx: {rx: float64 series of total_steps}}``
+        (fdtd_2d_batched.py:408-538).  As in the reference, fields persist, so
+        a second call continues the simulation and overwrites the series."""
+        self.advance(0, self.total_steps)
+        probe_np = self.probe_data.double().cpu().numpy()
+        P = len(self.probe_positions)
+        return {tx: {rx: probe_np[tx, rx, :] for rx in range(P)} for tx in range(self.batch)}
+
+    def run_cpu(self) -> Dict[int, Dict[int, np.ndarray]]:
+        """The reference's CPML-free variant (fdtd_2d_batched.py:540-611): no
+        CPML, fresh fields, H zeroed on the far edge, E on all edges.  In this
+        framework it runs on the GPU (a CPML thickness of 0 gives exactly that
+        region map); it does not touch this solver's state."""
+        twin = BatchedFDTD2D(self.nx, self.ny, self.dx, self.total_steps, 0, self.source_positions,
+                             self.probe_positions, self.frequency, self.delay_factor,
+                             courant=None if self.dt == self.dx / (C_0 * np.sqrt(2.0)) * 0.99 else self.dt * C_0 / self.dx,
+                             waveform=self._waveform_override, device=str(self.device), use_graph=self.use_graph)
+        twin._eps_r[:] = self._eps_r
+        twin._sigma_e[:] = self._sigma_e
+        return twin.run()
+
+    # -- S-parameters (dft.py:55-103, s_params.py:70-137) ---------------------
+    def s_matrix(self, frequencies: Optional[Sequence[float]] = None) -> np.ndarray:
+        """Complex S[f, rx, tx] = sum_n probe[tx, rx, n] e^{-j w n dt} dt of the
+        last run, computed on the device."""
+        freqs = self.frequencies if frequencies is None else np.asarray(frequencies, np.float64)
+        if freqs is None:
+            raise ValueError("no frequencies given")
+        from .spectral import dft
+        return dft(self.probe_data[:, :len(self.probe_positions)], freqs, self.dt).cpu().numpy().astype(np.complex128)
+
+    # -- state views in the reference layout (B, nx, ny) ----------------------
+    def _cur(self) -> int:
+        return lib().ceep2d_plan_current_buffer(self._plan) if self._built else 0
+
+    @property
+    def ez(self):
+        return self._ez[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+
+    @property
+    def hx(self):
+        return self._hx[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+
+    @property
+    def hy(self):
+        return self._hy[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+
+    def reset(self) -> None:
+        """Zero every field, psi and ADE state (not in the reference: lets one
+        solver be reused for a new phantom without reallocating)."""
+        if not self._built:
+            return
+        for t in (self._ez + self._hx + self._hy + self._psi_hy + self._psi_hx +
+                  [self._psi_ezx, self._psi_ezy, self._j, self._j_prev, self.probe_data]):
+            if t is not None:
+                t.zero_()
+        check(lib().ceep2d_plan_reset(self._plan), "ceep2d_plan_reset")
+
+    def material_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
+        """Device tensors (coef, dteps, ade_coef) for the given (nx, ny) maps in
+        this solver's layout, for ``load_material_tensors``."""
+        eps_add, ade = physics.ade_coefficients(self.dt, debye, lorentz, (self.nx, self.ny))
+        ca, cb = physics.update_coefficients(eps_r, sigma_e, self.dt, eps_add if ade.shape[0] else None)
+        dev = self.device
+        coef = torch.as_tensor(np.ascontiguousarray(np.stack([ca.T, cb.T], -1)), dtype=torch.float32).to(dev)
+        dteps = torch.as_tensor(np.ascontiguousarray((self.dt / (np.asarray(eps_r) * EPS_0)).T),
+                                dtype=torch.float32).to(dev)
+        ade_t = (torch.as_tensor(np.ascontiguousarray(ade.transpose(0, 2, 1, 3)), dtype=torch.float32).to(dev)
+                 if ade.shape[0] else None)
+        return coef, dteps, ade_t
+
+    def load_material_tensors(self, mats) -> None:
+        """Device-to-device copy of precomputed material tensors into the plan's
+        buffers (no host traffic); the pole count must match the first build."""
+        if not self._built:
+            self._build()
+        coef, dteps, ade_t = mats
+        self._coef.copy_(coef, non_blocking=True)
+        self._dteps.copy_(dteps, non_blocking=True)
+        if (ade_t is None) != (self._ade_coef is None):
+            raise ValueError("ADE pole count differs from the built solver")
+        if ade_t is not None:
+            self._ade_coef.copy_(ade_t, non_blocking=True)
+
+    def update_materials(self) -> None:
+        """Re-upload ca/cb/dteps (and ADE coefficients) after editing
+        ``_eps_r``/``_sigma_e``/poles on a built solver."""
+        if not self._built:
+            return
+        eps_add, ade = physics.ade_coefficients(self.dt, self._debye, self._lorentz, (self.nx, self.ny))
+        if ade.shape[0] != (0 if self._ade_coef is None else self._ade_coef.shape[0]):
+            raise ValueError("the number of ADE poles cannot change after the first run()")
+        ca, cb = physics.update_coefficients(self._eps_r, self._sigma_e, self.dt, eps_add if ade.shape[0] else None)
+        self._coef.copy_(torch.as_tensor(np.stack([ca.T, cb.T], -1), dtype=torch.float32))
+        self._dteps.copy_(torch.as_tensor((self.dt / (self._eps_r * EPS_0)).T, dtype=torch.float32))
+        if ade.shape[0]:
+            self._ade_coef.copy_(torch.as_tensor(ade.transpose(0, 2, 1, 3), dtype=torch.float32))

@@ -1,0 +1,154 @@
+/*
+ * ceep_b200 — C ABI of the B200-native batched multistatic FDTD path.
+ *
+ * Drop-in boundary for the hot path of the reference project
+ * (shahzaibshazoo/ceep-v1).  The reference has no FFI: its seam is the Python
+ * solver classes plus the global array-module switch.  Each entry point below
+ * replaces one piece of that path; the reference location is cited beside it.
+ *
+ * Conventions
+ *   - Every buffer argument is a DEVICE pointer owned by the caller (in the
+ *     Python host code: torch tensors).  The library never allocates device
+ *     memory, never calls exit/abort, and never synchronises the device
+ *     except where a function says so.
+ *   - Field layout is (y, x, tx) in 2D and (z, y, x, tx) in 3D, tx innermost,
+ *     tx padded to `ntx_pad` (a multiple of 4; a multiple of 32 above 32).
+ *   - Functions return 0 on success or a ceep_status code; the message of
+ *     the last failure on the calling thread is returned by ceep_last_error().
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).
+ *   - A plan is not thread-safe; use one plan per host thread.
+ */
+#ifndef CEEP_B200_H
+#define CEEP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ceep_status {
+  CEEP_OK = 0,
+  CEEP_ERR_INVALID = 1,     /* bad argument (sizes, positions, null pointer) */
+  CEEP_ERR_CUDA = 2,        /* a CUDA runtime call failed                    */
+  CEEP_ERR_UNSUPPORTED = 3, /* configuration outside what is compiled in     */
+  CEEP_ERR_TIMEOUT = 4,     /* a bounded device wait gave up                 */
+  CEEP_ERR_NONFINITE = 5    /* NaN/Inf found by the sentinel                 */
+} ceep_status;
+
+/* Library version and last error (thread-local message). */
+int ceep_version(void);
+const char* ceep_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * 2D TMz batched FDTD.
+ * Replaces BatchedFDTD2D.run()'s time loop, src/ceep/solvers/fdtd_2d_batched.py:454-526
+ * (interior H :471-483, _apply_h_cpml :272-334, interior E :491-498,
+ *  _apply_e_cpml :336-406, edge zeroing :503-507, source :509-515,
+ *  probes :517-526), with the Debye/Lorentz ADE of
+ *  src/ceep/materials/dispersive.py:364-404 composed into the interior E update.
+ * ---------------------------------------------------------------------- */
+typedef struct ceep2d_desc {
+  int32_t nx, ny;          /* grid (x, y)                                    */
+  int32_t cpml;            /* CPML thickness n (0, or 2 <= n)                */
+  int32_t ntx, ntx_pad;    /* transmit events and padded lane count          */
+  int32_t nprobe;          /* receivers                                      */
+  int32_t nsteps;          /* length of waveform and of each probe series    */
+  int32_t n_debye, n_lorentz; /* ADE poles per cell (0..2 each)              */
+  float db;                /* dt / mu0                                       */
+  float inv_dx;            /* 1 / dx (dx == dy)                              */
+  float dt;                /* time step (ADE dE/dt)                          */
+  /* ping-pong state, each (ny, nx, ntx_pad) float; [k] = buffer k          */
+  float* ez[2];
+  float* hx[2];
+  float* hy[2];
+  /* H-CPML psi, ping-pong: x strips (ny, 2n, ntx_pad), y strips (2n, nx, ntx_pad) */
+  float* psi_hy[2];
+  float* psi_hx[2];
+  /* E-CPML psi, in place, same shapes as above                               */
+  float* psi_ezx;
+  float* psi_ezy;
+  /* ADE currents, in place: (poles, ny, nx, ntx_pad); Lorentz keeps J^{n-1}  */
+  float* j;                /* n_debye + n_lorentz planes                     */
+  float* j_prev;           /* n_lorentz planes                               */
+  const float* coef;       /* (ny, nx, 2): ca, cb                            */
+  const float* dteps;      /* (ny, nx): dt / (eps_r eps0) for E-CPML         */
+  const float* ade_coef;   /* (poles, ny, nx, 4): Debye k1,k2,gamma ; Lorentz k1,k2,k3 */
+  const float* cpml_b;     /* (n)                                            */
+  const float* cpml_c;     /* (n)                                            */
+  const int32_t* src_xy;   /* (ntx, 2) source cell per transmit event        */
+  const int32_t* prb_xy;   /* (nprobe, 2)                                    */
+  const uint8_t* row_flags;/* (ny): bit0 a source on this row, bit1 a probe  */
+  const float* waveform;   /* (nsteps)                                       */
+  float* probes;           /* (ntx, nprobe, nsteps) output series            */
+  int32_t rows_per_block;  /* 0 = library default                           */
+} ceep2d_desc;
+
+typedef struct ceep2d_plan ceep2d_plan;
+
+/* Validate the descriptor and build a plan (host memory only). */
+int ceep2d_plan_create(const ceep2d_desc* desc, ceep2d_plan** out);
+/* Advance `nsteps` steps starting at global step `step0` (buffer parity is
+ * step0 & 1).  use_graph != 0 captures the launches once per (step0, nsteps)
+ * and replays the CUDA graph on later calls. */
+int ceep2d_plan_run(ceep2d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+int ceep2d_plan_destroy(ceep2d_plan* plan);
+/* Number of kernel launches one step issues. */
+int ceep2d_launches_per_step(const ceep2d_plan* plan);
+/* Which ping-pong buffer (0 or 1) holds the current state; reset sets it to 0
+ * (the caller zeroes the state buffers). */
+int ceep2d_plan_current_buffer(const ceep2d_plan* plan);
+int ceep2d_plan_reset(ceep2d_plan* plan);
+/* sizeof(ceep2d_desc), for binding layers to check their struct mirror. */
+int64_t ceep2d_desc_size(void);
+
+/* ------------------------------------------------------------------------
+ * On-device DFT of the probe series into the S-matrix.
+ * Replaces the DFTMonitor accumulation of src/ceep/solvers/dft.py:55-90 run
+ * over every (tx, rx) series, laid out as MultistaticSParameters.s_matrix
+ * (src/ceep/solvers/s_params.py:77-79): out[f, rx, tx] (complex64).
+ *   series  : (ntx, nprobe, nsteps) float
+ *   twiddle : (nfreq, nsteps) float2 = (cos(w n dt) dt, -sin(w n dt) dt),
+ *             built in FP64 on the host and rounded once
+ *   s_out   : (nfreq, nprobe, ntx) float2
+ * ---------------------------------------------------------------------- */
+int ceep_dft(const float* series, const float* twiddle, float* s_out,
+             int32_t ntx, int32_t nprobe, int32_t nsteps, int32_t nfreq, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Frequency-domain delay-and-sum image.
+ * Replaces DelayAndSumBeamformer._reconstruct_das,
+ * src/ceep/imaging/beamforming.py:210-257 (delays :146-182, pixel positions
+ * :73-83, velocity :144).
+ *   s       : (nfreq, nant, nant) float2, s[f, rx, tx] (frequency-masked)
+ *   kfreq   : (nfreq) float, 2*pi*f / v
+ *   ant_xy  : (nant, 2) float, antenna positions in metres
+ *   px0,py0 : position of pixel (0,0) in metres; pix = pixel pitch
+ *   work    : caller scratch, ceep_das_workspace_bytes() bytes
+ *   image   : (nx_pix, ny_pix) float, |sum|, normalised to (I-min)/max when
+ *             normalize != 0
+ * ---------------------------------------------------------------------- */
+int64_t ceep_das_workspace_bytes(int32_t nx_pix, int32_t ny_pix, int32_t nfreq);
+int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
+             int32_t nfreq, int32_t nant, int32_t nx_pix, int32_t ny_pix,
+             float px0, float py0, float pix, int normalize,
+             void* work, float* image, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Time-domain delay-and-sum image.
+ * Replaces das_imaging, scripts/verify_dataset_with_das.py:37-103:
+ * pixel (i,j) at (i*dx, j*dx); for tx != rx, idx = int((|a_tx-p|+|a_rx-p|)/C/dt)
+ * with dt = 1/(4 f) and C = 3e8; image += |s[tx, rx, idx]| when in range.
+ * Distances and the index are computed in FP64 without contraction so the
+ * truncation agrees with NumPy; |s| is accumulated in FP64.
+ *   s      : (nant, nant, ntime) complex64 as float2, s[tx, rx, t]
+ *   ant_xy : (nant, 2) double, metres
+ *   image  : (grid, grid) float, image[i, j] for pixel (i*dx, j*dx)
+ * ---------------------------------------------------------------------- */
+int ceep_das_time(const float* s, const double* ant_xy, int32_t nant, int32_t ntime,
+                  int32_t grid, double dx, double frequency, float* image, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CEEP_B200_H */
