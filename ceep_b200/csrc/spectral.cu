@@ -183,7 +183,10 @@ __global__ void __launch_bounds__(1024) das_finish_kernel(const float2* __restri
 
 // --------------------------------------------------------------------------
 // Time-domain DAS (scripts/verify_dataset_with_das.py:37-103), one thread per
-// pixel.  FP64 without contraction for the delay index (int() truncation).
+// pixel.  The delay index is truncated like int() in FP64, so every rounding
+// matters: |v| is sqrt(fma(v1, v1, v0*v0)), the rounding sequence of
+// np.linalg.norm on a 2-vector (its BLAS dot product), then the two sums and
+// divisions in the reference's order.
 // --------------------------------------------------------------------------
 __global__ void das_time_kernel(const float2* __restrict__ s, const double* __restrict__ ant, int nant, int ntime,
                                 int grid, double dx, double dt, float* __restrict__ image) {
@@ -195,11 +198,11 @@ __global__ void das_time_kernel(const float2* __restrict__ s, const double* __re
   double acc = 0.0;
   for (int tx = 0; tx < nant; ++tx) {
     const double ax = __dsub_rn(ant[2 * tx], px), ay = __dsub_rn(ant[2 * tx + 1], py);
-    const double dtx = __dsqrt_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)));
+    const double dtx = __dsqrt_rn(__fma_rn(ay, ay, __dmul_rn(ax, ax)));
     for (int rx = 0; rx < nant; ++rx) {
       if (rx == tx) continue;
       const double bx = __dsub_rn(ant[2 * rx], px), by = __dsub_rn(ant[2 * rx + 1], py);
-      const double drx = __dsqrt_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)));
+      const double drx = __dsqrt_rn(__fma_rn(by, by, __dmul_rn(bx, bx)));
       const double t = __ddiv_rn(__ddiv_rn(__dadd_rn(dtx, drx), C), dt);
       const long long idx = (long long)t;  // truncation toward zero, as int()
       if (idx >= 0 && idx < ntime) {

@@ -139,8 +139,9 @@ int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
  * Replaces das_imaging, scripts/verify_dataset_with_das.py:37-103:
  * pixel (i,j) at (i*dx, j*dx); for tx != rx, idx = int((|a_tx-p|+|a_rx-p|)/C/dt)
  * with dt = 1/(4 f) and C = 3e8; image += |s[tx, rx, idx]| when in range.
- * Distances and the index are computed in FP64 without contraction so the
- * truncation agrees with NumPy; |s| is accumulated in FP64.
+ * Distances and the index are computed in FP64 with NumPy's rounding sequence
+ * (|v| = sqrt(fma(v1, v1, v0*v0))) so the truncation agrees with the
+ * reference; |s| is accumulated in FP64.
  *   s      : (nant, nant, ntime) complex64 as float2, s[tx, rx, t]
  *   ant_xy : (nant, 2) double, metres
  *   image  : (grid, grid) float, image[i, j] for pixel (i*dx, j*dx)

@@ -175,6 +175,13 @@ def gen_das_time():
     img = v.das_imaging(s, pos, 2e9, G, dx)
     _save("das_time_small", s=s, positions=pos, frequency=np.float64(2e9),
           grid_size=np.int64(G), dx=np.float64(dx), image=img)
+    # grid-aligned geometry: many delays fall exactly on sample boundaries
+    N, T, G, dx = 4, 64, 24, 3.75e-3
+    pos = np.array([[0.0, 0.0], [0.0375, 0.0], [0.0, 0.075], [0.0375, 0.0375]])
+    s = np.arange(N * N * T, dtype=np.float64).reshape(N, N, T) % 97 + 1.0
+    img = v.das_imaging(s.astype(complex), pos, 2e9, G, dx)
+    _save("das_time_aligned", s=s, positions=pos, frequency=np.float64(2e9),
+          grid_size=np.int64(G), dx=np.float64(dx), image=img)
 
 
 def gen_ade():

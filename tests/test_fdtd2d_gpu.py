@@ -229,8 +229,13 @@ def test_linearity_at_full_size(cuda_device):
     for s in (a, b):
         s.set_material_circle(300, 300, 150, 40.0, 0.5)
         s.run()
-    # scaling by a power of two is exact in binary floating point
-    assert torch.equal(4.0 * a.probe_data, b.probe_data)
+    # scaling by a power of two commutes with every rounding except in the
+    # subnormal range (the far tail of the wave front), so outside it the
+    # results agree bit for bit
+    pa, pb = 4.0 * a.probe_data, b.probe_data
+    normal = pa.abs() > 1e-30
+    assert torch.equal(pa[normal], pb[normal])
+    assert rel_l2(pa.cpu().numpy(), pb.cpu().numpy()) < 1e-7
     assert torch.isfinite(a.probe_data).all()
 
 

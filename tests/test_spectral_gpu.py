@@ -75,13 +75,11 @@ def test_das_time_against_reference(cuda_device):
     np.testing.assert_allclose(img, g["image"], rtol=2e-6, atol=0)
 
 
-def test_das_time_index_truncation_matches_numpy(cuda_device):
+def test_das_time_index_truncation_matches_reference(cuda_device):
     """Grid-aligned geometry where many delays land exactly on sample
-    boundaries; the FP64 index must truncate exactly like int()."""
+    boundaries; the FP64 index must truncate exactly like the reference's int()."""
     from ceep_b200 import das_time
-    N, T, G, dx = 4, 64, 24, 3.75e-3
-    pos = np.array([[0.0, 0.0], [0.0375, 0.0], [0.0, 0.075], [0.0375, 0.0375]])
-    s = np.arange(N * N * T, dtype=np.float64).reshape(N, N, T) % 97 + 1.0
-    ref = osp.das_time(s, pos, 2e9, G, dx)
-    img = das_time(torch.as_tensor(s, dtype=torch.complex64, device=cuda_device), pos, 2e9, G, dx).cpu().numpy()
-    np.testing.assert_array_equal(img, ref.astype(np.float32))
+    g = load_golden("das_time_aligned")
+    s = torch.as_tensor(g["s"], dtype=torch.complex64, device=cuda_device)
+    img = das_time(s, g["positions"], float(g["frequency"]), int(g["grid_size"]), float(g["dx"])).cpu().numpy()
+    np.testing.assert_array_equal(img, g["image"].astype(np.float32))
