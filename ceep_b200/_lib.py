@@ -24,9 +24,9 @@ class Desc2D(C.Structure):
         ("db", C.c_float), ("inv_dx", C.c_float), ("dt", C.c_float),
         ("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hy", P * 2), ("psi_hx", P * 2),
         ("psi_ezx", P), ("psi_ezy", P), ("j", P), ("j_prev", P),
-        ("coef", P), ("dteps", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
+        ("coef", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
         ("src_xy", P), ("prb_xy", P), ("row_flags", P), ("waveform", P), ("probes", P),
-        ("rows_per_block", I32),
+        ("status", P), ("rows_per_block", I32),
     ]
 
 
@@ -41,6 +41,7 @@ _SIGS = {
     "ceep2d_plan_current_buffer": (C.c_int, [P]),
     "ceep2d_plan_reset": (C.c_int, [P]),
     "ceep2d_desc_size": (I64, []),
+    "ceep2d_plan_rows": (C.c_int, [P]),
     "ceep_dft": (C.c_int, [P, P, P, I32, I32, I32, I32, P]),
     "ceep_das_workspace_bytes": (I64, [I32, I32, I32]),
     "ceep_das": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),

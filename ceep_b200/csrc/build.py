@@ -19,7 +19,7 @@ ROOT = os.path.dirname(PKG)
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libceep_b200.so")
 SOURCES = ["capi.cu", "fdtd2d.cu", "spectral.cu"]
-HEADERS = ["common.cuh", "fdtd2d.cuh", "capi_internal.h"]
+HEADERS = ["common.cuh", "fdtd2d.cuh", "tma.cuh", "capi_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -56,12 +56,11 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
     return fail(CEEP_ERR_INVALID, "ntx=%d ntx_pad=%d (pad must be a multiple of 4 and >= ntx)", d->ntx,
                 d->ntx_pad);
   const int lanes = d->ntx_pad / 4;
-  const int group = lanes <= 8 ? lanes : 8;
+  const int L = lanes <= 8 ? lanes : 8;
   if (lanes > 8 && lanes % 8)
     return fail(CEEP_ERR_INVALID, "ntx_pad=%d above 32 must be a multiple of 32", d->ntx_pad);
-  if (group != 1 && group != 2 && group != 4 && group != 8)
-    return fail(CEEP_ERR_INVALID, "ntx_pad=%d: lanes per cell must be 1, 2, 4 or 8 (pad to 4, 8, 16, 32)",
-                d->ntx_pad);
+  if (L != 1 && L != 2 && L != 4 && L != 8)
+    return fail(CEEP_ERR_INVALID, "ntx_pad=%d: pad to 4, 8, 16 or a multiple of 32", d->ntx_pad);
   if (d->n_debye < 0 || d->n_lorentz < 0 || d->n_debye + d->n_lorentz > 2)
     return fail(CEEP_ERR_UNSUPPORTED, "ADE poles: at most 2 per cell (debye=%d lorentz=%d)", d->n_debye,
                 d->n_lorentz);
@@ -69,7 +68,7 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   for (int k = 0; k < 2; ++k)
     if (!d->ez[k] || !d->hx[k] || !d->hy[k]) return fail(CEEP_ERR_INVALID, "null field buffer");
   if (n > 0 && (!d->psi_hx[0] || !d->psi_hx[1] || !d->psi_hy[0] || !d->psi_hy[1] || !d->psi_ezx ||
-                !d->psi_ezy || !d->cpml_b || !d->cpml_c || !d->dteps))
+                !d->psi_ezy || !d->cpml_b || !d->cpml_c))
     return fail(CEEP_ERR_INVALID, "null CPML buffer");
   if (d->n_debye + d->n_lorentz > 0 && (!d->j || !d->ade_coef || (d->n_lorentz && !d->j_prev)))
     return fail(CEEP_ERR_INVALID, "null ADE buffer");
@@ -80,11 +79,18 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   if (!pl) return fail(CEEP_ERR_INVALID, "host allocation failed");
   ceep::Fdtd2dParams& p = pl->p;
   p.nx = d->nx; p.ny = d->ny; p.n = n;
-  p.ntx = d->ntx; p.lanes = lanes; p.lanes_per_group = group;
+  p.ntx = d->ntx; p.L = L; p.groups = lanes / L;
   p.nprobe = d->nprobe; p.nsteps = d->nsteps;
   p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
-  p.rows = d->rows_per_block > 0 ? d->rows_per_block : 16;
+  p.rows = d->rows_per_block > 0 ? d->rows_per_block : 0;
   p.db = d->db; p.db_dx = d->db * d->inv_dx; p.inv_dx = d->inv_dx; p.dt = d->dt;
+  const long long cells = (long long)d->nx * d->ny;
+  const int np = d->n_debye + d->n_lorentz;
+  p.gs_field = cells * L;
+  p.gs_psi_x = (long long)d->ny * 2 * (n > 0 ? n : 1) * L;
+  p.gs_psi_y = (long long)2 * (n > 0 ? n : 1) * d->nx * L;
+  p.gs_j = cells * np * L;
+  p.gs_jp = cells * d->n_lorentz * L;
   for (int k = 0; k < 2; ++k) {
     p.ez[k] = reinterpret_cast<float4*>(d->ez[k]);
     p.hx[k] = reinterpret_cast<float4*>(d->hx[k]);
@@ -96,10 +102,16 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   p.psi_ezy = reinterpret_cast<float4*>(d->psi_ezy);
   p.j = reinterpret_cast<float4*>(d->j);
   p.j_prev = reinterpret_cast<float4*>(d->j_prev);
-  p.coef = d->coef; p.dteps = d->dteps; p.ade_coef = d->ade_coef;
+  p.coef = d->coef; p.ade_coef = d->ade_coef;
   p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
   p.src_xy = d->src_xy; p.prb_xy = d->prb_xy; p.row_flags = d->row_flags;
   p.waveform = d->waveform; p.probes = d->probes;
+  p.status = d->status;
+  cudaError_t ce = ceep::fdtd2d_configure(p);
+  if (ce != cudaSuccess) {
+    delete pl;
+    return ceep::cuda_fail(ce, "fdtd2d_configure");
+  }
   *out = pl;
   return CEEP_OK;
 }
@@ -155,6 +167,7 @@ extern "C" int ceep2d_plan_reset(ceep2d_plan* pl) {
   return CEEP_OK;
 }
 extern "C" int64_t ceep2d_desc_size(void) { return (int64_t)sizeof(ceep2d_desc); }
+extern "C" int ceep2d_plan_rows(const ceep2d_plan* pl) { return pl ? pl->p.rows : 0; }
 
 extern "C" int ceep2d_plan_destroy(ceep2d_plan* pl) {
   if (!pl) return CEEP_OK;

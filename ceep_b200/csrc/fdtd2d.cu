@@ -1,4 +1,4 @@
-// Fused 2D TMz batched FDTD step for sm_100a.
+// Fused 2D TMz batched FDTD step for sm_100a, TMA-pipelined.
 //
 // One launch advances every transmit event by one full time step:
 //   H phase   interior Hx/Hy + graded-CPML psi recurrences on the four strips
@@ -16,267 +16,446 @@
 //       1..n and ny-n..ny-1 (columns >= 1) get  -dt/(eps_r eps0)*psi_y, with no
 //       ca factor; then the four edges are zeroed, the source added, probes read.
 //
-// Layout: every field is (y, x, tx) with tx innermost and padded to a
-// multiple of 4, so one float4 holds four transmit events of one cell and a
-// warp reads 32 consecutive float4 (512 B) per field and row.  All cell
-// coefficients (ca, cb, CPML, ADE) are loaded once per cell and serve every
-// transmit event in the float4s of that cell.
+// Layout: every per-TX array is (group, y, x, L float4) with tx innermost, so
+// one float4 holds four transmit events of one cell; a group is <= 32 TX.
+// Per-cell coefficients (ca, cb, dt/eps; ADE k's) are one float4 per cell and
+// serve every transmit event of that cell.
 //
-// Fusion: E(x,y) needs H^{n+1/2} at (x-1,y) and (x,y-1).  Each thread walks
-// a column segment upward in y, carrying Hx(x,y-1) and Ez(x,y+1) in
-// registers, and recomputes Hy(x-1,y) from Ez (two extra FMAs per TX) rather
-// than waiting for its neighbour.  Fields and the H-psi arrays are ping-pong
-// buffered (read [p], write [p^1]) so these halo recomputes never race with
-// the owner's write; the E-psi and ADE arrays are touched only by their
-// owner and are updated in place.
+// Schedule: a block owns a column strip of CX cells and a segment of rows.
+// One producer thread streams each row's slices (Ez with a one-cell halo on
+// both sides, Hx, Hy with the left halo, coefficients, ADE currents) from HBM
+// into a kStages-deep shared-memory ring with 1D bulk copies (cp.async.bulk,
+// completion counted on an mbarrier); 128 consumer threads walk the rows
+// upward, one float4 each, carrying Hx(x, y-1) in registers.  Hy(x-1, y) is
+// recomputed from the staged Ez halo instead of being exchanged.  Fields and
+// the H-psi arrays are ping-pong buffered (read [p], write [p^1]) so halo
+// recomputes never race with the owner's write; E-psi and ADE currents are
+// touched only by their owner and are updated in place.  Results go straight
+// to HBM with coalesced 16-byte stores.
 //
-// Per cell-step DRAM traffic: Ez, Hx, Hy read and written once (24 B per TX)
-// plus 8 B of (ca, cb) per cell shared by all TX; strip cells add their psi.
+// Every mbarrier wait is bounded in time; on expiry the block records
+// CEEP_ERR_TIMEOUT in the status word, lets its copies in flight land, and
+// returns.
+#include "../../include/ceep_b200.h"
 #include "common.cuh"
 #include "fdtd2d.cuh"
+#include "tma.cuh"
 
 namespace ceep {
 
-// ------------------------------------------------------------------------
-// Per-cell updates.  `GEN` = false for blocks that lie entirely in the
-// interior of every region (no strips, no edges): the predicates fold away.
-// ------------------------------------------------------------------------
+constexpr int kConsumers = 128;
+constexpr int kStages = 4;
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s
 
-// Hx^{n+1/2}(x, y) from Ez(x,y), Ez(x,y+1)
+template <int L, int NP, int NL>
+struct Stage2d {
+  static constexpr int CX = kConsumers / L;
+  float4 ez[(CX + 2) * L];  // cells x0-1 .. x0+CX
+  float4 hx[CX * L];        // cells x0 .. x0+CX-1
+  float4 hy[(CX + 1) * L];  // cells x0-1 .. x0+CX-1
+  float4 coef[CX];          // ca, cb, dt/(eps_r eps0), 0
+  float4 ade[NP > 0 ? NP * CX : 1];
+  float4 j[NP > 0 ? NP * CX * L : 1];
+  float4 jp[NL > 0 ? NL * CX * L : 1];
+};
+
+template <int L, int NP, int NL>
+constexpr size_t stage_smem_bytes() {
+  return kStages * sizeof(Stage2d<L, NP, NL>) + 2 * kStages * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ void record_status(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// ------------------------------------------------------------------------
+// Per-cell H updates.  GEN = false for blocks entirely inside every region's
+// plain interior: the region predicates fold away.
+// ------------------------------------------------------------------------
 template <bool GEN>
-CEEP_D float4 hx_new(const Fdtd2dParams& p, int x, int y, int par, int l, float4 hx, float4 ez_c,
-                     float4 ez_up, bool write_psi) {
+CEEP_D float4 hx_new(const Fdtd2dParams& p, const float4* psi_in, float4* psi_out, int x, int y, int lo,
+                     float4 hx, float4 ez_c, float4 ez_up) {
   const int n = p.n;
   if (!GEN) return fma4(-p.db_dx, ez_up - ez_c, hx);
   if (y >= p.ny - 1) return hx;  // never updated
-  float4 d = ez_up - ez_c;
+  const float4 d = ez_up - ez_c;
   if (x >= n && x < p.nx - n && y >= n) hx = fma4(-p.db_dx, d, hx);
   int sy = -1, ci = 0;
   if (y < n) { sy = y; ci = y; }
   else if (y >= p.ny - n) { sy = n + (y - (p.ny - n)); ci = p.ny - 1 - y; }
   if (sy >= 0) {
-    size_t idx = ((size_t)sy * p.nx + x) * p.lanes + l;
-    float4 psi = ld4(p.psi_hx[par] + idx);
+    const size_t idx = ((size_t)sy * p.nx + x) * p.L + lo;
+    float4 psi = ld4(psi_in + idx);
     psi = p.cpml_b[ci] * psi + p.cpml_c[ci] * (d * f4(p.inv_dx));
-    if (write_psi) st4(p.psi_hx[par ^ 1] + idx, psi);
+    if (psi_out) st4(psi_out + idx, psi);
     hx = fma4(-p.db, psi, hx);
   }
   return hx;
 }
 
-// Hy^{n+1/2}(x, y) from Ez(x,y), Ez(x+1,y)
 template <bool GEN>
-CEEP_D float4 hy_new(const Fdtd2dParams& p, int x, int y, int par, int l, float4 hy, float4 ez_c,
-                     float4 ez_r, bool write_psi) {
+CEEP_D float4 hy_new(const Fdtd2dParams& p, const float4* psi_in, float4* psi_out, int x, int y, int lo,
+                     float4 hy, float4 ez_c, float4 ez_r) {
   const int n = p.n;
   if (!GEN) return fma4(p.db_dx, ez_r - ez_c, hy);
   if (x >= p.nx - 1) return hy;  // never updated
-  float4 d = ez_r - ez_c;
+  const float4 d = ez_r - ez_c;
   if (x >= n && y >= n && y < p.ny - n) hy = fma4(p.db_dx, d, hy);
   int sx = -1, ci = 0;
   if (x < n) { sx = x; ci = x; }
   else if (x >= p.nx - n) { sx = n + (x - (p.nx - n)); ci = p.nx - 1 - x; }
   if (sx >= 0) {
-    size_t idx = ((size_t)y * (2 * n) + sx) * p.lanes + l;
-    float4 psi = ld4(p.psi_hy[par] + idx);
+    const size_t idx = ((size_t)y * (2 * n) + sx) * p.L + lo;
+    float4 psi = ld4(psi_in + idx);
     psi = p.cpml_b[ci] * psi + p.cpml_c[ci] * (d * f4(p.inv_dx));
-    if (write_psi) st4(p.psi_hy[par ^ 1] + idx, psi);
+    if (psi_out) st4(psi_out + idx, psi);
     hy = fma4(p.db, psi, hy);
   }
   return hy;
 }
 
-// ADE on the interior E update (dispersive.py:364-404, fdtd_2d.py:163-178):
-//   E  = ca*E_old + cb*curl - cb*sum(gamma_p J_p)
-//   Debye   J = k1 J + k2 (E - E_old)/dt
-//   Lorentz J' = k1 J + k3 J_prev + k2 (E - E_old)/dt ; J_prev = J ; J = J'
-template <int ND, int NL>
-CEEP_D float4 ade_update(const Fdtd2dParams& p, size_t cell, int l, float4 e_new, float4 e_old, float cb) {
+// ------------------------------------------------------------------------
+// Producer: one thread, bulk copies of row slices into the stage ring.
+// ------------------------------------------------------------------------
+template <int L, int ND, int NL>
+CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty, int par,
+                    int x0, int y0, int y1, int rs, int nslots, int g) {
   constexpr int NP = ND + NL;
-  float4 J[NP > 0 ? NP : 1];
-  float4 k[NP > 0 ? NP : 1];
-  const size_t plane = (size_t)p.nx * p.ny;
-  float4 sum = f4(0.f);
-#pragma unroll
-  for (int q = 0; q < NP; ++q) {
-    k[q] = __ldg(reinterpret_cast<const float4*>(p.ade_coef) + q * plane + cell);
-    J[q] = p.j[(q * plane + cell) * p.lanes + l];
-    sum = (q < ND) ? fma4(k[q].z, J[q], sum) : sum + J[q];
-  }
-  e_new = e_new - cb * sum;
-  float4 dedt = (e_new - e_old) / p.dt;
-#pragma unroll
-  for (int q = 0; q < NP; ++q) {
-    float4* jp = p.j + (q * plane + cell) * p.lanes + l;
-    if (q < ND) {
-      *jp = k[q].x * J[q] + k[q].y * dedt;
-    } else {
-      float4* jq = p.j_prev + ((q - ND) * plane + cell) * p.lanes + l;
-      float4 jm = *jq;
-      *jp = k[q].x * J[q] + k[q].z * jm + k[q].y * dedt;
-      *jq = J[q];
+  constexpr int CX = kConsumers / L;
+  const int nx = p.nx;
+  const size_t gf = (size_t)g * p.gs_field;
+  const float4* ez = p.ez[par] + gf;
+  const float4* hx = p.hx[par] + gf;
+  const float4* hy = p.hy[par] + gf;
+  const float4* coef = reinterpret_cast<const float4*>(p.coef);
+  const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
+  const float4* J = p.j + (size_t)g * p.gs_j;
+  const float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
+  const size_t plane = (size_t)nx * p.ny;
+  const int xa = x0 > 0 ? x0 - 1 : 0;                   // first halo cell
+  const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;   // end of Ez slice
+  const int xe = x0 + CX < nx ? x0 + CX : nx;           // end of owned cells
+  const uint32_t row4 = L * 16;                          // bytes per cell
+  int issued = 0;
+  for (int k = 0; k < nslots; ++k) {
+    const int s = k % kStages, u = k / kStages;
+    if (u > 0 && !mbar_wait_bounded(&empty[s], (u - 1) & 1, kWaitLimitNs)) {
+      record_status(p.status, CEEP_ERR_TIMEOUT);
+      break;
     }
+    const int r = rs + k;
+    const bool pro = r < y0, tail = r >= y1;
+    uint32_t bytes = (uint32_t)(xb - xa) * row4;
+    if (!tail) bytes += (uint32_t)(xe - x0) * row4;
+    if (!pro && !tail) {
+      bytes += (uint32_t)(xe - xa) * row4 + (uint32_t)(xe - x0) * 16u * (1 + NP);
+      bytes += (uint32_t)(xe - x0) * row4 * (NP + NL);
+    }
+    Stage2d<L, NP, NL>& S = st[s];
+    mbar_arrive_expect_tx(&full[s], bytes);
+    const size_t rowc = (size_t)r * nx;
+    bulk_g2s(S.ez + (xa - (x0 - 1)) * L, ez + (rowc + xa) * L, (xb - xa) * row4, &full[s]);
+    if (!tail) bulk_g2s(S.hx, hx + (rowc + x0) * L, (xe - x0) * row4, &full[s]);
+    if (!pro && !tail) {
+      bulk_g2s(S.hy + (xa - (x0 - 1)) * L, hy + (rowc + xa) * L, (xe - xa) * row4, &full[s]);
+      bulk_g2s(S.coef, coef + rowc + x0, (xe - x0) * 16u, &full[s]);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        bulk_g2s(S.ade + q * CX, ade + q * plane + rowc + x0, (xe - x0) * 16u, &full[s]);
+        bulk_g2s(S.j + q * CX * L, J + (q * plane + rowc + x0) * L, (xe - x0) * row4, &full[s]);
+      }
+#pragma unroll
+      for (int q = 0; q < NL; ++q)
+        bulk_g2s(S.jp + q * CX * L, Jp + (q * plane + rowc + x0) * L, (xe - x0) * row4, &full[s]);
+    }
+    issued = k + 1;
   }
-  return e_new;
+  // Let every copy this thread issued land before it leaves (only matters on
+  // the timeout path: otherwise the consumers have waited on all of them).
+  for (int k = issued > kStages ? issued - kStages : 0; k < issued; ++k)
+    mbar_wait_bounded(&full[k % kStages], (k / kStages) & 1, kWaitLimitNs);
 }
 
+// ------------------------------------------------------------------------
+// Consumer: one float4 (4 TX) of one cell per thread, walking the rows.
+// ------------------------------------------------------------------------
 template <int L, bool GEN, int ND, int NL>
-CEEP_D void column_segment(const Fdtd2dParams& p, int x, int l, int y0, int y1, int step, int par) {
+CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty,
+                    int step, int par, int x0, int y0, int y1, int rs, int nslots, int g) {
+  constexpr int NP = ND + NL;
+  constexpr int CX = kConsumers / L;
   const int nx = p.nx, ny = p.ny, n = p.n;
-  const size_t rowstride = (size_t)nx * p.lanes;
-  const float4* ez = p.ez[par];
-  const float4* hxo = p.hx[par];
-  const float4* hyo = p.hy[par];
-  float4* ezw = p.ez[par ^ 1];
-  float4* hxw = p.hx[par ^ 1];
-  float4* hyw = p.hy[par ^ 1];
-  const size_t col = (size_t)x * p.lanes + l;
+  const int cx = threadIdx.x / L, lo = threadIdx.x % L;
+  const int x = x0 + cx;
+  const bool active = x < nx;
+  const int lane_warp = threadIdx.x & 31;
+  const size_t gf = (size_t)g * p.gs_field;
+  float4* ezw = p.ez[par ^ 1] + gf;
+  float4* hxw = p.hx[par ^ 1] + gf;
+  float4* hyw = p.hy[par ^ 1] + gf;
+  const float4* psi_hx_in = p.psi_hx[par] + (size_t)g * p.gs_psi_y;
+  float4* psi_hx_out = p.psi_hx[par ^ 1] + (size_t)g * p.gs_psi_y;
+  const float4* psi_hy_in = p.psi_hy[par] + (size_t)g * p.gs_psi_x;
+  float4* psi_hy_out = p.psi_hy[par ^ 1] + (size_t)g * p.gs_psi_x;
+  float4* psi_ezx = p.psi_ezx + (size_t)g * p.gs_psi_x;
+  float4* psi_ezy = p.psi_ezy + (size_t)g * p.gs_psi_y;
+  float4* J = p.j + (size_t)g * p.gs_j;
+  float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
+  const size_t plane = (size_t)nx * ny;
+  const int lane_g = g * L + lo;  // float4 lane across all groups (tx = 4*lane_g + c)
 
-  // prologue: Ez(x, y0) and Hx^{n+1/2}(x, y0-1)
-  float4 ez_c = ld4(ez + (size_t)y0 * rowstride + col);
+  // Warp-uniform bounded wait: if any lane gives up, the whole warp leaves.
+  auto wait = [&](int k) {
+    const bool ok = mbar_wait_bounded(&full[k % kStages], (k / kStages) & 1, kWaitLimitNs);
+    if (__any_sync(0xffffffffu, !ok)) {
+      if (lane_warp == 0) record_status(p.status, CEEP_ERR_TIMEOUT);
+      return false;
+    }
+    return true;
+  };
+  auto release = [&](int k) {
+    __syncwarp();
+    if (lane_warp == 0) mbar_arrive(&empty[k % kStages]);
+  };
+
+  if (!wait(0)) return;
+  int k = 0;
   float4 hx_prev = f4(0.f);
-  if (y0 >= 1) {
-    float4 ez_dn = ld4(ez + (size_t)(y0 - 1) * rowstride + col);
-    hx_prev = hx_new<GEN>(p, x, y0 - 1, par, l, ld4(hxo + (size_t)(y0 - 1) * rowstride + col), ez_dn, ez_c,
-                          false);
+  if (y0 > 0) {  // slot 0 holds row y0-1 (Ez, Hx): Hx^{n+1/2}(x, y0-1)
+    if (!wait(1)) return;
+    if (active) {
+      const Stage2d<L, NP, NL>& A = st[0];
+      const Stage2d<L, NP, NL>& Bn = st[1 % kStages];
+      hx_prev = hx_new<GEN>(p, psi_hx_in, nullptr, x, y0 - 1, lo, A.hx[cx * L + lo], A.ez[(cx + 1) * L + lo],
+                            Bn.ez[(cx + 1) * L + lo]);
+    }
+    release(0);
+    k = 1;
   }
 
-  for (int y = y0; y < y1; ++y) {
-    const size_t at = (size_t)y * rowstride + col;
-    const float4 ez_up = (!GEN || y + 1 < ny) ? ld4(ez + at + rowstride) : f4(0.f);
-    const float4 ez_r = (!GEN || x + 1 < nx) ? ld4(ez + at + p.lanes) : f4(0.f);
-    const float4 ez_l = (!GEN || x >= 1) ? ld4(ez + at - p.lanes) : f4(0.f);
+  for (int y = y0; y < y1; ++y, ++k) {
+    const bool has_up = k + 1 < nslots;
+    if (has_up && !wait(k + 1)) return;
+    const Stage2d<L, NP, NL>& A = st[k % kStages];
+    if (active) {
+      const float4 ez_c = A.ez[(cx + 1) * L + lo];
+      const float4 ez_up = has_up ? st[(k + 1) % kStages].ez[(cx + 1) * L + lo] : f4(0.f);
+      const float4 ez_r = A.ez[(cx + 2) * L + lo];
+      const float4 ez_l = A.ez[cx * L + lo];
+      const size_t at = ((size_t)y * nx + x) * L + lo;
 
-    // H phase (this cell, plus the recomputed Hy of the left neighbour)
-    const float4 hxn = hx_new<GEN>(p, x, y, par, l, ld4(hxo + at), ez_c, ez_up, true);
-    const float4 hyn = hy_new<GEN>(p, x, y, par, l, ld4(hyo + at), ez_c, ez_r, true);
-    float4 hyl = f4(0.f);
-    if (!GEN || x >= 1) hyl = hy_new<GEN>(p, x - 1, y, par, l, ld4(hyo + at - p.lanes), ez_l, ez_c, false);
-    st4(hxw + at, hxn);
-    st4(hyw + at, hyn);
+      // H phase: this cell, plus the recomputed Hy of the left neighbour
+      const float4 hxn = hx_new<GEN>(p, psi_hx_in, psi_hx_out, x, y, lo, A.hx[cx * L + lo], ez_c, ez_up);
+      const float4 hyn = hy_new<GEN>(p, psi_hy_in, psi_hy_out, x, y, lo, A.hy[(cx + 1) * L + lo], ez_c, ez_r);
+      float4 hyl = f4(0.f);
+      if (!GEN || x >= 1) hyl = hy_new<GEN>(p, psi_hy_in, nullptr, x - 1, y, lo, A.hy[cx * L + lo], ez_l, ez_c);
+      st4(hxw + at, hxn);
+      st4(hyw + at, hyn);
 
-    // E phase
-    const size_t cell = (size_t)y * nx + x;
-    float4 e = ez_c;
-    const bool f9 = !GEN || (x >= n + 1 && x < nx - n && y >= n + 1 && y < ny - n);
-    const float4 dhy = hyn - hyl;
-    const float4 dhx = hxn - hx_prev;
-    if (f9) {
-      const float2 c = __ldg(reinterpret_cast<const float2*>(p.coef) + cell);
-      float4 curl = dhy * f4(p.inv_dx) - dhx * f4(p.inv_dx);
-      float4 en = c.x * e + c.y * curl;
-      if constexpr (ND + NL > 0) en = ade_update<ND, NL>(p, cell, l, en, e, c.y);
-      e = en;
-    }
-    if (GEN && n > 0) {
-      // E-CPML x strips (fdtd_2d_batched.py:355-378)
-      int sx = -1, ci = 0;
-      if (y >= 1) {
-        if (x >= 1 && x <= n) { sx = x - 1; ci = x - 1; }
-        else if (x >= nx - n) { sx = n + (x - (nx - n)); ci = nx - 1 - x; }
+      // E phase
+      const float4 cf = A.coef[cx];
+      float4 e = ez_c;
+      const bool f9 = !GEN || (x >= n + 1 && x < nx - n && y >= n + 1 && y < ny - n);
+      const float4 dhy = hyn - hyl;
+      const float4 dhx = hxn - hx_prev;
+      if (f9) {
+        float4 en = cf.x * e + cf.y * (dhy * f4(p.inv_dx) - dhx * f4(p.inv_dx));
+        if constexpr (NP > 0) {
+          // ADE (dispersive.py:364-404, fdtd_2d.py:163-178):
+          //   E -= cb * sum(gamma_p J_p);  Debye J = k1 J + k2 dE/dt;
+          //   Lorentz J' = k1 J + k3 J_prev + k2 dE/dt, J_prev = J
+          float4 sum = f4(0.f);
+#pragma unroll
+          for (int q = 0; q < NP; ++q) {
+            const float4 jq = A.j[(q * CX + cx) * L + lo];
+            sum = (q < ND) ? fma4(A.ade[q * CX + cx].z, jq, sum) : sum + jq;
+          }
+          en = en - cf.y * sum;
+          const float4 dedt = (en - e) / p.dt;
+#pragma unroll
+          for (int q = 0; q < NP; ++q) {
+            const float4 kq = A.ade[q * CX + cx];
+            const float4 jq = A.j[(q * CX + cx) * L + lo];
+            const size_t ja = (q * plane + (size_t)y * nx + x) * L + lo;
+            if (q < ND) {
+              st4(J + ja, kq.x * jq + kq.y * dedt);
+            } else {
+              const float4 jm = A.jp[((q - ND) * CX + cx) * L + lo];
+              st4(J + ja, kq.x * jq + kq.z * jm + kq.y * dedt);
+              st4(Jp + ((q - ND) * plane + (size_t)y * nx + x) * L + lo, jq);
+            }
+          }
+        }
+        e = en;
       }
-      if (sx >= 0) {
-        float4* pp = p.psi_ezx + ((size_t)y * (2 * n) + sx) * p.lanes + l;
-        float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhy * f4(p.inv_dx));
-        *pp = psi;
-        e = fma4(__ldg(p.dteps + cell), psi, e);
-      }
-      // E-CPML y strips (fdtd_2d_batched.py:380-406)
-      int sy = -1;
-      if (x >= 1) {
-        if (y >= 1 && y <= n) { sy = y - 1; ci = y - 1; }
-        else if (y >= ny - n) { sy = n + (y - (ny - n)); ci = ny - 1 - y; }
-      }
-      if (sy >= 0) {
-        float4* pp = p.psi_ezy + ((size_t)sy * nx + x) * p.lanes + l;
-        float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhx * f4(p.inv_dx));
-        *pp = psi;
-        e = fma4(-__ldg(p.dteps + cell), psi, e);
-      }
-    }
-    if (GEN && (x == 0 || x == nx - 1 || y == 0 || y == ny - 1)) e = f4(0.f);
-
-    // soft source and probe record (fdtd_2d_batched.py:509-526)
-    const uint8_t flags = __ldg(p.row_flags + y);
-    if (flags) {
-      if (flags & 1) {
-        const float w = __ldg(p.waveform + step);
-        for (int s = 0; s < p.ntx; ++s) {
-          if ((s >> 2) == l && __ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y)
-            add_comp(e, s & 3, w);
+      if (GEN && n > 0) {
+        // E-CPML x strips (fdtd_2d_batched.py:355-378)
+        int sx = -1, ci = 0;
+        if (y >= 1) {
+          if (x >= 1 && x <= n) { sx = x - 1; ci = x - 1; }
+          else if (x >= nx - n) { sx = n + (x - (nx - n)); ci = nx - 1 - x; }
+        }
+        if (sx >= 0) {
+          float4* pp = psi_ezx + ((size_t)y * (2 * n) + sx) * L + lo;
+          const float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhy * f4(p.inv_dx));
+          *pp = psi;
+          e = fma4(cf.z, psi, e);
+        }
+        // E-CPML y strips (fdtd_2d_batched.py:380-406)
+        int sy = -1;
+        if (x >= 1) {
+          if (y >= 1 && y <= n) { sy = y - 1; ci = y - 1; }
+          else if (y >= ny - n) { sy = n + (y - (ny - n)); ci = ny - 1 - y; }
+        }
+        if (sy >= 0) {
+          float4* pp = psi_ezy + ((size_t)sy * nx + x) * L + lo;
+          const float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhx * f4(p.inv_dx));
+          *pp = psi;
+          e = fma4(-cf.z, psi, e);
         }
       }
-      if (flags & 2) {
-        for (int q = 0; q < p.nprobe; ++q) {
-          if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
+      if (GEN && (x == 0 || x == nx - 1 || y == 0 || y == ny - 1)) e = f4(0.f);
+
+      // soft source and probe record (fdtd_2d_batched.py:509-526)
+      const uint8_t flags = __ldg(p.row_flags + y);
+      if (flags) {
+        if (flags & 1) {
+          const float w = __ldg(p.waveform + step);
+          for (int s = 0; s < p.ntx; ++s)
+            if ((s >> 2) == lane_g && __ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y)
+              add_comp(e, s & 3, w);
+        }
+        if (flags & 2) {
+          for (int q = 0; q < p.nprobe; ++q) {
+            if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const int tx = 4 * l + c;
-              if (tx < p.ntx) p.probes[((size_t)tx * p.nprobe + q) * p.nsteps + step] = comp(e, c);
+              for (int c = 0; c < 4; ++c) {
+                const int tx = 4 * lane_g + c;
+                if (tx < p.ntx) p.probes[((size_t)tx * p.nprobe + q) * p.nsteps + step] = comp(e, c);
+              }
             }
           }
         }
       }
+      st4(ezw + at, e);
+      hx_prev = hxn;
     }
-    st4(ezw + at, e);
-
-    hx_prev = hxn;
-    ez_c = ez_up;
+    release(k);
   }
+  if (k < nslots) release(k);  // the Ez-only slot of row y1
 }
 
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kThreads2d) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
-  constexpr int CX = kThreads2d / L;  // cells per block along x
+__global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
+  using St = Stage2d<L, ND + NL, NL>;
+  constexpr int CX = kConsumers / L;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  St* st = reinterpret_cast<St*>(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * sizeof(St));
+  uint64_t* empty = full + kStages;
+
   const int x0 = blockIdx.x * CX;
-  const int x = x0 + threadIdx.x / L;
-  const int l = blockIdx.z * L + threadIdx.x % L;
   const int y0 = blockIdx.y * p.rows;
   const int y1 = min(y0 + p.rows, p.ny);
-  if (x >= p.nx) return;
+  const int g = blockIdx.z;
+  const int rs = y0 > 0 ? y0 - 1 : 0;
+  const int nslots = (y1 - rs) + (y1 < p.ny ? 1 : 0);
+
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumers / 32);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  if (threadIdx.x >= kConsumers) {
+    if (threadIdx.x == kConsumers) produce<L, ND, NL>(p, st, full, empty, par, x0, y0, y1, rs, nslots, g);
+    return;
+  }
   const int n = p.n;
-  // Block-uniform: every cell (and every recomputed halo H) of this block lies
-  // in the plain interior of all regions.
-  // (the far column/row is excluded too: Hy(nx-1), Hx(ny-1) are never updated
-  // and Ez there is an edge).
+  // Block-uniform: every owned cell (and every recomputed halo H) lies in the
+  // plain interior of all regions; the far column/row is excluded too
+  // (Hy(nx-1), Hx(ny-1) are never updated and Ez there is an edge).
   const int m = n > 1 ? n : 1;
   const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (y0 >= n + 1) && (y1 <= p.ny - m);
   if (interior)
-    column_segment<L, false, ND, NL>(p, x, l, y0, y1, step, par);
+    consume<L, false, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
   else
-    column_segment<L, true, ND, NL>(p, x, l, y0, y1, step, par);
+    consume<L, true, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
 }
 
 // ------------------------------------------------------------------------
+// Host side: launch configuration and the rows-per-block choice.
+// ------------------------------------------------------------------------
+template <int L, int ND, int NL>
+static cudaError_t configure_l(Fdtd2dParams& p) {
+  constexpr size_t smem = stage_smem_bytes<L, ND + NL, NL>();
+  auto kern = fdtd2d_step_kernel<L, ND, NL>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  p.smem = (int)smem;
+  if (p.rows > 0) return cudaSuccess;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConsumers + 32, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  // Pick the segment length whose grid fills whole waves best: cost ~ waves *
+  // (rows + 2), the +2 being the two halo rows every segment loads.
+  constexpr int CX = kConsumers / L;
+  const long slots = (long)sms * per_sm;
+  const long xb = (p.nx + CX - 1) / CX;
+  double best = 1e300;
+  int best_rows = 16;
+  for (int rows = 4; rows <= 128; ++rows) {
+    const long blocks = xb * ((p.ny + rows - 1) / rows) * p.groups;
+    const long waves = (blocks + slots - 1) / slots;
+    const double cost = (double)waves * (rows + 2);
+    if (cost < best - 1e-9) { best = cost; best_rows = rows; }
+  }
+  p.rows = best_rows;
+  return cudaSuccess;
+}
+
 template <int L, int ND, int NL>
 static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
-  constexpr int CX = kThreads2d / L;
-  dim3 grid((p.nx + CX - 1) / CX, (p.ny + p.rows - 1) / p.rows, p.lanes / L);
-  fdtd2d_step_kernel<L, ND, NL><<<grid, kThreads2d, 0, s>>>(p, step, par);
+  constexpr int CX = kConsumers / L;
+  dim3 grid((p.nx + CX - 1) / CX, (p.ny + p.rows - 1) / p.rows, p.groups);
+  fdtd2d_step_kernel<L, ND, NL><<<grid, kConsumers + 32, p.smem, s>>>(p, step, par);
   return cudaGetLastError();
 }
 
 template <int ND, int NL>
-static cudaError_t launch_ade(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
-  switch (p.lanes_per_group) {
-    case 1: return launch_l<1, ND, NL>(p, step, par, s);
-    case 2: return launch_l<2, ND, NL>(p, step, par, s);
-    case 4: return launch_l<4, ND, NL>(p, step, par, s);
-    default: return launch_l<8, ND, NL>(p, step, par, s);
+static cudaError_t dispatch_l(Fdtd2dParams& p, int step, int par, cudaStream_t s, bool configure) {
+  switch (p.L) {
+    case 1: return configure ? configure_l<1, ND, NL>(p) : launch_l<1, ND, NL>(p, step, par, s);
+    case 2: return configure ? configure_l<2, ND, NL>(p) : launch_l<2, ND, NL>(p, step, par, s);
+    case 4: return configure ? configure_l<4, ND, NL>(p) : launch_l<4, ND, NL>(p, step, par, s);
+    default: return configure ? configure_l<8, ND, NL>(p) : launch_l<8, ND, NL>(p, step, par, s);
   }
 }
 
-cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
-  const int key = p.n_debye * 3 + p.n_lorentz;
-  switch (key) {
-    case 0: return launch_ade<0, 0>(p, step, par, s);
-    case 1: return launch_ade<0, 1>(p, step, par, s);
-    case 2: return launch_ade<0, 2>(p, step, par, s);
-    case 3: return launch_ade<1, 0>(p, step, par, s);
-    case 4: return launch_ade<1, 1>(p, step, par, s);
-    case 6: return launch_ade<2, 0>(p, step, par, s);
+static cudaError_t dispatch(Fdtd2dParams& p, int step, int par, cudaStream_t s, bool configure) {
+  switch (p.n_debye * 3 + p.n_lorentz) {
+    case 0: return dispatch_l<0, 0>(p, step, par, s, configure);
+    case 1: return dispatch_l<0, 1>(p, step, par, s, configure);
+    case 2: return dispatch_l<0, 2>(p, step, par, s, configure);
+    case 3: return dispatch_l<1, 0>(p, step, par, s, configure);
+    case 4: return dispatch_l<1, 1>(p, step, par, s, configure);
+    case 6: return dispatch_l<2, 0>(p, step, par, s, configure);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t fdtd2d_configure(Fdtd2dParams& p) { return dispatch(p, 0, 0, nullptr, true); }
+
+cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
+  Fdtd2dParams q = p;
+  return dispatch(q, step, par, s, false);
 }
 
 }  // namespace ceep

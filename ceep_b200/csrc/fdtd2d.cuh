@@ -5,17 +5,18 @@
 
 namespace ceep {
 
-constexpr int kThreads2d = 128;
-
 struct Fdtd2dParams {
   int nx, ny, n;
   int ntx;              // real transmit events
-  int lanes;            // float4 per cell (ntx_pad / 4)
-  int lanes_per_group;  // float4 per cell handled by one block (grid.z = lanes / this)
+  int L;                // float4 per cell inside one TX group (1, 2, 4, 8)
+  int groups;           // TX groups (grid.z); all per-TX arrays are (group, ...)
   int nprobe, nsteps;
   int n_debye, n_lorentz;
-  int rows;             // rows of the column segment walked by one thread
+  int rows;             // rows of the column segment one block walks
+  int smem;             // dynamic shared memory per block
   float db, db_dx, inv_dx, dt;
+  // per-group strides in float4
+  long long gs_field, gs_psi_x, gs_psi_y, gs_j, gs_jp;
   float4* ez[2];
   float4* hx[2];
   float4* hy[2];
@@ -25,9 +26,8 @@ struct Fdtd2dParams {
   float4* psi_ezy;
   float4* j;
   float4* j_prev;
-  const float* coef;
-  const float* dteps;
-  const float* ade_coef;
+  const float* coef;      // (ny, nx) float4: ca, cb, dt/(eps_r eps0), 0
+  const float* ade_coef;  // (poles, ny, nx) float4
   const float* cpml_b;
   const float* cpml_c;
   const int32_t* src_xy;
@@ -35,8 +35,11 @@ struct Fdtd2dParams {
   const uint8_t* row_flags;
   const float* waveform;
   float* probes;
+  int* status;
 };
 
+// Set the kernel attributes and (if rows == 0) choose rows per block.
+cudaError_t fdtd2d_configure(Fdtd2dParams& p);
 // Launch one step reading buffer `par` and writing buffer `par ^ 1`.
 cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStream_t s);
 

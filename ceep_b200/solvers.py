@@ -159,35 +159,33 @@ class BatchedFDTD2D:
         nx, ny, n, B = self.nx, self.ny, self.cpml_n, self.batch
         BP = _pad_tx(B)
         self.ntx_pad = BP
+        G = BP // min(BP, 32)           # TX groups of at most 32 (kernel grid.z)
+        W = BP // G                     # floats per cell in one group
+        self._groups, self._gwidth = G, W
         dt = self.dt
         f32 = dict(dtype=torch.float32, device=dev)
-        eps_add, ade = physics.ade_coefficients(dt, self._debye, self._lorentz, (nx, ny))
-        ca, cb = physics.update_coefficients(self._eps_r, self._sigma_e, dt, eps_add if ade.shape[0] else None)
         to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
-        # (y, x) transposes of the reference's (x, y) maps
-        self._coef = to_dev(np.stack([ca.T, cb.T], axis=-1))
-        self._dteps = to_dev((dt / (self._eps_r * EPS_0)).T)
-        if ade.shape[0]:
-            self._ade_coef = to_dev(ade.transpose(0, 2, 1, 3))
-        else:
-            self._ade_coef = None
+        coef, ade = self._coef_maps(self._eps_r, self._sigma_e, self._debye, self._lorentz)
+        self._coef = to_dev(coef)
+        self._ade_coef = to_dev(ade) if ade.shape[0] else None
         b, c = physics.cpml_profile(n, self.dx, dt, self.cpml_R0, self.cpml_order)
         self._cpml_b, self._cpml_c = to_dev(b if n else np.zeros(1)), to_dev(c if n else np.zeros(1))
         w = (self._waveform_override if self._waveform_override is not None
              else physics.gaussian_derivative(self.total_steps, dt, self.frequency, self.delay_factor))
         self.waveform = to_dev(w)
-        field = lambda: torch.zeros((ny, nx, BP), **f32)
+        field = lambda: torch.zeros((G, ny, nx, W), **f32)
         self._ez = [field(), field()]
         self._hx = [field(), field()]
         self._hy = [field(), field()]
         nn = max(n, 1)
-        self._psi_hy = [torch.zeros((ny, 2 * nn, BP), **f32) for _ in range(2)]
-        self._psi_hx = [torch.zeros((2 * nn, nx, BP), **f32) for _ in range(2)]
-        self._psi_ezx = torch.zeros((ny, 2 * nn, BP), **f32)
-        self._psi_ezy = torch.zeros((2 * nn, nx, BP), **f32)
+        self._psi_hy = [torch.zeros((G, ny, 2 * nn, W), **f32) for _ in range(2)]
+        self._psi_hx = [torch.zeros((G, 2 * nn, nx, W), **f32) for _ in range(2)]
+        self._psi_ezx = torch.zeros((G, ny, 2 * nn, W), **f32)
+        self._psi_ezy = torch.zeros((G, 2 * nn, nx, W), **f32)
         nd, nl = len(self._debye), len(self._lorentz)
-        self._j = torch.zeros((nd + nl, ny, nx, BP), **f32) if nd + nl else None
-        self._j_prev = torch.zeros((nl, ny, nx, BP), **f32) if nl else None
+        self._j = torch.zeros((G, nd + nl, ny, nx, W), **f32) if nd + nl else None
+        self._j_prev = torch.zeros((G, nl, ny, nx, W), **f32) if nl else None
+        self._status = torch.zeros(1, dtype=torch.int32, device=dev)
         P = len(self.probe_positions)
         self._src = to_dev(np.array(self.source_positions, np.int32).reshape(-1, 2), torch.int32)
         self._prb = to_dev(np.array(self.probe_positions, np.int32).reshape(-1, 2), torch.int32)
@@ -208,10 +206,11 @@ class BatchedFDTD2D:
             d.psi_hy[k], d.psi_hx[k] = _ptr(self._psi_hy[k]), _ptr(self._psi_hx[k])
         d.psi_ezx, d.psi_ezy = _ptr(self._psi_ezx), _ptr(self._psi_ezy)
         d.j, d.j_prev = _ptr(self._j), _ptr(self._j_prev)
-        d.coef, d.dteps, d.ade_coef = _ptr(self._coef), _ptr(self._dteps), _ptr(self._ade_coef)
+        d.coef, d.ade_coef = _ptr(self._coef), _ptr(self._ade_coef)
         d.cpml_b, d.cpml_c = _ptr(self._cpml_b), _ptr(self._cpml_c)
         d.src_xy, d.prb_xy, d.row_flags = _ptr(self._src), _ptr(self._prb), _ptr(self._flags)
         d.waveform, d.probes = _ptr(self.waveform), _ptr(self.probe_data)
+        d.status = _ptr(self._status)
         d.rows_per_block = self.rows_per_block
         self._desc = d
         plan = C.c_void_p()
@@ -243,6 +242,7 @@ class BatchedFDTD2D:
         a second call continues the simulation and overwrites the series."""
         self.advance(0, self.total_steps)
         probe_np = self.probe_data.double().cpu().numpy()
+        self.check_status()
         P = len(self.probe_positions)
         return {tx: {rx: probe_np[tx, rx, :] for rx in range(P)} for tx in range(self.batch)}
 
@@ -273,17 +273,32 @@ class BatchedFDTD2D:
     def _cur(self) -> int:
         return lib().ceep2d_plan_current_buffer(self._plan) if self._built else 0
 
+    def _ref_view(self, t: torch.Tensor) -> torch.Tensor:
+        """(G, ny, nx, W) device array -> (B, nx, ny) in the reference's axis order."""
+        G, ny, nx, W = t.shape
+        v = t.permute(0, 3, 2, 1)                       # (G, W, nx, ny)
+        v = v.reshape(G * W, nx, ny) if G > 1 else v[0]
+        return v[:self.batch]
+
     @property
     def ez(self):
-        return self._ez[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+        return self._ref_view(self._ez[self._cur()]) if self._built else None
 
     @property
     def hx(self):
-        return self._hx[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+        return self._ref_view(self._hx[self._cur()]) if self._built else None
 
     @property
     def hy(self):
-        return self._hy[self._cur()][:, :, :self.batch].permute(2, 1, 0) if self._built else None
+        return self._ref_view(self._hy[self._cur()]) if self._built else None
+
+    def check_status(self) -> None:
+        """Raise if a bounded device wait gave up during an earlier launch."""
+        if self._built:
+            code = int(self._status.item())
+            if code:
+                self._status.zero_()
+                raise RuntimeError(f"fused step reported status {code} (bounded wait expired)")
 
     def reset(self) -> None:
         """Zero every field, psi and ADE state (not in the reference: lets one
@@ -296,42 +311,44 @@ class BatchedFDTD2D:
                 t.zero_()
         check(lib().ceep2d_plan_reset(self._plan), "ceep2d_plan_reset")
 
+    def _coef_maps(self, eps_r, sigma_e, debye=(), lorentz=()):
+        """Host FP64 -> (ny, nx, 4) float32 (ca, cb, dt/(eps_r eps0), 0) and
+        (poles, ny, nx, 4) ADE coefficients, in the kernel's (y, x) order."""
+        nx, ny, dt = self.nx, self.ny, self.dt
+        eps_add, ade = physics.ade_coefficients(dt, debye, lorentz, (nx, ny))
+        ca, cb = physics.update_coefficients(eps_r, sigma_e, dt, eps_add if ade.shape[0] else None)
+        dteps = dt / (np.asarray(eps_r, np.float64) * EPS_0)   # E-CPML scale, fdtd_2d_batched.py:348
+        coef = np.stack([ca.T, cb.T, dteps.T, np.zeros((ny, nx))], axis=-1).astype(np.float32)
+        return coef, ade.transpose(0, 2, 1, 3).astype(np.float32)
+
     def material_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
-        """Device tensors (coef, dteps, ade_coef) for the given (nx, ny) maps in
-        this solver's layout, for ``load_material_tensors``."""
-        eps_add, ade = physics.ade_coefficients(self.dt, debye, lorentz, (self.nx, self.ny))
-        ca, cb = physics.update_coefficients(eps_r, sigma_e, self.dt, eps_add if ade.shape[0] else None)
+        """Device tensors (coef, ade_coef) for the given (nx, ny) maps in this
+        solver's layout, for ``load_material_tensors``."""
+        coef, ade = self._coef_maps(eps_r, sigma_e, debye, lorentz)
         dev = self.device
-        coef = torch.as_tensor(np.ascontiguousarray(np.stack([ca.T, cb.T], -1)), dtype=torch.float32).to(dev)
-        dteps = torch.as_tensor(np.ascontiguousarray((self.dt / (np.asarray(eps_r) * EPS_0)).T),
-                                dtype=torch.float32).to(dev)
-        ade_t = (torch.as_tensor(np.ascontiguousarray(ade.transpose(0, 2, 1, 3)), dtype=torch.float32).to(dev)
-                 if ade.shape[0] else None)
-        return coef, dteps, ade_t
+        return (torch.as_tensor(np.ascontiguousarray(coef)).to(dev),
+                torch.as_tensor(np.ascontiguousarray(ade)).to(dev) if ade.shape[0] else None)
 
     def load_material_tensors(self, mats) -> None:
         """Device-to-device copy of precomputed material tensors into the plan's
         buffers (no host traffic); the pole count must match the first build."""
         if not self._built:
             self._build()
-        coef, dteps, ade_t = mats
-        self._coef.copy_(coef, non_blocking=True)
-        self._dteps.copy_(dteps, non_blocking=True)
+        coef, ade_t = mats
         if (ade_t is None) != (self._ade_coef is None):
             raise ValueError("ADE pole count differs from the built solver")
+        self._coef.copy_(coef, non_blocking=True)
         if ade_t is not None:
             self._ade_coef.copy_(ade_t, non_blocking=True)
 
     def update_materials(self) -> None:
-        """Re-upload ca/cb/dteps (and ADE coefficients) after editing
-        ``_eps_r``/``_sigma_e``/poles on a built solver."""
+        """Re-upload the coefficients after editing ``_eps_r``/``_sigma_e`` or the
+        poles on a built solver."""
         if not self._built:
             return
-        eps_add, ade = physics.ade_coefficients(self.dt, self._debye, self._lorentz, (self.nx, self.ny))
+        coef, ade = self._coef_maps(self._eps_r, self._sigma_e, self._debye, self._lorentz)
         if ade.shape[0] != (0 if self._ade_coef is None else self._ade_coef.shape[0]):
             raise ValueError("the number of ADE poles cannot change after the first run()")
-        ca, cb = physics.update_coefficients(self._eps_r, self._sigma_e, self.dt, eps_add if ade.shape[0] else None)
-        self._coef.copy_(torch.as_tensor(np.stack([ca.T, cb.T], -1), dtype=torch.float32))
-        self._dteps.copy_(torch.as_tensor((self.dt / (self._eps_r * EPS_0)).T, dtype=torch.float32))
+        self._coef.copy_(torch.as_tensor(coef))
         if ade.shape[0]:
-            self._ade_coef.copy_(torch.as_tensor(ade.transpose(0, 2, 1, 3), dtype=torch.float32))
+            self._ade_coef.copy_(torch.as_tensor(ade))

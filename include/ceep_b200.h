@@ -58,21 +58,24 @@ typedef struct ceep2d_desc {
   float db;                /* dt / mu0                                       */
   float inv_dx;            /* 1 / dx (dx == dy)                              */
   float dt;                /* time step (ADE dE/dt)                          */
-  /* ping-pong state, each (ny, nx, ntx_pad) float; [k] = buffer k          */
+  /* Per-TX arrays are split into groups of at most 32 transmit events:
+   * G = ntx_pad / min(ntx_pad, 32) groups, each group's array contiguous, so
+   * a field is (G, ny, nx, ntx_pad / G) floats (for ntx_pad <= 32 simply
+   * (ny, nx, ntx_pad)).
+   * ping-pong state, each (G, ny, nx, ntx_pad/G) float; [k] = buffer k      */
   float* ez[2];
   float* hx[2];
   float* hy[2];
-  /* H-CPML psi, ping-pong: x strips (ny, 2n, ntx_pad), y strips (2n, nx, ntx_pad) */
+  /* H-CPML psi, ping-pong: x strips (G, ny, 2n, .), y strips (G, 2n, nx, .) */
   float* psi_hy[2];
   float* psi_hx[2];
   /* E-CPML psi, in place, same shapes as above                               */
   float* psi_ezx;
   float* psi_ezy;
-  /* ADE currents, in place: (poles, ny, nx, ntx_pad); Lorentz keeps J^{n-1}  */
+  /* ADE currents, in place: (G, poles, ny, nx, .); Lorentz keeps J^{n-1}    */
   float* j;                /* n_debye + n_lorentz planes                     */
   float* j_prev;           /* n_lorentz planes                               */
-  const float* coef;       /* (ny, nx, 2): ca, cb                            */
-  const float* dteps;      /* (ny, nx): dt / (eps_r eps0) for E-CPML         */
+  const float* coef;       /* (ny, nx, 4): ca, cb, dt/(eps_r eps0), 0        */
   const float* ade_coef;   /* (poles, ny, nx, 4): Debye k1,k2,gamma ; Lorentz k1,k2,k3 */
   const float* cpml_b;     /* (n)                                            */
   const float* cpml_c;     /* (n)                                            */
@@ -81,7 +84,9 @@ typedef struct ceep2d_desc {
   const uint8_t* row_flags;/* (ny): bit0 a source on this row, bit1 a probe  */
   const float* waveform;   /* (nsteps)                                       */
   float* probes;           /* (ntx, nprobe, nsteps) output series            */
-  int32_t rows_per_block;  /* 0 = library default                           */
+  int32_t* status;         /* device word, 0 = ok; a bounded wait that gives
+                              up writes CEEP_ERR_TIMEOUT (may be NULL)        */
+  int32_t rows_per_block;  /* 0 = chosen to fill whole waves of the GPU     */
 } ceep2d_desc;
 
 typedef struct ceep2d_plan ceep2d_plan;
@@ -101,6 +106,8 @@ int ceep2d_plan_current_buffer(const ceep2d_plan* plan);
 int ceep2d_plan_reset(ceep2d_plan* plan);
 /* sizeof(ceep2d_desc), for binding layers to check their struct mirror. */
 int64_t ceep2d_desc_size(void);
+/* Rows per block the plan launches with (chosen at creation when 0). */
+int ceep2d_plan_rows(const ceep2d_plan* plan);
 
 /* ------------------------------------------------------------------------
  * On-device DFT of the probe series into the S-matrix.
