@@ -284,8 +284,8 @@ def run_e2e(w, phantoms, pos, freqs, device):
                         np.asarray(pos, float) * w["dx"], w["das"], w["das"], w["nx"] // 2 * w["dx"] - 0.09,
                         w["ny"] // 2 * w["dx"] - 0.09, 0.18 / w["das"], 299_792_458.0).cpu().numpy()
         times.append(time.perf_counter() - t0)
-        h2d = (solver._coef.numel() + solver._dteps.numel() +
-               (solver._ade_coef.numel() if solver._ade_coef is not None else 0)) * 4 + S.size * 8
+        h2d = (solver._coef.numel() + (solver._ade_coef.numel() if solver._ade_coef is not None else 0)) * 4 \
+            + S.size * 8
         d2h = solver.probe_data.numel() * 4 + S.size * 8 + img.size * 4
     cell_steps = w["nx"] * w["ny"] * w["steps"] * w["ntx"]
     return {"value": round(len(times) * cell_steps / sum(times) / 1e9, 3), "unit": "GCell-steps/s",

@@ -84,6 +84,7 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
   p.rows = d->rows_per_block > 0 ? d->rows_per_block : 0;
   p.db = d->db; p.db_dx = d->db * d->inv_dx; p.inv_dx = d->inv_dx; p.dt = d->dt;
+  p.inv_dt = (float)(1.0 / (double)d->dt);
   const long long cells = (long long)d->nx * d->ny;
   const int np = d->n_debye + d->n_lorentz;
   p.gs_field = cells * L;

@@ -22,16 +22,18 @@
 // serve every transmit event of that cell.
 //
 // Schedule: a block owns a column strip of CX cells and a segment of rows.
-// One producer thread streams each row's slices (Ez with a one-cell halo on
-// both sides, Hx, Hy with the left halo, coefficients, ADE currents) from HBM
-// into a kStages-deep shared-memory ring with 1D bulk copies (cp.async.bulk,
-// completion counted on an mbarrier); 128 consumer threads walk the rows
-// upward, one float4 each, carrying Hx(x, y-1) in registers.  Hy(x-1, y) is
-// recomputed from the staged Ez halo instead of being exchanged.  Fields and
-// the H-psi arrays are ping-pong buffered (read [p], write [p^1]) so halo
-// recomputes never race with the owner's write; E-psi and ADE currents are
-// touched only by their owner and are updated in place.  Results go straight
-// to HBM with coalesced 16-byte stores.
+// One producer thread streams each row's slices -- Ez with a one-cell halo on
+// both sides, Hx, Hy with the left halo, coefficients, ADE currents, and the
+// CPML psi slices where the block touches a strip -- from HBM into a
+// kStages-deep shared-memory ring with 1D bulk copies (cp.async.bulk,
+// completion counted on an mbarrier).  128 consumer threads walk the rows
+// upward, one float4 each, carrying Hx(x, y-1) in registers; every operand
+// they read comes from shared memory, every result goes straight to HBM with
+// coalesced 16-byte stores.  Hy(x-1, y) is recomputed from the staged Ez halo
+// instead of being exchanged.  Fields and the H-psi arrays are ping-pong
+// buffered (read [p], write [p^1]) so halo recomputes never race with the
+// owner's write; E-psi and ADE currents are read once per launch by their
+// owner's copy and written back in place.
 //
 // Every mbarrier wait is bounded in time; on expiry the block records
 // CEEP_ERR_TIMEOUT in the status word, lets its copies in flight land, and
@@ -44,16 +46,21 @@
 namespace ceep {
 
 constexpr int kConsumers = 128;
-constexpr int kStages = 4;
-constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s
+constexpr int kStages = 3;
+constexpr int kMaxRows = 64;                        // rows per block (row masks are 64-bit)
+constexpr uint64_t kWaitLimitNs = 1000000000ull;    // 1 s
 
 template <int L, int NP, int NL>
 struct Stage2d {
   static constexpr int CX = kConsumers / L;
-  float4 ez[(CX + 2) * L];  // cells x0-1 .. x0+CX
-  float4 hx[CX * L];        // cells x0 .. x0+CX-1
-  float4 hy[(CX + 1) * L];  // cells x0-1 .. x0+CX-1
-  float4 coef[CX];          // ca, cb, dt/(eps_r eps0), 0
+  float4 ez[(CX + 2) * L];   // cells x0-1 .. x0+CX
+  float4 hx[CX * L];         // cells x0 .. x0+CX-1
+  float4 hy[(CX + 1) * L];   // cells x0-1 .. x0+CX-1
+  float4 coef[CX];           // ca, cb, dt/(eps_r eps0), 0
+  float4 phx[CX * L];        // H psi of the y strips (for Hx), cells x0..
+  float4 pey[CX * L];        // E psi of the y strips, cells x0..
+  float4 phy[(CX + 1) * L];  // H psi of the x strips (for Hy), cells x0-1..
+  float4 pex[CX * L];        // E psi of the x strips, cells x0..
   float4 ade[NP > 0 ? NP * CX : 1];
   float4 j[NP > 0 ? NP * CX * L : 1];
   float4 jp[NL > 0 ? NL * CX * L : 1];
@@ -68,47 +75,61 @@ __device__ __forceinline__ void record_status(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
+// Strip bookkeeping shared by producer and consumers.
+struct Strips {
+  int n, nx, ny;
+  // H psi of the y strips (Hx): row -> strip row, or -1
+  __device__ int hy_row(int y) const {
+    if (y < n) return y;
+    if (y >= ny - n && y < ny - 1) return n + (y - (ny - n));
+    return -1;
+  }
+  // E psi of the y strips: row -> strip row, or -1 (rows 1..n and ny-n..ny-1)
+  __device__ int ey_row(int y) const {
+    if (y >= 1 && y <= n) return y - 1;
+    if (n > 0 && y >= ny - n) return n + (y - (ny - n));
+    return -1;
+  }
+};
+
 // ------------------------------------------------------------------------
 // Per-cell H updates.  GEN = false for blocks entirely inside every region's
-// plain interior: the region predicates fold away.
+// plain interior: the region predicates fold away.  `psi` is the staged old
+// psi value of this cell (read only when the cell is in a strip).
 // ------------------------------------------------------------------------
 template <bool GEN>
-CEEP_D float4 hx_new(const Fdtd2dParams& p, const float4* psi_in, float4* psi_out, int x, int y, int lo,
-                     float4 hx, float4 ez_c, float4 ez_up) {
+CEEP_D float4 hx_new(const Fdtd2dParams& p, float4 psi, float4* psi_out, int x, int y, float4 hx, float4 ez_c,
+                     float4 ez_up) {
   const int n = p.n;
   if (!GEN) return fma4(-p.db_dx, ez_up - ez_c, hx);
   if (y >= p.ny - 1) return hx;  // never updated
   const float4 d = ez_up - ez_c;
   if (x >= n && x < p.nx - n && y >= n) hx = fma4(-p.db_dx, d, hx);
-  int sy = -1, ci = 0;
-  if (y < n) { sy = y; ci = y; }
-  else if (y >= p.ny - n) { sy = n + (y - (p.ny - n)); ci = p.ny - 1 - y; }
-  if (sy >= 0) {
-    const size_t idx = ((size_t)sy * p.nx + x) * p.L + lo;
-    float4 psi = ld4(psi_in + idx);
+  int ci = -1;
+  if (y < n) ci = y;
+  else if (y >= p.ny - n) ci = p.ny - 1 - y;
+  if (ci >= 0) {
     psi = p.cpml_b[ci] * psi + p.cpml_c[ci] * (d * f4(p.inv_dx));
-    if (psi_out) st4(psi_out + idx, psi);
+    if (psi_out) st4(psi_out, psi);
     hx = fma4(-p.db, psi, hx);
   }
   return hx;
 }
 
 template <bool GEN>
-CEEP_D float4 hy_new(const Fdtd2dParams& p, const float4* psi_in, float4* psi_out, int x, int y, int lo,
-                     float4 hy, float4 ez_c, float4 ez_r) {
+CEEP_D float4 hy_new(const Fdtd2dParams& p, float4 psi, float4* psi_out, int x, int y, float4 hy, float4 ez_c,
+                     float4 ez_r) {
   const int n = p.n;
   if (!GEN) return fma4(p.db_dx, ez_r - ez_c, hy);
   if (x >= p.nx - 1) return hy;  // never updated
   const float4 d = ez_r - ez_c;
   if (x >= n && y >= n && y < p.ny - n) hy = fma4(p.db_dx, d, hy);
-  int sx = -1, ci = 0;
-  if (x < n) { sx = x; ci = x; }
-  else if (x >= p.nx - n) { sx = n + (x - (p.nx - n)); ci = p.nx - 1 - x; }
-  if (sx >= 0) {
-    const size_t idx = ((size_t)y * (2 * n) + sx) * p.L + lo;
-    float4 psi = ld4(psi_in + idx);
+  int ci = -1;
+  if (x < n) ci = x;
+  else if (x >= p.nx - n) ci = p.nx - 1 - x;
+  if (ci >= 0) {
     psi = p.cpml_b[ci] * psi + p.cpml_c[ci] * (d * f4(p.inv_dx));
-    if (psi_out) st4(psi_out + idx, psi);
+    if (psi_out) st4(psi_out, psi);
     hy = fma4(p.db, psi, hy);
   }
   return hy;
@@ -122,7 +143,8 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
                     int x0, int y0, int y1, int rs, int nslots, int g) {
   constexpr int NP = ND + NL;
   constexpr int CX = kConsumers / L;
-  const int nx = p.nx;
+  const int nx = p.nx, ny = p.ny, n = p.n;
+  const Strips sp{n, nx, ny};
   const size_t gf = (size_t)g * p.gs_field;
   const float4* ez = p.ez[par] + gf;
   const float4* hx = p.hx[par] + gf;
@@ -131,11 +153,20 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
   const float4* J = p.j + (size_t)g * p.gs_j;
   const float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
-  const size_t plane = (size_t)nx * p.ny;
-  const int xa = x0 > 0 ? x0 - 1 : 0;                   // first halo cell
-  const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;   // end of Ez slice
-  const int xe = x0 + CX < nx ? x0 + CX : nx;           // end of owned cells
-  const uint32_t row4 = L * 16;                          // bytes per cell
+  const float4* psi_hx = p.psi_hx[par] + (size_t)g * p.gs_psi_y;
+  const float4* psi_hy = p.psi_hy[par] + (size_t)g * p.gs_psi_x;
+  const float4* psi_ezx = p.psi_ezx + (size_t)g * p.gs_psi_x;
+  const float4* psi_ezy = p.psi_ezy + (size_t)g * p.gs_psi_y;
+  const size_t plane = (size_t)nx * ny;
+  const int xa = x0 > 0 ? x0 - 1 : 0;                  // first halo cell
+  const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;  // end of the Ez slice
+  const int xe = x0 + CX < nx ? x0 + CX : nx;          // end of the owned cells
+  const uint32_t cb = L * 16;                           // bytes of one cell's float4s
+  // x-strip cell ranges of this block (empty when lo >= hi)
+  const int hl0 = xa, hl1 = min(xe, n);                                  // H, left  (sx = x)
+  const int hr0 = max(xa, nx - n), hr1 = min(xe, nx - 1);                // H, right (sx = n + x - (nx-n))
+  const int el0 = max(x0, 1), el1 = min(xe, n + 1);                      // E, left  (sx = x - 1)
+  const int er0 = max(x0, nx - n), er1 = xe;                             // E, right
   int issued = 0;
   for (int k = 0; k < nslots; ++k) {
     const int s = k % kStages, u = k / kStages;
@@ -144,29 +175,41 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
       break;
     }
     const int r = rs + k;
-    const bool pro = r < y0, tail = r >= y1;
-    uint32_t bytes = (uint32_t)(xb - xa) * row4;
-    if (!tail) bytes += (uint32_t)(xe - x0) * row4;
-    if (!pro && !tail) {
-      bytes += (uint32_t)(xe - xa) * row4 + (uint32_t)(xe - x0) * 16u * (1 + NP);
-      bytes += (uint32_t)(xe - x0) * row4 * (NP + NL);
-    }
+    const bool pro = r < y0, tail = r >= y1, body = !pro && !tail;
+    const int shy = sp.hy_row(r), sey = sp.ey_row(r);
     Stage2d<L, NP, NL>& S = st[s];
-    mbar_arrive_expect_tx(&full[s], bytes);
     const size_t rowc = (size_t)r * nx;
-    bulk_g2s(S.ez + (xa - (x0 - 1)) * L, ez + (rowc + xa) * L, (xb - xa) * row4, &full[s]);
-    if (!tail) bulk_g2s(S.hx, hx + (rowc + x0) * L, (xe - x0) * row4, &full[s]);
-    if (!pro && !tail) {
-      bulk_g2s(S.hy + (xa - (x0 - 1)) * L, hy + (rowc + xa) * L, (xe - xa) * row4, &full[s]);
-      bulk_g2s(S.coef, coef + rowc + x0, (xe - x0) * 16u, &full[s]);
-#pragma unroll
-      for (int q = 0; q < NP; ++q) {
-        bulk_g2s(S.ade + q * CX, ade + q * plane + rowc + x0, (xe - x0) * 16u, &full[s]);
-        bulk_g2s(S.j + q * CX * L, J + (q * plane + rowc + x0) * L, (xe - x0) * row4, &full[s]);
+    const size_t rowp = (size_t)r * 2 * n;
+    // Two passes over the same list: count the bytes, then issue the copies.
+    for (int pass = 0; pass < 2; ++pass) {
+      uint32_t bytes = 0;
+      auto cp = [&](void* dst, const void* src, uint32_t nb) {
+        if (nb == 0) return;
+        if (pass) bulk_g2s(dst, src, nb, &full[s]);
+        else bytes += nb;
+      };
+      cp(S.ez + (xa - (x0 - 1)) * L, ez + (rowc + xa) * L, (xb - xa) * cb);
+      if (!tail) {
+        cp(S.hx, hx + (rowc + x0) * L, (xe - x0) * cb);
+        if (shy >= 0) cp(S.phx, psi_hx + ((size_t)shy * nx + x0) * L, (xe - x0) * cb);
       }
+      if (body) {
+        cp(S.hy + (xa - (x0 - 1)) * L, hy + (rowc + xa) * L, (xe - xa) * cb);
+        cp(S.coef, coef + rowc + x0, (xe - x0) * 16u);
+        if (sey >= 0) cp(S.pey, psi_ezy + ((size_t)sey * nx + x0) * L, (xe - x0) * cb);
+        if (hl1 > hl0) cp(S.phy + (hl0 - (x0 - 1)) * L, psi_hy + (rowp + hl0) * L, (hl1 - hl0) * cb);
+        if (hr1 > hr0) cp(S.phy + (hr0 - (x0 - 1)) * L, psi_hy + (rowp + n + hr0 - (nx - n)) * L, (hr1 - hr0) * cb);
+        if (el1 > el0) cp(S.pex + (el0 - x0) * L, psi_ezx + (rowp + el0 - 1) * L, (el1 - el0) * cb);
+        if (er1 > er0) cp(S.pex + (er0 - x0) * L, psi_ezx + (rowp + n + er0 - (nx - n)) * L, (er1 - er0) * cb);
 #pragma unroll
-      for (int q = 0; q < NL; ++q)
-        bulk_g2s(S.jp + q * CX * L, Jp + (q * plane + rowc + x0) * L, (xe - x0) * row4, &full[s]);
+        for (int q = 0; q < NP; ++q) {
+          cp(S.ade + q * CX, ade + q * plane + rowc + x0, (xe - x0) * 16u);
+          cp(S.j + q * CX * L, J + (q * plane + rowc + x0) * L, (xe - x0) * cb);
+        }
+#pragma unroll
+        for (int q = 0; q < NL; ++q) cp(S.jp + q * CX * L, Jp + (q * plane + rowc + x0) * L, (xe - x0) * cb);
+      }
+      if (!pass) mbar_arrive_expect_tx(&full[s], bytes);
     }
     issued = k + 1;
   }
@@ -185,6 +228,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   constexpr int NP = ND + NL;
   constexpr int CX = kConsumers / L;
   const int nx = p.nx, ny = p.ny, n = p.n;
+  const Strips sp{n, nx, ny};
   const int cx = threadIdx.x / L, lo = threadIdx.x % L;
   const int x = x0 + cx;
   const bool active = x < nx;
@@ -193,9 +237,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   float4* ezw = p.ez[par ^ 1] + gf;
   float4* hxw = p.hx[par ^ 1] + gf;
   float4* hyw = p.hy[par ^ 1] + gf;
-  const float4* psi_hx_in = p.psi_hx[par] + (size_t)g * p.gs_psi_y;
   float4* psi_hx_out = p.psi_hx[par ^ 1] + (size_t)g * p.gs_psi_y;
-  const float4* psi_hy_in = p.psi_hy[par] + (size_t)g * p.gs_psi_x;
   float4* psi_hy_out = p.psi_hy[par ^ 1] + (size_t)g * p.gs_psi_x;
   float4* psi_ezx = p.psi_ezx + (size_t)g * p.gs_psi_x;
   float4* psi_ezy = p.psi_ezy + (size_t)g * p.gs_psi_y;
@@ -203,6 +245,18 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
   const size_t plane = (size_t)nx * ny;
   const int lane_g = g * L + lo;  // float4 lane across all groups (tx = 4*lane_g + c)
+  // x-strip membership of this cell (H: Hy at x and x-1; E: Ez at x)
+  const int hxs = (x < n) ? x : (x >= nx - n && x < nx - 1) ? n + (x - (nx - n)) : -1;
+  const int ex_s = (x >= 1 && x <= n) ? x - 1 : (x >= nx - n) ? n + (x - (nx - n)) : -1;
+  const int ex_c = (x >= 1 && x <= n) ? x - 1 : nx - 1 - x;
+
+  // Source/probe rows of this segment as bit masks (rows <= 64).
+  uint64_t src_rows = 0, prb_rows = 0;
+  for (int y = y0; y < y1; ++y) {
+    const uint8_t f = __ldg(p.row_flags + y);
+    if (f & 1) src_rows |= 1ull << (y - y0);
+    if (f & 2) prb_rows |= 1ull << (y - y0);
+  }
 
   // Warp-uniform bounded wait: if any lane gives up, the whole warp leaves.
   auto wait = [&](int k) {
@@ -221,13 +275,12 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   if (!wait(0)) return;
   int k = 0;
   float4 hx_prev = f4(0.f);
-  if (y0 > 0) {  // slot 0 holds row y0-1 (Ez, Hx): Hx^{n+1/2}(x, y0-1)
+  if (y0 > 0) {  // slot 0 holds row y0-1 (Ez, Hx, H psi): Hx^{n+1/2}(x, y0-1)
     if (!wait(1)) return;
     if (active) {
       const Stage2d<L, NP, NL>& A = st[0];
-      const Stage2d<L, NP, NL>& Bn = st[1 % kStages];
-      hx_prev = hx_new<GEN>(p, psi_hx_in, nullptr, x, y0 - 1, lo, A.hx[cx * L + lo], A.ez[(cx + 1) * L + lo],
-                            Bn.ez[(cx + 1) * L + lo]);
+      hx_prev = hx_new<GEN>(p, A.phx[cx * L + lo], nullptr, x, y0 - 1, A.hx[cx * L + lo], A.ez[(cx + 1) * L + lo],
+                            st[1 % kStages].ez[(cx + 1) * L + lo]);
     }
     release(0);
     k = 1;
@@ -238,17 +291,22 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
     if (has_up && !wait(k + 1)) return;
     const Stage2d<L, NP, NL>& A = st[k % kStages];
     if (active) {
-      const float4 ez_c = A.ez[(cx + 1) * L + lo];
-      const float4 ez_up = has_up ? st[(k + 1) % kStages].ez[(cx + 1) * L + lo] : f4(0.f);
-      const float4 ez_r = A.ez[(cx + 2) * L + lo];
-      const float4 ez_l = A.ez[cx * L + lo];
+      const int i0 = (cx + 1) * L + lo;  // this cell in the halo'd slices
+      const float4 ez_c = A.ez[i0];
+      const float4 ez_up = has_up ? st[(k + 1) % kStages].ez[i0] : f4(0.f);
       const size_t at = ((size_t)y * nx + x) * L + lo;
+      const int shy = GEN ? sp.hy_row(y) : -1;
+      const int sey = GEN ? sp.ey_row(y) : -1;
 
       // H phase: this cell, plus the recomputed Hy of the left neighbour
-      const float4 hxn = hx_new<GEN>(p, psi_hx_in, psi_hx_out, x, y, lo, A.hx[cx * L + lo], ez_c, ez_up);
-      const float4 hyn = hy_new<GEN>(p, psi_hy_in, psi_hy_out, x, y, lo, A.hy[(cx + 1) * L + lo], ez_c, ez_r);
+      const float4 hxn = hx_new<GEN>(p, A.phx[cx * L + lo],
+                                     shy >= 0 ? psi_hx_out + ((size_t)shy * nx + x) * L + lo : nullptr, x, y,
+                                     A.hx[cx * L + lo], ez_c, ez_up);
+      const float4 hyn = hy_new<GEN>(p, A.phy[i0], hxs >= 0 ? psi_hy_out + ((size_t)y * 2 * n + hxs) * L + lo : nullptr,
+                                     x, y, A.hy[i0], ez_c, A.ez[i0 + L]);
       float4 hyl = f4(0.f);
-      if (!GEN || x >= 1) hyl = hy_new<GEN>(p, psi_hy_in, nullptr, x - 1, y, lo, A.hy[cx * L + lo], ez_l, ez_c);
+      if (!GEN || x >= 1)
+        hyl = hy_new<GEN>(p, A.phy[i0 - L], nullptr, x - 1, y, A.hy[i0 - L], A.ez[i0 - L], ez_c);
       st4(hxw + at, hxn);
       st4(hyw + at, hyn);
 
@@ -271,7 +329,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
             sum = (q < ND) ? fma4(A.ade[q * CX + cx].z, jq, sum) : sum + jq;
           }
           en = en - cf.y * sum;
-          const float4 dedt = (en - e) / p.dt;
+          const float4 dedt = (en - e) * f4(p.inv_dt);
 #pragma unroll
           for (int q = 0; q < NP; ++q) {
             const float4 kq = A.ade[q * CX + cx];
@@ -290,49 +348,35 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
       }
       if (GEN && n > 0) {
         // E-CPML x strips (fdtd_2d_batched.py:355-378)
-        int sx = -1, ci = 0;
-        if (y >= 1) {
-          if (x >= 1 && x <= n) { sx = x - 1; ci = x - 1; }
-          else if (x >= nx - n) { sx = n + (x - (nx - n)); ci = nx - 1 - x; }
-        }
-        if (sx >= 0) {
-          float4* pp = psi_ezx + ((size_t)y * (2 * n) + sx) * L + lo;
-          const float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhy * f4(p.inv_dx));
-          *pp = psi;
+        if (y >= 1 && ex_s >= 0) {
+          const float4 psi = p.cpml_b[ex_c] * A.pex[cx * L + lo] + p.cpml_c[ex_c] * (dhy * f4(p.inv_dx));
+          st4(psi_ezx + ((size_t)y * 2 * n + ex_s) * L + lo, psi);
           e = fma4(cf.z, psi, e);
         }
         // E-CPML y strips (fdtd_2d_batched.py:380-406)
-        int sy = -1;
-        if (x >= 1) {
-          if (y >= 1 && y <= n) { sy = y - 1; ci = y - 1; }
-          else if (y >= ny - n) { sy = n + (y - (ny - n)); ci = ny - 1 - y; }
-        }
-        if (sy >= 0) {
-          float4* pp = psi_ezy + ((size_t)sy * nx + x) * L + lo;
-          const float4 psi = p.cpml_b[ci] * (*pp) + p.cpml_c[ci] * (dhx * f4(p.inv_dx));
-          *pp = psi;
+        if (x >= 1 && sey >= 0) {
+          const int ci = (y <= n) ? y - 1 : ny - 1 - y;
+          const float4 psi = p.cpml_b[ci] * A.pey[cx * L + lo] + p.cpml_c[ci] * (dhx * f4(p.inv_dx));
+          st4(psi_ezy + ((size_t)sey * nx + x) * L + lo, psi);
           e = fma4(-cf.z, psi, e);
         }
       }
       if (GEN && (x == 0 || x == nx - 1 || y == 0 || y == ny - 1)) e = f4(0.f);
 
       // soft source and probe record (fdtd_2d_batched.py:509-526)
-      const uint8_t flags = __ldg(p.row_flags + y);
-      if (flags) {
-        if (flags & 1) {
-          const float w = __ldg(p.waveform + step);
-          for (int s = 0; s < p.ntx; ++s)
-            if ((s >> 2) == lane_g && __ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y)
-              add_comp(e, s & 3, w);
-        }
-        if (flags & 2) {
-          for (int q = 0; q < p.nprobe; ++q) {
-            if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
+      if ((src_rows >> (y - y0)) & 1) {
+        const float w = __ldg(p.waveform + step);
+        for (int s = 0; s < p.ntx; ++s)
+          if ((s >> 2) == lane_g && __ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y)
+            add_comp(e, s & 3, w);
+      }
+      if ((prb_rows >> (y - y0)) & 1) {
+        for (int q = 0; q < p.nprobe; ++q) {
+          if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
 #pragma unroll
-              for (int c = 0; c < 4; ++c) {
-                const int tx = 4 * lane_g + c;
-                if (tx < p.ntx) p.probes[((size_t)tx * p.nprobe + q) * p.nsteps + step] = comp(e, c);
-              }
+            for (int c = 0; c < 4; ++c) {
+              const int tx = 4 * lane_g + c;
+              if (tx < p.ntx) p.probes[((size_t)tx * p.nprobe + q) * p.nsteps + step] = comp(e, c);
             }
           }
         }
@@ -397,6 +441,7 @@ static cudaError_t configure_l(Fdtd2dParams& p) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   p.smem = (int)smem;
+  if (p.rows > kMaxRows) p.rows = kMaxRows;
   if (p.rows > 0) return cudaSuccess;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
@@ -411,7 +456,7 @@ static cudaError_t configure_l(Fdtd2dParams& p) {
   const long xb = (p.nx + CX - 1) / CX;
   double best = 1e300;
   int best_rows = 16;
-  for (int rows = 4; rows <= 128; ++rows) {
+  for (int rows = 4; rows <= kMaxRows; ++rows) {
     const long blocks = xb * ((p.ny + rows - 1) / rows) * p.groups;
     const long waves = (blocks + slots - 1) / slots;
     const double cost = (double)waves * (rows + 2);

@@ -14,7 +14,7 @@ struct Fdtd2dParams {
   int n_debye, n_lorentz;
   int rows;             // rows of the column segment one block walks
   int smem;             // dynamic shared memory per block
-  float db, db_dx, inv_dx, dt;
+  float db, db_dx, inv_dx, dt, inv_dt;
   // per-group strides in float4
   long long gs_field, gs_psi_x, gs_psi_y, gs_j, gs_jp;
   float4* ez[2];
