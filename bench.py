@@ -214,9 +214,11 @@ def run_ours(args, w):
         peak, peak_src = 6650.0, "fallback"
     achieved = bytes_step / (launch_ms * 1e-3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "fdtd2d_step_head600_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", f"fdtd2d_step_{args.workload}.md")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("bytes_per_launch")
+        for line in open(tpath):
+            if line.startswith("dram_bytes_per_launch"):
+                traffic = int(line.split("=")[1])
 
     # -- end to end through the public API with host buffers
     e2e = None
