@@ -291,3 +291,75 @@ extern "C" int ceep_das_time(const float* s, const double* ant_xy, int32_t nant,
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "das_time_kernel launch");
 }
+
+// --------------------------------------------------------------------------
+// Delay-and-sum without a caller workspace.
+//
+// Some callers cannot hand this library any device memory: for example an
+// imaging pipeline that reserves all of its GPU memory in its own pool at
+// start-up and must not allocate while a scan is running, or a host
+// application whose allocator this library cannot reach.  For them the
+// partial sums of ceep_das live in one fixed array that the library itself
+// declares at file scope, so the call needs no cudaMalloc at all.
+//
+// Facts a caller must know:
+//  * The array holds kDasNoAllocScratch complex partial sums (2 MiB).  Every
+//    GPU that loads this library keeps that much memory reserved until the
+//    process exits.  Images whose (frequency chunks x pixels) exceed it are
+//    rejected with CEEP_ERR_UNSUPPORTED before anything is launched.
+//  * In host code the array's name is only a host-side stand-in; its device
+//    address is looked up with cudaGetSymbolAddress on the first call made
+//    on each device (with that device current) and cached.  That first call
+//    therefore does set-up work and should be made before any stream capture.
+//  * Every call on a device shares the one array.  Two calls whose kernels
+//    overlap on the GPU (different streams, no ordering between them) race
+//    on it and give wrong images; order them on one stream or serialise them.
+//  * Nothing in the array needs to start at zero: the partial-sum kernel
+//    writes every entry that the finishing kernel later reads, so the
+//    contents a previous call left behind are never used.
+// --------------------------------------------------------------------------
+namespace ceep {
+constexpr int64_t kDasNoAllocScratch = 262144;  // float2 entries = 2 MiB
+static __device__ __align__(256) float2 g_das_noalloc_scratch[kDasNoAllocScratch];
+}  // namespace ceep
+
+#include <mutex>
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_das_scratch_mu;
+void* g_das_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int64_t ceep_das_noalloc_capacity(void) { return ceep::kDasNoAllocScratch; }
+
+extern "C" int ceep_das_noalloc(const float* s, const float* kfreq, const float* ant_xy, int32_t nfreq,
+                                int32_t nant, int32_t nx_pix, int32_t ny_pix, float px0, float py0, float pix,
+                                int normalize, float* image, void* stream) {
+  if (!s || !kfreq || !ant_xy || !image) return fail(CEEP_ERR_INVALID, "ceep_das_noalloc: null pointer");
+  if (nfreq < 1 || nant < 1 || nx_pix < 1 || ny_pix < 1)
+    return fail(CEEP_ERR_INVALID, "ceep_das_noalloc: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix,
+                ny_pix);
+  const int64_t need = ceep_das_workspace_bytes(nx_pix, ny_pix, nfreq) / (int64_t)sizeof(float2);
+  if (need > ceep::kDasNoAllocScratch)
+    return fail(CEEP_ERR_UNSUPPORTED,
+                "ceep_das_noalloc: %dx%d pixels x %d frequencies need %lld partial sums, the fixed scratch holds "
+                "%lld; use ceep_das with a workspace",
+                nx_pix, ny_pix, nfreq, (long long)need, (long long)ceep::kDasNoAllocScratch);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "ceep_das_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(CEEP_ERR_UNSUPPORTED, "ceep_das_noalloc: device %d", dev);
+  void* scratch;
+  {
+    std::lock_guard<std::mutex> lock(g_das_scratch_mu);
+    if (!g_das_scratch_ptr[dev]) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, ceep::g_das_noalloc_scratch);
+      if (e != cudaSuccess || !ptr) return ceep::cuda_fail(e, "ceep_das_noalloc: cudaGetSymbolAddress");
+      g_das_scratch_ptr[dev] = ptr;
+    }
+    scratch = g_das_scratch_ptr[dev];
+  }
+  return ceep_das(s, kfreq, ant_xy, nfreq, nant, nx_pix, ny_pix, px0, py0, pix, normalize, scratch, image, stream);
+}

@@ -142,6 +142,25 @@ int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
              void* work, float* image, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Frequency-domain delay-and-sum for callers that cannot allocate device
+ * memory.  No counterpart in the reference: it exists for hosts that own all
+ * GPU memory through their own pool (for example a scanner pipeline that
+ * reserves its memory at start-up and may not allocate mid-scan) and so
+ * cannot pass ceep_das a workspace.  Same arguments and result as ceep_das
+ * without `work`; the partial sums live in a fixed 2 MiB array inside the
+ * library (ceep_das_noalloc_capacity() complex entries) that every GPU which
+ * loads the library keeps until exit.  Larger problems are rejected with
+ * CEEP_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address (make it before any stream capture); calls that overlap on
+ * the GPU share the array and race.  Calls no allocating routine.
+ * ---------------------------------------------------------------------- */
+int64_t ceep_das_noalloc_capacity(void);
+int ceep_das_noalloc(const float* s, const float* kfreq, const float* ant_xy,
+                     int32_t nfreq, int32_t nant, int32_t nx_pix, int32_t ny_pix,
+                     float px0, float py0, float pix, int normalize,
+                     float* image, void* stream);
+
+/* ------------------------------------------------------------------------
  * Time-domain delay-and-sum image.
  * Replaces das_imaging, scripts/verify_dataset_with_das.py:37-103:
  * pixel (i,j) at (i*dx, j*dx); for tx != rx, idx = int((|a_tx-p|+|a_rx-p|)/C/dt)
