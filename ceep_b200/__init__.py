@@ -2,12 +2,14 @@
 
 Public API:
     BatchedFDTD2D                      2D TMz batched solver (fdtd_2d_batched.py)
+    BatchedFDTD3D                      3D Yee batched solver (fdtd_3d_batched.py)
     MultistaticSParameters, ImagingRegion, DelayAndSumBeamformer, dft, das_time
 The compute runs in ``_lib/libceep_b200.so`` (sm_100a); there is no CPU path.
 """
 from .solvers import BatchedFDTD2D
+from .solvers3d import BatchedFDTD3D
 from .spectral import (DelayAndSumBeamformer, ImagingRegion, MultistaticSParameters, das_image, das_time,
                        dft)
 
-__all__ = ["BatchedFDTD2D", "MultistaticSParameters", "ImagingRegion", "DelayAndSumBeamformer", "dft",
+__all__ = ["BatchedFDTD2D", "BatchedFDTD3D", "MultistaticSParameters", "ImagingRegion", "DelayAndSumBeamformer", "dft",
            "das_image", "das_time"]

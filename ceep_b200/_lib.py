@@ -30,6 +30,19 @@ class Desc2D(C.Structure):
     ]
 
 
+class Desc3D(C.Structure):
+    """Mirror of ``ceep3d_desc``."""
+    _fields_ = [
+        ("nx", I32), ("ny", I32), ("nz", I32), ("cpml", I32), ("ntx", I32), ("ntx_pad", I32),
+        ("nprobe", I32), ("nsteps", I32), ("n_debye", I32), ("n_lorentz", I32),
+        ("inv_dx", C.c_float), ("dt", C.c_float),
+        ("ex", P), ("ey", P), ("ez", P), ("hx", P), ("hy", P), ("hz", P),
+        ("psi_hxy", P), ("psi_hzy", P), ("psi_hyx", P), ("psi_hzx", P), ("psi_hxz", P), ("psi_hyz", P),
+        ("j", P), ("j_prev", P), ("coef", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
+        ("src_xyz", P), ("prb_xyz", P), ("waveform", P), ("probes", P), ("z_rows", I32),
+    ]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "ceep_version": (C.c_int, []),
@@ -42,6 +55,10 @@ _SIGS = {
     "ceep2d_plan_reset": (C.c_int, [P]),
     "ceep2d_desc_size": (I64, []),
     "ceep2d_plan_rows": (C.c_int, [P]),
+    "ceep3d_plan_create": (C.c_int, [C.POINTER(Desc3D), C.POINTER(P)]),
+    "ceep3d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
+    "ceep3d_plan_destroy": (C.c_int, [P]),
+    "ceep3d_desc_size": (I64, []),
     "ceep_dft": (C.c_int, [P, P, P, I32, I32, I32, I32, P]),
     "ceep_das_workspace_bytes": (I64, [I32, I32, I32]),
     "ceep_das": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),
@@ -71,8 +88,8 @@ def lib():
             fn = getattr(h, name)
             fn.restype = res
             fn.argtypes = args
-        if h.ceep2d_desc_size() != C.sizeof(Desc2D):
-            raise ImportError("ceep2d_desc layout mismatch between header and binding")
+        if h.ceep2d_desc_size() != C.sizeof(Desc2D) or h.ceep3d_desc_size() != C.sizeof(Desc3D):
+            raise ImportError("descriptor layout mismatch between header and binding")
         _lib = h
     return _lib
 

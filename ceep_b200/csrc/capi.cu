@@ -178,3 +178,115 @@ extern "C" int ceep2d_plan_destroy(ceep2d_plan* pl) {
 }
 
 extern "C" int ceep2d_launches_per_step(const ceep2d_plan* pl) { return pl ? 1 : 0; }
+
+// --------------------------------------------------------------------------
+// 3D plan
+// --------------------------------------------------------------------------
+#include "fdtd3d.cuh"
+
+struct ceep3d_plan {
+  ceep::Fdtd3dParams p;
+  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+};
+
+extern "C" int64_t ceep3d_desc_size(void) { return (int64_t)sizeof(ceep3d_desc); }
+
+extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
+  if (!d || !out) return fail(CEEP_ERR_INVALID, "ceep3d_plan_create: null argument");
+  *out = nullptr;
+  const int n = d->cpml;
+  if (n == 1 || n < 0) return fail(CEEP_ERR_INVALID, "cpml thickness must be 0 or >= 2 (got %d)", n);
+  if (d->nx < 2 * n + 2 || d->ny < 2 * n + 2 || d->nz < 2 * n + 2 || d->nx < 3 || d->ny < 3 || d->nz < 3)
+    return fail(CEEP_ERR_INVALID, "grid %dx%dx%d must exceed twice the CPML (%d) by 2", d->nx, d->ny, d->nz, n);
+  if (d->ntx < 1 || d->ntx_pad < d->ntx || d->ntx_pad % 4)
+    return fail(CEEP_ERR_INVALID, "ntx=%d ntx_pad=%d", d->ntx, d->ntx_pad);
+  const int lanes = d->ntx_pad / 4;
+  const int L = lanes <= 8 ? lanes : 8;
+  if ((lanes > 8 && lanes % 8) || (L != 1 && L != 2 && L != 4 && L != 8))
+    return fail(CEEP_ERR_INVALID, "ntx_pad=%d: pad to 4, 8, 16 or a multiple of 32", d->ntx_pad);
+  if (d->n_debye < 0 || d->n_lorentz < 0 || d->n_debye + d->n_lorentz > 2)
+    return fail(CEEP_ERR_UNSUPPORTED, "ADE poles: at most 2 per cell");
+  if (d->nsteps < 1 || d->nprobe < 0) return fail(CEEP_ERR_INVALID, "nsteps/nprobe");
+  if (!d->ex || !d->ey || !d->ez || !d->hx || !d->hy || !d->hz || !d->coef || !d->src_xyz || !d->waveform ||
+      (d->nprobe && (!d->prb_xyz || !d->probes)))
+    return fail(CEEP_ERR_INVALID, "null field/coefficient/source/probe buffer");
+  if (n > 0 && (!d->psi_hxy || !d->psi_hzy || !d->psi_hyx || !d->psi_hzx || !d->psi_hxz || !d->psi_hyz ||
+                !d->cpml_b || !d->cpml_c))
+    return fail(CEEP_ERR_INVALID, "null CPML buffer");
+  if (d->n_debye + d->n_lorentz > 0 && (!d->j || !d->ade_coef || (d->n_lorentz && !d->j_prev)))
+    return fail(CEEP_ERR_INVALID, "null ADE buffer");
+  ceep3d_plan* pl = new (std::nothrow) ceep3d_plan();
+  if (!pl) return fail(CEEP_ERR_INVALID, "host allocation failed");
+  ceep::Fdtd3dParams& p = pl->p;
+  p.nx = d->nx; p.ny = d->ny; p.nz = d->nz; p.n = n;
+  p.ntx = d->ntx; p.L = L; p.groups = lanes / L;
+  p.nprobe = d->nprobe; p.nsteps = d->nsteps;
+  p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
+  p.zrows = d->z_rows > 0 ? d->z_rows : 16;
+  p.zsegs = (d->nz + p.zrows - 1) / p.zrows;
+  const int nzi = d->nz - 2 * n - 1;
+  p.zsegs_e = nzi > 0 ? (nzi + p.zrows - 1) / p.zrows : 0;
+  p.inv_dx = d->inv_dx; p.dt = d->dt; p.inv_dt = (float)(1.0 / (double)d->dt);
+  const long long cells = (long long)d->nx * d->ny * d->nz;
+  const long long nn = n > 0 ? n : 1;
+  p.gs_field = cells * L;
+  p.gs_px = (long long)d->nz * d->ny * 2 * nn * L;
+  p.gs_py = (long long)d->nz * 2 * nn * d->nx * L;
+  p.gs_pz = 2 * nn * d->ny * (long long)d->nx * L;
+  p.gs_j = cells * 3 * (d->n_debye + d->n_lorentz) * L;
+  p.gs_jp = cells * 3 * d->n_lorentz * L;
+  auto f4p = [](float* q) { return reinterpret_cast<float4*>(q); };
+  p.ex = f4p(d->ex); p.ey = f4p(d->ey); p.ez = f4p(d->ez);
+  p.hx = f4p(d->hx); p.hy = f4p(d->hy); p.hz = f4p(d->hz);
+  p.psi_hxy = f4p(d->psi_hxy); p.psi_hzy = f4p(d->psi_hzy);
+  p.psi_hyx = f4p(d->psi_hyx); p.psi_hzx = f4p(d->psi_hzx);
+  p.psi_hxz = f4p(d->psi_hxz); p.psi_hyz = f4p(d->psi_hyz);
+  p.j = f4p(d->j); p.j_prev = f4p(d->j_prev);
+  p.coef = d->coef; p.ade_coef = d->ade_coef; p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
+  p.src_xyz = d->src_xyz; p.prb_xyz = d->prb_xyz; p.waveform = d->waveform; p.probes = d->probes;
+  *out = pl;
+  return CEEP_OK;
+}
+
+static int run_steps3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, cudaStream_t s) {
+  for (int64_t k = 0; k < nsteps; ++k) {
+    cudaError_t e = ceep::fdtd3d_launch_step(pl->p, (int)(step0 + k), s);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd3d step launch");
+  }
+  return CEEP_OK;
+}
+
+extern "C" int ceep3d_plan_run(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+  if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
+  if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
+    return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
+                (long long)(step0 + nsteps), pl->p.nsteps);
+  if (nsteps == 0) return CEEP_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!use_graph || s == nullptr) return run_steps3d(pl, step0, nsteps, s);
+  auto key = std::make_pair(step0, nsteps);
+  auto it = pl->graphs.find(key);
+  if (it == pl->graphs.end()) {
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
+    int rc = run_steps3d(pl, step0, nsteps, s);
+    e = cudaStreamEndCapture(s, &g);
+    if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphInstantiate");
+    it = pl->graphs.emplace(key, ex).first;
+  }
+  cudaError_t e = cudaGraphLaunch(it->second, s);
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "cudaGraphLaunch");
+}
+
+extern "C" int ceep3d_plan_destroy(ceep3d_plan* pl) {
+  if (!pl) return CEEP_OK;
+  for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  delete pl;
+  return CEEP_OK;
+}

@@ -1,0 +1,284 @@
+// Batched 3D Yee FDTD for sm_100a: one H kernel and one E kernel per step
+// (each a fused half-step), plus a one-block epilogue for sources/probes.
+//
+// Region semantics of the reference's BatchedFDTD3D.run()
+// (src/ceep/solvers/fdtd_3d_batched.py:886-985):
+//   H  interior boxes (:753-818):
+//        Hx on x in [n, nx-n), y in [n, ny-1), z in [n, nz-1)
+//        Hy on x in [n, nx-1), y in [n, ny-n), z in [n, nz-1)
+//        Hz on x in [n, nx-1), y in [n, ny-1), z in [n, nz-n)
+//      then the CPML faces in the order x, y, z (:398-586); each face's psi
+//      recurrence runs over the whole slab, low faces use forward and high
+//      faces backward differences:
+//        x faces: Hy -= db psi(dEz/dx) (z < nz-1), Hz += db psi(dEy/dx) (y < ny-1)
+//        y faces: Hx -= db psi(dEz/dy) (z < nz-1), Hz += db psi(dEx/dy) (x < nx-1)
+//        z faces: Hx += db psi(dEy/dz) (y < ny-1), Hy -= db psi(dEx/dz) (x < nx-1)
+//      each face update being H = da*H +/- db*psi on the already-updated H.
+//   E  only on [n+1, N-n)^3 (:820-884); the rest of E is never updated.
+//   E zeroed on the three low faces (:936-944), soft Ez source (:949-951),
+//   Ez probes (:956-958).
+// The E interior reads only H cells of the interior boxes, so the two
+// half-steps are separate launches that update their fields in place.
+//
+// Layout: (group, z, y, x, L float4), tx innermost.  A block is 128 threads =
+// 128/L cells of one x-row; each thread walks a z segment carrying the
+// z-neighbour planes in registers.  Per-cell coefficients are float4
+// (da, db, ca, cb).
+#include "../../include/ceep_b200.h"
+#include "common.cuh"
+#include "fdtd3d.cuh"
+
+namespace ceep {
+
+constexpr int kThreads3d = 128;
+
+// ---------------------------------------------------------------------------
+// H half-step
+// ---------------------------------------------------------------------------
+template <int L>
+__global__ void __launch_bounds__(kThreads3d) fdtd3d_h_kernel(const Fdtd3dParams p) {
+  constexpr int CX = kThreads3d / L;
+  const int x = blockIdx.x * CX + threadIdx.x / L;
+  const int lo = threadIdx.x % L;
+  const int y = blockIdx.y;
+  const int zseg = blockIdx.z % p.zsegs, g = blockIdx.z / p.zsegs;
+  const int z0 = zseg * p.zrows, z1 = min(z0 + p.zrows, p.nz);
+  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n;
+  if (x >= nx) return;
+  const size_t gs = (size_t)g * p.gs_field;
+  const float4* __restrict__ ex = p.ex + gs;
+  const float4* __restrict__ ey = p.ey + gs;
+  const float4* __restrict__ ez = p.ez + gs;
+  float4* hx = p.hx + gs;
+  float4* hy = p.hy + gs;
+  float4* hz = p.hz + gs;
+  const float4* coef = reinterpret_cast<const float4*>(p.coef);
+  const size_t sx = L, sy = (size_t)nx * L, sz = (size_t)ny * nx * L;  // float4 strides
+  const float inv = p.inv_dx;
+  const bool x_int_hx = x >= n && x < nx - n, x_int = x >= n && x < nx - 1;
+  const bool y_int_hy = y >= n && y < ny - n, y_int = y >= n && y < ny - 1;
+  const int xf = x < n ? x : (x >= nx - n ? n + (x - (nx - n)) : -1);   // x-face slot
+  const int xc = x < n ? x : nx - 1 - x;                                  // its coefficient
+  const int yf = y < n ? y : (y >= ny - n ? n + (y - (ny - n)) : -1);
+  const int yc = y < n ? y : ny - 1 - y;
+
+  size_t at = (size_t)z0 * sz + (size_t)y * sy + (size_t)x * sx + lo;
+  float4 exc = ld4(ex + at), eyc = ld4(ey + at), ezc = ld4(ez + at);
+  float4 exm = f4(0.f), eym = f4(0.f);
+  if (z0 > 0) { exm = ld4(ex + at - sz); eym = ld4(ey + at - sz); }
+  for (int z = z0; z < z1; ++z, at += sz) {
+    const bool up = z + 1 < nz;
+    const float4 exu = up ? ld4(ex + at + sz) : f4(0.f);
+    const float4 eyu = up ? ld4(ey + at + sz) : f4(0.f);
+    const float4 ezxp = x + 1 < nx ? ld4(ez + at + sx) : f4(0.f);
+    const float4 eyxp = x + 1 < nx ? ld4(ey + at + sx) : f4(0.f);
+    const float4 ezyp = y + 1 < ny ? ld4(ez + at + sy) : f4(0.f);
+    const float4 exyp = y + 1 < ny ? ld4(ex + at + sy) : f4(0.f);
+    const float4 cf = __ldg(coef + (size_t)z * ny * nx + (size_t)y * nx + x);  // da, db, ca, cb
+    float4 Hx = hx[at], Hy = hy[at], Hz = hz[at];
+    const bool z_int = z >= n && z < nz - 1, z_int_hz = z >= n && z < nz - n;
+    // interior boxes (fdtd_3d_batched.py:764-818)
+    if (x_int_hx && y_int && z_int) Hx = cf.x * Hx + cf.y * ((eyu - eyc) * f4(inv) - (ezyp - ezc) * f4(inv));
+    if (x_int && y_int_hy && z_int) Hy = cf.x * Hy + cf.y * ((ezxp - ezc) * f4(inv) - (exu - exc) * f4(inv));
+    if (x_int && y_int && z_int_hz) Hz = cf.x * Hz + cf.y * ((exyp - exc) * f4(inv) - (eyxp - eyc) * f4(inv));
+    if (n > 0) {
+      // x faces (:398-460)
+      if (xf >= 0) {
+        const bool lof = x < n;
+        const float4 ezn = lof ? ezxp : ld4(ez + at - sx);
+        const float4 eyn = lof ? eyxp : ld4(ey + at - sx);
+        const float4 dez = lof ? (ezn - ezc) * f4(inv) : (ezc - ezn) * f4(inv);
+        const float4 dey = lof ? (eyn - eyc) * f4(inv) : (eyc - eyn) * f4(inv);
+        const size_t pi = (((size_t)z * ny + y) * 2 * n + xf) * L + lo + (size_t)g * p.gs_px;
+        const float4 pa = p.cpml_b[xc] * p.psi_hxy[pi] + p.cpml_c[xc] * dez;
+        const float4 pb = p.cpml_b[xc] * p.psi_hzy[pi] + p.cpml_c[xc] * dey;
+        p.psi_hxy[pi] = pa;
+        p.psi_hzy[pi] = pb;
+        if (z < nz - 1) Hy = cf.x * Hy - cf.y * pa;
+        if (y < ny - 1) Hz = cf.x * Hz + cf.y * pb;
+      }
+      // y faces (:462-523)
+      if (yf >= 0) {
+        const bool lof = y < n;
+        const float4 ezn = lof ? ezyp : ld4(ez + at - sy);
+        const float4 exn = lof ? exyp : ld4(ex + at - sy);
+        const float4 dez = lof ? (ezn - ezc) * f4(inv) : (ezc - ezn) * f4(inv);
+        const float4 dex = lof ? (exn - exc) * f4(inv) : (exc - exn) * f4(inv);
+        const size_t pi = (((size_t)z * 2 * n + yf) * nx + x) * L + lo + (size_t)g * p.gs_py;
+        const float4 pa = p.cpml_b[yc] * p.psi_hyx[pi] + p.cpml_c[yc] * dez;
+        const float4 pb = p.cpml_b[yc] * p.psi_hzx[pi] + p.cpml_c[yc] * dex;
+        p.psi_hyx[pi] = pa;
+        p.psi_hzx[pi] = pb;
+        if (z < nz - 1) Hx = cf.x * Hx - cf.y * pa;
+        if (x < nx - 1) Hz = cf.x * Hz + cf.y * pb;
+      }
+      // z faces (:525-586)
+      const int zf = z < n ? z : (z >= nz - n ? n + (z - (nz - n)) : -1);
+      if (zf >= 0) {
+        const bool lof = z < n;
+        const int zc = lof ? z : nz - 1 - z;
+        const float4 dey = lof ? (eyu - eyc) * f4(inv) : (eyc - eym) * f4(inv);
+        const float4 dex = lof ? (exu - exc) * f4(inv) : (exc - exm) * f4(inv);
+        const size_t pi = (((size_t)zf * ny + y) * nx + x) * L + lo + (size_t)g * p.gs_pz;
+        const float4 pa = p.cpml_b[zc] * p.psi_hxz[pi] + p.cpml_c[zc] * dey;
+        const float4 pb = p.cpml_b[zc] * p.psi_hyz[pi] + p.cpml_c[zc] * dex;
+        p.psi_hxz[pi] = pa;
+        p.psi_hyz[pi] = pb;
+        if (y < ny - 1) Hx = cf.x * Hx + cf.y * pa;
+        if (x < nx - 1) Hy = cf.x * Hy - cf.y * pb;
+      }
+    }
+    hx[at] = Hx;
+    hy[at] = Hy;
+    hz[at] = Hz;
+    exm = exc; eym = eyc;
+    exc = exu; eyc = eyu;
+    ezc = up ? ld4(ez + at + sz) : f4(0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E half-step on the interior box, with the Debye/Lorentz currents of each
+// component (the 3D analogue of dispersive.py:364-404 / fdtd_2d.py:163-178).
+// ---------------------------------------------------------------------------
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kThreads3d) fdtd3d_e_kernel(const Fdtd3dParams p) {
+  constexpr int CX = kThreads3d / L;
+  constexpr int NP = ND + NL;
+  const int n = p.n, nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x = n + 1 + blockIdx.x * CX + threadIdx.x / L;
+  const int lo = threadIdx.x % L;
+  const int y = n + 1 + blockIdx.y;
+  const int zseg = blockIdx.z % p.zsegs_e, g = blockIdx.z / p.zsegs_e;
+  const int z0 = n + 1 + zseg * p.zrows, z1 = min(z0 + p.zrows, nz - n);
+  if (x >= nx - n) return;
+  const size_t gs = (size_t)g * p.gs_field;
+  float4* ex = p.ex + gs;
+  float4* ey = p.ey + gs;
+  float4* ez = p.ez + gs;
+  const float4* __restrict__ hx = p.hx + gs;
+  const float4* __restrict__ hy = p.hy + gs;
+  const float4* __restrict__ hz = p.hz + gs;
+  const float4* coef = reinterpret_cast<const float4*>(p.coef);
+  const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
+  const size_t sx = L, sy = (size_t)nx * L, sz = (size_t)ny * nx * L;
+  const size_t cells = (size_t)nx * ny * nz;
+  const float inv = p.inv_dx;
+  size_t at = (size_t)z0 * sz + (size_t)y * sy + (size_t)x * sx + lo;
+  float4 hxm = ld4(hx + at - sz), hym = ld4(hy + at - sz);
+  for (int z = z0; z < z1; ++z, at += sz) {
+    const float4 Hx = ld4(hx + at), Hy = ld4(hy + at), Hz = ld4(hz + at);
+    const float4 hzy = ld4(hz + at - sy), hzx = ld4(hz + at - sx);
+    const float4 hyx = ld4(hy + at - sx), hxy = ld4(hx + at - sy);
+    const size_t cell = (size_t)z * ny * nx + (size_t)y * nx + x;
+    const float4 cf = __ldg(coef + cell);
+    const float4 cx_ = (Hz - hzy) * f4(inv) - (Hy - hym) * f4(inv);
+    const float4 cy_ = (Hx - hxm) * f4(inv) - (Hz - hzx) * f4(inv);
+    const float4 cz_ = (Hy - hyx) * f4(inv) - (Hx - hxy) * f4(inv);
+    float4* E[3] = {ex + at, ey + at, ez + at};
+    const float4 curl[3] = {cx_, cy_, cz_};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float4 e0 = *E[c];
+      float4 e = cf.z * e0 + cf.w * curl[c];
+      if constexpr (NP > 0) {
+        const size_t jbase = (size_t)g * p.gs_j + (size_t)c * cells * L;
+        float4 sum = f4(0.f);
+        float4 jq[NP > 0 ? NP : 1];
+        float4 kq[NP > 0 ? NP : 1];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          kq[q] = __ldg(ade + q * cells + cell);
+          jq[q] = p.j[jbase + (size_t)q * 3 * cells * L + cell * L + lo];
+          sum = (q < ND) ? fma4(kq[q].z, jq[q], sum) : sum + jq[q];
+        }
+        e = e - cf.w * sum;
+        const float4 dedt = (e - e0) * f4(p.inv_dt);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          float4* jp = p.j + jbase + (size_t)q * 3 * cells * L + cell * L + lo;
+          if (q < ND) {
+            *jp = kq[q].x * jq[q] + kq[q].y * dedt;
+          } else {
+            float4* jm = p.j_prev + (size_t)g * p.gs_jp + (size_t)c * cells * L + (size_t)(q - ND) * 3 * cells * L +
+                         cell * L + lo;
+            const float4 jmv = *jm;
+            *jp = kq[q].x * jq[q] + kq[q].z * jmv + kq[q].y * dedt;
+            *jm = jq[q];
+          }
+        }
+      }
+      *E[c] = e;
+    }
+    hxm = Hx;
+    hym = Hy;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Epilogue: zero the low faces at source cells, add the source, read probes.
+// ---------------------------------------------------------------------------
+__global__ void fdtd3d_src_probe_kernel(const Fdtd3dParams p, int step) {
+  const int L = p.L;
+  const size_t sy = (size_t)p.nx * L, sz = (size_t)p.ny * p.nx * L;
+  float* ez = reinterpret_cast<float*>(p.ez);
+  const float w = p.waveform[step];
+  for (int b = threadIdx.x; b < p.ntx; b += blockDim.x) {
+    const int sxx = p.src_xyz[3 * b], syy = p.src_xyz[3 * b + 1], szz = p.src_xyz[3 * b + 2];
+    const int g = b / (4 * L), lane = b % (4 * L);
+    float* e = ez + 4 * ((size_t)g * p.gs_field + (size_t)szz * sz + (size_t)syy * sy + (size_t)sxx * L) + lane;
+    if (sxx == 0 || syy == 0 || szz == 0) *e = 0.f;
+    *e += w;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < p.ntx * p.nprobe; i += blockDim.x) {
+    const int b = i / p.nprobe, q = i % p.nprobe;
+    const int pxx = p.prb_xyz[3 * q], pyy = p.prb_xyz[3 * q + 1], pzz = p.prb_xyz[3 * q + 2];
+    const int g = b / (4 * L), lane = b % (4 * L);
+    p.probes[((size_t)b * p.nprobe + q) * p.nsteps + step] =
+        ez[4 * ((size_t)g * p.gs_field + (size_t)pzz * sz + (size_t)pyy * sy + (size_t)pxx * L) + lane];
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int L, int ND, int NL>
+static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s) {
+  constexpr int CX = kThreads3d / L;
+  dim3 gh((p.nx + CX - 1) / CX, p.ny, p.zsegs * p.groups);
+  fdtd3d_h_kernel<L><<<gh, kThreads3d, 0, s>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int ni = p.nx - 2 * p.n - 1, nj = p.ny - 2 * p.n - 1;
+  if (ni > 0 && nj > 0 && p.zsegs_e > 0) {
+    dim3 ge((ni + CX - 1) / CX, nj, p.zsegs_e * p.groups);
+    fdtd3d_e_kernel<L, ND, NL><<<ge, kThreads3d, 0, s>>>(p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  fdtd3d_src_probe_kernel<<<1, 256, 0, s>>>(p, step);
+  return cudaGetLastError();
+}
+
+template <int ND, int NL>
+static cudaError_t step_ade(const Fdtd3dParams& p, int step, cudaStream_t s) {
+  switch (p.L) {
+    case 1: return step_l<1, ND, NL>(p, step, s);
+    case 2: return step_l<2, ND, NL>(p, step, s);
+    case 4: return step_l<4, ND, NL>(p, step, s);
+    default: return step_l<8, ND, NL>(p, step, s);
+  }
+}
+
+cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s) {
+  switch (p.n_debye * 3 + p.n_lorentz) {
+    case 0: return step_ade<0, 0>(p, step, s);
+    case 1: return step_ade<0, 1>(p, step, s);
+    case 2: return step_ade<0, 2>(p, step, s);
+    case 3: return step_ade<1, 0>(p, step, s);
+    case 4: return step_ade<1, 1>(p, step, s);
+    case 6: return step_ade<2, 0>(p, step, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace ceep

@@ -110,6 +110,46 @@ int64_t ceep2d_desc_size(void);
 int ceep2d_plan_rows(const ceep2d_plan* plan);
 
 /* ------------------------------------------------------------------------
+ * 3D batched Yee FDTD.
+ * Replaces BatchedFDTD3D.run()'s time loop, src/ceep/solvers/fdtd_3d_batched.py:918-958
+ * (_update_h_fields :753-818, _apply_h_cpml_x/y/z :398-586,
+ *  _update_e_fields :820-884, low-face zeroing :936-944, source :949-951,
+ *  probes :956-958), with optional Debye/Lorentz currents on each E component.
+ * Three launches per step: H half-step, E half-step, source/probe epilogue;
+ * all state is updated in place.
+ * ---------------------------------------------------------------------- */
+typedef struct ceep3d_desc {
+  int32_t nx, ny, nz;
+  int32_t cpml;
+  int32_t ntx, ntx_pad, nprobe, nsteps;
+  int32_t n_debye, n_lorentz;
+  float inv_dx, dt;
+  /* fields, each (G, nz, ny, nx, ntx_pad/G) float, G = TX groups of <= 32 */
+  float *ex, *ey, *ez, *hx, *hy, *hz;
+  /* CPML psi: x faces (G, nz, ny, 2n, .), y faces (G, nz, 2n, nx, .),
+   * z faces (G, 2n, ny, nx, .); psi_hxy/psi_hzy act on Hy/Hz, psi_hyx/psi_hzx
+   * on Hx/Hz, psi_hxz/psi_hyz on Hx/Hy                                        */
+  float *psi_hxy, *psi_hzy, *psi_hyx, *psi_hzx, *psi_hxz, *psi_hyz;
+  float* j;                /* (G, poles, 3, nz, ny, nx, .)                   */
+  float* j_prev;           /* (G, n_lorentz, 3, nz, ny, nx, .)               */
+  const float* coef;       /* (nz, ny, nx, 4): da, db, ca, cb                */
+  const float* ade_coef;   /* (poles, nz, ny, nx, 4)                         */
+  const float* cpml_b;
+  const float* cpml_c;
+  const int32_t* src_xyz;  /* (ntx, 3) */
+  const int32_t* prb_xyz;  /* (nprobe, 3) */
+  const float* waveform;   /* (nsteps) */
+  float* probes;           /* (ntx, nprobe, nsteps) */
+  int32_t z_rows;          /* z segment per thread, 0 = default              */
+} ceep3d_desc;
+
+typedef struct ceep3d_plan ceep3d_plan;
+int ceep3d_plan_create(const ceep3d_desc* desc, ceep3d_plan** out);
+int ceep3d_plan_run(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+int ceep3d_plan_destroy(ceep3d_plan* plan);
+int64_t ceep3d_desc_size(void);
+
+/* ------------------------------------------------------------------------
  * On-device DFT of the probe series into the S-matrix.
  * Replaces the DFTMonitor accumulation of src/ceep/solvers/dft.py:55-90 run
  * over every (tx, rx) series, laid out as MultistaticSParameters.s_matrix

@@ -71,7 +71,7 @@ class Fdtd3DOracle:
         self.cb = ((dt / eps) / (1.0 + se)).astype(dtp)
         self.da = ((1.0 - sm) / (1.0 + sm)).astype(dtp)
         self.db = ((dt / mu) / (1.0 + sm)).astype(dtp)
-        b, c = cpml_profile(n, self.dx, dt, self.R0, self.order)
+        b, c = cpml_profile(n, self.dx, dt, self.R0, self.order) if n > 0 else (np.zeros(0), np.zeros(0))
         self.b, self.c = b.astype(dtp), c.astype(dtp)
         z = lambda *s: np.zeros(s, dtp)
         for f in ("ex", "ey", "ez", "hx", "hy", "hz"):

@@ -1,0 +1,119 @@
+"""Parity of the CUDA 3D path with the reference fixture and the oracle (1e-4 rel L2)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_l2
+from oracle.fdtd3d import Fdtd3DOracle
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _probes(out, B, P):
+    return np.array([[out[b][p] for p in range(P)] for b in range(B)])
+
+
+def test_small_against_reference(cuda_device):
+    from ceep_b200 import BatchedFDTD3D
+    g64, g32 = load_golden("fdtd3d_small_float64"), load_golden("fdtd3d_small_float32")
+    src = [tuple(int(v) for v in p) for p in g64["src"]]
+    prb = [tuple(int(v) for v in p) for p in g64["prb"]]
+    s = BatchedFDTD3D(20, 20, 20, 1e-3, 70, 4, src, prb, 2e9)
+    s.set_material_region(8, 14, 7, 13, 6, 12, eps_r=6.0, sigma_e=0.4, mu_r=1.5, sigma_m=200.0)
+    s.set_material_sphere(12, 10, 8, 3, eps_r=20.0, sigma_e=1.0)
+    np.testing.assert_array_equal(s._eps_r, g64["eps_r"])     # sphere quirk reproduced
+    out = _probes(s.run(), 3, 4)
+    assert rel_l2(out, g32["probes"]) < TOL
+    assert rel_l2(out, g64["probes"]) < TOL
+    for k in ("ex", "ey", "ez", "hx", "hy", "hz"):
+        assert rel_l2(getattr(s, k).cpu().numpy(), g64[k]) < TOL, k
+    assert abs(s.compute_energy() - float(g64["energy"])) / float(g64["energy"]) < TOL
+    # psi of the x faces: (G, nz, ny, 2n, W) -> reference (B, n, ny, nz)
+    psi = s._psi["hxy"][0, :, :, :, :3].permute(3, 2, 1, 0).cpu().numpy()
+    assert rel_l2(psi[:, :4], g64["psi_hxy_lo"]) < TOL
+    assert rel_l2(psi[:, 4:], g64["psi_hxy_hi"]) < TOL
+
+
+def test_sphere_non_cubic_raises_like_reference(cuda_device):
+    from ceep_b200 import BatchedFDTD3D
+    s = BatchedFDTD3D(22, 20, 18, 1e-3, 10, 4, [(10, 10, 9)], [(10, 10, 9)], 2e9)
+    with pytest.raises(IndexError):
+        s.set_material_sphere(11, 10, 9, 3, eps_r=5.0)
+
+
+CASES = [
+    # nx, ny, nz, n, steps, B, seed, sources in the shell
+    (18, 16, 14, 3, 60, 1, 0, False),
+    (24, 20, 22, 4, 80, 3, 1, True),
+    (16, 19, 17, 0, 50, 5, 2, True),
+    (21, 21, 21, 2, 70, 8, 3, False),
+    (20, 17, 23, 3, 40, 17, 4, True),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_random_against_oracle(cuda_device, case):
+    from ceep_b200 import BatchedFDTD3D
+    nx, ny, nz, n, steps, B, seed, shell = case
+    rng = np.random.default_rng(seed)
+    lo = 0 if shell else n + 1
+    src = [(int(rng.integers(lo, nx - lo)), int(rng.integers(lo, ny - lo)), int(rng.integers(lo, nz - lo)))
+           for _ in range(B)]
+    if shell:
+        src[0] = (0, ny // 2, nz // 3)
+    prb = [(int(rng.integers(0, nx)), int(rng.integers(0, ny)), int(rng.integers(0, nz))) for _ in range(4)] + [src[-1]]
+    shp = (nx, ny, nz)
+    eps = 1 + 9 * (rng.random(shp) < 0.3) * rng.random(shp)
+    sig = 0.5 * rng.random(shp) * (eps > 1)
+    mu = 1 + 0.5 * (rng.random(shp) < 0.1)
+    sm = 100.0 * (mu > 1)
+    o = Fdtd3DOracle(nx, ny, nz, 1e-3, steps, n, src, prb, 2e9, eps_r=eps, sigma_e=sig, mu_r=mu, sigma_m=sm)
+    o.run()
+    s = BatchedFDTD3D(nx, ny, nz, 1e-3, steps, n, src, prb, 2e9, z_rows=int(rng.integers(3, 9)))
+    s._eps_r[:], s._sigma_e[:], s._mu_r[:], s._sigma_m[:] = eps, sig, mu, sm
+    out = _probes(s.run(), B, len(prb))
+    assert rel_l2(out, o.probe_data) < TOL
+    for k in ("ez", "hx", "hy", "hz"):
+        assert rel_l2(getattr(s, k).cpu().numpy(), getattr(o, k)) < TOL, k
+    assert abs(s.compute_energy() - o.compute_energy()) / o.compute_energy() < TOL
+
+
+@pytest.mark.parametrize("kinds", [("d",), ("l", "d")])
+def test_ade_against_oracle(cuda_device, kinds):
+    from ceep_b200 import BatchedFDTD3D
+    nx = ny = nz = 22
+    n, T, B = 3, 70, 3
+    x, y, z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    m = (x - 11) ** 2 + (y - 10) ** 2 + (z - 12) ** 2 <= 6 ** 2
+    deb, lor = [], []
+    for k in kinds:
+        if k == "d":
+            deb.append((np.where(m, 25.0, 0.0), np.where(m, 8e-12, 0.0)))
+        else:
+            lor.append((np.where(m, 4.0, 0.0), np.where(m, 2 * np.pi * 8e9, 0.0), np.where(m, 2 * np.pi * 0.4e9, 0.0)))
+    eps, sig = np.where(m, 6.0, 1.0), np.where(m, 0.6, 0.0)
+    src = [(8, 9, 10), (14, 12, 11), (10, 15, 13)]
+    prb = src + [(11, 10, 12)]
+    o = Fdtd3DOracle(nx, ny, nz, 1e-3, T, n, src, prb, 2e9, eps_r=eps, sigma_e=sig,
+                     dispersion={"debye": deb, "lorentz": lor})
+    o.run()
+    s = BatchedFDTD3D(nx, ny, nz, 1e-3, T, n, src, prb, 2e9)
+    s._eps_r[:], s._sigma_e[:] = eps, sig
+    s.set_dispersion(debye=deb, lorentz=lor)
+    assert rel_l2(_probes(s.run(), B, len(prb)), o.probe_data) < TOL
+
+
+def test_graph_and_tx_permutation_bitwise(cuda_device):
+    from ceep_b200 import BatchedFDTD3D
+    rng = np.random.default_rng(9)
+    src = [(int(rng.integers(5, 19)), int(rng.integers(5, 17)), int(rng.integers(5, 15))) for _ in range(6)]
+    prb = src[:3]
+    res = []
+    for graph, order in ((True, range(6)), (False, range(6)), (True, [5, 3, 1, 0, 2, 4])):
+        s = BatchedFDTD3D(24, 22, 20, 1e-3, 45, 3, [src[i] for i in order], prb, 2e9, use_graph=graph)
+        s.set_material_region(8, 16, 8, 14, 6, 14, eps_r=7.0, sigma_e=0.3)
+        s.run()
+        res.append((list(order), s.probe_data.clone()))
+    assert torch.equal(res[0][1], res[1][1])
+    assert torch.equal(res[0][1][res[2][0]], res[2][1])
