@@ -2,7 +2,7 @@
 """Throughput of the batched multistatic FDTD path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload head600|disk200]
+                    [--workload head600|disk200|head192]
 
 A bench "step" is one complete head-imaging sample: the 800-step fused FDTD
 time loop for 16 transmit events with a one-pole Debye phantom, the DFT of
@@ -38,11 +38,33 @@ WORKLOADS = {
     # config 1 (the reference's CPU-runnable case): 200x200, 400 steps, 8 TX, disk
     "disk200": dict(nx=200, ny=200, dx=0.5e-3, steps=400, cpml=15, ntx=8, ring=70, nfreq=101, das=64,
                     debye=False),
+    # config 5: 192^3, 1 mm, 1000 steps, CPML 10, 8 z-directed TX/RX on a mid-plane
+    # ring, Debye ellipsoid shells with an inclusion, 101 frequencies
+    "head192": dict(dim=3, nx=192, ny=192, nz=192, dx=1e-3, steps=1000, cpml=10, ntx=8, ring=75, nfreq=101,
+                    das=64, debye=True),
 }
 PUBLISHED_GCELLS = 1.40  # README.md:60 of the reference: 600x600x16 TX x 800 steps in 3.3 s (T4)
 
 
 def algorithmic_bytes_per_step(w, n_debye):
+    if w.get("dim", 2) == 3:
+        return algorithmic_bytes_per_step_3d(w, n_debye)
+    return algorithmic_bytes_per_step_2d(w, n_debye)
+
+
+def algorithmic_bytes_per_step_3d(w, n_debye):
+    """Compulsory FP32 DRAM bytes of one 3D step: 48 B per cell-TX (six field
+    components read and written once), 16 B per cell for (da, db, ca, cb),
+    16 B per face cell-TX for its two psi, and per Debye pole 24 B per
+    interior cell-TX (three currents) plus 12 B per interior cell."""
+    nx, ny, nz, n, T = w["nx"], w["ny"], w["nz"], w["cpml"], w["ntx"]
+    cells = nx * ny * nz
+    faces = 2 * n * (ny * nz + nx * nz + nx * ny)
+    interior = (nx - 2 * n - 1) * (ny - 2 * n - 1) * (nz - 2 * n - 1)
+    return cells * (48 * T + 16) + faces * 16 * T + n_debye * interior * (24 * T + 12)
+
+
+def algorithmic_bytes_per_step_2d(w, n_debye):
     """Compulsory FP32 DRAM bytes of one fused step (read+write each state word
     once, coefficients once per cell): 24 B per cell-TX for Ez/Hx/Hy, 8 B per
     cell for (ca, cb), 16 B per strip cell-TX for the H and E psi of that
@@ -103,7 +125,28 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def build_inputs_3d(w, nsamples, device, seed0=1000):
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200.phantoms import HeadPhantom3D, ring_positions
+    c = w["nx"] // 2
+    pos = [(x, y, w["nz"] // 2) for x, y in ring_positions(w["ntx"], (c, w["ny"] // 2), w["ring"])]
+    freqs = np.linspace(0.5e9, 3.5e9, w["nfreq"])
+    solver = BatchedFDTD3D(w["nx"], w["ny"], w["nz"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
+                           frequencies=freqs, device=str(device))
+    phantoms, mats = [], []
+    for k in range(nsamples):
+        ph = HeadPhantom3D(w["nx"], w["ny"], w["nz"], w["dx"], seed=seed0 + k)
+        eps, sig = ph.get_eps_map_3d()
+        d = ph.get_dispersion()
+        mats.append(solver.material_tensors(eps, sig, d["debye"], d["lorentz"]))
+        phantoms.append(ph)
+    solver.set_phantom(phantoms[0])
+    return solver, pos, freqs, phantoms, mats
+
+
 def build_inputs(w, nsamples, device, seed0=1000):
+    if w.get("dim", 2) == 3:
+        return build_inputs_3d(w, nsamples, device, seed0)
     from ceep_b200 import BatchedFDTD2D
     from ceep_b200.phantoms import HeadPhantom2D, ring_positions
     pos = ring_positions(w["ntx"], (w["nx"] // 2, w["ny"] // 2), w["ring"])
@@ -137,8 +180,8 @@ def one_sample(solver, w, freqs, pos, das_ws, stream):
     solver.reset()
     solver.advance(0, w["steps"], stream=stream)
     S = dft(solver.probe_data, freqs, solver.dt)
-    half = 0.09
-    img = das_image(S, freqs, np.asarray(pos, float) * w["dx"], w["das"], w["das"],
+    half = 0.09 if w.get("dim", 2) == 2 else 0.07
+    img = das_image(S, freqs, np.asarray([p[:2] for p in pos], float) * w["dx"], w["das"], w["das"],
                     (w["nx"] // 2) * w["dx"] - half, (w["ny"] // 2) * w["dx"] - half, 2 * half / w["das"],
                     299_792_458.0, True, workspace=das_ws)
     return S, img
@@ -190,7 +233,7 @@ def run_ours(args, w):
         t = torch.tensor([total_ms], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    cell_steps = w["nx"] * w["ny"] * w["steps"] * w["ntx"]
+    cell_steps = w["nx"] * w["ny"] * w.get("nz", 1) * w["steps"] * w["ntx"]
     value = world * K * cell_steps / (total_ms * 1e-3) / 1e9
 
     # -- dominant kernel alone: the fused step, per-launch time over full loops
@@ -222,11 +265,11 @@ def run_ours(args, w):
 
     # -- end to end through the public API with host buffers
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and w.get("dim", 2) == 2:
         e2e = run_e2e(w, phantoms[:min(K, 3)], pos, freqs, device)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and w.get("dim", 2) == 2:
         cpu = cpu_baseline(w, sample_steps=args.cpu_steps)
 
     if world > 1:
@@ -240,16 +283,19 @@ def run_ours(args, w):
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": round(value / PUBLISHED_GCELLS, 2),
         "dtype": "f32", "data": "synthetic (seeded phantoms)",
-        "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "time_steps": w["steps"],
+        "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "nz": w.get("nz", 1),
+                   "time_steps": w["steps"],
                    "tx": w["ntx"], "cpml": w["cpml"], "debye_poles": n_debye, "dft_freqs": w["nfreq"],
                    "das": f"{w['das']}x{w['das']}", "parallelism": f"replicas{world}",
                    "l2": "flushed (256 MB write) before every sample; per-step working set > L2",
                    "sample": "fused time loop + DFT->S + DAS image"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "fdtd2d_step_kernel", "launch_ms": round(launch_ms, 5),
+                     "kernel": ("fdtd2d_step_kernel" if w.get("dim", 2) == 2 else
+                                "fdtd3d step: h + e + source/probe launches"),
+                     "launch_ms": round(launch_ms, 5),
                      "algorithmic_bytes_per_launch": bytes_step},
-        "gpu_launches": K * (w["steps"] + 3),
+        "gpu_launches": K * (w["steps"] * (1 if w.get("dim", 2) == 2 else 3) + 3),
         "clocks": clk.summary(),
     }
     if e2e:

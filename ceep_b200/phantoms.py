@@ -124,3 +124,68 @@ def ring_positions(n_ant: int, center: tuple, radius: float):
     scripts/generate_corrected_dataset.py:121-129 and arrays.py:114-124 do."""
     ang = np.linspace(0, 2 * np.pi, n_ant, endpoint=False)
     return [(int(center[0] + radius * np.cos(a)), int(center[1] + radius * np.sin(a))) for a in ang]
+
+
+@dataclass
+class HeadPhantom3D:
+    """Concentric ellipsoid shells (the 2D layer sequence, thicknesses from
+    head_models.py:541-545) with one seeded Debye pole per shell and a seeded
+    ellipsoidal inclusion of 0.8-1.5 cm; ``get_eps_map_3d`` feeds
+    ``BatchedFDTD3D.set_phantom``."""
+    nx: int = 192
+    ny: int = 192
+    nz: int = 192
+    dx: float = 1e-3
+    seed: int = 0
+    semi_axes: tuple = (0.070, 0.056, 0.060)
+    jitter: float = 0.05
+    eps_inf: tuple = (4.0, 40.0)
+    delta_eps: tuple = (10.0, 45.0)
+    tau: tuple = (5e-12, 15e-12)
+    sigma: tuple = (0.1, 2.5)
+    inclusion_radius: tuple = (0.8e-2, 1.5e-2)
+    inclusion_eps: tuple = (55.0, 65.0)
+    inclusion_sigma: tuple = (1.4, 1.8)
+
+    def __post_init__(self):
+        rng = np.random.default_rng(self.seed)
+        u = lambda r: float(rng.uniform(*r))
+        self.axes = tuple(a * (1 + rng.uniform(-self.jitter, self.jitter)) for a in self.semi_axes)
+        self.layer_params = {name: dict(eps_inf=u(self.eps_inf), delta_eps=u(self.delta_eps), tau=u(self.tau),
+                                         sigma=u(self.sigma)) for name in LAYERS}
+        r = u(self.inclusion_radius)
+        radii = (r, r * rng.uniform(0.7, 1.0), r * rng.uniform(0.7, 1.0))
+        inner = [a - sum(THICKNESS) - r for a in self.axes]
+        c = [rng.uniform(-0.6, 0.6) * max(v, 0.0) for v in inner]
+        self.inclusion = dict(center=c, radii=radii, eps=u(self.inclusion_eps), sigma=u(self.inclusion_sigma))
+        self._maps = None
+
+    def _build(self):
+        if self._maps is not None:
+            return self._maps
+        g = lambda n: (np.arange(n) - n // 2) * self.dx
+        x, y, z = np.meshgrid(g(self.nx), g(self.ny), g(self.nz), indexing="ij")
+        eps, sig = np.ones(x.shape), np.zeros(x.shape)
+        de, tau = np.zeros(x.shape), np.zeros(x.shape)
+        shrink = 0.0
+        for k, name in enumerate(LAYERS):
+            a, b, c = (v - shrink for v in self.axes)
+            m = (x / a) ** 2 + (y / b) ** 2 + (z / c) ** 2 <= 1.0
+            p = self.layer_params[name]
+            eps[m], sig[m], de[m], tau[m] = p["eps_inf"], p["sigma"], p["delta_eps"], p["tau"]
+            if k < len(THICKNESS):
+                shrink += THICKNESS[k]
+        inc = self.inclusion
+        (cx, cy, cz), (rx, ry, rz) = inc["center"], inc["radii"]
+        m = ((x - cx) / rx) ** 2 + ((y - cy) / ry) ** 2 + ((z - cz) / rz) ** 2 <= 1.0
+        eps[m], sig[m], de[m], tau[m] = inc["eps"], inc["sigma"], 0.0, 0.0
+        self._maps = (eps, sig, de, tau)
+        return self._maps
+
+    def get_eps_map_3d(self, frequency: float = 0.0):
+        eps, sig, _, _ = self._build()
+        return eps.copy(), sig.copy()
+
+    def get_dispersion(self):
+        _, _, de, tau = self._build()
+        return {"debye": [(de.copy(), tau.copy())], "lorentz": []}

@@ -240,6 +240,45 @@ class BatchedFDTD3D:
             return None if f is None else self._ref_view(f[name])
         raise AttributeError(name)
 
+    def reset(self) -> None:
+        """Zero all field, psi and ADE state (not in the reference; reuses buffers)."""
+        if not self._built:
+            return
+        for t in list(self._f.values()) + list(self._psi.values()) + [self._j, self._j_prev, self.probe_data]:
+            if t is not None:
+                t.zero_()
+
+    def material_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
+        """Device (coef, ade) tensors for the given maps, for ``load_material_tensors``."""
+        saved = (self._eps_r, self._sigma_e, self._debye, self._lorentz)
+        try:
+            self._eps_r, self._sigma_e = np.asarray(eps_r, np.float64), np.asarray(sigma_e, np.float64)
+            self._debye, self._lorentz = list(debye), list(lorentz)
+            coef, ade = self._coef_maps()
+        finally:
+            self._eps_r, self._sigma_e, self._debye, self._lorentz = saved
+        dev = self.device
+        return (torch.as_tensor(np.ascontiguousarray(coef)).to(dev),
+                torch.as_tensor(np.ascontiguousarray(ade)).to(dev) if ade.shape[0] else None)
+
+    def load_material_tensors(self, mats) -> None:
+        if not self._built:
+            self._build()
+        coef, ade = mats
+        if (ade is None) != (self._ade_coef is None):
+            raise ValueError("ADE pole count differs from the built solver")
+        self._coef.copy_(coef, non_blocking=True)
+        if ade is not None:
+            self._ade_coef.copy_(ade, non_blocking=True)
+
+    def update_materials(self) -> None:
+        if not self._built:
+            return
+        coef, ade = self._coef_maps()
+        self._coef.copy_(torch.as_tensor(coef))
+        if ade.shape[0]:
+            self._ade_coef.copy_(torch.as_tensor(ade))
+
     def compute_energy(self) -> float:
         """fdtd_3d_batched.py:987-1011 (sums in FP64 on the device)."""
         if not self._built:
