@@ -414,6 +414,13 @@ __global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const F
     mbar_init_fence();
   }
   __syncthreads();
+  // Programmatic dependent launch: let the next step's blocks be scheduled as
+  // this grid drains, and wait for the previous step's grid to finish (and
+  // its writes to be visible) before touching any field.  Every global read
+  // and write of this launch comes after the wait, which also protects the
+  // ping-pong buffer the previous step was still reading.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 
   if (threadIdx.x >= kConsumers) {
     if (threadIdx.x == kConsumers) produce<L, ND, NL>(p, st, full, empty, par, x0, y0, y1, rs, nslots, g);
@@ -470,8 +477,17 @@ template <int L, int ND, int NL>
 static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
   constexpr int CX = kConsumers / L;
   dim3 grid((p.nx + CX - 1) / CX, (p.ny + p.rows - 1) / p.rows, p.groups);
-  fdtd2d_step_kernel<L, ND, NL><<<grid, kConsumers + 32, p.smem, s>>>(p, step, par);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kConsumers + 32);
+  cfg.dynamicSmemBytes = p.smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fdtd2d_step_kernel<L, ND, NL>, p, step, par);
 }
 
 template <int ND, int NL>
