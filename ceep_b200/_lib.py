@@ -55,6 +55,13 @@ _SIGS = {
     "ceep2d_plan_reset": (C.c_int, [P]),
     "ceep2d_desc_size": (I64, []),
     "ceep2d_plan_rows": (C.c_int, [P]),
+    "ceep2d_plan_run_save": (C.c_int, [P, I64, I64, P, C.c_int, P, P, I64]),
+    "ceep2d_plan_set_current_buffer": (C.c_int, [P, C.c_int]),
+    "ceep2d_adjoint_create": (C.c_int, [P, P, C.POINTER(P)]),
+    "ceep2d_adjoint_run": (C.c_int, [P, I64, I64, P, P, I64, P]),
+    "ceep2d_adjoint_reset": (C.c_int, [P]),
+    "ceep2d_adjoint_destroy": (C.c_int, [P]),
+    "ceep2d_adjoint_desc_size": (I64, []),
     "ceep3d_plan_create": (C.c_int, [C.POINTER(Desc3D), C.POINTER(P)]),
     "ceep3d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
     "ceep3d_plan_destroy": (C.c_int, [P]),

@@ -1,0 +1,246 @@
+"""Checkpointed adjoint of the batched 2D solver and its torch.autograd.Function.
+
+The reference announces a differentiable solver but implements none
+(src/ceep/ai/__init__.py is a docstring).  Here the gradient of a loss on the
+probe series with respect to the per-cell eps_r, sigma and Debye delta_eps
+maps comes from the exact discrete adjoint of the fused forward step
+(``csrc/adjoint2d.cu``), run backwards in time:
+
+* the forward pass stores the full state every ``checkpoint_every`` steps;
+* for each segment, last first, the state is restored, the segment is
+  recomputed while the step kernel saves Ez and the Debye currents of every
+  step, and the transposed steps run back over it, accumulating d(loss)/d of
+  the per-cell update coefficients (ca, cb, k1, k2, gamma) in FP64;
+* the chain rule from those coefficients to (eps_r, sigma, delta_eps) runs in
+  torch FP64 through the same coefficient formulas as the forward
+  (src/ceep/solvers/fdtd_2d_batched.py:151-167, src/ceep/materials/dispersive.py:253-261).
+
+``checkpoint_every=1`` keeps every step (no recompute) when memory allows.
+Gradients are defined on the interior E region, where the coefficients act.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import torch
+
+from ._lib import check, lib
+from .constants import EPS_0
+from .solvers import BatchedFDTD2D, _ptr
+
+
+class _AdjDesc(C.Structure):
+    P = C.c_void_p
+    _fields_ = [("ez", P), ("hx", P * 2), ("hy", P * 2), ("psi_hx", P * 2), ("psi_hy", P * 2),
+                ("psi_ezx", P), ("psi_ezy", P), ("j", P), ("cy", P), ("cx", P), ("elin", P),
+                ("grad", P), ("probe_grad", P)]
+
+
+def coefficient_maps(eps_r, sigma, debye, dt):
+    """Differentiable (ca, cb, dt/(eps_r eps0), [(k1, k2, gamma)]) from (nx, ny) FP64 maps."""
+    eps = eps_r * EPS_0
+    poles = []
+    for de, tau in debye:
+        valid = tau > 0
+        den = 2.0 * tau + dt
+        z = torch.zeros_like(tau)
+        k1 = torch.where(valid, (2.0 * tau - dt) / den, z)
+        k2 = torch.where(valid, 2.0 * EPS_0 * de * dt / den, z)
+        g = torch.where(valid, (1.0 + k1) / 2.0, z)
+        eps = eps + k2 / 2.0
+        poles.append((k1, k2, g))
+    s = sigma * dt / (2.0 * eps)
+    return (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s), dt / (eps_r * EPS_0), poles
+
+
+class Adjoint2D:
+    """Gradient driver for one ``BatchedFDTD2D`` (Debye poles only)."""
+
+    def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50):
+        if solver._lorentz:
+            raise ValueError("the adjoint supports Debye poles only")
+        self.s = solver
+        self.K = max(1, int(checkpoint_every))
+        self._params = None
+        self._ckpt = {}
+
+    # -- parameters -------------------------------------------------------------
+    def set_parameters(self, eps_r: torch.Tensor, sigma: torch.Tensor, deps=None, tau=None) -> None:
+        """(nx, ny) maps in the reference's axis order; ``deps``/``tau`` are the
+        Debye maps of the solver's single pole when it has one."""
+        s = self.s
+        dev = s.device
+        f64 = lambda t: torch.as_tensor(t, dtype=torch.float64).to(dev)
+        eps_r, sigma = f64(eps_r), f64(sigma)
+        debye = []
+        if s._debye:
+            debye = [(f64(deps), f64(tau))]
+        self._params = (eps_r, sigma, debye)
+        if not s._built:
+            s._build()
+        ca, cb, dteps, poles = coefficient_maps(eps_r, sigma, debye, s.dt)
+        coef = torch.stack([ca, cb, dteps, torch.zeros_like(ca)], -1).transpose(0, 1)   # (ny, nx, 4)
+        s._coef.copy_(coef.to(torch.float32))
+        if poles:
+            ade = torch.stack([torch.stack([k1, k2, g, torch.zeros_like(k1)], -1).transpose(0, 1)
+                               for k1, k2, g in poles])
+            s._ade_coef.copy_(ade.to(torch.float32))
+
+    # -- forward with checkpoints ---------------------------------------------------
+    def _state(self):
+        s = self.s
+        cur = s._cur()
+        st = {"ez": s._ez[cur], "hx": s._hx[cur], "hy": s._hy[cur], "psi_hy": s._psi_hy[cur],
+              "psi_hx": s._psi_hx[cur], "psi_ezx": s._psi_ezx, "psi_ezy": s._psi_ezy}
+        if s._j is not None:
+            st["j"] = s._j
+        return st
+
+    def forward(self) -> torch.Tensor:
+        """Run all steps from a zero state, keeping checkpoints; returns the probe
+        series (ntx, nprobe, T) float32 on the device."""
+        s = self.s
+        s.reset()
+        T, K = s.total_steps, self.K
+        self._ckpt = {}
+        stream = torch.cuda.current_stream(s.device)
+        for a in range(0, T, K):
+            if K > 1 or a == 0:
+                self._ckpt[a] = {k: v.clone() for k, v in self._state().items()}
+            nst = min(K, T - a)
+            if K == 1:
+                break
+            s.advance(a, nst, stream=stream)
+        if K == 1:
+            # keep every step: one saving forward pass serves the whole adjoint
+            self._full = self._save_segment(0, T)
+        return s.probe_data[:, :len(s.probe_positions)].clone()
+
+    def _restore(self, a):
+        s = self.s
+        ck = self._ckpt[a]
+        s._ez[0].copy_(ck["ez"]); s._hx[0].copy_(ck["hx"]); s._hy[0].copy_(ck["hy"])
+        s._psi_hy[0].copy_(ck["psi_hy"]); s._psi_hx[0].copy_(ck["psi_hx"])
+        s._psi_ezx.copy_(ck["psi_ezx"]); s._psi_ezy.copy_(ck["psi_ezy"])
+        if "j" in ck:
+            s._j.copy_(ck["j"])
+        check(lib().ceep2d_plan_set_current_buffer(s._plan, 0), "ceep2d_plan_set_current_buffer")
+
+    def _save_segment(self, a, b):
+        """Restore step a, recompute [a, b) saving Ez and J of every step."""
+        s = self.s
+        self._restore(a)
+        G, W = s._groups, s._gwidth
+        slots = (s.total_steps if self.K == 1 else self.K) + 1
+        if getattr(self, "_seg", None) is None:
+            # allocated once: the recompute graphs are keyed on these addresses
+            seg_ez = torch.empty((slots, G, s.ny, s.nx, W), dtype=torch.float32, device=s.device)
+            seg_j = (torch.zeros((slots,) + tuple(s._j.shape), dtype=torch.float32, device=s.device)
+                     if s._j is not None else None)
+            self._seg = (seg_ez, seg_j)
+        seg_ez, seg_j = self._seg
+        seg_ez[0].copy_(s._ez[0])
+        if seg_j is not None:
+            seg_j[0].copy_(s._j)
+        stream = torch.cuda.current_stream(s.device)
+        check(lib().ceep2d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
+                                         seg_ez.data_ptr(), _ptr(seg_j), a), "ceep2d_plan_run_save")
+        return seg_ez, seg_j
+
+    # -- backward ------------------------------------------------------------------
+    def backward(self, grad_probes: torch.Tensor):
+        """d(loss)/d(eps_r, sigma, delta_eps) given d(loss)/d(probe series)."""
+        s = self.s
+        dev = s.device
+        T, K = s.total_steps, self.K
+        G, W = s._groups, s._gwidth
+        f32 = dict(dtype=torch.float32, device=dev)
+        z = lambda t: torch.zeros_like(t)
+        adj = {"ez": z(s._ez[0]), "hx": [z(s._hx[0]), z(s._hx[0])], "hy": [z(s._hy[0]), z(s._hy[0])],
+               "psi_hx": [z(s._psi_hx[0]), z(s._psi_hx[0])], "psi_hy": [z(s._psi_hy[0]), z(s._psi_hy[0])],
+               "psi_ezx": z(s._psi_ezx), "psi_ezy": z(s._psi_ezy),
+               "j": z(s._j) if s._j is not None else None,
+               "cy": z(s._ez[0]), "cx": z(s._ez[0]), "elin": z(s._ez[0])}
+        nd = len(s._debye)
+        grad = torch.zeros((2 + 3 * nd, s.ny, s.nx), dtype=torch.float64, device=dev)
+        gp = torch.zeros((s.batch, max(len(s.probe_positions), 1), T), **f32)
+        gp[:, :grad_probes.shape[1]] = grad_probes.to(torch.float32)
+        d = _AdjDesc()
+        d.ez = adj["ez"].data_ptr()
+        for k in range(2):
+            d.hx[k], d.hy[k] = adj["hx"][k].data_ptr(), adj["hy"][k].data_ptr()
+            d.psi_hx[k], d.psi_hy[k] = adj["psi_hx"][k].data_ptr(), adj["psi_hy"][k].data_ptr()
+        d.psi_ezx, d.psi_ezy, d.j = adj["psi_ezx"].data_ptr(), adj["psi_ezy"].data_ptr(), _ptr(adj["j"])
+        d.cy, d.cx, d.elin = adj["cy"].data_ptr(), adj["cx"].data_ptr(), adj["elin"].data_ptr()
+        d.grad, d.probe_grad = grad.data_ptr(), gp.data_ptr()
+        h = C.c_void_p()
+        check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
+        stream = torch.cuda.current_stream(dev)
+        try:
+            if K == 1:
+                seg_ez, seg_j = self._full
+                check(lib().ceep2d_adjoint_run(h, T, T, seg_ez.data_ptr(), _ptr(seg_j), 0,
+                                               C.c_void_p(stream.cuda_stream)), "ceep2d_adjoint_run")
+            else:
+                for a in sorted(self._ckpt, reverse=True):
+                    b = min(a + K, T)
+                    seg_ez, seg_j = self._save_segment(a, b)
+                    check(lib().ceep2d_adjoint_run(h, b, b - a, seg_ez.data_ptr(), _ptr(seg_j), a,
+                                                   C.c_void_p(stream.cuda_stream)), "ceep2d_adjoint_run")
+        finally:
+            lib().ceep2d_adjoint_destroy(h)
+        return self._chain(grad)
+
+    def _chain(self, grad):
+        """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""
+        eps_r, sigma, debye = self._params
+        inputs = [eps_r.detach().requires_grad_(True), sigma.detach().requires_grad_(True)]
+        deb = [(de.detach().requires_grad_(True), tau.detach()) for de, tau in debye]
+        inputs += [de for de, _ in deb]
+        with torch.enable_grad():
+            ca, cb, _, poles = coefficient_maps(inputs[0], inputs[1], deb, self.s.dt)
+            outs = [ca, cb]
+            gouts = [grad[0].t(), grad[1].t()]
+            for q, (k1, k2, g) in enumerate(poles):
+                outs += [k1, k2, g]
+                gouts += [grad[2 + 3 * q].t(), grad[3 + 3 * q].t(), grad[4 + 3 * q].t()]
+            grads = torch.autograd.grad(outs, inputs, gouts, allow_unused=True)
+        res = {"eps_r": grads[0], "sigma": grads[1]}
+        if deb:
+            res["deps"] = grads[2]
+        return res
+
+
+class FDTD2DProbes(torch.autograd.Function):
+    """probes = FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint): the probe
+    series of an ``Adjoint2D``'s solver as a differentiable function of the
+    (nx, ny) maps; ``deps``/``tau`` may be None for a non-dispersive solver."""
+
+    @staticmethod
+    def forward(ctx, eps_r, sigma, deps, tau, adjoint: Adjoint2D):
+        adjoint.set_parameters(eps_r, sigma, deps, tau)
+        ctx.adjoint = adjoint
+        ctx.has_deps = deps is not None
+        return adjoint.forward()
+
+    @staticmethod
+    def backward(ctx, grad_probes):
+        g = ctx.adjoint.backward(grad_probes.contiguous())
+        return (g["eps_r"], g["sigma"], g.get("deps") if ctx.has_deps else None, None, None)
+
+
+def probes_with_grad(eps_r, sigma, adjoint: Adjoint2D, deps=None, tau=None):
+    return FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint)
+
+
+def s_parameter_loss(probes: torch.Tensor, dt: float, frequencies, target: torch.Tensor):
+    """L = sum |S - S*|^2 over S[f, rx, tx] = sum_n probe[tx, rx, n] e^{-j w n dt} dt
+    (the running DFT of src/ceep/solvers/dft.py:55-90); returns (L, S)."""
+    import math
+    T = probes.shape[-1]
+    w = 2.0 * math.pi * torch.as_tensor(frequencies, dtype=torch.float64, device=probes.device)
+    ph = w[:, None] * (torch.arange(T, dtype=torch.float64, device=probes.device) * dt)[None, :]
+    tw = torch.complex(torch.cos(ph) * dt, -torch.sin(ph) * dt)
+    S = torch.einsum("bpt,ft->fpb", probes.to(torch.complex128), tw)
+    return (S - target).abs().pow(2).sum(), S

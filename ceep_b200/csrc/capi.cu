@@ -40,8 +40,8 @@ extern "C" const char* ceep_last_error(void) { return g_err; }
 struct ceep2d_plan {
   ceep::Fdtd2dParams p;
   int cur = 0;  // ping-pong buffer holding the current state
-  // captured step loops keyed by (step0, nsteps, starting buffer)
-  std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
+  // captured step loops keyed by (step0, nsteps, starting buffer, save buffers, save base)
+  std::map<std::tuple<int64_t, int64_t, int, const void*, const void*, int64_t>, cudaGraphExec_t> graphs;
 };
 
 extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
@@ -117,35 +117,42 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   return CEEP_OK;
 }
 
-static int run_steps(ceep2d_plan* pl, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
+static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
   for (int64_t k = 0; k < nsteps; ++k) {
-    cudaError_t e = ceep::fdtd2d_launch_step(pl->p, (int)(step0 + k), cur, s);
+    cudaError_t e = ceep::fdtd2d_launch_step(p, (int)(step0 + k), cur, s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd2d step launch");
     cur ^= 1;
   }
   return CEEP_OK;
 }
 
-extern "C" int ceep2d_plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph, float* save_ez,
+                    float* save_j, int64_t save_base) {
   if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
   if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
     return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
                 (long long)(step0 + nsteps), pl->p.nsteps);
+  if (save_ez && (save_base > step0 || (pl->p.n_debye + pl->p.n_lorentz > 0 && !save_j)))
+    return fail(CEEP_ERR_INVALID, "save buffers need save_base <= step0 and a J buffer when poles exist");
   if (nsteps == 0) return CEEP_OK;
+  ceep::Fdtd2dParams q = pl->p;
+  q.save_ez = reinterpret_cast<float4*>(save_ez);
+  q.save_j = save_ez ? reinterpret_cast<float4*>(save_j) : nullptr;
+  q.save_base = (int)save_base;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int cur = pl->cur;
   if (!use_graph || s == nullptr) {
-    int rc = run_steps(pl, step0, nsteps, cur, s);
+    int rc = run_steps(q, step0, nsteps, cur, s);
     if (rc == CEEP_OK) pl->cur = cur ^ (int)(nsteps & 1);
     return rc;
   }
-  auto key = std::make_tuple(step0, nsteps, cur);
+  auto key = std::make_tuple(step0, nsteps, cur, (const void*)save_ez, (const void*)q.save_j, save_base);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps(pl, step0, nsteps, cur, s);
+    int rc = run_steps(q, step0, nsteps, cur, s);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -158,6 +165,22 @@ extern "C" int ceep2d_plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, v
   cudaError_t e = cudaGraphLaunch(it->second, s);
   if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
   pl->cur = cur ^ (int)(nsteps & 1);
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+  return plan_run(pl, step0, nsteps, stream, use_graph, nullptr, nullptr, 0);
+}
+
+extern "C" int ceep2d_plan_run_save(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph,
+                                    float* save_ez, float* save_j, int64_t save_base) {
+  if (!save_ez) return fail(CEEP_ERR_INVALID, "ceep2d_plan_run_save: null save buffer");
+  return plan_run(pl, step0, nsteps, stream, use_graph, save_ez, save_j, save_base);
+}
+
+extern "C" int ceep2d_plan_set_current_buffer(ceep2d_plan* pl, int cur) {
+  if (!pl || (cur != 0 && cur != 1)) return fail(CEEP_ERR_INVALID, "bad plan or buffer index");
+  pl->cur = cur;
   return CEEP_OK;
 }
 
@@ -290,3 +313,82 @@ extern "C" int ceep3d_plan_destroy(ceep3d_plan* pl) {
   delete pl;
   return CEEP_OK;
 }
+
+// --------------------------------------------------------------------------
+// 2D adjoint
+// --------------------------------------------------------------------------
+#include "adjoint2d.cuh"
+
+struct ceep2d_adjoint {
+  ceep::Adjoint2dParams a;
+  int cur = 0;
+};
+
+extern "C" int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoint_desc* d, ceep2d_adjoint** out) {
+  if (!plan || !d || !out) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_create: null argument");
+  *out = nullptr;
+  if (plan->p.n_lorentz) return fail(CEEP_ERR_UNSUPPORTED, "adjoint: Lorentz poles are not supported");
+  if (!d->ez || !d->hx[0] || !d->hx[1] || !d->hy[0] || !d->hy[1] || !d->cy || !d->cx || !d->elin || !d->grad)
+    return fail(CEEP_ERR_INVALID, "adjoint: null state/scratch/gradient buffer");
+  if (plan->p.n > 0 && (!d->psi_hx[0] || !d->psi_hx[1] || !d->psi_hy[0] || !d->psi_hy[1] || !d->psi_ezx ||
+                        !d->psi_ezy))
+    return fail(CEEP_ERR_INVALID, "adjoint: null psi buffer");
+  if (plan->p.n_debye && !d->j) return fail(CEEP_ERR_INVALID, "adjoint: null current buffer");
+  if (plan->p.nprobe && !d->probe_grad) return fail(CEEP_ERR_INVALID, "adjoint: null probe gradient");
+  ceep2d_adjoint* ad = new (std::nothrow) ceep2d_adjoint();
+  if (!ad) return fail(CEEP_ERR_INVALID, "host allocation failed");
+  ceep::Adjoint2dParams& a = ad->a;
+  a.f = plan->p;
+  auto f4p = [](float* q) { return reinterpret_cast<float4*>(q); };
+  a.ez = f4p(d->ez);
+  for (int k = 0; k < 2; ++k) {
+    a.hx[k] = f4p(d->hx[k]);
+    a.hy[k] = f4p(d->hy[k]);
+    a.psi_hx[k] = f4p(d->psi_hx[k]);
+    a.psi_hy[k] = f4p(d->psi_hy[k]);
+  }
+  a.psi_ezx = f4p(d->psi_ezx);
+  a.psi_ezy = f4p(d->psi_ezy);
+  a.j = f4p(d->j);
+  a.cy = f4p(d->cy);
+  a.cx = f4p(d->cx);
+  a.elin = f4p(d->elin);
+  a.g = d->grad;
+  a.probe_grad = d->probe_grad;
+  *out = ad;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_adjoint_run(ceep2d_adjoint* ad, int64_t step_hi, int64_t nsteps, const float* seg_ez,
+                                  const float* seg_j, int64_t seg_base, void* stream) {
+  if (!ad || !seg_ez) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_run: null argument");
+  const ceep::Fdtd2dParams& f = ad->a.f;
+  if (nsteps < 0 || step_hi > f.nsteps || step_hi - nsteps < seg_base || (f.n_debye && !seg_j))
+    return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_run: steps [%lld, %lld) with segment base %lld",
+                (long long)(step_hi - nsteps), (long long)step_hi, (long long)seg_base);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t fslot = (size_t)f.groups * f.gs_field, jslot = (size_t)f.groups * f.gs_j;
+  const float4* E = reinterpret_cast<const float4*>(seg_ez);
+  const float4* J = reinterpret_cast<const float4*>(seg_j);
+  for (int64_t n = step_hi - 1; n >= step_hi - nsteps; --n) {
+    const size_t k = (size_t)(n - seg_base);
+    cudaError_t e = ceep::adjoint2d_launch_step(ad->a, (int)n, ad->cur, E + k * fslot, E + (k + 1) * fslot,
+                                                J ? J + k * jslot : nullptr, s);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "adjoint2d step launch");
+    ad->cur ^= 1;
+  }
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_adjoint_reset(ceep2d_adjoint* ad) {
+  if (!ad) return fail(CEEP_ERR_INVALID, "null adjoint");
+  ad->cur = 0;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_adjoint_destroy(ceep2d_adjoint* ad) {
+  delete ad;
+  return CEEP_OK;
+}
+
+extern "C" int64_t ceep2d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep2d_adjoint_desc); }

@@ -336,7 +336,10 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
             const float4 jq = A.j[(q * CX + cx) * L + lo];
             const size_t ja = (q * plane + (size_t)y * nx + x) * L + lo;
             if (q < ND) {
-              st4(J + ja, kq.x * jq + kq.y * dedt);
+              const float4 jnew = kq.x * jq + kq.y * dedt;
+              st4(J + ja, jnew);
+              if (p.save_j)
+                st4(p.save_j + (size_t)(step + 1 - p.save_base) * p.groups * p.gs_j + (size_t)g * p.gs_j + ja, jnew);
             } else {
               const float4 jm = A.jp[((q - ND) * CX + cx) * L + lo];
               st4(J + ja, kq.x * jq + kq.z * jm + kq.y * dedt);
@@ -382,6 +385,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
         }
       }
       st4(ezw + at, e);
+      if (p.save_ez) st4(p.save_ez + (size_t)(step + 1 - p.save_base) * p.groups * p.gs_field + gf + at, e);
       hx_prev = hxn;
     }
     release(k);

@@ -36,6 +36,11 @@ struct Fdtd2dParams {
   const float* waveform;
   float* probes;
   int* status;
+  // optional per-step save of Ez^{n+1} and J^{n+1} for the adjoint: slot
+  // (step + 1 - save_base) of arrays shaped like (slots, whole Ez) / (slots, whole J)
+  float4* save_ez;
+  float4* save_j;
+  int save_base;
 };
 
 // Set the kernel attributes and (if rows == 0) choose rows per block.

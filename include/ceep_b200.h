@@ -108,6 +108,52 @@ int ceep2d_plan_reset(ceep2d_plan* plan);
 int64_t ceep2d_desc_size(void);
 /* Rows per block the plan launches with (chosen at creation when 0). */
 int ceep2d_plan_rows(const ceep2d_plan* plan);
+/* As ceep2d_plan_run, and also store Ez^{n+1} (and J^{n+1} when the plan has
+ * Debye poles) of every step n into slot n + 1 - save_base of save_ez
+ * (slots, G, ny, nx, .) / save_j (slots, G, poles, ny, nx, .): the forward
+ * values the adjoint needs.  J entries outside the interior E region are
+ * never written (the caller zeroes the buffer once). */
+int ceep2d_plan_run_save(ceep2d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph,
+                         float* save_ez, float* save_j, int64_t save_base);
+/* Select which ping-pong buffer holds the current state (after the caller
+ * restores a checkpoint into it). */
+int ceep2d_plan_set_current_buffer(ceep2d_plan* plan, int cur);
+
+/* ------------------------------------------------------------------------
+ * Adjoint (reverse-mode) of the 2D step: no counterpart in the reference
+ * (src/ceep/ai/__init__.py only announces a differentiable solver).  It is
+ * the exact transpose of the fused step above, run backwards in time; per
+ * cell it accumulates (over transmit events and steps) the gradients of the
+ * loss with respect to ca, cb and the Debye k1, k2, gamma of each pole.
+ * Debye poles only (Lorentz: CEEP_ERR_UNSUPPORTED).
+ * ---------------------------------------------------------------------- */
+typedef struct ceep2d_adjoint_desc {
+  float* ez;               /* adjoint Ez, (G, ny, nx, .), in place           */
+  float* hx[2];            /* adjoint Hx / Hy, ping-pong                     */
+  float* hy[2];
+  float* psi_hx[2];        /* adjoint H-CPML psi, ping-pong (forward shapes) */
+  float* psi_hy[2];
+  float* psi_ezx;          /* adjoint E-CPML psi, in place                   */
+  float* psi_ezy;
+  float* j;                /* adjoint Debye currents, in place               */
+  float* cy;               /* scratch, each like Ez                          */
+  float* cx;
+  float* elin;
+  double* grad;            /* (2 + 3*n_debye, ny, nx): d/dca, d/dcb, then per
+                              pole d/dk1, d/dk2, d/dgamma; accumulated       */
+  const float* probe_grad; /* (ntx, nprobe, nsteps) dLoss/dprobe             */
+} ceep2d_adjoint_desc;
+
+typedef struct ceep2d_adjoint ceep2d_adjoint;
+int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoint_desc* desc, ceep2d_adjoint** out);
+/* Transposed steps n = step_hi-1 down to step_hi-nsteps.  Forward values come
+ * from a segment saved by ceep2d_plan_run_save: Ez^n is slot n - seg_base of
+ * seg_ez (slot 0 = the segment's starting state), J^n likewise. */
+int ceep2d_adjoint_run(ceep2d_adjoint* adj, int64_t step_hi, int64_t nsteps, const float* seg_ez,
+                       const float* seg_j, int64_t seg_base, void* stream);
+int ceep2d_adjoint_reset(ceep2d_adjoint* adj);
+int ceep2d_adjoint_destroy(ceep2d_adjoint* adj);
+int64_t ceep2d_adjoint_desc_size(void);
 
 /* ------------------------------------------------------------------------
  * 3D batched Yee FDTD.

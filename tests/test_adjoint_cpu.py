@@ -1,0 +1,69 @@
+"""Gradient oracle pins (CPU): the PyTorch restatement equals the NumPy oracle,
+and its autograd gradient equals central finite differences (h = 1e-3) of the
+FP64 oracle on 32 random interior cells for eps_r, sigma and Debye delta_eps."""
+import numpy as np
+import torch
+
+from oracle.fdtd2d import Fdtd2DOracle
+from oracle.spectral import running_dft
+from oracle.torch_fdtd2d import TorchFdtd2D, s_misfit_loss
+
+NX, NY, N, T = 36, 32, 4, 110
+SRC = [(12, 11), (23, 20)]
+PRB = [(12, 11), (23, 20), (18, 26)]
+FREQS = np.linspace(1e9, 3e9, 9)
+
+
+def _maps():
+    x, y = np.meshgrid(np.arange(NX), np.arange(NY), indexing="ij")
+    m = (x - 18) ** 2 + (y - 16) ** 2 <= 7 ** 2
+    return (np.where(m, 6.0, 1.0), np.where(m, 0.4, 0.0), np.where(m, 18.0, 0.0), np.where(m, 8e-12, 0.0), m)
+
+
+def _oracle_loss(eps, sig, de, tau, target):
+    o = Fdtd2DOracle(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9, eps_r=eps, sigma_e=sig,
+                     dispersion={"debye": [(de, tau)]})
+    o.run()
+    S = running_dft(o.probe_data, o.dt, FREQS)
+    return float(np.sum(np.abs(S - target) ** 2)), o
+
+
+def test_torch_restatement_equals_oracle():
+    eps, sig, de, tau, _ = _maps()
+    _, o = _oracle_loss(eps, sig, de, tau, 0.0)
+    t = TorchFdtd2D(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9)
+    tt = lambda a: torch.as_tensor(a, dtype=torch.float64)
+    p = t.run(tt(eps), tt(sig), [(tt(de), tt(tau))]).numpy()
+    assert np.abs(p - o.probe_data).max() <= 1e-12 * np.abs(o.probe_data).max()
+
+
+def test_autograd_matches_central_differences():
+    eps, sig, de, tau, m = _maps()
+    # target: a different inclusion
+    eps_t = eps.copy(); eps_t[15:21, 13:19] = 12.0
+    _, ot = _oracle_loss(eps_t, sig, de, tau, 0.0)
+    target = running_dft(ot.probe_data, ot.dt, FREQS)
+    t = TorchFdtd2D(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9)
+    e_ = torch.tensor(eps, dtype=torch.float64, requires_grad=True)
+    s_ = torch.tensor(sig, dtype=torch.float64, requires_grad=True)
+    d_ = torch.tensor(de, dtype=torch.float64, requires_grad=True)
+    probes = t.run(e_, s_, [(d_, torch.tensor(tau, dtype=torch.float64))])
+    loss, _ = s_misfit_loss(probes, t.dt, FREQS, torch.as_tensor(target))
+    loss.backward()
+    rng = np.random.default_rng(3)
+    cells = [tuple(c) for c in np.argwhere(m)[rng.choice(int(m.sum()), 32, replace=False)]]
+    h = 1e-3
+    for name, base, grad in (("eps_r", eps, e_.grad), ("sigma", sig, s_.grad), ("deps", de, d_.grad)):
+        fd, ad = [], []
+        for c in cells:
+            vals = []
+            for sgn in (1, -1):
+                arr = base.copy()
+                arr[c] += sgn * h
+                args = {"eps_r": (arr, sig, de), "sigma": (eps, arr, de), "deps": (eps, sig, arr)}[name]
+                vals.append(_oracle_loss(*args[:3], tau, target)[0])
+            fd.append((vals[0] - vals[1]) / (2 * h))
+            ad.append(float(grad[c]))
+        fd, ad = np.array(fd), np.array(ad)
+        err = np.linalg.norm(fd - ad) / np.linalg.norm(fd)
+        assert err < 1e-4, (name, err)

@@ -1,0 +1,106 @@
+"""The CUDA adjoint against autograd through the PyTorch FP64 restatement
+(itself pinned to central finite differences of the FP64 oracle on the CPU)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle.torch_fdtd2d import TorchFdtd2D, s_misfit_loss
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-3
+
+
+def _case(nx, ny, n, seed, debye=True):
+    rng = np.random.default_rng(seed)
+    x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    cx, cy = nx // 2, ny // 2
+    r = min(nx, ny) // 4
+    m = (x - cx) ** 2 + (y - cy) ** 2 <= r ** 2
+    eps = np.where(m, 6.0 + rng.random((nx, ny)), 1.0)
+    sig = np.where(m, 0.3 + 0.2 * rng.random((nx, ny)), 0.0)
+    de = np.where(m, 15.0 + 5 * rng.random((nx, ny)), 0.0) if debye else None
+    tau = np.where(m, 8e-12, 0.0) if debye else None
+    ang = 2 * np.pi * np.arange(4) / 4
+    ring = [(int(cx + (r + 6) * np.cos(a)), int(cy + (r + 6) * np.sin(a))) for a in ang]
+    return eps, sig, de, tau, m, ring
+
+
+def _gradients(nx, ny, n, T, seed, K, debye=True, ntx=3):
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad, s_parameter_loss
+    dev = torch.device("cuda")
+    eps, sig, de, tau, m, ring = _case(nx, ny, n, seed, debye)
+    src, prb = ring[:ntx], ring
+    freqs = np.linspace(1e9, 3e9, 11)
+    # target S from the same geometry with a changed inclusion (oracle-free: torch FP64)
+    t = TorchFdtd2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9, device=dev)
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    eps_t = eps.copy()
+    eps_t[nx // 2 - 3:nx // 2 + 3, ny // 2 - 2:ny // 2 + 4] += 4.0
+    deb_t = [(f64(de), f64(tau))] if debye else []
+    with torch.no_grad():
+        _, target = s_misfit_loss(t.run(f64(eps_t), f64(sig), deb_t), t.dt, freqs, 0.0)
+    # autograd through the FP64 restatement
+    e_, s_ = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
+    d_ = f64(de).requires_grad_(True) if debye else None
+    loss_ref, _ = s_misfit_loss(t.run(e_, s_, [(d_, f64(tau))] if debye else []), t.dt, freqs, target)
+    loss_ref.backward()
+    # CUDA forward + adjoint
+    s = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9)
+    if debye:
+        s.set_dispersion(debye=[(de, tau)])
+    adj = Adjoint2D(s, checkpoint_every=K)
+    e2, s2 = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
+    d2 = f64(de).requires_grad_(True) if debye else None
+    probes = probes_with_grad(e2, s2, adj, d2, f64(tau) if debye else None)
+    loss, _ = s_parameter_loss(probes.double(), s.dt, freqs, target)
+    loss.backward()
+    inner = np.zeros((nx, ny), bool)
+    inner[n + 1:nx - n, n + 1:ny - n] = True
+    out = {"loss": (float(loss), float(loss_ref)), "eps_r": (e2.grad, e_.grad), "sigma": (s2.grad, s_.grad)}
+    if debye:
+        out["deps"] = (d2.grad, d_.grad)
+    return out, inner
+
+
+def test_adjoint_matches_autograd(cuda_device):
+    out, inner = _gradients(96, 88, 8, 220, 1, K=25)
+    lo, lr = out["loss"]
+    assert abs(lo - lr) / lr < 1e-4
+    for k in ("eps_r", "sigma", "deps"):
+        g, gr = (v.detach().cpu().numpy() for v in out[k])
+        err = rel_l2(g[inner], gr[inner])
+        print(f"{k}: rel L2 vs autograd {err:.2e}")
+        assert err < TOL, (k, err)
+
+
+def test_adjoint_torch_check_128_300(cuda_device):
+    out, inner = _gradients(128, 128, 10, 300, 2, K=50, ntx=4)
+    for k in ("eps_r", "sigma", "deps"):
+        g, gr = (v.detach().cpu().numpy() for v in out[k])
+        assert rel_l2(g[inner], gr[inner]) < TOL, k
+
+
+def test_adjoint_without_dispersion(cuda_device):
+    out, inner = _gradients(64, 60, 6, 150, 3, K=10, debye=False)
+    for k in ("eps_r", "sigma"):
+        g, gr = (v.detach().cpu().numpy() for v in out[k])
+        assert rel_l2(g[inner], gr[inner]) < TOL, k
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(cuda_device):
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    eps, sig, de, tau, m, ring = _case(70, 66, 6, 5)
+    res = []
+    for K in (1, 7, 40):
+        s = BatchedFDTD2D(70, 66, 0.5e-3, 120, 6, ring[:3], ring, 2e9)
+        s.set_dispersion(debye=[(de, tau)])
+        adj = Adjoint2D(s, checkpoint_every=K)
+        e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+        p = probes_with_grad(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                             torch.tensor(tau, device="cuda"))
+        (p.double() ** 2).sum().backward()
+        res.append(e.grad.clone())
+    assert torch.equal(res[0], res[1]) and torch.equal(res[0], res[2])
