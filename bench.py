@@ -281,7 +281,7 @@ def run_ours(args, w):
         "metric": "batched FDTD GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(total_ms / K, 3),
         "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": round(value / PUBLISHED_GCELLS, 2),
+        "vs_baseline": round(value / PUBLISHED_GCELLS, 2) if args.workload == "head600" else None,
         "dtype": "f32", "data": "synthetic (seeded phantoms)",
         "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "nz": w.get("nz", 1),
                    "time_steps": w["steps"],
@@ -422,6 +422,77 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint_bench(args):
+    """Config 4: cost of a full S-misfit gradient (forward with checkpoints +
+    segment recompute + adjoint) relative to one plain forward, for several
+    checkpoint intervals.  400x400, 0.5 mm, 1000 steps, CPML 15, 16 TX/RX,
+    101 frequencies, one-pole Debye head phantom (scaled to the grid); target
+    S from the phantom with its disk, parameters from the phantom without it."""
+    import torch
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad, s_parameter_loss
+    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
+    dev = torch.device("cuda", 0)
+    nx = ny = 400
+    T, n = 1000, 15
+    pos = ring_positions(16, (nx // 2, ny // 2), 130)
+    freqs = np.linspace(0.5e9, 3.5e9, 101)
+    kw = dict(nx=nx, ny=ny, dx=0.5e-3, seed=7, semi_axes=(0.060, 0.047))
+    with_disk = HeadPhantom2D(p_disk=1.0, **kw)
+    no_disk = HeadPhantom2D(p_disk=0.0, **kw)
+    # the target
+    s = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, pos, pos, 2e9, frequencies=freqs, device=str(dev))
+    s.set_phantom(with_disk)
+    s.run()
+    target = torch.as_tensor(s.s_matrix(), device=dev)
+    eps, sig = no_disk.get_eps_map()
+    de, tau = no_disk.get_dispersion()["debye"][0]
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    # one plain forward (graph-replayed), the unit of cost
+    s2 = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, pos, pos, 2e9, device=str(dev))
+    s2.set_phantom(no_disk)
+    s2._build()
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def fwd():
+        s2.reset()
+        s2.advance(0, T, stream=stream)
+    t_fwd = timed(fwd, 3)
+    ratios = {}
+    for K in (1, 25, 50, 100):
+        sk = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, pos, pos, 2e9, device=str(dev))
+        sk.set_phantom(no_disk)
+        adj = Adjoint2D(sk, checkpoint_every=K)
+        e, g = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
+        d = f64(de).requires_grad_(True)
+
+        def grad_step():
+            e.grad = g.grad = d.grad = None
+            loss, _ = s_parameter_loss(probes_with_grad(e, g, adj, d, f64(tau)).double(), sk.dt, freqs, target)
+            loss.backward()
+        ratios[K] = timed(grad_step, 2) / t_fwd
+        del adj, sk
+        torch.cuda.empty_cache()
+    line = {"metric": "adjoint gradient cost vs forward", "value": round(ratios[50], 3), "unit": "x forward",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded phantom)",
+            "config": {"workload": "adjoint400", "nx": nx, "ny": ny, "time_steps": T, "tx": 16, "cpml": n,
+                       "debye_poles": 1, "dft_freqs": 101, "loss": "sum |S - S*|^2",
+                       "grad": "eps_r, sigma, debye delta_eps"},
+            "forward_ms": round(t_fwd, 3), "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args, w):
     """A few fused steps of one sample, launched without a graph, then the DFT
     and DAS once: the small command that ncu captures."""
@@ -447,7 +518,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS) + ["adjoint400"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=12)
@@ -456,6 +527,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.workload == "adjoint400":
+        run_adjoint_bench(args)
+        return
     w = WORKLOADS[args.workload]
     if args.profile:
         run_profile(args, w)

@@ -205,7 +205,11 @@ class Adjoint2D:
             for q, (k1, k2, g) in enumerate(poles):
                 outs += [k1, k2, g]
                 gouts += [grad[2 + 3 * q].t(), grad[3 + 3 * q].t(), grad[4 + 3 * q].t()]
-            grads = torch.autograd.grad(outs, inputs, gouts, allow_unused=True)
+            # k1 and gamma depend on tau only, which is held fixed
+            keep = [i for i, o in enumerate(outs) if o.requires_grad]
+            grads = torch.autograd.grad([outs[i] for i in keep], inputs, [gouts[i] for i in keep],
+                                        allow_unused=True)
+        grads = [torch.zeros_like(x) if gr is None else gr for gr, x in zip(grads, inputs)]
         res = {"eps_r": grads[0], "sigma": grads[1]}
         if deb:
             res["deps"] = grads[2]
