@@ -493,6 +493,87 @@ def run_adjoint_bench(args):
     print(json.dumps(line), flush=True)
 
 
+def _pack_solvers(count, device, seed=2024):
+    """Config-3 phantoms: nx, ny in {256..768 step 32}, steps in [600, 1200],
+    8-16 TX, one third with a two-pole Lorentz model instead of Debye."""
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.phantoms import HeadPhantom2D, LorentzHeadPhantom2D, ring_positions
+    rng = np.random.default_rng(seed)
+    sizes = np.arange(256, 769, 32)
+    out = []
+    for k in range(count):
+        nx, ny = int(rng.choice(sizes)), int(rng.choice(sizes))
+        steps, ntx = int(rng.integers(600, 1201)), int(rng.integers(8, 17))
+        scale = min(nx, ny) / 600.0
+        cls = LorentzHeadPhantom2D if k % 3 == 2 else HeadPhantom2D
+        ph = cls(nx=nx, ny=ny, dx=0.5e-3, seed=seed + k, semi_axes=(0.09 * scale, 0.07 * scale))
+        pos = ring_positions(ntx, (nx // 2, ny // 2), 0.36 * min(nx, ny))
+        s = BatchedFDTD2D(nx, ny, 0.5e-3, steps, 15, pos, pos, 2e9, device=str(device))
+        s.set_phantom(ph)
+        out.append(s)
+    return out
+
+
+def run_pack_bench(args):
+    """Config 3: aggregate GCell-steps/s of one packed, graph-replayed run of
+    all phantoms against per-phantom run() calls of the single-grid kernel."""
+    import torch
+    from ceep_b200.packed import PackedBatch2D
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    count = args.pack_count
+    # baseline: per-phantom run() on a sample (fresh solver = what a caller does)
+    sample = _pack_solvers(count, dev)[:: max(1, count // args.pack_sample)]
+    t_fresh = t_replay = cs_sample = 0.0
+    for s in sample:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run()
+        torch.cuda.synchronize()
+        t_fresh += time.perf_counter() - t0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.reset()
+        a.record(stream)
+        s.advance(0, s.total_steps, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        t_replay += a.elapsed_time(b) / 1e3
+        cs_sample += s.nx * s.ny * s.total_steps * s.batch
+    del sample
+    torch.cuda.empty_cache()
+    solvers = _pack_solvers(count, dev)
+    pk = PackedBatch2D(solvers)
+    timings = pk.autotune(candidates=(12, 16, 24, 32), probe_steps=30)
+    pk.reset()
+    pk.advance(0, pk.max_steps, stream)          # graph capture of the full run
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        pk.reset()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pk.advance(0, pk.max_steps, stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1e3)
+    for s in solvers:
+        s.check_status()
+    value = pk.cell_steps / float(np.median(times)) / 1e9
+    base_fresh = cs_sample / t_fresh / 1e9
+    base_replay = cs_sample / t_replay / 1e9
+    line = {"metric": "packed uneven batch GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
+            "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded phantoms)",
+            "config": {"workload": "pack256", "phantoms": count, "sizes": "256..768 step 32", "time_steps": "600..1200",
+                       "tx": "8..16", "lorentz_fraction": "1/3", "cpml": 15, "tile_rows": pk.rows,
+                       "cell_steps": pk.cell_steps},
+            "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
+            "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
+            "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),
+            "baseline_sample": len(range(0, count, max(1, count // args.pack_sample)))}
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args, w):
     """A few fused steps of one sample, launched without a graph, then the DFT
     and DAS once: the small command that ncu captures."""
@@ -518,7 +599,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS) + ["adjoint400"])
+    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS) + ["adjoint400", "pack256"])
+    ap.add_argument("--pack-count", type=int, default=256)
+    ap.add_argument("--pack-sample", type=int, default=32)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=12)
@@ -529,6 +612,9 @@ def main():
         args.warmup = 3
     if args.workload == "adjoint400":
         run_adjoint_bench(args)
+        return
+    if args.workload == "pack256":
+        run_pack_bench(args)
         return
     w = WORKLOADS[args.workload]
     if args.profile:

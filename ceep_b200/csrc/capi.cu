@@ -392,3 +392,197 @@ extern "C" int ceep2d_adjoint_destroy(ceep2d_adjoint* ad) {
 }
 
 extern "C" int64_t ceep2d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep2d_adjoint_desc); }
+
+// --------------------------------------------------------------------------
+// Packed multi-phantom 2D launch
+// --------------------------------------------------------------------------
+#include <algorithm>
+#include <vector>
+
+namespace {
+struct PackClass {
+  int L, nd, nl;
+  ceep::PackTile* tiles;            // device (inside the caller's workspace)
+  std::vector<int> active_by_step;  // tiles active at each step (a prefix)
+};
+size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+}  // namespace
+
+struct ceep2d_pack {
+  std::vector<ceep2d_plan*> plans;
+  ceep::Fdtd2dParams* params = nullptr;  // device
+  std::vector<PackClass> classes;
+  int max_steps = 0;
+  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+};
+
+static int pack_layout(ceep2d_plan* const* plans, int32_t count, size_t* bytes,
+                       std::vector<std::vector<std::pair<int, int>>>* cls_out,
+                       std::vector<std::tuple<int, int, int>>* keys_out) {
+  if (!plans || count < 1) return fail(CEEP_ERR_INVALID, "pack: no plans");
+  std::vector<std::tuple<int, int, int>> keys;
+  std::vector<std::vector<std::pair<int, int>>> cls;  // per class: (nsteps, plan index)
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i]) return fail(CEEP_ERR_INVALID, "pack: null plan %d", i);
+    const ceep::Fdtd2dParams& p = plans[i]->p;
+    auto key = std::make_tuple(p.L, p.n_debye, p.n_lorentz);
+    auto it = std::find(keys.begin(), keys.end(), key);
+    if (it == keys.end()) {
+      keys.push_back(key);
+      cls.emplace_back();
+      it = keys.end() - 1;
+    }
+    cls[it - keys.begin()].push_back({p.nsteps, i});
+  }
+  size_t b = align16(sizeof(ceep::Fdtd2dParams) * count);
+  for (auto& c : cls) {
+    size_t tiles = 0;
+    for (auto& e : c) {
+      const ceep::Fdtd2dParams& p = plans[e.second]->p;
+      const int cx = ceep::fdtd2d_cells_per_block(p.L);
+      tiles += (size_t)((p.nx + cx - 1) / cx) * ((p.ny + p.rows - 1) / p.rows) * p.groups;
+    }
+    b += align16(tiles * sizeof(ceep::PackTile));
+  }
+  *bytes = b;
+  if (cls_out) *cls_out = cls;
+  if (keys_out) *keys_out = keys;
+  return CEEP_OK;
+}
+
+extern "C" int64_t ceep2d_pack_workspace_bytes(ceep2d_plan* const* plans, int32_t count) {
+  size_t b = 0;
+  return pack_layout(plans, count, &b, nullptr, nullptr) == CEEP_OK ? (int64_t)b : -1;
+}
+
+extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void* workspace, int64_t bytes,
+                                  void* stream, ceep2d_pack** out) {
+  if (!out || !workspace) return fail(CEEP_ERR_INVALID, "pack: null argument");
+  *out = nullptr;
+  size_t need = 0;
+  std::vector<std::vector<std::pair<int, int>>> cls;
+  std::vector<std::tuple<int, int, int>> keys;
+  int rc = pack_layout(plans, count, &need, &cls, &keys);
+  if (rc != CEEP_OK) return rc;
+  if ((size_t)bytes < need) return fail(CEEP_ERR_INVALID, "pack: workspace %lld < %zu bytes", (long long)bytes, need);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ceep2d_pack* pk = new (std::nothrow) ceep2d_pack();
+  if (!pk) return fail(CEEP_ERR_INVALID, "host allocation failed");
+  pk->plans.assign(plans, plans + count);
+  char* ws = static_cast<char*>(workspace);
+  pk->params = reinterpret_cast<ceep::Fdtd2dParams*>(ws);
+  std::vector<ceep::Fdtd2dParams> hp(count);
+  for (int i = 0; i < count; ++i) {
+    hp[i] = plans[i]->p;
+    pk->max_steps = std::max(pk->max_steps, hp[i].nsteps);
+  }
+  // host staging vectors must outlive the asynchronous copies: synchronise below
+  std::vector<std::vector<ceep::PackTile>> host_tiles(cls.size());
+  size_t off = align16(sizeof(ceep::Fdtd2dParams) * count);
+  for (size_t c = 0; c < cls.size(); ++c) {
+    auto& v = cls[c];
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+      return a.first > b.first;  // longest runs first: the active tiles stay a prefix
+    });
+    PackClass pc;
+    pc.L = std::get<0>(keys[c]);
+    pc.nd = std::get<1>(keys[c]);
+    pc.nl = std::get<2>(keys[c]);
+    std::vector<ceep::PackTile>& tl = host_tiles[c];
+    std::vector<std::pair<int, size_t>> ends;  // (nsteps, tiles so far)
+    for (auto& e : v) {
+      const ceep::Fdtd2dParams& p = hp[e.second];
+      const int cx = ceep::fdtd2d_cells_per_block(p.L);
+      for (int g = 0; g < p.groups; ++g)
+        for (int y0 = 0; y0 < p.ny; y0 += p.rows)
+          for (int x0 = 0; x0 < p.nx; x0 += cx) tl.push_back({e.second, x0, y0, g});
+      ends.push_back({p.nsteps, tl.size()});
+    }
+    pc.active_by_step.assign(pk->max_steps, 0);
+    for (int t = 0; t < pk->max_steps; ++t) {
+      size_t a = 0;
+      for (auto& en : ends)
+        if (en.first > t) a = en.second;
+      pc.active_by_step[t] = (int)a;
+    }
+    pc.tiles = reinterpret_cast<ceep::PackTile*>(ws + off);
+    off += align16(tl.size() * sizeof(ceep::PackTile));
+    pk->classes.push_back(pc);
+  }
+  cudaError_t e = cudaMemcpyAsync(pk->params, hp.data(), sizeof(ceep::Fdtd2dParams) * count,
+                                  cudaMemcpyHostToDevice, s);
+  for (size_t c = 0; c < cls.size() && e == cudaSuccess; ++c)
+    e = cudaMemcpyAsync(pk->classes[c].tiles, host_tiles[c].data(), host_tiles[c].size() * sizeof(ceep::PackTile),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    delete pk;
+    return ceep::cuda_fail(e, "pack: table upload");
+  }
+  for (auto* pl : pk->plans) pl->cur = 0;
+  *out = pk;
+  return CEEP_OK;
+}
+
+static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream_t s) {
+  for (int64_t t = step0; t < step0 + nsteps; ++t)
+    for (auto& c : pk->classes) {
+      const int act = c.active_by_step[t];
+      if (act == 0) continue;
+      cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, act, pk->params, (int)t, s);
+      if (e != cudaSuccess) return ceep::cuda_fail(e, "packed step launch");
+    }
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+  if (!pk) return fail(CEEP_ERR_INVALID, "null pack");
+  if (step0 < 0 || nsteps < 0 || step0 + nsteps > pk->max_steps)
+    return fail(CEEP_ERR_INVALID, "pack: steps [%lld, %lld) outside [0, %d)", (long long)step0,
+                (long long)(step0 + nsteps), pk->max_steps);
+  for (auto* pl : pk->plans)
+    if ((pl->cur != (int)(std::min<int64_t>(step0, pl->p.nsteps) & 1)))
+      return fail(CEEP_ERR_INVALID, "pack: a plan's state is not at step %lld", (long long)step0);
+  if (nsteps == 0) return CEEP_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = CEEP_OK;
+  if (!use_graph || s == nullptr) {
+    rc = pack_steps(pk, step0, nsteps, s);
+  } else {
+    auto key = std::make_pair(step0, nsteps);
+    auto it = pk->graphs.find(key);
+    if (it == pk->graphs.end()) {
+      cudaGraph_t g;
+      cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
+      rc = pack_steps(pk, step0, nsteps, s);
+      e = cudaStreamEndCapture(s, &g);
+      if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphInstantiate");
+      it = pk->graphs.emplace(key, ex).first;
+    }
+    cudaError_t e = cudaGraphLaunch(it->second, s);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
+  }
+  if (rc == CEEP_OK)
+    for (auto* pl : pk->plans) pl->cur = (int)(std::min<int64_t>(step0 + nsteps, pl->p.nsteps) & 1);
+  return rc;
+}
+
+extern "C" int ceep2d_pack_tiles(const ceep2d_pack* pk, int32_t step) {
+  if (!pk || step < 0 || step >= pk->max_steps) return -1;
+  int n = 0;
+  for (auto& c : pk->classes) n += c.active_by_step[step];
+  return n;
+}
+
+extern "C" int ceep2d_pack_destroy(ceep2d_pack* pk) {
+  if (!pk) return CEEP_OK;
+  for (auto& kv : pk->graphs) cudaGraphExecDestroy(kv.second);
+  delete pk;
+  return CEEP_OK;
+}

@@ -393,19 +393,17 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   if (k < nslots) release(k);  // the Ez-only slot of row y1
 }
 
+// One block's work for one time step: a column strip of CX cells starting at
+// x0, rows [y0, y0 + rows), TX group g.  Shared by the single-grid kernel and
+// the packed multi-phantom kernel.
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
+CEEP_D void step_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
   using St = Stage2d<L, ND + NL, NL>;
   constexpr int CX = kConsumers / L;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   St* st = reinterpret_cast<St*>(smem_raw);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * sizeof(St));
   uint64_t* empty = full + kStages;
-
-  const int x0 = blockIdx.x * CX;
-  const int y0 = blockIdx.y * p.rows;
   const int y1 = min(y0 + p.rows, p.ny);
-  const int g = blockIdx.z;
   const int rs = y0 > 0 ? y0 - 1 : 0;
   const int nslots = (y1 - rs) + (y1 < p.ny ? 1 : 0);
 
@@ -421,7 +419,7 @@ __global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const F
   // Programmatic dependent launch: let the next step's blocks be scheduled as
   // this grid drains, and wait for the previous step's grid to finish (and
   // its writes to be visible) before touching any field.  Every global read
-  // and write of this launch comes after the wait, which also protects the
+  // and write of field state comes after the wait, which also protects the
   // ping-pong buffer the previous step was still reading.
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -440,6 +438,29 @@ __global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const F
     consume<L, false, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
   else
     consume<L, true, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+}
+
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int CX = kConsumers / L;
+  step_block<L, ND, NL>(p, step, par, blockIdx.x * CX, blockIdx.y * p.rows, blockIdx.z, smem_raw);
+}
+
+// Many phantoms in one launch: block b runs tile tiles[b] of phantom
+// tiles[b].phantom, whose parameters are staged into shared memory first
+// (they are constant, so this happens before the dependency wait).
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kConsumers + 32, 4)
+    fdtd2d_packed_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(16) Fdtd2dParams sp;
+  const PackTile t = tiles[blockIdx.x];
+  const int* src = reinterpret_cast<const int*>(params + t.phantom);
+  int* dst = reinterpret_cast<int*>(&sp);
+  for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  step_block<L, ND, NL>(sp, step, step & 1, t.x0, t.y0, t.g, smem_raw);
 }
 
 // ------------------------------------------------------------------------
@@ -493,6 +514,56 @@ static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, fdtd2d_step_kernel<L, ND, NL>, p, step, par);
 }
+
+template <int L, int ND, int NL>
+static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step,
+                                   cudaStream_t s) {
+  constexpr size_t smem = stage_smem_bytes<L, ND + NL, NL>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(fdtd2d_packed_kernel<L, ND, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(kConsumers + 32);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, fdtd2d_packed_kernel<L, ND, NL>, tiles, params, step);
+}
+
+template <int ND, int NL>
+static cudaError_t packed_l(int L, const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step,
+                            cudaStream_t s) {
+  switch (L) {
+    case 1: return launch_packed_l<1, ND, NL>(tiles, ntiles, params, step, s);
+    case 2: return launch_packed_l<2, ND, NL>(tiles, ntiles, params, step, s);
+    case 4: return launch_packed_l<4, ND, NL>(tiles, ntiles, params, step, s);
+    default: return launch_packed_l<8, ND, NL>(tiles, ntiles, params, step, s);
+  }
+}
+
+cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
+                                 const Fdtd2dParams* params, int step, cudaStream_t s) {
+  switch (n_debye * 3 + n_lorentz) {
+    case 0: return packed_l<0, 0>(L, tiles, ntiles, params, step, s);
+    case 1: return packed_l<0, 1>(L, tiles, ntiles, params, step, s);
+    case 2: return packed_l<0, 2>(L, tiles, ntiles, params, step, s);
+    case 3: return packed_l<1, 0>(L, tiles, ntiles, params, step, s);
+    case 4: return packed_l<1, 1>(L, tiles, ntiles, params, step, s);
+    case 6: return packed_l<2, 0>(L, tiles, ntiles, params, step, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int fdtd2d_cells_per_block(int L) { return kConsumers / L; }
 
 template <int ND, int NL>
 static cudaError_t dispatch_l(Fdtd2dParams& p, int step, int par, cudaStream_t s, bool configure) {

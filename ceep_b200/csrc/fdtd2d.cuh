@@ -43,6 +43,19 @@ struct Fdtd2dParams {
   int save_base;
 };
 
+// One tile of a packed multi-phantom launch.
+struct PackTile {
+  int phantom;  // index into the parameter array
+  int x0, y0;   // first cell column and row of the tile
+  int g;        // TX group
+};
+
+// Launch one step of every tile in `tiles` (all of one lane width L and one
+// ADE shape), each block reading its phantom's parameters from `params`.
+cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
+                                 const Fdtd2dParams* params, int step, cudaStream_t s);
+int fdtd2d_cells_per_block(int L);
+
 // Set the kernel attributes and (if rows == 0) choose rows per block.
 cudaError_t fdtd2d_configure(Fdtd2dParams& p);
 // Launch one step reading buffer `par` and writing buffer `par ^ 1`.

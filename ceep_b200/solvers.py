@@ -226,6 +226,24 @@ class BatchedFDTD2D:
                 pass
             self._plan = None
 
+    def set_rows_per_block(self, rows: int) -> None:
+        """Rebuild the launch plan with a given tile height (0 = automatic);
+        buffers and state are kept, the state restarts from zero."""
+        self.rows_per_block = int(rows)
+        if not self._built:
+            return
+        lib().ceep2d_plan_destroy(self._plan)
+        self._plan = None
+        self._desc.rows_per_block = self.rows_per_block
+        plan = C.c_void_p()
+        check(lib().ceep2d_plan_create(C.byref(self._desc), C.byref(plan)), "ceep2d_plan_create")
+        self._plan = plan
+        self.reset()
+
+    @property
+    def plan_rows(self) -> int:
+        return lib().ceep2d_plan_rows(self._plan) if self._built else 0
+
     # -- time loop ------------------------------------------------------------
     def advance(self, step0: int = 0, nsteps: Optional[int] = None, stream=None) -> None:
         """Launch steps [step0, step0+nsteps) on ``stream`` without synchronising."""

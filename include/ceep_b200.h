@@ -120,6 +120,28 @@ int ceep2d_plan_run_save(ceep2d_plan* plan, int64_t step0, int64_t nsteps, void*
 int ceep2d_plan_set_current_buffer(ceep2d_plan* plan, int cur);
 
 /* ------------------------------------------------------------------------
+ * Packed launch of many 2D plans (phantoms of uneven size, step count, TX
+ * count and ADE model).  No counterpart in the reference, which runs one
+ * BatchedFDTD2D per phantom (scripts/generate_corrected_dataset.py:139-149).
+ * Each time step is one launch per (lane width, ADE shape) class covering the
+ * tiles of every plan of that class still running; plans are ordered by
+ * decreasing step count so the running tiles form a prefix of the class's
+ * tile table.  Per-plan parameters and tile tables live in the caller's
+ * workspace (ceep2d_pack_workspace_bytes); every plan must be at step 0
+ * (freshly created or reset) when the pack is created.
+ * ---------------------------------------------------------------------- */
+typedef struct ceep2d_pack ceep2d_pack;
+int64_t ceep2d_pack_workspace_bytes(ceep2d_plan* const* plans, int32_t count);
+int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void* workspace, int64_t bytes,
+                       void* stream, ceep2d_pack** out);
+/* Steps [step0, step0 + nsteps) of the longest plan; shorter plans stop at
+ * their own step count.  use_graph != 0 captures and replays a CUDA graph. */
+int ceep2d_pack_run(ceep2d_pack* pack, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+/* Number of tiles (blocks) launched at `step`, over all classes. */
+int ceep2d_pack_tiles(const ceep2d_pack* pack, int32_t step);
+int ceep2d_pack_destroy(ceep2d_pack* pack);
+
+/* ------------------------------------------------------------------------
  * Adjoint (reverse-mode) of the 2D step: no counterpart in the reference
  * (src/ceep/ai/__init__.py only announces a differentiable solver).  It is
  * the exact transpose of the fused step above, run backwards in time; per
