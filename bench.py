@@ -230,9 +230,8 @@ def run_ours(args, w):
     ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(np.sum(ms))
     if world > 1:
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        from ceep_b200.distributed import max_time_ms
+        total_ms = max_time_ms(total_ms, device)
     cell_steps = w["nx"] * w["ny"] * w.get("nz", 1) * w["steps"] * w["ntx"]
     value = world * K * cell_steps / (total_ms * 1e-3) / 1e9
 
@@ -574,11 +573,37 @@ def run_pack_bench(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_adjoint(args):
+    """One gradient (forward with one checkpoint segment + adjoint) of a
+    400x400, 16-TX Debye case over --profile steps, launched without graphs."""
+    import torch
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
+    dev = torch.device("cuda", 0)
+    T = args.profile
+    pos = ring_positions(16, (200, 200), 130)
+    ph = HeadPhantom2D(nx=400, ny=400, dx=0.5e-3, seed=7, semi_axes=(0.060, 0.047))
+    s = BatchedFDTD2D(400, 400, 0.5e-3, T, 15, pos, pos, 2e9, device=str(dev), use_graph=False)
+    s.set_phantom(ph)
+    eps, sig = ph.get_eps_map()
+    de, tau = ph.get_dispersion()["debye"][0]
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    e = f64(eps).requires_grad_(True)
+    p = probes_with_grad(e, f64(sig), Adjoint2D(s, checkpoint_every=T), f64(de), f64(tau))
+    (p.double() ** 2).sum().backward()
+    torch.cuda.synchronize()
+    print("profile run done", flush=True)
+
+
 def run_profile(args, w):
     """A few fused steps of one sample, launched without a graph, then the DFT
-    and DAS once: the small command that ncu captures."""
+    and DAS once: the small command that ncu captures.  With --small the 3D
+    workload shrinks to 128^3 (state ~0.6 GB) for multi-pass captures."""
     import torch
     device = torch.device("cuda", 0)
+    if args.small and w.get("dim", 2) == 3:
+        w = dict(w, nx=128, ny=128, nz=128, ring=50)
     solver, pos, freqs, _, mats = build_inputs(w, 1, device)
     solver.use_graph = False
     solver.load_material_tensors(mats[0])
@@ -587,7 +612,8 @@ def run_profile(args, w):
     das_ws = torch.empty(1 << 20, dtype=torch.uint8, device=device)
     from ceep_b200.spectral import das_image, dft
     S = dft(solver.probe_data, freqs, solver.dt)
-    das_image(S, freqs, np.asarray(pos, float) * w["dx"], w["das"], w["das"], 0.06, 0.06, 0.18 / w["das"],
+    das_image(S, freqs, np.asarray([p[:2] for p in pos], float) * w["dx"], w["das"], w["das"], 0.06, 0.06,
+              0.18 / w["das"],
               299_792_458.0, True, workspace=das_ws)
     torch.cuda.synchronize()
     print("profile run done", flush=True)
@@ -602,6 +628,7 @@ def main():
     ap.add_argument("--workload", default="head600", choices=list(WORKLOADS) + ["adjoint400", "pack256"])
     ap.add_argument("--pack-count", type=int, default=256)
     ap.add_argument("--pack-sample", type=int, default=32)
+    ap.add_argument("--small", action="store_true", help="with --profile: a smaller 3D grid")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=12)
@@ -611,7 +638,10 @@ def main():
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.workload == "adjoint400":
-        run_adjoint_bench(args)
+        if args.profile:
+            run_profile_adjoint(args)
+        else:
+            run_adjoint_bench(args)
         return
     if args.workload == "pack256":
         run_pack_bench(args)
