@@ -135,7 +135,9 @@ def build_inputs_3d(w, nsamples, device, seed0=1000):
                            frequencies=freqs, device=str(device))
     phantoms, mats = [], []
     for k in range(nsamples):
-        ph = HeadPhantom3D(w["nx"], w["ny"], w["nz"], w["dx"], seed=seed0 + k)
+        sc = min(w["nx"], w["ny"], w["nz"]) / 192.0           # shells scaled to the grid
+        ph = HeadPhantom3D(w["nx"], w["ny"], w["nz"], w["dx"], seed=seed0 + k,
+                           semi_axes=(0.070 * sc, 0.056 * sc, 0.060 * sc))
         eps, sig = ph.get_eps_map_3d()
         d = ph.get_dispersion()
         mats.append(solver.material_tensors(eps, sig, d["debye"], d["lorentz"]))
