@@ -46,7 +46,18 @@
 namespace ceep {
 
 constexpr int kConsumers = 128;
-constexpr int kStages = 3;
+// Ring depth and the resident blocks per SM the registers are budgeted for.
+// The consumer holds two slots (its row and the next row's Ez), so kStages - 2
+// row slices per block are in flight while it computes.  Measured on the
+// 600x600x16 Debye step: 3 stages x 4 blocks/SM 43.2 us, 4 x 3 42.7 us,
+// 5 x 2 49.6 us, 6 x 2 52.5 us.
+#ifndef CEEP_STAGES
+#define CEEP_STAGES 4
+#endif
+#ifndef CEEP_MIN_BLOCKS
+#define CEEP_MIN_BLOCKS 3
+#endif
+constexpr int kStages = CEEP_STAGES;
 constexpr int kMaxRows = 64;                        // rows per block (row masks are 64-bit)
 constexpr uint64_t kWaitLimitNs = 1000000000ull;    // 1 s
 
@@ -441,7 +452,7 @@ CEEP_D void step_block(const Fdtd2dParams& p, int step, int par, int x0, int y0,
 }
 
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
+__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int CX = kConsumers / L;
   step_block<L, ND, NL>(p, step, par, blockIdx.x * CX, blockIdx.y * p.rows, blockIdx.z, smem_raw);
@@ -451,7 +462,7 @@ __global__ void __launch_bounds__(kConsumers + 32, 4) fdtd2d_step_kernel(const F
 // tiles[b].phantom, whose parameters are staged into shared memory first
 // (they are constant, so this happens before the dependency wait).
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kConsumers + 32, 4)
+__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
     fdtd2d_packed_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(16) Fdtd2dParams sp;
