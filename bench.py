@@ -483,6 +483,13 @@ def run_adjoint_bench(args):
             loss, _ = s_parameter_loss(probes_with_grad(e, g, adj, d, f64(tau)).double(), sk.dt, freqs, target)
             loss.backward()
         ratios[K] = timed(grad_step, 2) / t_fwd
+        if K == 1:
+            # split of one gradient: the forward that saves Ez/J of every step,
+            # and the backward (adjoint steps + chain rule)
+            adj.set_parameters(e.detach(), g.detach(), d.detach(), f64(tau))
+            gprobe = torch.randn((len(pos), len(pos), T), dtype=torch.float32, device=dev)
+            split = {"forward_save_ms": timed(adj.forward, 2),
+                     "backward_ms": timed(lambda: adj.backward(gprobe), 2)}
         del adj, sk
         torch.cuda.empty_cache()
     line = {"metric": "adjoint gradient cost vs forward", "value": round(ratios[50], 3), "unit": "x forward",
@@ -490,7 +497,8 @@ def run_adjoint_bench(args):
             "config": {"workload": "adjoint400", "nx": nx, "ny": ny, "time_steps": T, "tx": 16, "cpml": n,
                        "debye_poles": 1, "dft_freqs": 101, "loss": "sum |S - S*|^2",
                        "grad": "eps_r, sigma, debye delta_eps"},
-            "forward_ms": round(t_fwd, 3), "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()}}
+            "forward_ms": round(t_fwd, 3), "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()},
+            "every_step_kept": {k: round(v, 3) for k, v in split.items()}}
     print(json.dumps(line), flush=True)
 
 

@@ -32,9 +32,13 @@ from .solvers import BatchedFDTD2D, _ptr
 
 class _AdjDesc(C.Structure):
     P = C.c_void_p
-    _fields_ = [("ez", P), ("hx", P * 2), ("hy", P * 2), ("psi_hx", P * 2), ("psi_hy", P * 2),
-                ("psi_ezx", P), ("psi_ezy", P), ("j", P), ("cy", P), ("cx", P), ("elin", P),
-                ("grad", P), ("probe_grad", P)]
+    _fields_ = [("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hx", P * 2), ("psi_hy", P * 2),
+                ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("grad", P), ("probe_grad", P)]
+
+
+def grad_width(n_debye: int) -> int:
+    """Per-cell gradient slots of the adjoint: 2 + 3 per pole, rounded up to even."""
+    return (2 + 3 * n_debye + 1) // 2 * 2
 
 
 def coefficient_maps(eps_r, sigma, debye, dt):
@@ -62,6 +66,7 @@ class Adjoint2D:
             raise ValueError("the adjoint supports Debye poles only")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
+        self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
         self._ckpt = {}
 
@@ -156,26 +161,23 @@ class Adjoint2D:
         T, K = s.total_steps, self.K
         G, W = s._groups, s._gwidth
         f32 = dict(dtype=torch.float32, device=dev)
-        z = lambda t: torch.zeros_like(t)
-        adj = {"ez": z(s._ez[0]), "hx": [z(s._hx[0]), z(s._hx[0])], "hy": [z(s._hy[0]), z(s._hy[0])],
-               "psi_hx": [z(s._psi_hx[0]), z(s._psi_hx[0])], "psi_hy": [z(s._psi_hy[0]), z(s._psi_hy[0])],
-               "psi_ezx": z(s._psi_ezx), "psi_ezy": z(s._psi_ezy),
-               "j": z(s._j) if s._j is not None else None,
-               "cy": z(s._ez[0]), "cx": z(s._ez[0]), "elin": z(s._ez[0])}
+        pair = lambda t: [torch.zeros_like(t), torch.zeros_like(t)] if t is not None else [None, None]
+        adj = {"ez": pair(s._ez[0]), "hx": pair(s._hx[0]), "hy": pair(s._hy[0]), "psi_hx": pair(s._psi_hx[0]),
+               "psi_hy": pair(s._psi_hy[0]), "psi_ezx": pair(s._psi_ezx), "psi_ezy": pair(s._psi_ezy),
+               "j": pair(s._j)}
         nd = len(s._debye)
-        grad = torch.zeros((2 + 3 * nd, s.ny, s.nx), dtype=torch.float64, device=dev)
+        kp = grad_width(nd)
+        grad = torch.zeros((G, s.ny, s.nx, kp), dtype=torch.float64, device=dev)
         gp = torch.zeros((s.batch, max(len(s.probe_positions), 1), T), **f32)
         gp[:, :grad_probes.shape[1]] = grad_probes.to(torch.float32)
         d = _AdjDesc()
-        d.ez = adj["ez"].data_ptr()
-        for k in range(2):
-            d.hx[k], d.hy[k] = adj["hx"][k].data_ptr(), adj["hy"][k].data_ptr()
-            d.psi_hx[k], d.psi_hy[k] = adj["psi_hx"][k].data_ptr(), adj["psi_hy"][k].data_ptr()
-        d.psi_ezx, d.psi_ezy, d.j = adj["psi_ezx"].data_ptr(), adj["psi_ezy"].data_ptr(), _ptr(adj["j"])
-        d.cy, d.cx, d.elin = adj["cy"].data_ptr(), adj["cx"].data_ptr(), adj["elin"].data_ptr()
+        for name, bufs in adj.items():
+            arr = getattr(d, name)
+            arr[0], arr[1] = _ptr(bufs[0]), _ptr(bufs[1])
         d.grad, d.probe_grad = grad.data_ptr(), gp.data_ptr()
         h = C.c_void_p()
         check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
+        self.launch_rows = lib().ceep2d_adjoint_rows(h)
         stream = torch.cuda.current_stream(dev)
         try:
             if K == 1:
@@ -190,7 +192,8 @@ class Adjoint2D:
                                                    C.c_void_p(stream.cuda_stream)), "ceep2d_adjoint_run")
         finally:
             lib().ceep2d_adjoint_destroy(h)
-        return self._chain(grad)
+        # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
+        return self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])
 
     def _chain(self, grad):
         """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""

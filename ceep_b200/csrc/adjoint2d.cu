@@ -1,31 +1,50 @@
-// Exact discrete adjoint of the fused 2D step (sm_100a).
+// Exact discrete adjoint of the fused 2D step (sm_100a): one launch per step.
 //
 // The forward step (fdtd2d.cu, after fdtd_2d_batched.py:454-526) is a chain
-// of linear maps; its transpose, applied in reverse order, is split into two
-// launches per step:
+// of linear maps; the transposed step applies their transposes in reverse
+// order.  Per cell it has two halves:
 //
-//   A  E-phase adjoint (pointwise): probe gradient injection, edge zeroing,
-//      transposed E-CPML psi recurrences, transposed interior E update and
-//      Debye current recurrence.  Writes the adjoints of the two curls (cy of
-//      Hy(x)-Hy(x-1), cx of Hx(y)-Hx(y-1)) and the pointwise part of the E
-//      adjoint to scratch, and adds this step's per-cell parameter gradients:
-//        dE1/dca = E^n, dE1/dcb = (E1 - ca E^n)/cb, dJ'/dk1 = J^n,
-//        dJ'/dk2 = (E1 - E^n)/dt, dE1/dgamma = -cb J^n,
-//      where E1 is the interior update (E^{n+1} minus the source).
-//   B  H-phase adjoint (5-point gather): transposed curls, transposed H
-//      updates including the strip psi recurrences, and the gather of the
-//      E adjoint from the H differences E(x+1)-E(x), E(y+1)-E(y).
+//   E half (pointwise): probe-gradient injection, edge zeroing, transposed
+//     E-CPML psi recurrences, transposed interior E update and Debye current
+//     recurrence.  It yields the adjoints of the two curls at the cell (cy of
+//     Hy(x)-Hy(x-1), cx of Hx(y)-Hx(y-1)) and the pointwise part of the E
+//     adjoint, and adds this step's per-cell parameter gradients:
+//       dE1/dca = E^n, dE1/dcb = (E1 - ca E^n)/cb, dJ'/dk1 = J^n,
+//       dJ'/dk2 = (E1 - E^n)/dt, dE1/dgamma = -cb J^n,
+//     where E1 is the interior update (E^{n+1} minus the source).
+//   H half (5-point): transposed curls and H updates with the strip psi
+//     recurrences, and the gather of the E adjoint from the H differences
+//     E(x+1)-E(x), E(y+1)-E(y) of the cell and of its left and lower
+//     neighbours.
+//
+// Schedule (the forward kernel's): a block owns a column strip of CX cells
+// and a segment of rows; one producer thread streams each row's slices into a
+// shared-memory ring with 1D bulk copies (cp.async.bulk, no multicast); 128
+// consumer threads walk the rows upward.  At row y a thread runs the E half
+// of row y+1 and the H half of row y, so the curl adjoints never leave the
+// chip: cx(y) and the lower neighbour's contribution to the E adjoint are
+// carried in registers, cy of the left and right neighbours comes from the
+// neighbouring lanes by shuffle, and the lanes at a warp edge recompute the
+// one neighbour cy they miss from the staged row (which carries a one-cell
+// halo).  The rows just below and above the segment are recomputed (E half,
+// cx only), never exchanged; every adjoint array is ping-pong buffered so
+// those recomputes read values no other block is writing.
 //
 // Gradients are exact for the interior E region (where the update
 // coefficients act); the E-CPML scale dt/(eps_r eps0) of strip cells is not
 // differentiated (the ADE and phantom live in the interior by construction).
+// Every mbarrier wait is bounded in time; on expiry the block records
+// CEEP_ERR_TIMEOUT in the status word and returns.
 #include "../../include/ceep_b200.h"
 #include "adjoint2d.cuh"
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ceep {
 
-constexpr int kAdjThreads = 256;
+constexpr int kAdjConsumers = 128;
+constexpr int kAdjMaxRows = 62;                  // rows + the two neighbour rows fit a 64-bit row mask
+constexpr uint64_t kAdjWaitNs = 1000000000ull;   // 1 s
 
 template <int L>
 CEEP_D float lane_sum(float v) {
@@ -34,282 +53,586 @@ CEEP_D float lane_sum(float v) {
   return v;
 }
 CEEP_D float dot4(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
-
-// ---------------------------------------------------------------------------
-template <int L, int ND>
-__global__ void __launch_bounds__(kAdjThreads) adjoint2d_e_kernel(const Adjoint2dParams a, int step,
-                                                                  const float4* __restrict__ ez_n,
-                                                                  const float4* __restrict__ ez_np1,
-                                                                  const float4* __restrict__ j_n) {
-  const Fdtd2dParams& p = a.f;
-  const int nx = p.nx, ny = p.ny, n = p.n;
-  const long long total = (long long)p.groups * ny * nx * L;
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  // Threads past the end still take part in the lane reductions (whole warps).
-  const bool valid = id < total;
-  const long long idc = valid ? id : total - 1;
-  const int lo = (int)(idc % L);
-  const long long cell_g = idc / L;
-  const int x = (int)(cell_g % nx);
-  const int y = (int)((cell_g / nx) % ny);
-  const int g = (int)(cell_g / ((long long)nx * ny));
-  const size_t cell = (size_t)y * nx + x;
-  const size_t plane = (size_t)nx * ny;
-  const int lane_g = g * L + lo;
-  const float4 cf = __ldg(reinterpret_cast<const float4*>(p.coef) + cell);  // ca, cb, dt/eps
-  const float inv = p.inv_dx;
-
-  float4 E = a.ez[idc];
-  // probe gradient injection: p_n = E after step n at the probe cells
-  if (__ldg(p.row_flags + y) & 2) {
-    for (int q = 0; q < p.nprobe; ++q)
-      if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int tx = 4 * lane_g + c;
-          if (tx < p.ntx) add_comp(E, c, __ldg(a.probe_grad + ((size_t)tx * p.nprobe + q) * p.nsteps + step));
-        }
-      }
-  }
-  if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1) E = f4(0.f);
-
-  float4 cyv = f4(0.f), cxv = f4(0.f), elin = E;
-  const size_t gy = (size_t)g * p.gs_psi_y, gx = (size_t)g * p.gs_psi_x;
-  if (n > 0) {
-    // transposed E-CPML, y strips: PEY' = b PEY + c inv cX ; E3 = E2 - dteps PEY'
-    int sy = -1, ci = 0;
-    if (x >= 1) {
-      if (y >= 1 && y <= n) { sy = y - 1; ci = y - 1; }
-      else if (y >= ny - n) { sy = n + (y - (ny - n)); ci = ny - 1 - y; }
-    }
-    if (sy >= 0) {
-      float4* pp = a.psi_ezy + gy + ((size_t)sy * nx + x) * L + lo;
-      const float4 tot = *pp - cf.z * E;
-      if (valid) *pp = p.cpml_b[ci] * tot;
-      cxv = (p.cpml_c[ci] * inv) * tot;
-    }
-    // transposed E-CPML, x strips: PEX' = b PEX + c inv cY ; E2 = E1 + dteps PEX'
-    int sx = -1;
-    if (y >= 1) {
-      if (x >= 1 && x <= n) { sx = x - 1; ci = x - 1; }
-      else if (x >= nx - n) { sx = n + (x - (nx - n)); ci = nx - 1 - x; }
-    }
-    if (sx >= 0) {
-      float4* pp = a.psi_ezx + gx + ((size_t)y * 2 * n + sx) * L + lo;
-      const float4 tot = *pp + cf.z * E;
-      if (valid) *pp = p.cpml_b[ci] * tot;
-      cyv = (p.cpml_c[ci] * inv) * tot;
-    }
-  }
-  const bool f9 = x >= n + 1 && x < nx - n && y >= n + 1 && y < ny - n;
-  const bool atomic = p.groups > 1;
-  const size_t gstride = plane;
-  float gv[2 + 3 * ND];
-#pragma unroll
-  for (int k = 0; k < 2 + 3 * ND; ++k) gv[k] = 0.f;
-  if (f9) {
-    // E1 = ca E + cb inv (cY - cX) - cb sum(gamma J);  J' = k1 J + k2 (E1 - E)/dt
-    float4 e1 = ez_np1[idc];
-    if (__ldg(p.row_flags + y) & 1) {  // the forward added the source after E1
-      const float w = __ldg(p.waveform + step);
-      for (int s = 0; s < p.ntx; ++s)
-        if ((s >> 2) == lane_g && __ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y)
-          add_comp(e1, s & 3, -w);
-    }
-    const float4 en = ez_n[idc];
-    float4 e1tot = E;
-    float4 jin[ND > 0 ? ND : 1], jn[ND > 0 ? ND : 1];
-    float4 kq[ND > 0 ? ND : 1];
-#pragma unroll
-    for (int q = 0; q < ND; ++q) {
-      kq[q] = __ldg(reinterpret_cast<const float4*>(p.ade_coef) + q * plane + cell);
-      const size_t ja = (size_t)g * p.gs_j + (q * plane + cell) * L + lo;
-      jin[q] = a.j[ja];
-      jn[q] = j_n[ja];
-      e1tot = fma4(kq[q].y * p.inv_dt, jin[q], e1tot);
-    }
-    elin = cf.x * e1tot;
-#pragma unroll
-    for (int q = 0; q < ND; ++q) {
-      elin = fma4(-kq[q].y * p.inv_dt, jin[q], elin);
-      const size_t ja = (size_t)g * p.gs_j + (q * plane + cell) * L + lo;
-      if (valid) a.j[ja] = kq[q].x * jin[q] - (cf.y * kq[q].z) * e1tot;
-    }
-    cyv = (cf.y * inv) * e1tot;
-    cxv = (-cf.y * inv) * e1tot;
-    // parameter gradients of this step (this thread's four transmit events)
-    gv[0] = dot4(e1tot, en);
-    gv[1] = dot4(e1tot, (e1 - cf.x * en)) / cf.y;
-#pragma unroll
-    for (int q = 0; q < ND; ++q) {
-      gv[2 + 3 * q] = dot4(jin[q], jn[q]);
-      gv[3 + 3 * q] = dot4(jin[q], (e1 - en) * f4(p.inv_dt));
-      gv[4 + 3 * q] = -cf.y * dot4(e1tot, jn[q]);
-    }
-  }
-  // Sum over the L threads of the cell (warp-uniform: every lane of the warp
-  // runs the shuffles); the first thread of the cell adds to the accumulator.
-#pragma unroll
-  for (int k = 0; k < 2 + 3 * ND; ++k) {
-    const float v = lane_sum<L>(valid ? gv[k] : 0.f);
-    if (valid && f9 && lo == 0) {
-      double* dst = a.g + (size_t)k * gstride + cell;
-      if (atomic)
-        atomicAdd(dst, (double)v);
-      else
-        *dst += (double)v;
-    }
-  }
-  if (valid) {
-    a.cy[idc] = cyv;
-    a.cx[idc] = cxv;
-    a.elin[idc] = elin;
-  }
+CEEP_D float4 shfl_up4(float4 v, int d) {
+  return make_float4(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d),
+                     __shfl_up_sync(0xffffffffu, v.z, d), __shfl_up_sync(0xffffffffu, v.w, d));
+}
+CEEP_D float4 shfl_down4(float4 v, int d) {
+  return make_float4(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d),
+                     __shfl_down_sync(0xffffffffu, v.z, d), __shfl_down_sync(0xffffffffu, v.w, d));
 }
 
-// ---------------------------------------------------------------------------
-// H-phase adjoint.  u_y(c) = A_y Y'* + kappa_x PHY'*, u_x(c) = -A_x X'* + kappa_y PHX'*
-// are the adjoints of E(c+x)-E(c) and E(c+y)-E(c).
-// ---------------------------------------------------------------------------
-struct HAdjoint {
-  float4 tot;   // adjoint of H' (total)
-  float4 psi;   // adjoint of the old psi (written back)
-  float4 u;     // adjoint of the forward difference
-  bool strip;
+// One slot of the ring: the slices of one row.  Halo'd slices hold cells
+// x0-1 .. x0+CX, left-halo'd ones x0-1 .. x0+CX-1, the rest x0 .. x0+CX-1.
+// The CPML psi slices are not staged: only strip cells read them, straight
+// from the read half of their ping-pong pair, which keeps a stage small
+// enough for three blocks per SM.
+template <int L, int ND>
+struct AdjStage {
+  static constexpr int CX = kAdjConsumers / L;
+  static constexpr int H = CX + 2;
+  static constexpr int NQ = ND > 0 ? ND : 1;
+  float4 le[H * L];          // adjoint Ez (halo'd)
+  float4 lj[NQ * H * L];     // adjoint Debye currents (halo'd)
+  float4 coef[H];            // ca, cb, dt/(eps_r eps0), 0 (halo'd)
+  float4 ade[NQ * H];        // k1, k2, gamma, 0 (halo'd)
+  float4 en[CX * L];         // forward Ez^n
+  float4 e1[CX * L];         // forward Ez^{n+1}
+  float4 jn[NQ * CX * L];    // forward J^n
+  float4 lhx[CX * L];        // adjoint Hx
+  float4 lhy[(CX + 1) * L];  // adjoint Hy (left-halo'd)
 };
 
-CEEP_D HAdjoint hy_adjoint(const Fdtd2dParams& p, int x, int y, float4 yin, float4 cy_c, float4 cy_r,
-                           float4 psi_in) {
-  HAdjoint r;
-  r.tot = yin + cy_c - cy_r;
-  const int n = p.n;
-  const float A = (x >= n && x < p.nx - 1 && y >= n && y < p.ny - n) ? p.db_dx : 0.f;
-  int ci = -1;
-  if (x < n) ci = x;
-  else if (x >= p.nx - n && x < p.nx - 1) ci = p.nx - 1 - x;
-  r.strip = ci >= 0;
+// Four stages where three blocks of them fit an SM, else three.
+template <int L, int ND>
+__host__ __device__ constexpr int adj_stages() {
+  return 4 * sizeof(AdjStage<L, ND>) <= 74 * 1024 ? 4 : 3;
+}
+template <int L, int ND>
+__host__ __device__ constexpr size_t adj_smem_bytes() {
+  return adj_stages<L, ND>() * sizeof(AdjStage<L, ND>) + 2 * adj_stages<L, ND>() * sizeof(uint64_t);
+}
+
+CEEP_D void adj_status(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// Region predicates of the forward step (fdtd2d.cu) for one cell.
+struct AdjRegions {
+  int n, nx, ny;
+  CEEP_D bool f9(int x, int y) const { return x >= n + 1 && x < nx - n && y >= n + 1 && y < ny - n; }
+  CEEP_D bool edge(int x, int y) const { return x == 0 || x == nx - 1 || y == 0 || y == ny - 1; }
+  // E-CPML y strips (rows 1..n, ny-n..ny-1): strip row or -1, profile index
+  CEEP_D int ey_row(int y) const {
+    return (y >= 1 && y <= n) ? y - 1 : (n > 0 && y >= ny - n) ? n + (y - (ny - n)) : -1;
+  }
+  CEEP_D int ey_ci(int y) const { return y <= n ? y - 1 : ny - 1 - y; }
+  // E-CPML x strips (columns 1..n, nx-n..nx-1)
+  CEEP_D int ex_col(int x) const {
+    return (x >= 1 && x <= n) ? x - 1 : (n > 0 && x >= nx - n) ? n + (x - (nx - n)) : -1;
+  }
+  CEEP_D int ex_ci(int x) const { return x <= n ? x - 1 : nx - 1 - x; }
+  // H-CPML y strips of Hx (rows y < n, ny-n <= y < ny-1)
+  CEEP_D int hy_row(int y) const { return y < n ? y : (y >= ny - n && y < ny - 1) ? n + (y - (ny - n)) : -1; }
+  // H-CPML x strips of Hy (columns x < n, nx-n <= x < nx-1)
+  CEEP_D int hx_col(int x) const { return x < n ? x : (x >= nx - n && x < nx - 1) ? n + (x - (nx - n)) : -1; }
+};
+
+// Transposed H update of one cell.  tot = adjoint of H' in total, u = adjoint
+// of the forward difference the update reads, psi = adjoint of the old psi
+// (strip cells, s >= 0 = strip index).
+struct HAdj {
+  float4 tot, psi, u;
+  int s;
+};
+
+// Hy' = Hy + A (E(x+1) - E(x)) [+ db psi'],  psi' = b psi + c/dx (E(x+1) - E(x))
+// `psi_src` is this TX group's read half of the psi array, `lo` the lane.
+template <bool GEN>
+CEEP_D HAdj hy_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, float4 lhy, float4 cy_c, float4 cy_r,
+                   const float4* psi_src, int lo) {
+  HAdj r;
+  r.tot = lhy + cy_c - cy_r;
+  r.s = -1;
+  if (!GEN) {
+    r.u = p.db_dx * r.tot;
+    return r;
+  }
+  const float A = (x >= p.n && x < p.nx - 1 && y >= p.n && y < p.ny - p.n) ? p.db_dx : 0.f;
   r.u = A * r.tot;
-  r.psi = psi_in;
-  if (r.strip) {
-    const float4 pt = fma4(p.db, r.tot, psi_in);
+  r.s = rg.hx_col(x);
+  if (r.s >= 0) {
+    const int ci = x < p.n ? x : p.nx - 1 - x;
+    const float4 psi = __ldg(psi_src + ((size_t)y * 2 * p.n + r.s) * (p.L) + lo);
+    const float4 pt = fma4(p.db, r.tot, psi);
     r.psi = p.cpml_b[ci] * pt;
     r.u = fma4(p.cpml_c[ci] * p.inv_dx, pt, r.u);
   }
   return r;
 }
 
-CEEP_D HAdjoint hx_adjoint(const Fdtd2dParams& p, int x, int y, float4 xin, float4 cx_c, float4 cx_u,
-                           float4 psi_in) {
-  HAdjoint r;
-  r.tot = xin + cx_c - cx_u;
-  const int n = p.n;
-  const float A = (x >= n && x < p.nx - n && y >= n && y < p.ny - 1) ? p.db_dx : 0.f;
-  int ci = -1;
-  if (y < n) ci = y;
-  else if (y >= p.ny - n && y < p.ny - 1) ci = p.ny - 1 - y;
-  r.strip = ci >= 0;
-  r.u = -A * r.tot;
-  r.psi = psi_in;
-  if (r.strip) {
-    const float4 pt = fma4(-p.db, r.tot, psi_in);
+// Hx' = Hx - A (E(y+1) - E(y)) [- db psi'],  psi' = b psi + c/dx (E(y+1) - E(y))
+template <bool GEN>
+CEEP_D HAdj hx_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, float4 lhx, float4 cx_c, float4 cx_u,
+                   const float4* psi_src, int lo) {
+  HAdj r;
+  r.tot = lhx + cx_c - cx_u;
+  r.s = -1;
+  if (!GEN) {
+    r.u = (-p.db_dx) * r.tot;
+    return r;
+  }
+  const float A = (x >= p.n && x < p.nx - p.n && y >= p.n && y < p.ny - 1) ? p.db_dx : 0.f;
+  r.u = (-A) * r.tot;
+  r.s = rg.hy_row(y);
+  if (r.s >= 0) {
+    const int ci = y < p.n ? y : p.ny - 1 - y;
+    const float4 psi = __ldg(psi_src + ((size_t)r.s * p.nx + x) * (p.L) + lo);
+    const float4 pt = fma4(-p.db, r.tot, psi);
     r.psi = p.cpml_b[ci] * pt;
     r.u = fma4(p.cpml_c[ci] * p.inv_dx, pt, r.u);
   }
   return r;
 }
 
-template <int L>
-__global__ void __launch_bounds__(kAdjThreads) adjoint2d_h_kernel(const Adjoint2dParams a, int par) {
+// p_n = Ez after step n at the probe cells: its adjoint enters here.
+CEEP_D void inject_probes(const Adjoint2dParams& a, float4& E, int x, int y, int lane_g, int step) {
+  const Fdtd2dParams& p = a.f;
+  for (int q = 0; q < p.nprobe; ++q)
+    if (__ldg(p.prb_xy + 2 * q) == x && __ldg(p.prb_xy + 2 * q + 1) == y) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int tx = 4 * lane_g + c;
+        if (tx < p.ntx) add_comp(E, c, __ldg(a.probe_grad + ((size_t)tx * p.nprobe + q) * p.nsteps + step));
+      }
+    }
+}
+
+// ------------------------------------------------------------------------
+// Producer: one thread, bulk copies of row slices into the stage ring.
+// Every row: adjoint Ez and J, coefficients (halo'd).  Rows of the segment
+// and the one below it: adjoint Hx.  Rows of the segment: forward Ez^n,
+// Ez^{n+1}, J^n and adjoint Hy.
+// ------------------------------------------------------------------------
+template <int L, int ND>
+CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty, int par,
+                        const float4* ez_n, const float4* ez_np1, const float4* j_n, int x0, int y0, int y1, int rs,
+                        int nslots, int g) {
+  using St = AdjStage<L, ND>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
+  const Fdtd2dParams& p = a.f;
+  const int nx = p.nx;
+  const size_t gf = (size_t)g * p.gs_field, gj = (size_t)g * p.gs_j;
+  const size_t plane = (size_t)nx * p.ny;
+  const float4* coef = reinterpret_cast<const float4*>(p.coef);
+  const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
+  const int xa = x0 > 0 ? x0 - 1 : 0;                  // first halo'd cell
+  const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;  // end of the halo'd cells
+  const int xe = x0 + CX < nx ? x0 + CX : nx;          // end of the owned cells
+  const int ha = xa - (x0 - 1);                         // slot index of cell xa
+  const uint32_t cb = L * 16;
+  int issued = 0;
+  for (int k = 0; k < nslots; ++k) {
+    const int s = k % NS, u = k / NS;
+    if (u > 0 && !mbar_wait_bounded(&empty[s], (u - 1) & 1, kAdjWaitNs)) {
+      adj_status(p.status, CEEP_ERR_TIMEOUT);
+      break;
+    }
+    const int r = rs + k;
+    const bool tail = r >= y1, body = r >= y0 && !tail;
+    St& S = st[s];
+    const size_t rowc = (size_t)r * nx;
+    for (int pass = 0; pass < 2; ++pass) {
+      uint32_t bytes = 0;
+      auto cp = [&](void* dst, const void* src, uint32_t nb) {
+        if (nb == 0) return;
+        if (pass) bulk_g2s(dst, src, nb, &full[s]);
+        else bytes += nb;
+      };
+      cp(S.le + ha * L, a.ez[par] + gf + (rowc + xa) * L, (xb - xa) * cb);
+      cp(S.coef + ha, coef + rowc + xa, (xb - xa) * 16u);
+#pragma unroll
+      for (int q = 0; q < ND; ++q) {
+        cp(S.ade + q * H + ha, ade + q * plane + rowc + xa, (xb - xa) * 16u);
+        cp(S.lj + (q * H + ha) * L, a.j[par] + gj + (q * plane + rowc + xa) * L, (xb - xa) * cb);
+      }
+      if (!tail) cp(S.lhx, a.hx[par] + gf + (rowc + x0) * L, (xe - x0) * cb);
+      if (body) {
+        cp(S.en, ez_n + gf + (rowc + x0) * L, (xe - x0) * cb);
+        cp(S.e1, ez_np1 + gf + (rowc + x0) * L, (xe - x0) * cb);
+#pragma unroll
+        for (int q = 0; q < ND; ++q) cp(S.jn + q * CX * L, j_n + gj + (q * plane + rowc + x0) * L, (xe - x0) * cb);
+        cp(S.lhy + ha * L, a.hy[par] + gf + (rowc + xa) * L, (xe - xa) * cb);
+      }
+      if (!pass) mbar_arrive_expect_tx(&full[s], bytes);
+    }
+    issued = k + 1;
+  }
+  // Let every copy this thread issued land before it leaves.
+  for (int k = issued > NS ? issued - NS : 0; k < issued; ++k)
+    mbar_wait_bounded(&full[k % NS], (k / NS) & 1, kAdjWaitNs);
+}
+
+// E-half results of one cell carried between rows.
+struct AdjE {
+  float4 cx, cy;  // adjoints of the two curls at the cell
+  float4 cye;     // warp-edge lanes: cy of the neighbour across the warp edge
+  float4 elin;    // pointwise part of the E adjoint
+};
+
+// ------------------------------------------------------------------------
+// Consumer: one float4 (4 TX) of one cell per thread, walking the rows.
+// GEN = false for blocks whose cells, halo cells and neighbour rows all lie
+// in the plain interior of every region.
+// ------------------------------------------------------------------------
+template <int L, int ND, bool GEN>
+CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty, int step,
+                        int par, int x0, int y0, int y1, int rs, int nslots, int g) {
+  using St = AdjStage<L, ND>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
+  constexpr int KG = 2 + 3 * ND, KP = adjoint2d_grad_width(ND);
   const Fdtd2dParams& p = a.f;
   const int nx = p.nx, ny = p.ny, n = p.n;
-  const long long total = (long long)p.groups * ny * nx * L;
-  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= total) return;
-  const int lo = (int)(id % L);
-  const long long cell_g = id / L;
-  const int x = (int)(cell_g % nx);
-  const int y = (int)((cell_g / nx) % ny);
-  const int g = (int)(cell_g / ((long long)nx * ny));
-  const size_t sxs = L, sys = (size_t)nx * L;
-  const size_t gx = (size_t)g * p.gs_psi_x, gy = (size_t)g * p.gs_psi_y;
-  const float4* yin = a.hy[par];
-  const float4* xin = a.hx[par];
-  const float4 zero = f4(0.f);
-  auto psi_y_at = [&](int xx, int yy) -> size_t {  // x-strip psi slot of cell (xx, yy), or ~0
-    if (n == 0) return ~(size_t)0;
-    if (xx < n) return gx + ((size_t)yy * 2 * n + xx) * L + lo;
-    if (xx >= nx - n && xx < nx - 1) return gx + ((size_t)yy * 2 * n + n + (xx - (nx - n))) * L + lo;
-    return ~(size_t)0;
+  const AdjRegions rg{n, nx, ny};
+  const int cx = threadIdx.x / L, lo = threadIdx.x % L;
+  const int x = x0 + cx;
+  const bool active = x < nx;
+  const int lw = threadIdx.x & 31;
+  const int lane_g = g * L + lo;
+  const float inv = p.inv_dx;
+  const size_t plane = (size_t)nx * ny, gf = (size_t)g * p.gs_field;
+  const int me = cx * L + lo;        // this cell in the plain slices
+  const int mh = (cx + 1) * L + lo;  // this cell in the halo'd slices
+  // read and write halves of the psi pairs, at this TX group
+  const float4* pex_r = a.psi_ezx[par] + (size_t)g * p.gs_psi_x;
+  const float4* pey_r = a.psi_ezy[par] + (size_t)g * p.gs_psi_y;
+  const float4* phy_r = a.psi_hy[par] + (size_t)g * p.gs_psi_x;
+  const float4* phx_r = a.psi_hx[par] + (size_t)g * p.gs_psi_y;
+
+  // Probe cells of this column and of the neighbour column an edge lane
+  // recomputes, and this lane's source cells, among rows rs .. rs + nslots - 1
+  // (<= 64) as bit masks; found once, before the first wait.
+  const int xn = lw < L ? x - 1 : (lw >= 32 - L ? x + 1 : x);
+  uint64_t prb_own = 0, prb_nb = 0, src_own = 0;
+  for (int q = 0; q < p.nprobe; ++q) {
+    const int px = __ldg(p.prb_xy + 2 * q), py = __ldg(p.prb_xy + 2 * q + 1) - rs;
+    if (py >= 0 && py < nslots) {
+      if (px == x) prb_own |= 1ull << py;
+      if (px == xn) prb_nb |= 1ull << py;
+    }
+  }
+  for (int s = 4 * lane_g; s < 4 * lane_g + 4 && s < p.ntx; ++s) {
+    const int sx = __ldg(p.src_xy + 2 * s), sy = __ldg(p.src_xy + 2 * s + 1) - rs;
+    if (sx == x && sy >= 0 && sy < nslots) src_own |= 1ull << sy;
+  }
+
+  auto wait = [&](int k) {
+    const bool ok = mbar_wait_bounded(&full[k % NS], (k / NS) & 1, kAdjWaitNs);
+    if (__any_sync(0xffffffffu, !ok)) {
+      if (lw == 0) adj_status(p.status, CEEP_ERR_TIMEOUT);
+      return false;
+    }
+    return true;
   };
-  auto psi_x_at = [&](int xx, int yy) -> size_t {  // y-strip psi slot, or ~0
-    if (n == 0) return ~(size_t)0;
-    if (yy < n) return gy + ((size_t)yy * nx + xx) * L + lo;
-    if (yy >= ny - n && yy < ny - 1) return gy + ((size_t)(n + (yy - (ny - n))) * nx + xx) * L + lo;
-    return ~(size_t)0;
+  auto release = [&](int k) {
+    __syncwarp();
+    if (lw == 0) mbar_arrive(&empty[k % NS]);
+  };
+  // adjoint Ez of halo'd cell i (cell xc) of row r after probe injection and edge zeroing
+  auto e_adj = [&](const St& S, int i, int xc, int r) {
+    float4 E = S.le[i * L + lo];
+    if (((xc == x ? prb_own : prb_nb) >> (r - rs)) & 1) inject_probes(a, E, xc, r, lane_g, step);
+    if (GEN && rg.edge(xc, r)) E = f4(0.f);
+    return E;
+  };
+  // sum over poles of (k2/dt) * adjoint J at halo'd cell i
+  auto jsum = [&](const St& S, int i) {
+    float4 s = f4(0.f);
+#pragma unroll
+    for (int q = 0; q < ND; ++q) s = fma4(S.ade[q * H + i].y * p.inv_dt, S.lj[(q * H + i) * L + lo], s);
+    return s;
+  };
+  // cy of halo'd cell i (cell xc) of row r
+  auto cy_at = [&](const St& S, int i, int xc, int r) {
+    const float4 E = e_adj(S, i, xc, r);
+    const float4 cf = S.coef[i];
+    if (!GEN || rg.f9(xc, r)) return (cf.y * inv) * (E + jsum(S, i));
+    if (n > 0 && r >= 1) {
+      const int sx = rg.ex_col(xc);
+      if (sx >= 0)
+        return (p.cpml_c[rg.ex_ci(xc)] * inv) * fma4(cf.z, E, __ldg(pex_r + ((size_t)r * 2 * n + sx) * L + lo));
+    }
+    return f4(0.f);
+  };
+  // cx of this cell in a neighbour row (r = y0 - 1 or y1)
+  auto cx_row = [&](const St& S, int r) {
+    if (!active) return f4(0.f);
+    const float4 E = e_adj(S, cx + 1, x, r);
+    const float4 cf = S.coef[cx + 1];
+    if (!GEN || rg.f9(x, r)) return (-cf.y * inv) * (E + jsum(S, cx + 1));
+    if (n > 0 && x >= 1) {
+      const int sy = rg.ey_row(r);
+      if (sy >= 0)
+        return (p.cpml_c[rg.ey_ci(r)] * inv) * fma4(-cf.z, E, __ldg(pey_r + ((size_t)sy * nx + x) * L + lo));
+    }
+    return f4(0.f);
+  };
+  // E half of this cell in row r of the segment: writes the new adjoint J and
+  // E psi, adds the gradients; every lane of the warp must call it.
+  auto e_half = [&](const St& S, int r) {
+    AdjE o{f4(0.f), f4(0.f), f4(0.f), f4(0.f)};
+    float gv[KG];
+#pragma unroll
+    for (int k = 0; k < KG; ++k) gv[k] = 0.f;
+    const bool f9 = active && (!GEN || rg.f9(x, r));
+    if (active) {
+      const float4 E = e_adj(S, cx + 1, x, r);
+      const float4 cf = S.coef[cx + 1];
+      o.elin = E;
+      if (f9) {
+        // E1 = ca E + cb/dx (cY - cX) - cb sum(gamma J);  J' = k1 J + k2 (E1 - E)/dt
+        float4 e1 = S.e1[me];
+        if ((src_own >> (r - rs)) & 1) {  // the forward added the source after E1
+          const float w = __ldg(p.waveform + step);
+          for (int s = 4 * lane_g; s < 4 * lane_g + 4 && s < p.ntx; ++s)
+            if (__ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == r) add_comp(e1, s & 3, -w);
+        }
+        const float4 en = S.en[me];
+        const float4 e1tot = E + jsum(S, cx + 1);
+        float4 elin = cf.x * e1tot;
+        const float4 dedt = (e1 - en) * f4(p.inv_dt);
+#pragma unroll
+        for (int q = 0; q < ND; ++q) {
+          const float4 kq = S.ade[q * H + cx + 1];
+          const float4 jin = S.lj[(q * H + cx + 1) * L + lo];
+          const float4 jn = S.jn[q * CX * L + me];
+          elin = fma4(-kq.y * p.inv_dt, jin, elin);
+          st4(a.j[par ^ 1] + (size_t)g * p.gs_j + (q * plane + (size_t)r * nx + x) * L + lo,
+              kq.x * jin - (cf.y * kq.z) * e1tot);
+          gv[2 + 3 * q] = dot4(jin, jn);
+          gv[3 + 3 * q] = dot4(jin, dedt);
+          gv[4 + 3 * q] = -cf.y * dot4(e1tot, jn);
+        }
+        o.elin = elin;
+        o.cy = (cf.y * inv) * e1tot;
+        o.cx = (-cf.y * inv) * e1tot;
+        gv[0] = dot4(e1tot, en);
+        gv[1] = __fdividef(dot4(e1tot, e1 - cf.x * en), cf.y);
+      } else if (GEN && n > 0) {
+        // transposed E-CPML: PEY' = b PEY + c/dx cX, E -= dteps PEY';
+        //                    PEX' = b PEX + c/dx cY, E += dteps PEX'
+        const int sy = rg.ey_row(r);
+        if (x >= 1 && sy >= 0) {
+          const int ci = rg.ey_ci(r);
+          const float4 tot = fma4(-cf.z, E, __ldg(pey_r + ((size_t)sy * nx + x) * L + lo));
+          st4(a.psi_ezy[par ^ 1] + (size_t)g * p.gs_psi_y + ((size_t)sy * nx + x) * L + lo, p.cpml_b[ci] * tot);
+          o.cx = (p.cpml_c[ci] * inv) * tot;
+        }
+        const int sx = rg.ex_col(x);
+        if (r >= 1 && sx >= 0) {
+          const int ci = rg.ex_ci(x);
+          const float4 tot = fma4(cf.z, E, __ldg(pex_r + ((size_t)r * 2 * n + sx) * L + lo));
+          st4(a.psi_ezx[par ^ 1] + (size_t)g * p.gs_psi_x + ((size_t)r * 2 * n + sx) * L + lo, p.cpml_b[ci] * tot);
+          o.cy = (p.cpml_c[ci] * inv) * tot;
+        }
+      }
+    }
+    // sum over the L lanes of the cell; lane k % L adds gradient k (each
+    // address receives one add per launch, so the order is fixed)
+    double* gw = a.g + ((size_t)g * plane + (size_t)r * nx + x) * KP;
+#pragma unroll
+    for (int k = 0; k < KG; ++k) {
+      const float v = lane_sum<L>(gv[k]);
+      if (f9 && (k % L) == lo) atomicAdd(gw + k, (double)v);
+    }
+    if (lw < L || lw >= 32 - L) {
+      const int dx = lw < L ? -1 : 1;
+      if (x + dx >= 0 && x + dx < nx) o.cye = cy_at(S, cx + 1 + dx, x + dx, r);
+    }
+    return o;
+  };
+  // H half of this cell in row y; every lane of the warp must call it.
+  auto h_half = [&](const St& S, int y, const AdjE& c, float4 cx_up, float4& d_u) {
+    float4 cy_l = shfl_up4(c.cy, L), cy_r = shfl_down4(c.cy, L);
+    if (lw < L) cy_l = c.cye;
+    if (lw >= 32 - L) cy_r = c.cye;
+    if (!active) return;
+    const size_t at = ((size_t)y * nx + x) * L + lo;
+    const HAdj ry = hy_adj<GEN>(p, rg, x, y, S.lhy[mh], c.cy, cy_r, phy_r, lo);
+    const HAdj rx = hx_adj<GEN>(p, rg, x, y, S.lhx[me], c.cx, cx_up, phx_r, lo);
+    st4(a.hy[par ^ 1] + gf + at, ry.tot);
+    st4(a.hx[par ^ 1] + gf + at, rx.tot);
+    if (GEN && ry.s >= 0)
+      st4(a.psi_hy[par ^ 1] + (size_t)g * p.gs_psi_x + ((size_t)y * 2 * n + ry.s) * L + lo, ry.psi);
+    if (GEN && rx.s >= 0) st4(a.psi_hx[par ^ 1] + (size_t)g * p.gs_psi_y + ((size_t)rx.s * nx + x) * L + lo, rx.psi);
+    float4 e = c.elin - ry.u - rx.u + d_u;
+    if (!GEN || x >= 1) e = e + hy_adj<GEN>(p, rg, x - 1, y, S.lhy[mh - L], cy_l, c.cy, phy_r, lo).u;
+    st4(a.ez[par ^ 1] + gf + at, e);
+    d_u = rx.u;
   };
 
-  const float4 cy_c = a.cy[id];
-  const float4 cx_c = a.cx[id];
-  // this cell
-  const size_t py = psi_y_at(x, y), px = psi_x_at(x, y);
-  const HAdjoint ry = hy_adjoint(p, x, y, yin[id], cy_c, x + 1 < nx ? a.cy[id + sxs] : zero,
-                                 py != ~(size_t)0 ? a.psi_hy[par][py] : zero);
-  const HAdjoint rx = hx_adjoint(p, x, y, xin[id], cx_c, y + 1 < ny ? a.cx[id + sys] : zero,
-                                 px != ~(size_t)0 ? a.psi_hx[par][px] : zero);
-  a.hy[par ^ 1][id] = ry.tot;
-  a.hx[par ^ 1][id] = rx.tot;
-  if (ry.strip) a.psi_hy[par ^ 1][py] = ry.psi;
-  if (rx.strip) a.psi_hx[par ^ 1][px] = rx.psi;
-  // neighbours' forward differences that involve this cell's E
-  float4 e = a.elin[id] - ry.u - rx.u;
-  if (x >= 1) {
-    const size_t pyl = psi_y_at(x - 1, y);
-    const HAdjoint l = hy_adjoint(p, x - 1, y, yin[id - sxs], a.cy[id - sxs], cy_c,
-                                  pyl != ~(size_t)0 ? a.psi_hy[par][pyl] : zero);
-    e = e + l.u;
+  if (!wait(0)) return;
+  int k = 0;
+  AdjE c;
+  float4 d_u = f4(0.f);  // adjoint of E(x, y) - E(x, y-1) from the Hx update of the row below
+  if (y0 > 0) {          // slot 0 holds row y0-1
+    const float4 pcx = cx_row(st[0], y0 - 1);
+    if (!wait(1)) return;
+    c = e_half(st[1 % NS], y0);
+    if (active) d_u = hx_adj<GEN>(p, rg, x, y0 - 1, st[0].lhx[me], pcx, c.cx, phx_r, lo).u;
+    release(0);
+    k = 1;
+  } else {
+    c = e_half(st[0], y0);
   }
-  if (y >= 1) {
-    const size_t pxd = psi_x_at(x, y - 1);
-    const HAdjoint d = hx_adjoint(p, x, y - 1, xin[id - sys], a.cx[id - sys], cx_c,
-                                  pxd != ~(size_t)0 ? a.psi_hx[par][pxd] : zero);
-    e = e + d.u;
+  for (int y = y0; y < y1; ++y, ++k) {
+    const bool has_up = k + 1 < nslots;
+    if (has_up && !wait(k + 1)) return;
+    AdjE up{f4(0.f), f4(0.f), f4(0.f), f4(0.f)};
+    if (y + 1 < y1) up = e_half(st[(k + 1) % NS], y + 1);
+    else if (has_up) up.cx = cx_row(st[(k + 1) % NS], y + 1);
+    h_half(st[k % NS], y, c, up.cx, d_u);
+    c = up;
+    release(k);
   }
-  a.ez[id] = e;
+  if (k < nslots) release(k);  // the row above the segment
 }
 
-// ---------------------------------------------------------------------------
+// Tile b of a gx x gy grid of column strips x row segments, in the order the
+// block scheduler should start them: the two edge columns (CPML x strips on
+// every row, the costliest tiles), then the first and last segments of the
+// other columns, then the rest.  A bijection of [0, gx*gy).
+CEEP_D void adj_tile(int b, int gx, int gy, int& bx, int& by) {
+  if (gx <= 2) {
+    bx = b % gx;
+    by = b / gx;
+    return;
+  }
+  if (b < 2 * gy) {
+    bx = (b & 1) ? gx - 1 : 0;
+    by = b >> 1;
+    return;
+  }
+  int r = b - 2 * gy;
+  const int ic = gx - 2;
+  if (gy <= 2) {
+    bx = 1 + r % ic;
+    by = r / ic;
+  } else if (r < 2 * ic) {
+    bx = 1 + (r >> 1);
+    by = (r & 1) ? gy - 1 : 0;
+  } else {
+    r -= 2 * ic;
+    bx = 1 + r % ic;
+    by = 1 + r / ic;
+  }
+}
+
+template <int L, int ND>
+__global__ void __launch_bounds__(kAdjConsumers + 32, 3)
+    adjoint2d_step_kernel(const Adjoint2dParams a, int step, int par, const float4* __restrict__ ez_n,
+                          const float4* __restrict__ ez_np1, const float4* __restrict__ j_n) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  using St = AdjStage<L, ND>;
+  constexpr int NS = adj_stages<L, ND>(), CX = St::CX;
+  St* st = reinterpret_cast<St*>(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * sizeof(St));
+  uint64_t* empty = full + NS;
+  const int nx = a.f.nx, ny = a.f.ny, n = a.f.n;
+  int bx, by;
+  adj_tile(blockIdx.x, (nx + CX - 1) / CX, (ny + a.rows - 1) / a.rows, bx, by);
+  const int x0 = bx * CX, y0 = by * a.rows, g = blockIdx.y;
+  const int y1 = min(y0 + a.rows, ny);
+  const int rs = y0 > 0 ? y0 - 1 : 0;
+  const int nslots = (y1 - rs) + (y1 < ny ? 1 : 0);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kAdjConsumers / 32);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  // Programmatic dependent launch, as in the forward step: every access to
+  // adjoint state comes after the wait for the previous step's grid.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (threadIdx.x >= kAdjConsumers) {
+    if (threadIdx.x == kAdjConsumers)
+      adj_produce<L, ND>(a, st, full, empty, par, ez_n, ez_np1, j_n, x0, y0, y1, rs, nslots, g);
+    return;
+  }
+  // Block-uniform: own cells, the halo cells x0-1 and x0+CX and the rows
+  // y0-1 and y1 all lie in the interior E region, off the edges, and the own
+  // cells (and x0-1) in the plain H interior.
+  const int m = n > 1 ? n : 1;
+  const bool interior = x0 >= n + 2 && x0 + CX + 1 <= nx - m && y0 >= n + 2 && y1 + 1 <= ny - m;
+  if (interior)
+    adj_consume<L, ND, false>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+  else
+    adj_consume<L, ND, true>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+}
+
+// ------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------
+// Tiles cost unequal time (CPML strips, probe rows), so a launch is cut into
+// about three waves of tiles, started costliest first, for the block
+// scheduler to balance; segments stay >= 8 rows so the two neighbour rows
+// each one recomputes stay a small overhead.
+static int adjoint2d_rows(int nx, int ny, int groups, int cells_per_block, long slots) {
+  const long xb = (nx + cells_per_block - 1) / cells_per_block;
+  for (int rows = kAdjMaxRows; rows > 8; --rows)
+    if (xb * ((ny + rows - 1) / rows) * groups >= 3 * slots) return rows;
+  return 8;
+}
+
+template <int L, int ND>
+static cudaError_t configure_l(Adjoint2dParams& a) {
+  constexpr size_t smem = adj_smem_bytes<L, ND>();
+  auto kern = adjoint2d_step_kernel<L, ND>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  a.smem = (int)smem;
+  if (a.rows > kAdjMaxRows) a.rows = kAdjMaxRows;
+  if (a.rows > 0) return cudaSuccess;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kAdjConsumers + 32, smem);
+  if (e != cudaSuccess) return e;
+  a.rows = adjoint2d_rows(a.f.nx, a.f.ny, a.f.groups, kAdjConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm));
+  return cudaSuccess;
+}
+
 template <int L, int ND>
 static cudaError_t launch_l(const Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
                             const float4* j_n, cudaStream_t s) {
-  const long long total = (long long)a.f.groups * a.f.ny * a.f.nx * L;
-  const unsigned blocks = (unsigned)((total + kAdjThreads - 1) / kAdjThreads);
-  adjoint2d_e_kernel<L, ND><<<blocks, kAdjThreads, 0, s>>>(a, step, ez_n, ez_np1, j_n);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  adjoint2d_h_kernel<L><<<blocks, kAdjThreads, 0, s>>>(a, par);
-  return cudaGetLastError();
+  constexpr int CX = kAdjConsumers / L;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(((a.f.nx + CX - 1) / CX) * ((a.f.ny + a.rows - 1) / a.rows), a.f.groups);
+  cfg.blockDim = dim3(kAdjConsumers + 32);
+  cfg.dynamicSmemBytes = a.smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, adjoint2d_step_kernel<L, ND>, a, step, par, ez_n, ez_np1, j_n);
 }
 
 template <int ND>
-static cudaError_t launch_nd(const Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
-                             const float4* j_n, cudaStream_t s) {
+static cudaError_t dispatch_l(Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
+                              const float4* j_n, cudaStream_t s, bool configure) {
   switch (a.f.L) {
-    case 1: return launch_l<1, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 2: return launch_l<2, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 4: return launch_l<4, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    default: return launch_l<8, ND>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 1: return configure ? configure_l<1, ND>(a) : launch_l<1, ND>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 2: return configure ? configure_l<2, ND>(a) : launch_l<2, ND>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 4: return configure ? configure_l<4, ND>(a) : launch_l<4, ND>(a, step, par, ez_n, ez_np1, j_n, s);
+    default: return configure ? configure_l<8, ND>(a) : launch_l<8, ND>(a, step, par, ez_n, ez_np1, j_n, s);
   }
+}
+
+static cudaError_t dispatch(Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
+                            const float4* j_n, cudaStream_t s, bool configure) {
+  if (a.f.n_lorentz != 0) return cudaErrorInvalidValue;
+  switch (a.f.n_debye) {
+    case 0: return dispatch_l<0>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 1: return dispatch_l<1>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 2: return dispatch_l<2>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t adjoint2d_configure(Adjoint2dParams& a) {
+  return dispatch(a, 0, 0, nullptr, nullptr, nullptr, nullptr, true);
 }
 
 cudaError_t adjoint2d_launch_step(const Adjoint2dParams& a, int step, int par, const float4* ez_n,
                                   const float4* ez_np1, const float4* j_n, cudaStream_t s) {
-  if (a.f.n_lorentz != 0) return cudaErrorInvalidValue;
-  switch (a.f.n_debye) {
-    case 0: return launch_nd<0>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 1: return launch_nd<1>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 2: return launch_nd<2>(a, step, par, ez_n, ez_np1, j_n, s);
-    default: return cudaErrorInvalidValue;
-  }
+  Adjoint2dParams q = a;
+  return dispatch(q, step, par, ez_n, ez_np1, j_n, s, false);
 }
 
 }  // namespace ceep

@@ -1,4 +1,4 @@
-// Parameters of the 2D adjoint (transposed) step kernels.
+// Parameters of the fused 2D adjoint (transposed) step kernel.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -9,28 +9,33 @@ namespace ceep {
 
 struct Adjoint2dParams {
   Fdtd2dParams f;       // geometry, coefficients, CPML profile, sources, probes of the forward plan
-  // adjoint state (same layouts as the forward state)
-  float4* ez;           // in place
-  float4* hx[2];        // ping-pong
+  int rows;             // rows of the column segment one block walks
+  int smem;             // dynamic shared memory per block
+  // adjoint state, every array ping-pong (read [p], write [p ^ 1]) with the
+  // layouts of the forward state
+  float4* ez[2];
+  float4* hx[2];
   float4* hy[2];
-  float4* psi_hx[2];    // ping-pong (y strips)
-  float4* psi_hy[2];    // ping-pong (x strips)
-  float4* psi_ezx;      // in place
-  float4* psi_ezy;      // in place
-  float4* j;            // in place, (G, poles, ny, nx, L)
-  // scratch written by the E-phase kernel and read by the H-phase kernel
-  float4* cy;           // adjoint of curl_y = Hy(x) - Hy(x-1)
-  float4* cx;           // adjoint of curl_x = Hx(y) - Hx(y-1)
-  float4* elin;         // pointwise part of the E adjoint
-  // per-cell parameter gradients, summed over transmit events and steps
-  double* g;            // (2 + 3*poles, ny, nx): ca, cb, then per pole k1, k2, gamma
+  float4* psi_hx[2];    // y strips
+  float4* psi_hy[2];    // x strips
+  float4* psi_ezx[2];
+  float4* psi_ezy[2];
+  float4* j[2];         // (G, poles, ny, nx, L)
+  // per-cell parameter gradients of each TX group, summed over steps:
+  // (G, ny, nx, KP) with KP = 2 + 3*poles rounded up to even; per cell ca, cb,
+  // then per pole k1, k2, gamma (and a zero pad)
+  double* g;
   const float* probe_grad;  // (ntx, nprobe, nsteps) dLoss/dprobe
 };
 
+__host__ __device__ constexpr int adjoint2d_grad_width(int n_debye) { return (2 + 3 * n_debye + 1) & ~1; }
+
+// Kernel attributes and rows per block (when a.rows == 0).
+cudaError_t adjoint2d_configure(Adjoint2dParams& a);
 // One adjoint step for forward step `step`: reads the adjoint of the state
-// after the step, writes the adjoint of the state before it.  ez_n / ez_np1 /
-// j_n are the forward Ez before and after the step and J before it (layout of
-// the forward fields).  `par` is the adjoint H ping-pong buffer to read.
+// after the step from buffer `par`, writes the adjoint of the state before it
+// into buffer `par ^ 1`.  ez_n / ez_np1 / j_n are the forward Ez before and
+// after the step and J before it (layout of the forward fields).
 cudaError_t adjoint2d_launch_step(const Adjoint2dParams& a, int step, int par, const float4* ez_n,
                                   const float4* ez_np1, const float4* j_n, cudaStream_t s);
 

@@ -328,33 +328,37 @@ extern "C" int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoi
   if (!plan || !d || !out) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_create: null argument");
   *out = nullptr;
   if (plan->p.n_lorentz) return fail(CEEP_ERR_UNSUPPORTED, "adjoint: Lorentz poles are not supported");
-  if (!d->ez || !d->hx[0] || !d->hx[1] || !d->hy[0] || !d->hy[1] || !d->cy || !d->cx || !d->elin || !d->grad)
-    return fail(CEEP_ERR_INVALID, "adjoint: null state/scratch/gradient buffer");
-  if (plan->p.n > 0 && (!d->psi_hx[0] || !d->psi_hx[1] || !d->psi_hy[0] || !d->psi_hy[1] || !d->psi_ezx ||
-                        !d->psi_ezy))
-    return fail(CEEP_ERR_INVALID, "adjoint: null psi buffer");
-  if (plan->p.n_debye && !d->j) return fail(CEEP_ERR_INVALID, "adjoint: null current buffer");
+  for (int k = 0; k < 2; ++k) {
+    if (!d->ez[k] || !d->hx[k] || !d->hy[k] || !d->grad)
+      return fail(CEEP_ERR_INVALID, "adjoint: null state/gradient buffer");
+    if (plan->p.n > 0 && (!d->psi_hx[k] || !d->psi_hy[k] || !d->psi_ezx[k] || !d->psi_ezy[k]))
+      return fail(CEEP_ERR_INVALID, "adjoint: null psi buffer");
+    if (plan->p.n_debye && !d->j[k]) return fail(CEEP_ERR_INVALID, "adjoint: null current buffer");
+  }
   if (plan->p.nprobe && !d->probe_grad) return fail(CEEP_ERR_INVALID, "adjoint: null probe gradient");
   ceep2d_adjoint* ad = new (std::nothrow) ceep2d_adjoint();
   if (!ad) return fail(CEEP_ERR_INVALID, "host allocation failed");
   ceep::Adjoint2dParams& a = ad->a;
   a.f = plan->p;
+  a.rows = 0;
   auto f4p = [](float* q) { return reinterpret_cast<float4*>(q); };
-  a.ez = f4p(d->ez);
   for (int k = 0; k < 2; ++k) {
+    a.ez[k] = f4p(d->ez[k]);
     a.hx[k] = f4p(d->hx[k]);
     a.hy[k] = f4p(d->hy[k]);
     a.psi_hx[k] = f4p(d->psi_hx[k]);
     a.psi_hy[k] = f4p(d->psi_hy[k]);
+    a.psi_ezx[k] = f4p(d->psi_ezx[k]);
+    a.psi_ezy[k] = f4p(d->psi_ezy[k]);
+    a.j[k] = f4p(d->j[k]);
   }
-  a.psi_ezx = f4p(d->psi_ezx);
-  a.psi_ezy = f4p(d->psi_ezy);
-  a.j = f4p(d->j);
-  a.cy = f4p(d->cy);
-  a.cx = f4p(d->cx);
-  a.elin = f4p(d->elin);
   a.g = d->grad;
   a.probe_grad = d->probe_grad;
+  cudaError_t e = ceep::adjoint2d_configure(a);
+  if (e != cudaSuccess) {
+    delete ad;
+    return ceep::cuda_fail(e, "adjoint2d configure");
+  }
   *out = ad;
   return CEEP_OK;
 }
@@ -392,6 +396,8 @@ extern "C" int ceep2d_adjoint_destroy(ceep2d_adjoint* ad) {
 }
 
 extern "C" int64_t ceep2d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep2d_adjoint_desc); }
+
+extern "C" int ceep2d_adjoint_rows(const ceep2d_adjoint* ad) { return ad ? ad->a.rows : 0; }
 
 // --------------------------------------------------------------------------
 // Packed multi-phantom 2D launch

@@ -491,22 +491,23 @@ static cudaError_t configure_l(Fdtd2dParams& p) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConsumers + 32, smem);
   if (e != cudaSuccess) return e;
-  if (per_sm < 1) per_sm = 1;
-  // Pick the segment length whose grid fills whole waves best: cost ~ waves *
-  // (rows + 2), the +2 being the two halo rows every segment loads.
-  constexpr int CX = kConsumers / L;
-  const long slots = (long)sms * per_sm;
-  const long xb = (p.nx + CX - 1) / CX;
+  p.rows = choose_rows(p.nx, p.ny, p.groups, kConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm), kMaxRows);
+  return cudaSuccess;
+}
+
+// The segment length whose grid fills whole waves best: cost ~ waves *
+// (rows + 2), the +2 being the two neighbour rows every segment loads.
+int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int max_rows) {
+  const long xb = (nx + cells_per_block - 1) / cells_per_block;
   double best = 1e300;
-  int best_rows = 16;
-  for (int rows = 4; rows <= kMaxRows; ++rows) {
-    const long blocks = xb * ((p.ny + rows - 1) / rows) * p.groups;
+  int best_rows = 16 < max_rows ? 16 : max_rows;
+  for (int rows = 4; rows <= max_rows; ++rows) {
+    const long blocks = xb * ((ny + rows - 1) / rows) * groups;
     const long waves = (blocks + slots - 1) / slots;
     const double cost = (double)waves * (rows + 2);
     if (cost < best - 1e-9) { best = cost; best_rows = rows; }
   }
-  p.rows = best_rows;
-  return cudaSuccess;
+  return best_rows;
 }
 
 template <int L, int ND, int NL>

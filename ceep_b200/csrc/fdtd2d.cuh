@@ -55,6 +55,8 @@ struct PackTile {
 cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
                                  const Fdtd2dParams* params, int step, cudaStream_t s);
 int fdtd2d_cells_per_block(int L);
+// Rows per block for a column-strip x row-segment grid of `slots` resident blocks.
+int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int max_rows);
 
 // Set the kernel attributes and (if rows == 0) choose rows per block.
 cudaError_t fdtd2d_configure(Fdtd2dParams& p);

@@ -43,6 +43,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// As mbar_try_wait, but the thread may be suspended (up to `hint_ns`) until
+// the phase completes instead of returning at once: a waiting warp then
+// takes no issue slots from the warps that have work.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -51,12 +66,14 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 
 // Bounded wait: returns false if the phase did not complete within
 // `limit_ns` (the caller records the failure and leaves the pipeline).
+// Each suspended try_wait lasts at most ~1 ms, so the bound is checked
+// often enough.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63) == 0 && global_timer_ns() - t0 > limit_ns) return false;
+  for (;;) {
+    if (mbar_try_wait_suspend(bar, parity, 1000000u)) return true;
+    if (global_timer_ns() - t0 > limit_ns) return false;
   }
 }
 

@@ -147,22 +147,23 @@ int ceep2d_pack_destroy(ceep2d_pack* pack);
  * the exact transpose of the fused step above, run backwards in time; per
  * cell it accumulates (over transmit events and steps) the gradients of the
  * loss with respect to ca, cb and the Debye k1, k2, gamma of each pole.
- * Debye poles only (Lorentz: CEEP_ERR_UNSUPPORTED).
+ * Debye poles only (Lorentz: CEEP_ERR_UNSUPPORTED).  One launch per step.
+ * Every adjoint state array is a ping-pong pair shaped like the forward's
+ * (both halves zeroed by the caller before the first run).
  * ---------------------------------------------------------------------- */
 typedef struct ceep2d_adjoint_desc {
-  float* ez;               /* adjoint Ez, (G, ny, nx, .), in place           */
-  float* hx[2];            /* adjoint Hx / Hy, ping-pong                     */
+  float* ez[2];            /* adjoint Ez, (G, ny, nx, .)                     */
+  float* hx[2];            /* adjoint Hx / Hy                                */
   float* hy[2];
-  float* psi_hx[2];        /* adjoint H-CPML psi, ping-pong (forward shapes) */
+  float* psi_hx[2];        /* adjoint H-CPML psi (forward shapes)            */
   float* psi_hy[2];
-  float* psi_ezx;          /* adjoint E-CPML psi, in place                   */
-  float* psi_ezy;
-  float* j;                /* adjoint Debye currents, in place               */
-  float* cy;               /* scratch, each like Ez                          */
-  float* cx;
-  float* elin;
-  double* grad;            /* (2 + 3*n_debye, ny, nx): d/dca, d/dcb, then per
-                              pole d/dk1, d/dk2, d/dgamma; accumulated       */
+  float* psi_ezx[2];       /* adjoint E-CPML psi                             */
+  float* psi_ezy[2];
+  float* j[2];             /* adjoint Debye currents                         */
+  double* grad;            /* (G, ny, nx, KP), KP = 2 + 3*n_debye rounded up
+                              to even: per TX group and cell d/dca, d/dcb,
+                              then per pole d/dk1, d/dk2, d/dgamma, then a
+                              zero pad; accumulated                          */
   const float* probe_grad; /* (ntx, nprobe, nsteps) dLoss/dprobe             */
 } ceep2d_adjoint_desc;
 
@@ -176,6 +177,8 @@ int ceep2d_adjoint_run(ceep2d_adjoint* adj, int64_t step_hi, int64_t nsteps, con
 int ceep2d_adjoint_reset(ceep2d_adjoint* adj);
 int ceep2d_adjoint_destroy(ceep2d_adjoint* adj);
 int64_t ceep2d_adjoint_desc_size(void);
+/* Rows of the segment one block of the adjoint walks per step. */
+int ceep2d_adjoint_rows(const ceep2d_adjoint* adj);
 
 /* ------------------------------------------------------------------------
  * 3D batched Yee FDTD.

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4
 
 
-def _case(nx, ny, n, seed, debye=True):
+def _case(nx, ny, n, seed, debye=True, nring=4):
     rng = np.random.default_rng(seed)
     x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
     cx, cy = nx // 2, ny // 2
@@ -21,12 +21,12 @@ def _case(nx, ny, n, seed, debye=True):
     sig = np.where(m, 0.3 + 0.2 * rng.random((nx, ny)), 0.0)
     de = np.where(m, 15.0 + 5 * rng.random((nx, ny)), 0.0) if debye else None
     tau = np.where(m, 8e-12, 0.0) if debye else None
-    ang = 2 * np.pi * np.arange(4) / 4
+    ang = 2 * np.pi * np.arange(nring) / nring
     ring = [(int(cx + (r + 6) * np.cos(a)), int(cy + (r + 6) * np.sin(a))) for a in ang]
     return eps, sig, de, tau, m, ring
 
 
-def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp"):
+def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp", nring=4):
     """Gradient of the same scalar through the CUDA adjoint and through autograd
     of the FP64 restatement.  loss="vjp": sum(probes * G) for a fixed random G,
     which tests the transposed Jacobian alone; loss="misfit": the S-parameter
@@ -34,7 +34,7 @@ def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp"):
     from ceep_b200 import BatchedFDTD2D
     from ceep_b200.adjoint import Adjoint2D, probes_with_grad, s_parameter_loss
     dev = torch.device("cuda")
-    eps, sig, de, tau, m, ring = _case(nx, ny, n, seed, debye)
+    eps, sig, de, tau, m, ring = _case(nx, ny, n, seed, debye, nring)
     src, prb = ring[:ntx], ring
     freqs = np.linspace(1e9, 3e9, 11)
     t = TorchFdtd2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9, device=dev)
@@ -83,6 +83,19 @@ def test_adjoint_vjp_matches_autograd(cuda_device):
 
 def test_adjoint_torch_check_128_300(cuda_device):
     out, inner = _run_both(128, 128, 10, 300, 2, K=50, ntx=4)
+    _check(out, inner, ("eps_r", "sigma", "deps"), TOL)
+
+
+def test_adjoint_16tx_interior_blocks(cuda_device):
+    """16 TX (four float4 lanes per cell, 32-cell blocks): most blocks lie in
+    the plain interior and take the kernel path without region tests."""
+    out, inner = _run_both(112, 112, 8, 160, 6, K=20, ntx=16, nring=16)
+    _check(out, inner, ("eps_r", "sigma", "deps"), TOL)
+
+
+def test_adjoint_two_tx_groups(cuda_device):
+    """37 TX: two TX groups, whose per-group gradient sums are added."""
+    out, inner = _run_both(100, 92, 7, 140, 7, K=1, ntx=37, nring=37)
     _check(out, inner, ("eps_r", "sigma", "deps"), TOL)
 
 
