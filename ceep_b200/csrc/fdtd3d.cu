@@ -35,16 +35,11 @@ constexpr int kThreads3d = 128;
 // ---------------------------------------------------------------------------
 // H half-step
 // ---------------------------------------------------------------------------
-template <int L>
-__global__ void __launch_bounds__(kThreads3d) fdtd3d_h_kernel(const Fdtd3dParams p) {
-  constexpr int CX = kThreads3d / L;
-  const int x = blockIdx.x * CX + threadIdx.x / L;
-  const int lo = threadIdx.x % L;
-  const int y = blockIdx.y;
-  const int zseg = blockIdx.z % p.zsegs, g = blockIdx.z / p.zsegs;
-  const int z0 = zseg * p.zrows, z1 = min(z0 + p.zrows, p.nz);
+// GEN = false for blocks whose cells all lie inside the three H interior
+// boxes and off every CPML face: the region tests and face code fold away.
+template <int L, bool GEN>
+__device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, int y, int g, int z0, int z1) {
   const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n;
-  if (x >= nx) return;
   const size_t gs = (size_t)g * p.gs_field;
   const float4* __restrict__ ex = p.ex + gs;
   const float4* __restrict__ ey = p.ey + gs;
@@ -76,12 +71,15 @@ __global__ void __launch_bounds__(kThreads3d) fdtd3d_h_kernel(const Fdtd3dParams
     const float4 exyp = y + 1 < ny ? ld4(ex + at + sy) : f4(0.f);
     const float4 cf = __ldg(coef + (size_t)z * ny * nx + (size_t)y * nx + x);  // da, db, ca, cb
     float4 Hx = hx[at], Hy = hy[at], Hz = hz[at];
-    const bool z_int = z >= n && z < nz - 1, z_int_hz = z >= n && z < nz - n;
+    const bool z_int = !GEN || (z >= n && z < nz - 1), z_int_hz = !GEN || (z >= n && z < nz - n);
     // interior boxes (fdtd_3d_batched.py:764-818)
-    if (x_int_hx && y_int && z_int) Hx = cf.x * Hx + cf.y * ((eyu - eyc) * f4(inv) - (ezyp - ezc) * f4(inv));
-    if (x_int && y_int_hy && z_int) Hy = cf.x * Hy + cf.y * ((ezxp - ezc) * f4(inv) - (exu - exc) * f4(inv));
-    if (x_int && y_int && z_int_hz) Hz = cf.x * Hz + cf.y * ((exyp - exc) * f4(inv) - (eyxp - eyc) * f4(inv));
-    if (n > 0) {
+    if (!GEN || (x_int_hx && y_int && z_int))
+      Hx = cf.x * Hx + cf.y * ((eyu - eyc) * f4(inv) - (ezyp - ezc) * f4(inv));
+    if (!GEN || (x_int && y_int_hy && z_int))
+      Hy = cf.x * Hy + cf.y * ((ezxp - ezc) * f4(inv) - (exu - exc) * f4(inv));
+    if (!GEN || (x_int && y_int && z_int_hz))
+      Hz = cf.x * Hz + cf.y * ((exyp - exc) * f4(inv) - (eyxp - eyc) * f4(inv));
+    if (GEN && n > 0) {
       // x faces (:398-460)
       if (xf >= 0) {
         const bool lof = x < n;
@@ -137,12 +135,33 @@ __global__ void __launch_bounds__(kThreads3d) fdtd3d_h_kernel(const Fdtd3dParams
   }
 }
 
+template <int L>
+__global__ void __launch_bounds__(kThreads3d, 6) fdtd3d_h_kernel(const Fdtd3dParams p) {
+  constexpr int CX = kThreads3d / L;
+  const int x0 = blockIdx.x * CX;
+  const int x = x0 + threadIdx.x / L;
+  const int lo = threadIdx.x % L;
+  const int y = blockIdx.y;
+  const int zseg = blockIdx.z % p.zsegs, g = blockIdx.z / p.zsegs;
+  const int z0 = zseg * p.zrows, z1 = min(z0 + p.zrows, p.nz);
+  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n;
+  if (x >= nx) return;
+  // every cell of the block in all three interior boxes and on no face:
+  // x in [n, nx-n), y in [n, ny-n), z in [n, nz-n) with n >= 1 (nx-n <= nx-1)
+  const int m = n > 1 ? n : 1;
+  const bool interior = x0 >= n && x0 + CX <= nx - m && y >= n && y < ny - m && z0 >= n && z1 <= nz - m;
+  if (interior)
+    h_segment<L, false>(p, x, lo, y, g, z0, z1);
+  else
+    h_segment<L, true>(p, x, lo, y, g, z0, z1);
+}
+
 // ---------------------------------------------------------------------------
 // E half-step on the interior box, with the Debye/Lorentz currents of each
 // component (the 3D analogue of dispersive.py:364-404 / fdtd_2d.py:163-178).
 // ---------------------------------------------------------------------------
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kThreads3d) fdtd3d_e_kernel(const Fdtd3dParams p) {
+__global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dParams p) {
   constexpr int CX = kThreads3d / L;
   constexpr int NP = ND + NL;
   const int n = p.n, nx = p.nx, ny = p.ny, nz = p.nz;
