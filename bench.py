@@ -64,7 +64,7 @@ def algorithmic_bytes_per_step_3d(w, n_debye):
     return cells * (48 * T + 16) + faces * 16 * T + n_debye * interior * (24 * T + 12)
 
 
-def algorithmic_bytes_per_step_2d(w, n_debye):
+def algorithmic_bytes_per_step_2d(w, n_debye, n_lorentz=0):
     """Compulsory FP32 DRAM bytes of one fused step (read+write each state word
     once, coefficients once per cell): 24 B per cell-TX for Ez/Hx/Hy, 8 B per
     cell for (ca, cb), 16 B per strip cell-TX for the H and E psi of that
@@ -78,7 +78,17 @@ def algorithmic_bytes_per_step_2d(w, n_debye):
     b = cells * (24 * T + 8)
     b += (xstrip + ystrip) * (16 * T + 4)
     b += n_debye * interior * (8 * T + 12)
+    b += n_lorentz * interior * (16 * T + 12)   # J and J_prev read+write, (k1, k2, k3)
     return b
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json, else
+    the pool's earlier measurement (6650 GB/s)."""
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return json.load(open(peaks_path))["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
 
 
 class ClockSampler:
@@ -250,12 +260,7 @@ def run_ours(args, w):
         per_launch.append(a.elapsed_time(b) / w["steps"])
     launch_ms = float(np.median(per_launch))
     bytes_step = algorithmic_bytes_per_step(w, n_debye)
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peak = json.load(open(peaks_path))["hbm_gbs"]
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = hbm_peak()
     achieved = bytes_step / (launch_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", f"fdtd2d_step_{args.workload}.md")
@@ -568,6 +573,12 @@ def run_pack_bench(args):
     for s in solvers:
         s.check_status()
     value = pk.cell_steps / float(np.median(times)) / 1e9
+    # roofline of the whole packed run: compulsory bytes of every phantom's
+    # steps (real TX counts, not the padded lanes) over the run's time
+    alg = sum(algorithmic_bytes_per_step_2d({"nx": s.nx, "ny": s.ny, "cpml": s.cpml_n, "ntx": s.batch},
+                                            len(s._debye), len(s._lorentz)) * s.total_steps for s in solvers)
+    peak, peak_src = hbm_peak()
+    achieved = alg / float(np.median(times)) / 1e9
     base_fresh = cs_sample / t_fresh / 1e9
     base_replay = cs_sample / t_replay / 1e9
     line = {"metric": "packed uneven batch GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
@@ -576,6 +587,9 @@ def run_pack_bench(args):
             "config": {"workload": "pack256", "phantoms": count, "sizes": "256..768 step 32", "time_steps": "600..1200",
                        "tx": "8..16", "lorentz_fraction": "1/3", "cpml": 15, "tile_rows": pk.rows,
                        "cell_steps": pk.cell_steps},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 3), "peak_source": peak_src,
+                         "algorithmic_bytes": int(alg), "kernel": "fdtd2d_packed_kernel (whole run)"},
             "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
             "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
             "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),
