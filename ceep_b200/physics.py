@@ -87,6 +87,83 @@ def update_coefficients(eps_r, sigma_e, dt, eps_add=None):
     return (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s)
 
 
+def _f64(a, device):
+    import torch
+    return torch.as_tensor(np.asarray(a, np.float64)).to(device)
+
+
+def ade_tensors(dt: float, debye=(), lorentz=(), shape=None, device=None):
+    """ade_coefficients evaluated with torch in FP64 on `device`: every
+    expression is the NumPy one above with the same operation order (one
+    IEEE-rounded op per torch call, no fusion), so the maps are bit-identical.
+    Returns eps_add and a (poles, *shape, 4) FP64 tensor."""
+    import torch
+    bc = lambda a: torch.broadcast_to(_f64(a, device), shape)
+    eps_add = torch.zeros(shape, dtype=torch.float64, device=device)
+    zero = torch.zeros((), dtype=torch.float64, device=device)
+    poles = []
+    for de, tau in debye:
+        de, tau = bc(de), bc(tau)
+        v = tau > 0
+        den = 2.0 * tau + dt
+        k1 = (2.0 * tau - dt) / den
+        k2 = (2.0 * EPS_0 * de * dt) / den
+        poles.append(torch.stack([torch.where(v, k1, zero), torch.where(v, k2, zero),
+                                  torch.where(v, (1.0 + k1) / 2.0, zero), torch.zeros_like(k1)], -1))
+        eps_add = torch.where(v, eps_add + k2 / 2.0, eps_add)
+    for de, w0, dl in lorentz:
+        de, w0, d = bc(de), bc(w0), bc(dl)
+        v = w0 > 0
+        w02, dt2 = w0 * w0, dt * dt
+        den = 4.0 + 2.0 * d * dt + w02 * dt2
+        k2 = 2.0 * EPS_0 * de * w02 * dt2 / den
+        k1 = (8.0 - 2.0 * w02 * dt2) / den
+        k3 = -(4.0 - 2.0 * d * dt + w02 * dt2) / den
+        poles.append(torch.stack([torch.where(v, k1, zero), torch.where(v, k2, zero),
+                                  torch.where(v, k3, zero), torch.zeros_like(k1)], -1))
+        eps_add = torch.where(v, eps_add + k2 / 2.0, eps_add)
+    ade = torch.stack(poles) if poles else torch.zeros((0,) + tuple(shape) + (4,), dtype=torch.float64,
+                                                       device=device)
+    return eps_add, ade
+
+
+def coefficient_tensors(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=None):
+    """2D: ade_coefficients + update_coefficients on the device (see
+    ade_tensors), in the kernel layout: coef (ny, nx, 4) float32 = (ca, cb,
+    dt/(eps_r eps0), 0) and ade (poles, ny, nx, 4) float32.  Only the (nx, ny)
+    FP64 maps cross the host link."""
+    import torch
+    eps_r = _f64(eps_r, device)
+    eps_add, ade = ade_tensors(dt, debye, lorentz, eps_r.shape, eps_r.device)
+    eps = eps_r * EPS_0
+    if ade.shape[0]:
+        eps = eps + eps_add
+    s = torch.broadcast_to(_f64(sigma_e, eps_r.device), eps_r.shape) * dt / (2.0 * eps)
+    ca, cb = (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s)
+    dteps = dt / (eps_r * EPS_0)
+    coef = torch.stack([ca.t(), cb.t(), dteps.t(), torch.zeros_like(ca).t()], -1).float().contiguous()
+    return coef, ade.transpose(1, 2).float().contiguous()
+
+
+def coefficient_tensors_3d(eps_r, sigma_e, mu_r, sigma_m, dt: float, debye=(), lorentz=(), device=None):
+    """3D (fdtd_3d_batched.py:281-296 with the ADE eps): coef (nz, ny, nx, 4)
+    float32 = (da, db, ca, cb) and ade (poles, nz, ny, nx, 4) float32 from
+    (nx, ny, nz) FP64 maps, on the device with the host formulas' operation order."""
+    import torch
+    eps_r = _f64(eps_r, device)
+    dev, shp = eps_r.device, eps_r.shape
+    bc = lambda a: torch.broadcast_to(_f64(a, dev), shp)
+    eps_add, ade = ade_tensors(dt, debye, lorentz, shp, dev)
+    eps = eps_r * EPS_0 + eps_add
+    mu = bc(mu_r) * MU_0
+    se = bc(sigma_e) * dt / (2.0 * eps)
+    sm = bc(sigma_m) * dt / (2.0 * mu)
+    ca, cb = (1.0 - se) / (1.0 + se), (dt / eps) / (1.0 + se)
+    da, db = (1.0 - sm) / (1.0 + sm), (dt / mu) / (1.0 + sm)
+    coef = torch.stack([da, db, ca, cb], -1).permute(2, 1, 0, 3).float().contiguous()
+    return coef, ade.permute(0, 3, 2, 1, 4).float().contiguous()
+
+
 def dft_twiddles(frequencies, nsteps: int, dt: float) -> np.ndarray:
     """(F, T, 2) float32: (cos(w n dt) dt, -sin(w n dt) dt), the running-DFT
     weights of dft.py:75-90, evaluated in FP64 (no FP32 phase accumulation)."""
@@ -96,4 +173,5 @@ def dft_twiddles(frequencies, nsteps: int, dt: float) -> np.ndarray:
 
 
 __all__ = ["gaussian_derivative", "modulated_gaussian", "cpml_profile", "ade_coefficients",
-           "update_coefficients", "dft_twiddles", "C_0", "EPS_0", "MU_0"]
+           "update_coefficients", "ade_tensors", "coefficient_tensors", "coefficient_tensors_3d", "dft_twiddles",
+           "C_0", "EPS_0", "MU_0"]

@@ -165,9 +165,9 @@ class BatchedFDTD2D:
         dt = self.dt
         f32 = dict(dtype=torch.float32, device=dev)
         to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
-        coef, ade = self._coef_maps(self._eps_r, self._sigma_e, self._debye, self._lorentz)
-        self._coef = to_dev(coef)
-        self._ade_coef = to_dev(ade) if ade.shape[0] else None
+        coef, ade = self._coef_tensors(self._eps_r, self._sigma_e, self._debye, self._lorentz)
+        self._coef = coef
+        self._ade_coef = ade if ade.shape[0] else None
         b, c = physics.cpml_profile(n, self.dx, dt, self.cpml_R0, self.cpml_order)
         self._cpml_b, self._cpml_c = to_dev(b if n else np.zeros(1)), to_dev(c if n else np.zeros(1))
         w = (self._waveform_override if self._waveform_override is not None
@@ -329,23 +329,18 @@ class BatchedFDTD2D:
                 t.zero_()
         check(lib().ceep2d_plan_reset(self._plan), "ceep2d_plan_reset")
 
-    def _coef_maps(self, eps_r, sigma_e, debye=(), lorentz=()):
-        """Host FP64 -> (ny, nx, 4) float32 (ca, cb, dt/(eps_r eps0), 0) and
-        (poles, ny, nx, 4) ADE coefficients, in the kernel's (y, x) order."""
-        nx, ny, dt = self.nx, self.ny, self.dt
-        eps_add, ade = physics.ade_coefficients(dt, debye, lorentz, (nx, ny))
-        ca, cb = physics.update_coefficients(eps_r, sigma_e, dt, eps_add if ade.shape[0] else None)
-        dteps = dt / (np.asarray(eps_r, np.float64) * EPS_0)   # E-CPML scale, fdtd_2d_batched.py:348
-        coef = np.stack([ca.T, cb.T, dteps.T, np.zeros((ny, nx))], axis=-1).astype(np.float32)
-        return coef, ade.transpose(0, 2, 1, 3).astype(np.float32)
+    def _coef_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
+        """(nx, ny) FP64 maps -> device (ny, nx, 4) float32 (ca, cb, dt/(eps_r eps0), 0)
+        and (poles, ny, nx, 4) ADE coefficients, in the kernel's (y, x) order;
+        FP64 arithmetic on the device, bit-identical to the host formulas
+        (fdtd_2d_batched.py:151-167, dispersive.py:240-339)."""
+        return physics.coefficient_tensors(eps_r, sigma_e, self.dt, debye, lorentz, self.device)
 
     def material_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
         """Device tensors (coef, ade_coef) for the given (nx, ny) maps in this
         solver's layout, for ``load_material_tensors``."""
-        coef, ade = self._coef_maps(eps_r, sigma_e, debye, lorentz)
-        dev = self.device
-        return (torch.as_tensor(np.ascontiguousarray(coef)).to(dev),
-                torch.as_tensor(np.ascontiguousarray(ade)).to(dev) if ade.shape[0] else None)
+        coef, ade = self._coef_tensors(eps_r, sigma_e, debye, lorentz)
+        return coef, (ade if ade.shape[0] else None)
 
     def load_material_tensors(self, mats) -> None:
         """Device-to-device copy of precomputed material tensors into the plan's
@@ -364,9 +359,9 @@ class BatchedFDTD2D:
         poles on a built solver."""
         if not self._built:
             return
-        coef, ade = self._coef_maps(self._eps_r, self._sigma_e, self._debye, self._lorentz)
+        coef, ade = self._coef_tensors(self._eps_r, self._sigma_e, self._debye, self._lorentz)
         if ade.shape[0] != (0 if self._ade_coef is None else self._ade_coef.shape[0]):
             raise ValueError("the number of ADE poles cannot change after the first run()")
-        self._coef.copy_(torch.as_tensor(coef))
+        self._coef.copy_(coef)
         if ade.shape[0]:
-            self._ade_coef.copy_(torch.as_tensor(ade))
+            self._ade_coef.copy_(ade)

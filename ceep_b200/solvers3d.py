@@ -126,17 +126,11 @@ class BatchedFDTD3D:
 
     # -- build ---------------------------------------------------------------
     def _coef_maps(self):
-        dt = self.dt
-        shp = (self.nx, self.ny, self.nz)
-        eps_add, ade = physics.ade_coefficients(dt, self._debye, self._lorentz, shp)
-        eps = self._eps_r * EPS_0 + eps_add
-        mu = self._mu_r * MU_0
-        se = self._sigma_e * dt / (2.0 * eps)
-        sm = self._sigma_m * dt / (2.0 * mu)
-        ca, cb = (1.0 - se) / (1.0 + se), (dt / eps) / (1.0 + se)            # fdtd_3d_batched.py:287-290
-        da, db = (1.0 - sm) / (1.0 + sm), (dt / mu) / (1.0 + sm)
-        coef = np.stack([da, db, ca, cb], -1).transpose(2, 1, 0, 3).astype(np.float32)   # (z, y, x, 4)
-        return coef, ade.transpose(0, 3, 2, 1, 4).astype(np.float32)
+        """Device (nz, ny, nx, 4) float32 (da, db, ca, cb) and (poles, nz, ny,
+        nx, 4) ADE coefficients (fdtd_3d_batched.py:281-296), computed in FP64
+        on the device with the host formulas (bit-identical)."""
+        return physics.coefficient_tensors_3d(self._eps_r, self._sigma_e, self._mu_r, self._sigma_m, self.dt,
+                                              self._debye, self._lorentz, self.device)
 
     def _build(self):
         dev = self.device
@@ -151,8 +145,8 @@ class BatchedFDTD3D:
         f32 = dict(dtype=torch.float32, device=dev)
         to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
         coef, ade = self._coef_maps()
-        self._coef = to_dev(coef)
-        self._ade_coef = to_dev(ade) if ade.shape[0] else None
+        self._coef = coef
+        self._ade_coef = ade if ade.shape[0] else None
         b, c = physics.cpml_profile(n, self.dx, self.dt)
         self._cpml_b, self._cpml_c = to_dev(b if n else np.zeros(1)), to_dev(c if n else np.zeros(1))
         w = (self._waveform_override if self._waveform_override is not None
@@ -257,9 +251,7 @@ class BatchedFDTD3D:
             coef, ade = self._coef_maps()
         finally:
             self._eps_r, self._sigma_e, self._debye, self._lorentz = saved
-        dev = self.device
-        return (torch.as_tensor(np.ascontiguousarray(coef)).to(dev),
-                torch.as_tensor(np.ascontiguousarray(ade)).to(dev) if ade.shape[0] else None)
+        return coef, (ade if ade.shape[0] else None)
 
     def load_material_tensors(self, mats) -> None:
         if not self._built:
@@ -275,9 +267,9 @@ class BatchedFDTD3D:
         if not self._built:
             return
         coef, ade = self._coef_maps()
-        self._coef.copy_(torch.as_tensor(coef))
+        self._coef.copy_(coef)
         if ade.shape[0]:
-            self._ade_coef.copy_(torch.as_tensor(ade))
+            self._ade_coef.copy_(ade)
 
     def compute_energy(self) -> float:
         """fdtd_3d_batched.py:987-1011 (sums in FP64 on the device)."""

@@ -26,13 +26,30 @@ def _stream(device):
     return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
+_TWIDDLES = {}  # (frequencies, T, dt, device) -> device (F, T, 2) float32; a few entries
+
+
+def _twiddles(frequencies, T: int, dt: float, device) -> torch.Tensor:
+    """The running-DFT weights on the device, built once per (frequencies, T,
+    dt): repeated S computations of a dataset reuse them."""
+    f = np.ascontiguousarray(np.asarray(frequencies, np.float64))
+    key = (f.tobytes(), int(T), float(dt), str(device))
+    tw = _TWIDDLES.get(key)
+    if tw is None:
+        if len(_TWIDDLES) >= 8:
+            _TWIDDLES.pop(next(iter(_TWIDDLES)))
+        tw = torch.as_tensor(physics.dft_twiddles(f, T, dt)).to(device)
+        _TWIDDLES[key] = tw
+    return tw
+
+
 def dft(series: torch.Tensor, frequencies: Sequence[float], dt: float) -> torch.Tensor:
     """series (ntx, nprobe, T) float32 CUDA tensor -> (F, nprobe, ntx) complex64."""
     if not series.is_cuda:
         raise ValueError("series must be a CUDA tensor")
     series = series.contiguous().float()
     B, P, T = series.shape
-    tw = torch.as_tensor(physics.dft_twiddles(frequencies, T, dt)).to(series.device)
+    tw = _twiddles(frequencies, T, dt, series.device)
     out = torch.empty((len(frequencies), P, B, 2), dtype=torch.float32, device=series.device)
     check(lib().ceep_dft(series.data_ptr(), tw.data_ptr(), out.data_ptr(), B, P, T, len(frequencies),
                          _stream(series.device)), "ceep_dft")
