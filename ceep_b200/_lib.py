@@ -23,7 +23,7 @@ class Desc2D(C.Structure):
         ("nprobe", I32), ("nsteps", I32), ("n_debye", I32), ("n_lorentz", I32),
         ("db", C.c_float), ("inv_dx", C.c_float), ("dt", C.c_float),
         ("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hy", P * 2), ("psi_hx", P * 2),
-        ("psi_ezx", P), ("psi_ezy", P), ("j", P), ("j_prev", P),
+        ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("j_prev", P * 2),
         ("coef", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
         ("src_xy", P), ("prb_xy", P), ("row_flags", P), ("waveform", P), ("probes", P),
         ("status", P), ("rows_per_block", I32),

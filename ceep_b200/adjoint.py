@@ -97,9 +97,9 @@ class Adjoint2D:
         s = self.s
         cur = s._cur()
         st = {"ez": s._ez[cur], "hx": s._hx[cur], "hy": s._hy[cur], "psi_hy": s._psi_hy[cur],
-              "psi_hx": s._psi_hx[cur], "psi_ezx": s._psi_ezx, "psi_ezy": s._psi_ezy}
+              "psi_hx": s._psi_hx[cur], "psi_ezx": s._psi_ezx[cur], "psi_ezy": s._psi_ezy[cur]}
         if s._j is not None:
-            st["j"] = s._j
+            st["j"] = s._j[cur]
         return st
 
     def forward(self) -> torch.Tensor:
@@ -127,9 +127,9 @@ class Adjoint2D:
         ck = self._ckpt[a]
         s._ez[0].copy_(ck["ez"]); s._hx[0].copy_(ck["hx"]); s._hy[0].copy_(ck["hy"])
         s._psi_hy[0].copy_(ck["psi_hy"]); s._psi_hx[0].copy_(ck["psi_hx"])
-        s._psi_ezx.copy_(ck["psi_ezx"]); s._psi_ezy.copy_(ck["psi_ezy"])
+        s._psi_ezx[0].copy_(ck["psi_ezx"]); s._psi_ezy[0].copy_(ck["psi_ezy"])
         if "j" in ck:
-            s._j.copy_(ck["j"])
+            s._j[0].copy_(ck["j"])
         check(lib().ceep2d_plan_set_current_buffer(s._plan, 0), "ceep2d_plan_set_current_buffer")
 
     def _save_segment(self, a, b):
@@ -141,13 +141,13 @@ class Adjoint2D:
         if getattr(self, "_seg", None) is None:
             # allocated once: the recompute graphs are keyed on these addresses
             seg_ez = torch.empty((slots, G, s.ny, s.nx, W), dtype=torch.float32, device=s.device)
-            seg_j = (torch.zeros((slots,) + tuple(s._j.shape), dtype=torch.float32, device=s.device)
+            seg_j = (torch.zeros((slots,) + tuple(s._j[0].shape), dtype=torch.float32, device=s.device)
                      if s._j is not None else None)
             self._seg = (seg_ez, seg_j)
         seg_ez, seg_j = self._seg
         seg_ez[0].copy_(s._ez[0])
         if seg_j is not None:
-            seg_j[0].copy_(s._j)
+            seg_j[0].copy_(s._j[0])
         stream = torch.cuda.current_stream(s.device)
         check(lib().ceep2d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
                                          seg_ez.data_ptr(), _ptr(seg_j), a), "ceep2d_plan_run_save")
@@ -163,8 +163,8 @@ class Adjoint2D:
         f32 = dict(dtype=torch.float32, device=dev)
         pair = lambda t: [torch.zeros_like(t), torch.zeros_like(t)] if t is not None else [None, None]
         adj = {"ez": pair(s._ez[0]), "hx": pair(s._hx[0]), "hy": pair(s._hy[0]), "psi_hx": pair(s._psi_hx[0]),
-               "psi_hy": pair(s._psi_hy[0]), "psi_ezx": pair(s._psi_ezx), "psi_ezy": pair(s._psi_ezy),
-               "j": pair(s._j)}
+               "psi_hy": pair(s._psi_hy[0]), "psi_ezx": pair(s._psi_ezx[0]), "psi_ezy": pair(s._psi_ezy[0]),
+               "j": pair(s._j[0] if s._j is not None else None)}
         nd = len(s._debye)
         kp = grad_width(nd)
         grad = torch.zeros((G, s.ny, s.nx, kp), dtype=torch.float64, device=dev)

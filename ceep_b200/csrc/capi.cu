@@ -67,11 +67,12 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   if (d->nsteps < 1 || d->nprobe < 0) return fail(CEEP_ERR_INVALID, "nsteps/nprobe");
   for (int k = 0; k < 2; ++k)
     if (!d->ez[k] || !d->hx[k] || !d->hy[k]) return fail(CEEP_ERR_INVALID, "null field buffer");
-  if (n > 0 && (!d->psi_hx[0] || !d->psi_hx[1] || !d->psi_hy[0] || !d->psi_hy[1] || !d->psi_ezx ||
-                !d->psi_ezy || !d->cpml_b || !d->cpml_c))
-    return fail(CEEP_ERR_INVALID, "null CPML buffer");
-  if (d->n_debye + d->n_lorentz > 0 && (!d->j || !d->ade_coef || (d->n_lorentz && !d->j_prev)))
-    return fail(CEEP_ERR_INVALID, "null ADE buffer");
+  for (int k = 0; k < 2; ++k) {
+    if (n > 0 && (!d->psi_hx[k] || !d->psi_hy[k] || !d->psi_ezx[k] || !d->psi_ezy[k] || !d->cpml_b || !d->cpml_c))
+      return fail(CEEP_ERR_INVALID, "null CPML buffer");
+    if (d->n_debye + d->n_lorentz > 0 && (!d->j[k] || !d->ade_coef || (d->n_lorentz && !d->j_prev[k])))
+      return fail(CEEP_ERR_INVALID, "null ADE buffer");
+  }
   if (!d->coef || !d->src_xy || !d->row_flags || !d->waveform || (d->nprobe && (!d->prb_xy || !d->probes)))
     return fail(CEEP_ERR_INVALID, "null coefficient/source/probe buffer");
 
@@ -98,11 +99,11 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
     p.hy[k] = reinterpret_cast<float4*>(d->hy[k]);
     p.psi_hy[k] = reinterpret_cast<float4*>(d->psi_hy[k]);
     p.psi_hx[k] = reinterpret_cast<float4*>(d->psi_hx[k]);
+    p.psi_ezx[k] = reinterpret_cast<float4*>(d->psi_ezx[k]);
+    p.psi_ezy[k] = reinterpret_cast<float4*>(d->psi_ezy[k]);
+    p.j[k] = reinterpret_cast<float4*>(d->j[k]);
+    p.j_prev[k] = reinterpret_cast<float4*>(d->j_prev[k]);
   }
-  p.psi_ezx = reinterpret_cast<float4*>(d->psi_ezx);
-  p.psi_ezy = reinterpret_cast<float4*>(d->psi_ezy);
-  p.j = reinterpret_cast<float4*>(d->j);
-  p.j_prev = reinterpret_cast<float4*>(d->j_prev);
   p.coef = d->coef; p.ade_coef = d->ade_coef;
   p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
   p.src_xy = d->src_xy; p.prb_xy = d->prb_xy; p.row_flags = d->row_flags;

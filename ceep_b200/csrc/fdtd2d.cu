@@ -30,10 +30,9 @@
 // upward, one float4 each, carrying Hx(x, y-1) in registers; every operand
 // they read comes from shared memory, every result goes straight to HBM with
 // coalesced 16-byte stores.  Hy(x-1, y) is recomputed from the staged Ez halo
-// instead of being exchanged.  Fields and the H-psi arrays are ping-pong
-// buffered (read [p], write [p^1]) so halo recomputes never race with the
-// owner's write; E-psi and ADE currents are read once per launch by their
-// owner's copy and written back in place.
+// instead of being exchanged.  Every state array (fields, psi, ADE currents)
+// is ping-pong buffered (read [p], write [p^1]), so a block may read any
+// neighbour's old values while the neighbour writes its new ones.
 //
 // Every mbarrier wait is bounded in time; on expiry the block records
 // CEEP_ERR_TIMEOUT in the status word, lets its copies in flight land, and
@@ -162,12 +161,12 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   const float4* hy = p.hy[par] + gf;
   const float4* coef = reinterpret_cast<const float4*>(p.coef);
   const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
-  const float4* J = p.j + (size_t)g * p.gs_j;
-  const float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
+  const float4* J = p.j[par] + (size_t)g * p.gs_j;
+  const float4* Jp = p.j_prev[par] + (size_t)g * p.gs_jp;
   const float4* psi_hx = p.psi_hx[par] + (size_t)g * p.gs_psi_y;
   const float4* psi_hy = p.psi_hy[par] + (size_t)g * p.gs_psi_x;
-  const float4* psi_ezx = p.psi_ezx + (size_t)g * p.gs_psi_x;
-  const float4* psi_ezy = p.psi_ezy + (size_t)g * p.gs_psi_y;
+  const float4* psi_ezx = p.psi_ezx[par] + (size_t)g * p.gs_psi_x;
+  const float4* psi_ezy = p.psi_ezy[par] + (size_t)g * p.gs_psi_y;
   const size_t plane = (size_t)nx * ny;
   const int xa = x0 > 0 ? x0 - 1 : 0;                  // first halo cell
   const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;  // end of the Ez slice
@@ -250,10 +249,10 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   float4* hyw = p.hy[par ^ 1] + gf;
   float4* psi_hx_out = p.psi_hx[par ^ 1] + (size_t)g * p.gs_psi_y;
   float4* psi_hy_out = p.psi_hy[par ^ 1] + (size_t)g * p.gs_psi_x;
-  float4* psi_ezx = p.psi_ezx + (size_t)g * p.gs_psi_x;
-  float4* psi_ezy = p.psi_ezy + (size_t)g * p.gs_psi_y;
-  float4* J = p.j + (size_t)g * p.gs_j;
-  float4* Jp = p.j_prev + (size_t)g * p.gs_jp;
+  float4* psi_ezx = p.psi_ezx[par ^ 1] + (size_t)g * p.gs_psi_x;
+  float4* psi_ezy = p.psi_ezy[par ^ 1] + (size_t)g * p.gs_psi_y;
+  float4* J = p.j[par ^ 1] + (size_t)g * p.gs_j;
+  float4* Jp = p.j_prev[par ^ 1] + (size_t)g * p.gs_jp;
   const size_t plane = (size_t)nx * ny;
   const int lane_g = g * L + lo;  // float4 lane across all groups (tx = 4*lane_g + c)
   // x-strip membership of this cell (H: Hy at x and x-1; E: Ez at x)

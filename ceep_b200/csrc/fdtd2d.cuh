@@ -22,10 +22,10 @@ struct Fdtd2dParams {
   float4* hy[2];
   float4* psi_hy[2];
   float4* psi_hx[2];
-  float4* psi_ezx;
-  float4* psi_ezy;
-  float4* j;
-  float4* j_prev;
+  float4* psi_ezx[2];
+  float4* psi_ezy[2];
+  float4* j[2];
+  float4* j_prev[2];
   const float* coef;      // (ny, nx) float4: ca, cb, dt/(eps_r eps0), 0
   const float* ade_coef;  // (poles, ny, nx) float4
   const float* cpml_b;

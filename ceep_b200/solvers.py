@@ -180,11 +180,11 @@ class BatchedFDTD2D:
         nn = max(n, 1)
         self._psi_hy = [torch.zeros((G, ny, 2 * nn, W), **f32) for _ in range(2)]
         self._psi_hx = [torch.zeros((G, 2 * nn, nx, W), **f32) for _ in range(2)]
-        self._psi_ezx = torch.zeros((G, ny, 2 * nn, W), **f32)
-        self._psi_ezy = torch.zeros((G, 2 * nn, nx, W), **f32)
+        self._psi_ezx = [torch.zeros((G, ny, 2 * nn, W), **f32) for _ in range(2)]
+        self._psi_ezy = [torch.zeros((G, 2 * nn, nx, W), **f32) for _ in range(2)]
         nd, nl = len(self._debye), len(self._lorentz)
-        self._j = torch.zeros((G, nd + nl, ny, nx, W), **f32) if nd + nl else None
-        self._j_prev = torch.zeros((G, nl, ny, nx, W), **f32) if nl else None
+        self._j = [torch.zeros((G, nd + nl, ny, nx, W), **f32) for _ in range(2)] if nd + nl else None
+        self._j_prev = [torch.zeros((G, nl, ny, nx, W), **f32) for _ in range(2)] if nl else None
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
         P = len(self.probe_positions)
         self._src = to_dev(np.array(self.source_positions, np.int32).reshape(-1, 2), torch.int32)
@@ -204,8 +204,10 @@ class BatchedFDTD2D:
         for k in range(2):
             d.ez[k], d.hx[k], d.hy[k] = _ptr(self._ez[k]), _ptr(self._hx[k]), _ptr(self._hy[k])
             d.psi_hy[k], d.psi_hx[k] = _ptr(self._psi_hy[k]), _ptr(self._psi_hx[k])
-        d.psi_ezx, d.psi_ezy = _ptr(self._psi_ezx), _ptr(self._psi_ezy)
-        d.j, d.j_prev = _ptr(self._j), _ptr(self._j_prev)
+        for k in range(2):
+            d.psi_ezx[k], d.psi_ezy[k] = _ptr(self._psi_ezx[k]), _ptr(self._psi_ezy[k])
+            d.j[k] = _ptr(self._j[k]) if self._j is not None else None
+            d.j_prev[k] = _ptr(self._j_prev[k]) if self._j_prev is not None else None
         d.coef, d.ade_coef = _ptr(self._coef), _ptr(self._ade_coef)
         d.cpml_b, d.cpml_c = _ptr(self._cpml_b), _ptr(self._cpml_c)
         d.src_xy, d.prb_xy, d.row_flags = _ptr(self._src), _ptr(self._prb), _ptr(self._flags)
@@ -323,8 +325,8 @@ class BatchedFDTD2D:
         solver be reused for a new phantom without reallocating)."""
         if not self._built:
             return
-        for t in (self._ez + self._hx + self._hy + self._psi_hy + self._psi_hx +
-                  [self._psi_ezx, self._psi_ezy, self._j, self._j_prev, self.probe_data]):
+        for t in (self._ez + self._hx + self._hy + self._psi_hy + self._psi_hx + self._psi_ezx + self._psi_ezy +
+                  (self._j or []) + (self._j_prev or []) + [self.probe_data]):
             if t is not None:
                 t.zero_()
         check(lib().ceep2d_plan_reset(self._plan), "ceep2d_plan_reset")

@@ -69,12 +69,12 @@ typedef struct ceep2d_desc {
   /* H-CPML psi, ping-pong: x strips (G, ny, 2n, .), y strips (G, 2n, nx, .) */
   float* psi_hy[2];
   float* psi_hx[2];
-  /* E-CPML psi, in place, same shapes as above                               */
-  float* psi_ezx;
-  float* psi_ezy;
-  /* ADE currents, in place: (G, poles, ny, nx, .); Lorentz keeps J^{n-1}    */
-  float* j;                /* n_debye + n_lorentz planes                     */
-  float* j_prev;           /* n_lorentz planes                               */
+  /* E-CPML psi, ping-pong, same shapes as above                             */
+  float* psi_ezx[2];
+  float* psi_ezy[2];
+  /* ADE currents, ping-pong: (G, poles, ny, nx, .); Lorentz keeps J^{n-1}   */
+  float* j[2];             /* n_debye + n_lorentz planes                     */
+  float* j_prev[2];        /* n_lorentz planes                               */
   const float* coef;       /* (ny, nx, 4): ca, cb, dt/(eps_r eps0), 0        */
   const float* ade_coef;   /* (poles, ny, nx, 4): Debye k1,k2,gamma ; Lorentz k1,k2,k3 */
   const float* cpml_b;     /* (n)                                            */

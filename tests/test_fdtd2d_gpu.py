@@ -44,7 +44,7 @@ def test_small_against_reference_fp32_and_fp64(cuda_device):
     psi_hy = s._psi_hy[cur][0, :, :, :3].permute(2, 1, 0).cpu().numpy()   # (B, 2n, ny)
     assert rel_l2(psi_hy[:, :n], g64["psi_hxy_lo"]) < TOL
     assert rel_l2(psi_hy[:, n:2 * n - 1], g64["psi_hxy_hi"][:, :n - 1]) < TOL
-    psi_ezy = s._psi_ezy[0, :, :, :3].permute(2, 1, 0).cpu().numpy()        # (B, nx, 2n)
+    psi_ezy = s._psi_ezy[cur][0, :, :, :3].permute(2, 1, 0).cpu().numpy()   # (B, nx, 2n)
     assert rel_l2(psi_ezy[:, :, :n], g64["psi_ezy_lo"]) < TOL
     assert rel_l2(psi_ezy[:, :, n:], g64["psi_ezy_hi"]) < TOL
 
