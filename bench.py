@@ -213,6 +213,9 @@ def run_ours(args, w):
     torch.cuda.set_device(device)
     K, W = args.steps, args.warmup
     solver, pos, freqs, phantoms, mats = build_inputs(w, K + W, device, seed0=1000 + 97 * rank)
+    tblock = args.temporal_block if w.get("dim", 2) == 2 else 1
+    if tblock != 1:
+        solver.set_temporal_block(tblock)
     solver._build()
     stream = torch.cuda.current_stream(device)
     das_ws = torch.empty(1 << 20, dtype=torch.uint8, device=device)
@@ -247,7 +250,10 @@ def run_ours(args, w):
     cell_steps = w["nx"] * w["ny"] * w.get("nz", 1) * w["steps"] * w["ntx"]
     value = world * K * cell_steps / (total_ms * 1e-3) / 1e9
 
-    # -- dominant kernel alone: the fused step, per-launch time over full loops
+    # -- dominant kernel alone: the fused step kernel (one or two steps per
+    # launch), per-launch time over full loops; each launch reads and writes
+    # every state word once, so its algorithmic bytes are one step's formula
+    launches = solver.launches(w["steps"]) if w.get("dim", 2) == 2 else w["steps"]
     per_launch = []
     for k in range(3):
         flush.zero_()
@@ -257,7 +263,7 @@ def run_ours(args, w):
         solver.advance(0, w["steps"], stream=stream)
         b.record(stream)
         torch.cuda.synchronize()
-        per_launch.append(a.elapsed_time(b) / w["steps"])
+        per_launch.append(a.elapsed_time(b) / launches)
     launch_ms = float(np.median(per_launch))
     bytes_step = algorithmic_bytes_per_step(w, n_debye)
     peak, peak_src = hbm_peak()
@@ -272,7 +278,7 @@ def run_ours(args, w):
     # -- end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e and w.get("dim", 2) == 2:
-        e2e = run_e2e(w, phantoms[:min(K, 3)], pos, freqs, device)
+        e2e = run_e2e(w, phantoms[:min(K, 3)], pos, freqs, device, tblock)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and w.get("dim", 2) == 2:
@@ -297,11 +303,13 @@ def run_ours(args, w):
                    "sample": "fused time loop + DFT->S + DAS image"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic, "peak_source": peak_src,
-                     "kernel": ("fdtd2d_step_kernel" if w.get("dim", 2) == 2 else
+                     "kernel": (("fdtd2d_step2_kernel (two steps per launch)" if tblock == 2 else
+                                 "fdtd2d_step_kernel") if w.get("dim", 2) == 2 else
                                 "fdtd3d step: h + e + source/probe launches"),
+                     "steps_per_launch": tblock,
                      "launch_ms": round(launch_ms, 5),
                      "algorithmic_bytes_per_launch": bytes_step},
-        "gpu_launches": K * (w["steps"] * (1 if w.get("dim", 2) == 2 else 3) + 3),
+        "gpu_launches": K * ((launches if w.get("dim", 2) == 2 else 3 * w["steps"]) + 3),
         "clocks": clk.summary(),
     }
     if e2e:
@@ -326,7 +334,7 @@ class _HostMaps:
         return self.dispersion
 
 
-def run_e2e(w, phantoms, pos, freqs, device):
+def run_e2e(w, phantoms, pos, freqs, device, tblock=1):
     """Public-API path per sample: host phantom maps -> set_phantom ->
     update_materials (H2D of the FP64 maps) -> run() (D2H of every series) ->
     s_matrix() (D2H) -> DAS image (D2H)."""
@@ -334,7 +342,7 @@ def run_e2e(w, phantoms, pos, freqs, device):
     from ceep_b200 import BatchedFDTD2D
     from ceep_b200.spectral import das_image
     solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
-                           frequencies=freqs, device=str(device))
+                           frequencies=freqs, device=str(device), temporal_block=tblock)
     phantoms = [None if ph is None else _HostMaps(ph) for ph in phantoms]
     if phantoms[0] is not None:
         solver.set_phantom(phantoms[0])
@@ -647,6 +655,8 @@ def run_profile(args, w):
         w = dict(w, nx=128, ny=128, nz=128, ring=50)
     solver, pos, freqs, _, mats = build_inputs(w, 1, device)
     solver.use_graph = False
+    if w.get("dim", 2) == 2 and args.temporal_block != 1:
+        solver.set_temporal_block(args.temporal_block)
     solver.load_material_tensors(mats[0])
     stream = torch.cuda.current_stream(device)
     solver.advance(0, min(args.profile, w["steps"]), stream=stream)
@@ -671,6 +681,8 @@ def main():
     ap.add_argument("--pack-sample", type=int, default=32)
     ap.add_argument("--small", action="store_true", help="with --profile: a smaller 3D grid")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--temporal-block", type=int, default=2, choices=(1, 2),
+                    help="2D steps per kernel launch (2 = temporal block of two)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--profile", type=int, default=0,

@@ -51,6 +51,9 @@ _SIGS = {
     "ceep2d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
     "ceep2d_plan_destroy": (C.c_int, [P]),
     "ceep2d_launches_per_step": (C.c_int, [P]),
+    "ceep2d_plan_set_temporal_block": (C.c_int, [P, C.c_int]),
+    "ceep2d_plan_temporal_block": (C.c_int, [P]),
+    "ceep2d_plan_launches": (I64, [P, I64]),
     "ceep2d_plan_current_buffer": (C.c_int, [P]),
     "ceep2d_plan_reset": (C.c_int, [P]),
     "ceep2d_desc_size": (I64, []),

@@ -39,9 +39,10 @@ extern "C" const char* ceep_last_error(void) { return g_err; }
 // --------------------------------------------------------------------------
 struct ceep2d_plan {
   ceep::Fdtd2dParams p;
-  int cur = 0;  // ping-pong buffer holding the current state
-  // captured step loops keyed by (step0, nsteps, starting buffer, save buffers, save base)
-  std::map<std::tuple<int64_t, int64_t, int, const void*, const void*, int64_t>, cudaGraphExec_t> graphs;
+  int cur = 0;       // ping-pong buffer holding the current state
+  int tblock = 1;    // steps per launch (1, or 2 with the temporal-block kernel)
+  // captured step loops keyed by (step0, nsteps, starting buffer, save buffers, save base, steps per launch)
+  std::map<std::tuple<int64_t, int64_t, int, const void*, const void*, int64_t, int>, cudaGraphExec_t> graphs;
 };
 
 extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
@@ -84,6 +85,7 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   p.nprobe = d->nprobe; p.nsteps = d->nsteps;
   p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
   p.rows = d->rows_per_block > 0 ? d->rows_per_block : 0;
+  p.rows_fixed = p.rows;
   p.db = d->db; p.db_dx = d->db * d->inv_dx; p.inv_dx = d->inv_dx; p.dt = d->dt;
   p.inv_dt = (float)(1.0 / (double)d->dt);
   const long long cells = (long long)d->nx * d->ny;
@@ -118,10 +120,19 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   return CEEP_OK;
 }
 
-static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
-  for (int64_t k = 0; k < nsteps; ++k) {
-    cudaError_t e = ceep::fdtd2d_launch_step(p, (int)(step0 + k), cur, s);
+// Launch steps [step0, step0 + nsteps): pairs through the two-step kernel when
+// tblock == 2, the rest one step at a time.  Every launch reads buffer `cur`
+// and writes the other.
+static int64_t launch_count(int64_t nsteps, int tblock) { return tblock == 2 ? (nsteps + 1) / 2 : nsteps; }
+
+static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, int tblock,
+                     cudaStream_t s) {
+  for (int64_t k = 0; k < nsteps;) {
+    const bool two = tblock == 2 && k + 1 < nsteps;
+    cudaError_t e = two ? ceep::fdtd2d_launch_step2(p, (int)(step0 + k), cur, s)
+                        : ceep::fdtd2d_launch_step(p, (int)(step0 + k), cur, s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd2d step launch");
+    k += two ? 2 : 1;
     cur ^= 1;
   }
   return CEEP_OK;
@@ -142,18 +153,19 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
   q.save_base = (int)save_base;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int cur = pl->cur;
+  const int cur_after = cur ^ (int)(launch_count(nsteps, pl->tblock) & 1);
   if (!use_graph || s == nullptr) {
-    int rc = run_steps(q, step0, nsteps, cur, s);
-    if (rc == CEEP_OK) pl->cur = cur ^ (int)(nsteps & 1);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, s);
+    if (rc == CEEP_OK) pl->cur = cur_after;
     return rc;
   }
-  auto key = std::make_tuple(step0, nsteps, cur, (const void*)save_ez, (const void*)q.save_j, save_base);
+  auto key = std::make_tuple(step0, nsteps, cur, (const void*)save_ez, (const void*)q.save_j, save_base, pl->tblock);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps(q, step0, nsteps, cur, s);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, s);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -165,7 +177,7 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
   }
   cudaError_t e = cudaGraphLaunch(it->second, s);
   if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
-  pl->cur = cur ^ (int)(nsteps & 1);
+  pl->cur = cur_after;
   return CEEP_OK;
 }
 
@@ -202,6 +214,19 @@ extern "C" int ceep2d_plan_destroy(ceep2d_plan* pl) {
 }
 
 extern "C" int ceep2d_launches_per_step(const ceep2d_plan* pl) { return pl ? 1 : 0; }
+
+extern "C" int ceep2d_plan_set_temporal_block(ceep2d_plan* pl, int steps) {
+  if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
+  if (steps != 1 && steps != 2) return fail(CEEP_ERR_INVALID, "temporal block of %d steps (1 or 2)", steps);
+  pl->tblock = steps;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_temporal_block(const ceep2d_plan* pl) { return pl ? pl->tblock : 0; }
+
+extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
+  return (!pl || nsteps < 0) ? 0 : launch_count(nsteps, pl->tblock);
+}
 
 // --------------------------------------------------------------------------
 // 3D plan

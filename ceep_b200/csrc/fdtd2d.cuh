@@ -14,6 +14,8 @@ struct Fdtd2dParams {
   int n_debye, n_lorentz;
   int rows;             // rows of the column segment one block walks
   int smem;             // dynamic shared memory per block
+  int rows2, smem2;     // the same for the two-step kernel
+  int rows_fixed;       // tile height the caller asked for (0 = chosen per kernel)
   float db, db_dx, inv_dx, dt, inv_dt;
   // per-group strides in float4
   long long gs_field, gs_psi_x, gs_psi_y, gs_j, gs_jp;
@@ -62,5 +64,9 @@ int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int
 cudaError_t fdtd2d_configure(Fdtd2dParams& p);
 // Launch one step reading buffer `par` and writing buffer `par ^ 1`.
 cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStream_t s);
+// Launch steps `step` and `step + 1` in one kernel (temporal block of two),
+// reading buffer `par` and writing buffer `par ^ 1` (and the adjoint's saved
+// Ez/J of both steps when the save pointers are set).
+cudaError_t fdtd2d_launch_step2(const Fdtd2dParams& p, int step, int par, cudaStream_t s);
 
 }  // namespace ceep

@@ -52,7 +52,7 @@ class BatchedFDTD2D:
                  frequency: float, delay_factor: float = 5.0, *, courant: Optional[float] = None,
                  cpml_R0: float = 1e-8, cpml_order: int = 3, waveform: Optional[np.ndarray] = None,
                  frequencies: Optional[Sequence[float]] = None, device: str = "cuda",
-                 rows_per_block: int = 0, use_graph: bool = True):
+                 rows_per_block: int = 0, use_graph: bool = True, temporal_block: int = 2):
         self.nx, self.ny = int(nx), int(ny)
         self.dx = self.dy = float(dx)
         self.total_steps = int(total_steps)
@@ -74,6 +74,7 @@ class BatchedFDTD2D:
         self.device = torch.device(device)
         self.rows_per_block = int(rows_per_block)
         self.use_graph = bool(use_graph)
+        self.temporal_block = int(temporal_block)   # steps per kernel launch (1 or 2)
         self._built = False
         self._plan = None
         self._validate()
@@ -218,6 +219,7 @@ class BatchedFDTD2D:
         plan = C.c_void_p()
         check(lib().ceep2d_plan_create(C.byref(d), C.byref(plan)), "ceep2d_plan_create")
         self._plan = plan
+        check(lib().ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
         self._built = True
 
     def __del__(self):
@@ -240,7 +242,25 @@ class BatchedFDTD2D:
         plan = C.c_void_p()
         check(lib().ceep2d_plan_create(C.byref(self._desc), C.byref(plan)), "ceep2d_plan_create")
         self._plan = plan
+        check(lib().ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
         self.reset()
+
+    def set_temporal_block(self, steps: int) -> None:
+        """Steps per kernel launch: 1, or 2 (two steps per launch, each state
+        word read and written once per pair; same arithmetic as 1)."""
+        if steps not in (1, 2):
+            raise ValueError("temporal block must be 1 or 2 steps")
+        self.temporal_block = int(steps)
+        if self._built:
+            check(lib().ceep2d_plan_set_temporal_block(self._plan, self.temporal_block),
+                  "ceep2d_plan_set_temporal_block")
+
+    def launches(self, nsteps: Optional[int] = None) -> int:
+        """Kernel launches that advancing `nsteps` steps (default: all) issues."""
+        nsteps = self.total_steps if nsteps is None else int(nsteps)
+        if not self._built:
+            return nsteps if self.temporal_block == 1 else (nsteps + 1) // 2
+        return int(lib().ceep2d_plan_launches(self._plan, nsteps))
 
     @property
     def plan_rows(self) -> int:

@@ -93,13 +93,22 @@ typedef struct ceep2d_plan ceep2d_plan;
 
 /* Validate the descriptor and build a plan (host memory only). */
 int ceep2d_plan_create(const ceep2d_desc* desc, ceep2d_plan** out);
-/* Advance `nsteps` steps starting at global step `step0` (buffer parity is
- * step0 & 1).  use_graph != 0 captures the launches once per (step0, nsteps)
- * and replays the CUDA graph on later calls. */
+/* Advance `nsteps` steps starting at global step `step0`.  use_graph != 0
+ * captures the launches once per (step0, nsteps) and replays the CUDA graph on
+ * later calls.  Every launch (one or two steps) reads the current ping-pong
+ * buffer and writes the other one. */
 int ceep2d_plan_run(ceep2d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
 int ceep2d_plan_destroy(ceep2d_plan* plan);
-/* Number of kernel launches one step issues. */
+/* Number of kernel launches one step issues with a temporal block of 1. */
 int ceep2d_launches_per_step(const ceep2d_plan* plan);
+/* Steps per launch: 1 (one fused step per launch), or 2 (temporal block of
+ * two: each state word is read once and written once per two steps; the
+ * same arithmetic, bit-identical results).  No counterpart in the reference.
+ * A new plan uses 1; the Python solver sets 2. */
+int ceep2d_plan_set_temporal_block(ceep2d_plan* plan, int steps);
+int ceep2d_plan_temporal_block(const ceep2d_plan* plan);
+/* Kernel launches a ceep2d_plan_run of `nsteps` steps issues. */
+int64_t ceep2d_plan_launches(const ceep2d_plan* plan, int64_t nsteps);
 /* Which ping-pong buffer (0 or 1) holds the current state; reset sets it to 0
  * (the caller zeroes the state buffers). */
 int ceep2d_plan_current_buffer(const ceep2d_plan* plan);
