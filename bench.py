@@ -269,7 +269,8 @@ def run_ours(args, w):
     peak, peak_src = hbm_peak()
     achieved = bytes_step / (launch_ms * 1e-3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"fdtd2d_step_{args.workload}.md")
+    kname = "fdtd2d_step2" if tblock == 2 else "fdtd2d_step"
+    tpath = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}.md")
     if os.path.exists(tpath):
         for line in open(tpath):
             if line.startswith("dram_bytes_per_launch"):
