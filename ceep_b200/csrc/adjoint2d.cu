@@ -478,36 +478,6 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
   if (k < nslots) release(k);  // the row above the segment
 }
 
-// Tile b of a gx x gy grid of column strips x row segments, in the order the
-// block scheduler should start them: the two edge columns (CPML x strips on
-// every row, the costliest tiles), then the first and last segments of the
-// other columns, then the rest.  A bijection of [0, gx*gy).
-CEEP_D void adj_tile(int b, int gx, int gy, int& bx, int& by) {
-  if (gx <= 2) {
-    bx = b % gx;
-    by = b / gx;
-    return;
-  }
-  if (b < 2 * gy) {
-    bx = (b & 1) ? gx - 1 : 0;
-    by = b >> 1;
-    return;
-  }
-  int r = b - 2 * gy;
-  const int ic = gx - 2;
-  if (gy <= 2) {
-    bx = 1 + r % ic;
-    by = r / ic;
-  } else if (r < 2 * ic) {
-    bx = 1 + (r >> 1);
-    by = (r & 1) ? gy - 1 : 0;
-  } else {
-    r -= 2 * ic;
-    bx = 1 + r % ic;
-    by = 1 + r / ic;
-  }
-}
-
 template <int L, int ND>
 __global__ void __launch_bounds__(kAdjConsumers + 32, 3)
     adjoint2d_step_kernel(const Adjoint2dParams a, int step, int par, const float4* __restrict__ ez_n,
@@ -520,7 +490,7 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, 3)
   uint64_t* empty = full + NS;
   const int nx = a.f.nx, ny = a.f.ny, n = a.f.n;
   int bx, by;
-  adj_tile(blockIdx.x, (nx + CX - 1) / CX, (ny + a.rows - 1) / a.rows, bx, by);
+  tile_costliest_first(blockIdx.x, (nx + CX - 1) / CX, (ny + a.rows - 1) / a.rows, bx, by);
   const int x0 = bx * CX, y0 = by * a.rows, g = blockIdx.y;
   const int y1 = min(y0 + a.rows, ny);
   const int rs = y0 > 0 ? y0 - 1 : 0;

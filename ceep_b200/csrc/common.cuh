@@ -51,6 +51,36 @@ CEEP_D void add_comp(float4& v, int i, float s) {
   if (i == 0) v.x += s; else if (i == 1) v.y += s; else if (i == 2) v.z += s; else v.w += s;
 }
 
+// Tile b of a gx x gy grid (columns x rows of tiles) in the order the block
+// scheduler should start them: the two edge columns (CPML x strips on every
+// row, the costliest tiles), then the first and last rows of tiles of the
+// other columns, then the rest.  A bijection of [0, gx*gy).
+CEEP_D void tile_costliest_first(int b, int gx, int gy, int& bx, int& by) {
+  if (gx <= 2) {
+    bx = b % gx;
+    by = b / gx;
+    return;
+  }
+  if (b < 2 * gy) {
+    bx = (b & 1) ? gx - 1 : 0;
+    by = b >> 1;
+    return;
+  }
+  int r = b - 2 * gy;
+  const int ic = gx - 2;
+  if (gy <= 2) {
+    bx = 1 + r % ic;
+    by = r / ic;
+  } else if (r < 2 * ic) {
+    bx = 1 + (r >> 1);
+    by = (r & 1) ? gy - 1 : 0;
+  } else {
+    r -= 2 * ic;
+    bx = 1 + r % ic;
+    by = 1 + r / ic;
+  }
+}
+
 // Streaming loads/stores.  Field state is read once and written once per
 // step, so the read-only path with an L1 hint is used for neighbours that
 // other threads of the same block also read.

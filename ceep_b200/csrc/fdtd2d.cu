@@ -798,6 +798,8 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   Exch2<L>* xr = reinterpret_cast<Exch2<L>*>(empty + kStages2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(xr + 2);
   const int ny = p.ny, n = p.n;
+  // row-major tile order: neighbouring tiles, which share halo rows and
+  // columns, run close together in time (their halos hit in L2)
   const int x0 = (int)blockIdx.x * (CX - 2) - 1;  // first thread column; outputs x0+1 .. x0+CX-2
   const int y0 = blockIdx.y * p.rows2, g = blockIdx.z;
   const int y1 = min(y0 + p.rows2, ny);
