@@ -182,6 +182,89 @@ __global__ void __launch_bounds__(1024) das_finish_kernel(const float2* __restri
 }
 
 // --------------------------------------------------------------------------
+// Frequency-domain DMAS (beamforming.py:259-313).  One block per pixel, one
+// thread per transmit/receive pair k = tx * N + rx (the reference's loop
+// order): the thread accumulates the delayed pair signal
+//   s_k = sum_f S[f, rx, tx] a_tx(f) a_rx(f),  a_n(f) = exp(-j k_f d_n),
+// with the antenna phasors of a chunk of frequencies built once per pixel in
+// shared memory (the DAS kernel's factorisation).  The block then forms the
+// ordered pair sum  sum_{k1<k2} s_k1 conj(s_k2) = sum_k s_k conj(R_k),
+// R_k = sum_{k'>k} s_k', from an inclusive suffix scan over k, and writes the
+// complex result; das_finish_kernel takes |.| and normalises.
+// --------------------------------------------------------------------------
+constexpr int kDmasMaxAnt = 32;  // N^2 <= 1024 pairs, one thread each
+constexpr int kDmasFreqChunk = 32;
+
+__global__ void __launch_bounds__(1024) dmas_kernel(const float2* __restrict__ S, const float* __restrict__ kf,
+                                                    const float* __restrict__ ant, int F, int N, int nyp, float px0,
+                                                    float py0, float pix, float2* __restrict__ out) {
+  extern __shared__ float2 dm_smem[];
+  float2* a = dm_smem;                          // (N, kDmasFreqChunk) phasors
+  float2* scan = dm_smem + N * kDmasFreqChunk;  // (blockDim.x) pair signals, then suffix sums
+  __shared__ float d[kDmasMaxAnt];
+  __shared__ float2 wsum[32];
+  const int pid = blockIdx.x, i = pid / nyp, j = pid % nyp;
+  const float px = px0 + i * pix, py = py0 + j * pix;
+  const int K = N * N, t = threadIdx.x;
+  if (t < N) d[t] = hypotf(px - ant[2 * t], py - ant[2 * t + 1]);
+  __syncthreads();
+  const int tx = t / N, rx = t % N;
+  float sx = 0.f, sy = 0.f;
+  for (int f0 = 0; f0 < F; f0 += kDmasFreqChunk) {
+    const int fc = min(kDmasFreqChunk, F - f0);
+    for (int e = t; e < N * fc; e += blockDim.x) {
+      const int nn = e / fc, ff = e % fc;
+      float sn, cs;
+      sincosf(-kf[f0 + ff] * d[nn], &sn, &cs);
+      a[nn * kDmasFreqChunk + ff] = make_float2(cs, sn);
+    }
+    __syncthreads();
+    if (t < K) {
+      for (int ff = 0; ff < fc; ++ff) {
+        const float2 v = __ldg(S + ((size_t)(f0 + ff) * N + rx) * N + tx);
+        const float2 at = a[tx * kDmasFreqChunk + ff], ar = a[rx * kDmasFreqChunk + ff];
+        const float ph_x = at.x * ar.x - at.y * ar.y, ph_y = at.x * ar.y + at.y * ar.x;
+        sx += v.x * ph_x - v.y * ph_y;
+        sy += v.x * ph_y + v.y * ph_x;
+      }
+    }
+    __syncthreads();
+  }
+  // inclusive suffix scan: scan[k] = sum_{k' >= k} s_k'
+  scan[t] = t < K ? make_float2(sx, sy) : make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int off = 1; off < K; off <<= 1) {
+    const float2 v = t + off < K ? scan[t + off] : make_float2(0.f, 0.f);
+    __syncthreads();
+    scan[t].x += v.x;
+    scan[t].y += v.y;
+    __syncthreads();
+  }
+  // s_k conj(R_k), R_k = scan[k + 1]
+  float ax = 0.f, ay = 0.f;
+  if (t + 1 < K) {
+    const float2 r = scan[t + 1];
+    ax = sx * r.x + sy * r.y;
+    ay = sy * r.x - sx * r.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+  if ((t & 31) == 0) wsum[t / 32] = make_float2(ax, ay);
+  __syncthreads();
+  if (t < 32) {
+    const int nw = blockDim.x / 32;
+    float2 v = t < nw ? wsum[t] : make_float2(0.f, 0.f);
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if (t == 0) out[pid] = v;
+  }
+}
+
+// --------------------------------------------------------------------------
 // Time-domain DAS (scripts/verify_dataset_with_das.py:37-103), one thread per
 // pixel.  The delay index is truncated like int() in FP64, so every rounding
 // matters: |v| is sqrt(fma(v1, v1, v0*v0)), the rounding sequence of
@@ -275,6 +358,33 @@ extern "C" int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
 #undef CEEP_DAS_LAUNCH
   if (e != cudaSuccess) return ceep::cuda_fail(e, "das_partial_kernel launch");
   ceep::das_finish_kernel<<<1, 1024, 0, st>>>(partial, chunks, npix, normalize, image);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "das_finish_kernel launch");
+}
+
+extern "C" int64_t ceep_dmas_workspace_bytes(int32_t nx_pix, int32_t ny_pix) {
+  return nx_pix > 0 && ny_pix > 0 ? (int64_t)nx_pix * ny_pix * (int64_t)sizeof(float2) : 0;
+}
+
+extern "C" int ceep_dmas(const float* s, const float* kfreq, const float* ant_xy, int32_t nfreq, int32_t nant,
+                         int32_t nx_pix, int32_t ny_pix, float px0, float py0, float pix, int normalize, void* work,
+                         float* image, void* stream) {
+  if (!s || !kfreq || !ant_xy || !work || !image) return fail(CEEP_ERR_INVALID, "ceep_dmas: null pointer");
+  if (nfreq < 1 || nant < 1 || nx_pix < 1 || ny_pix < 1)
+    return fail(CEEP_ERR_INVALID, "ceep_dmas: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix, ny_pix);
+  if (nant > ceep::kDmasMaxAnt)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_dmas: %d antennas (at most %d)", nant, ceep::kDmasMaxAnt);
+  const int npix = nx_pix * ny_pix;
+  const int K = nant * nant;
+  const int threads = ((K + 31) / 32) * 32;
+  const size_t smem = ((size_t)nant * ceep::kDmasFreqChunk + threads) * sizeof(float2);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float2* acc = static_cast<float2*>(work);
+  ceep::dmas_kernel<<<npix, threads, smem, st>>>(reinterpret_cast<const float2*>(s), kfreq, ant_xy, nfreq, nant,
+                                                 ny_pix, px0, py0, pix, acc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "dmas_kernel launch");
+  ceep::das_finish_kernel<<<1, 1024, 0, st>>>(acc, 1, npix, normalize, image);
   e = cudaGetLastError();
   return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "das_finish_kernel launch");
 }

@@ -3,9 +3,8 @@
 * ``dft``                  — S[f, rx, tx] from probe series (dft.py:55-90 over
                              every pair, s_params.py:77-79 layout)
 * ``MultistaticSParameters`` — the reference container (s_params.py:70-231)
-* ``ImagingRegion``, ``DelayAndSumBeamformer`` — beamforming.py:42-257 with the
-  DAS sum evaluated by the CUDA kernel (DMAS stays on the host: it is the
-  next row of the imaging side and not on the measured path)
+* ``ImagingRegion``, ``DelayAndSumBeamformer`` — beamforming.py:42-313 with the
+  DAS and DMAS sums evaluated by CUDA kernels
 * ``das_time``             — scripts/verify_dataset_with_das.py:37-103 on the device
 """
 from __future__ import annotations
@@ -96,10 +95,15 @@ class MultistaticSParameters:
                                       self.antenna_positions, self.background_subtracted)
 
     def subtract_background(self, background: "MultistaticSParameters") -> "MultistaticSParameters":
+        """s_params.py:202-231; with a device tensor on either side the
+        difference is formed on that device."""
         if not np.array_equal(self.frequencies, background.frequencies):
             raise ValueError("Frequency points must match")
-        return MultistaticSParameters(self.frequencies, self.s_matrix - background.s_matrix,
-                                      self.antenna_positions, True)
+        a, b = self.s_matrix, background.s_matrix
+        if isinstance(a, torch.Tensor) or isinstance(b, torch.Tensor):
+            dev = a.device if isinstance(a, torch.Tensor) else b.device
+            a, b = torch.as_tensor(a).to(dev), torch.as_tensor(b).to(dev)
+        return MultistaticSParameters(self.frequencies, a - b, self.antenna_positions, True)
 
 
 @dataclass
@@ -143,8 +147,29 @@ def das_image(S: torch.Tensor, frequencies: Sequence[float], antenna_xy_m: np.nd
     return img
 
 
+def dmas_image(S: torch.Tensor, frequencies: Sequence[float], antenna_xy_m: np.ndarray, nx_pix: int, ny_pix: int,
+               px0: float, py0: float, pix: float, velocity: float, normalize: bool = True,
+               workspace: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """|sum_{k1<k2} s_k1 conj(s_k2)| over the delayed pair signals
+    s_k = sum_f S[f, rx, tx] exp(-j 2 pi f (d_tx + d_rx)/v), k = tx*N + rx, on
+    the device (beamforming.py:259-313).  S: (F, N, N) complex CUDA tensor,
+    already frequency-masked."""
+    dev = S.device
+    F, N, _ = S.shape
+    Sr = torch.view_as_real(S.to(torch.complex64).contiguous())
+    k = torch.as_tensor((2.0 * np.pi * np.asarray(frequencies, np.float64) / velocity).astype(np.float32)).to(dev)
+    ant = torch.as_tensor(np.asarray(antenna_xy_m, np.float32).reshape(N, 2)).to(dev)
+    need = lib().ceep_dmas_workspace_bytes(nx_pix, ny_pix)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = torch.empty(max(need, 8), dtype=torch.uint8, device=dev)
+    img = torch.empty((nx_pix, ny_pix), dtype=torch.float32, device=dev)
+    check(lib().ceep_dmas(Sr.data_ptr(), k.data_ptr(), ant.data_ptr(), F, N, nx_pix, ny_pix, px0, py0, pix,
+                          int(normalize), workspace.data_ptr(), img.data_ptr(), _stream(dev)), "ceep_dmas")
+    return img
+
+
 class DelayAndSumBeamformer:
-    """beamforming.py:86-257; ``reconstruct('das')`` runs on the device."""
+    """beamforming.py:86-313; ``reconstruct('das')`` and ``reconstruct('dmas')`` run on the device."""
 
     def __init__(self, s_parameters: MultistaticSParameters, antenna_positions, imaging_region: ImagingRegion,
                  frequency_range: Optional[Tuple[float, float]] = None, device: str = "cuda"):
@@ -169,44 +194,18 @@ class DelayAndSumBeamformer:
         return (np.hypot(*(p - tx)) + np.hypot(*(p - rx))) / self.velocity
 
     def reconstruct(self, method: str = "das", normalize: bool = True) -> np.ndarray:
-        if method == "das":
-            S = torch.as_tensor(np.asarray(self.s_params.s_matrix)[self.freq_mask]).to(self.device)
-            ant = np.asarray([p[:2] for p in self.antenna_positions], np.float64) * self.dx
-            r = self.region
-            img = das_image(S, self.frequencies, ant, r.nx, r.ny, r.x_range[0] * r.dx, r.y_range[0] * r.dx, r.dx,
-                            self.velocity, normalize)
-            return img.double().cpu().numpy()
-        if method == "dmas":
-            return self._reconstruct_dmas(normalize)
-        raise ValueError(f"Unknown method: {method}")
-
-    def _reconstruct_dmas(self, normalize: bool) -> np.ndarray:
-        """beamforming.py:259-313 (host; the DMAS is not on the device path)."""
-        r = self.region
-        px = (r.x_range[0] + np.arange(r.nx)) * r.dx
-        py = (r.y_range[0] + np.arange(r.ny)) * r.dx
-        PX, PY = np.meshgrid(px, py, indexing="ij")
+        if method not in ("das", "dmas"):
+            raise ValueError(f"Unknown method: {method}")
+        S = self.s_params.s_matrix
+        S = (S[torch.as_tensor(self.freq_mask)] if isinstance(S, torch.Tensor)
+             else np.asarray(S)[self.freq_mask])
+        S = torch.as_tensor(S).to(self.device)
         ant = np.asarray([p[:2] for p in self.antenna_positions], np.float64) * self.dx
-        d = np.stack([np.hypot(PX - a[0], PY - a[1]) for a in ant])
-        S = np.asarray(self.s_params.s_matrix)[self.freq_mask]
-        f = self.frequencies
-        sig = []
-        for tx in range(len(ant)):
-            for rx in range(len(ant)):
-                ph = np.exp(-1j * 2 * np.pi * f[:, None, None] * ((d[tx] + d[rx]) / self.velocity)[None])
-                sig.append(np.sum(S[:, rx, tx][:, None, None] * ph, axis=0))
-        sig = np.stack(sig)
-        acc = np.zeros(PX.shape, complex)
-        csum = np.conj(sig.sum(0))
-        for k in range(sig.shape[0]):
-            csum = csum - np.conj(sig[k])
-            acc += sig[k] * csum
-        img = np.abs(acc)
-        if normalize:
-            img = img - img.min()
-            if img.max() > 0:
-                img = img / img.max()
-        return img
+        r = self.region
+        image = das_image if method == "das" else dmas_image
+        img = image(S, self.frequencies, ant, r.nx, r.ny, r.x_range[0] * r.dx, r.y_range[0] * r.dx, r.dx,
+                    self.velocity, normalize)
+        return img.double().cpu().numpy()
 
 
 def das_time(s: torch.Tensor, antenna_positions_m: np.ndarray, frequency: float, grid_size: int,

@@ -262,6 +262,20 @@ int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
              void* work, float* image, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Frequency-domain delay-multiply-and-sum image.
+ * Replaces DelayAndSumBeamformer._reconstruct_dmas,
+ * src/ceep/imaging/beamforming.py:259-313: per pixel the delayed signal of
+ * every (tx, rx) pair (k = tx * nant + rx, tx == rx included), then
+ * |sum_{k1<k2} s_k1 conj(s_k2)|, normalised like ceep_das.  Same arguments
+ * as ceep_das (nant <= 32); work = ceep_dmas_workspace_bytes() bytes.
+ * ---------------------------------------------------------------------- */
+int64_t ceep_dmas_workspace_bytes(int32_t nx_pix, int32_t ny_pix);
+int ceep_dmas(const float* s, const float* kfreq, const float* ant_xy,
+              int32_t nfreq, int32_t nant, int32_t nx_pix, int32_t ny_pix,
+              float px0, float py0, float pix, int normalize,
+              void* work, float* image, void* stream);
+
+/* ------------------------------------------------------------------------
  * Frequency-domain delay-and-sum for callers that cannot allocate device
  * memory.  No counterpart in the reference: it exists for hosts that own all
  * GPU memory through their own pool (for example a scanner pipeline that
