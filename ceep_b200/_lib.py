@@ -80,6 +80,7 @@ _SIGS = {
     "ceep_das": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),
     "ceep_das_time": (C.c_int, [P, P, I32, I32, I32, C.c_double, C.c_double, P, P]),
     "ceep_dmas_workspace_bytes": (I64, [I32, I32]),
+    "ceep_brain_phantom_2d": (C.c_int, [I32, I32, I32, C.c_double, P, P, P, P, P, P, P]),
     "ceep_dmas": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),
     "ceep_das_noalloc_capacity": (I64, []),
     "ceep_das_noalloc": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P]),

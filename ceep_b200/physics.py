@@ -89,6 +89,8 @@ def update_coefficients(eps_r, sigma_e, dt, eps_add=None):
 
 def _f64(a, device):
     import torch
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device if device is not None else a.device, dtype=torch.float64)
     return torch.as_tensor(np.asarray(a, np.float64)).to(device)
 
 

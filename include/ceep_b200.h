@@ -309,6 +309,24 @@ int ceep_das_noalloc(const float* s, const float* kfreq, const float* ant_xy,
 int ceep_das_time(const float* s, const double* ant_xy, int32_t nant, int32_t ntime,
                   int32_t grid, double dx, double frequency, float* image, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Brain phantom rasteriser for dataset generation.
+ * Replaces BrainPhantom2D.get_eps_map with the fixed tissue table
+ * (src/ceep/phantoms/head_models.py:519-631, use_gabriel_database=False)
+ * and the hemorrhage mask of scripts/generate_corrected_dataset.py:110-118,
+ * for `batch` phantoms at once, on the device.
+ *   radii   : HOST (5) outer radius in metres of skin, skull, csf, grey, white
+ *   tissue  : HOST (6, 2) (eps_r, sigma) of skin, skull, csf, grey, white, blood
+ *   hem     : device (batch, 3) hemorrhage centre (metres from the grid centre
+ *             cell nx/2, ny/2) and radius; radius < 0 = no hemorrhage
+ *   eps_out, sigma_out, mask_out : (batch, nx, ny) FP64 (mask_out may be NULL)
+ * Distances are FP64 in the reference's operation order, so every cell lands
+ * in the same layer as with NumPy.
+ * ---------------------------------------------------------------------- */
+int ceep_brain_phantom_2d(int32_t batch, int32_t nx, int32_t ny, double dx, const double* radii,
+                          const double* tissue, const double* hem, double* eps_out, double* sigma_out,
+                          double* mask_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,10 @@ das_small         DelayAndSumBeamformer DAS and DMAS on a 6-antenna S-matrix
 das_time_small    das_imaging (scripts/verify_dataset_with_das.py)
 ade2d_small       batched step composed with DispersiveManager (Debye pole 0,
                   Lorentz pole 1), 44x40, CPML 5, 2 TX, 220 steps
+brain_phantom     BrainPhantom2D.get_eps_map (fixed tissue table) for a
+                  head-sized 400x380 grid with and without hemorrhage, and
+                  the 64x64 dataset-generator grid; hemorrhage masks as
+                  scripts/generate_corrected_dataset.py builds them
 """
 from __future__ import annotations
 
@@ -254,8 +258,36 @@ def gen_ade():
           j1=np.stack([np.asarray(m.j_ez[1]) for m in mgrs]))
 
 
+def gen_brain_phantom():
+    """BrainPhantom2D maps and the dataset generator's hemorrhage mask."""
+    import_reference(np.float64)
+    from ceep.phantoms import BrainPhantom2D
+    cases = [  # nx, ny, dx, hemorrhage (cm) or None, radius (cm), head radius (cm)
+        (400, 380, 0.5e-3, (2.1, -1.3), 1.2, 9.0),
+        (400, 380, 0.5e-3, None, 1.0, 9.0),
+        (64, 64, 0.5e-3, (0.4, -0.25), 0.6, 9.0),
+        (90, 70, 1e-3, (-0.9, 0.7), 0.45, 4.0),
+    ]
+    out = {}
+    for k, (nx, ny, dx, loc, rad, head) in enumerate(cases):
+        ph = BrainPhantom2D(nx=nx, ny=ny, dx=dx, hemorrhage_location=loc, hemorrhage_radius=rad,
+                            head_radius_cm=head, use_gabriel_database=False)
+        eps, sig = ph.get_eps_map(2e9)
+        mask = np.zeros((nx, ny))
+        if loc is not None:  # generate_corrected_dataset.py:110-118
+            cx, cy = nx // 2, ny // 2
+            xg, yg = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+            r = np.sqrt(((xg - cx) * dx - loc[0] * 1e-2) ** 2 + ((yg - cy) * dx - loc[1] * 1e-2) ** 2)
+            mask[r <= rad * 1e-2] = 1.0
+        out[f"eps_{k}"], out[f"sigma_{k}"], out[f"mask_{k}"] = eps, sig, mask
+        out[f"case_{k}"] = np.array([nx, ny, dx, np.nan if loc is None else loc[0],
+                                     np.nan if loc is None else loc[1], rad, head])
+    _save("brain_phantom", **out)
+
+
 JOBS = {
     "ceep_results": gen_ceep_results,
+    "brain_phantom": gen_brain_phantom,
     "small": lambda: (gen_small(np.float64), gen_small(np.float32)),
     "cfg1": lambda: (gen_cfg1(np.float64), gen_cfg1(np.float32)),
     "runcpu": gen_runcpu,

@@ -140,3 +140,20 @@ def test_ade_composition():
     assert rel_l2(o.probe_data, g["probes"]) < 1e-13
     assert rel_l2(o.j_deb[0], g["j0"]) < 1e-12
     assert rel_l2(o.j_lor[0], g["j1"]) < 1e-12
+
+
+def test_brain_phantom_oracle_against_reference():
+    """oracle/phantoms.py against BrainPhantom2D (fixed tissue table) and the
+    dataset generator's hemorrhage mask, bit for bit."""
+    from oracle.phantoms import brain_phantom_maps, hemorrhage_mask
+    g = load_golden("brain_phantom")
+    k = 0
+    while f"case_{k}" in g:
+        nx, ny, dx, hx, hy, rad, head = g[f"case_{k}"]
+        loc = None if np.isnan(hx) else (hx, hy)
+        eps, sig = brain_phantom_maps(int(nx), int(ny), dx, loc, rad, head)
+        np.testing.assert_array_equal(eps, g[f"eps_{k}"])
+        np.testing.assert_array_equal(sig, g[f"sigma_{k}"])
+        np.testing.assert_array_equal(hemorrhage_mask(int(nx), int(ny), dx, loc, rad), g[f"mask_{k}"])
+        k += 1
+    assert k == 4
