@@ -33,7 +33,8 @@ from .solvers import BatchedFDTD2D, _ptr
 class _AdjDesc(C.Structure):
     P = C.c_void_p
     _fields_ = [("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hx", P * 2), ("psi_hy", P * 2),
-                ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("grad", P), ("probe_grad", P)]
+                ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("grad", P), ("probe_grad", P),
+                ("grad_tau", C.c_int32)]
 
 
 def grad_width(n_debye: int) -> int:
@@ -59,13 +60,19 @@ def coefficient_maps(eps_r, sigma, debye, dt):
 
 
 class Adjoint2D:
-    """Gradient driver for one ``BatchedFDTD2D`` (Debye poles only)."""
+    """Gradient driver for one ``BatchedFDTD2D`` (Debye poles only).
 
-    def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50):
+    ``grad_tau`` adds d(loss)/d(tau) for a dispersive solver.  Without it tau
+    is held fixed: the update coefficients k1 and gamma depend on tau alone,
+    so their gradients are never formed and the forward pass does not keep
+    the Debye currents of every step (one field less to write and read)."""
+
+    def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False):
         if solver._lorentz:
             raise ValueError("the adjoint supports Debye poles only")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
+        self.grad_tau = bool(grad_tau)
         self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
         self._ckpt = {}
@@ -133,7 +140,8 @@ class Adjoint2D:
         check(lib().ceep2d_plan_set_current_buffer(s._plan, 0), "ceep2d_plan_set_current_buffer")
 
     def _save_segment(self, a, b):
-        """Restore step a, recompute [a, b) saving Ez and J of every step."""
+        """Restore step a, recompute [a, b) saving Ez (and, for tau gradients,
+        J) of every step."""
         s = self.s
         self._restore(a)
         G, W = s._groups, s._gwidth
@@ -142,7 +150,7 @@ class Adjoint2D:
             # allocated once: the recompute graphs are keyed on these addresses
             seg_ez = torch.empty((slots, G, s.ny, s.nx, W), dtype=torch.float32, device=s.device)
             seg_j = (torch.zeros((slots,) + tuple(s._j[0].shape), dtype=torch.float32, device=s.device)
-                     if s._j is not None else None)
+                     if s._j is not None and self.grad_tau else None)
             self._seg = (seg_ez, seg_j)
         seg_ez, seg_j = self._seg
         seg_ez[0].copy_(s._ez[0])
@@ -175,6 +183,7 @@ class Adjoint2D:
             arr = getattr(d, name)
             arr[0], arr[1] = _ptr(bufs[0]), _ptr(bufs[1])
         d.grad, d.probe_grad = grad.data_ptr(), gp.data_ptr()
+        d.grad_tau = int(self.grad_tau)
         h = C.c_void_p()
         check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
         self.launch_rows = lib().ceep2d_adjoint_rows(h)
@@ -199,8 +208,10 @@ class Adjoint2D:
         """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""
         eps_r, sigma, debye = self._params
         inputs = [eps_r.detach().requires_grad_(True), sigma.detach().requires_grad_(True)]
-        deb = [(de.detach().requires_grad_(True), tau.detach()) for de, tau in debye]
+        deb = [(de.detach().requires_grad_(True), tau.detach().requires_grad_(self.grad_tau)) for de, tau in debye]
         inputs += [de for de, _ in deb]
+        if self.grad_tau:
+            inputs += [tau for _, tau in deb]
         with torch.enable_grad():
             ca, cb, _, poles = coefficient_maps(inputs[0], inputs[1], deb, self.s.dt)
             outs = [ca, cb]
@@ -208,7 +219,7 @@ class Adjoint2D:
             for q, (k1, k2, g) in enumerate(poles):
                 outs += [k1, k2, g]
                 gouts += [grad[2 + 3 * q].t(), grad[3 + 3 * q].t(), grad[4 + 3 * q].t()]
-            # k1 and gamma depend on tau only, which is held fixed
+            # without grad_tau, k1 and gamma depend on fixed inputs only
             keep = [i for i, o in enumerate(outs) if o.requires_grad]
             grads = torch.autograd.grad([outs[i] for i in keep], inputs, [gouts[i] for i in keep],
                                         allow_unused=True)
@@ -216,6 +227,8 @@ class Adjoint2D:
         res = {"eps_r": grads[0], "sigma": grads[1]}
         if deb:
             res["deps"] = grads[2]
+            if self.grad_tau:
+                res["tau"] = grads[3]
         return res
 
 
@@ -234,7 +247,8 @@ class FDTD2DProbes(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_probes):
         g = ctx.adjoint.backward(grad_probes.contiguous())
-        return (g["eps_r"], g["sigma"], g.get("deps") if ctx.has_deps else None, None, None)
+        return (g["eps_r"], g["sigma"], g.get("deps") if ctx.has_deps else None,
+                g.get("tau") if ctx.has_deps else None, None)
 
 
 def probes_with_grad(eps_r, sigma, adjoint: Adjoint2D, deps=None, tau=None):

@@ -241,7 +241,8 @@ CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
         cp(S.en, ez_n + gf + (rowc + x0) * L, (xe - x0) * cb);
         cp(S.e1, ez_np1 + gf + (rowc + x0) * L, (xe - x0) * cb);
 #pragma unroll
-        for (int q = 0; q < ND; ++q) cp(S.jn + q * CX * L, j_n + gj + (q * plane + rowc + x0) * L, (xe - x0) * cb);
+        if (a.grad_tau)
+          for (int q = 0; q < ND; ++q) cp(S.jn + q * CX * L, j_n + gj + (q * plane + rowc + x0) * L, (xe - x0) * cb);
         cp(S.lhy + ha * L, a.hy[par] + gf + (rowc + xa) * L, (xe - xa) * cb);
       }
       if (!pass) mbar_arrive_expect_tx(&full[s], bytes);
@@ -385,13 +386,15 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
         for (int q = 0; q < ND; ++q) {
           const float4 kq = S.ade[q * H + cx + 1];
           const float4 jin = S.lj[(q * H + cx + 1) * L + lo];
-          const float4 jn = S.jn[q * CX * L + me];
           elin = fma4(-kq.y * p.inv_dt, jin, elin);
           st4(a.j[par ^ 1] + (size_t)g * p.gs_j + (q * plane + (size_t)r * nx + x) * L + lo,
               kq.x * jin - (cf.y * kq.z) * e1tot);
-          gv[2 + 3 * q] = dot4(jin, jn);
           gv[3 + 3 * q] = dot4(jin, dedt);
-          gv[4 + 3 * q] = -cf.y * dot4(e1tot, jn);
+          if (a.grad_tau) {  // k1 and gamma depend on tau alone
+            const float4 jn = S.jn[q * CX * L + me];
+            gv[2 + 3 * q] = dot4(jin, jn);
+            gv[4 + 3 * q] = -cf.y * dot4(e1tot, jn);
+          }
         }
         o.elin = elin;
         o.cy = (cf.y * inv) * e1tot;
@@ -422,6 +425,7 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
     double* gw = a.g + ((size_t)g * plane + (size_t)r * nx + x) * KP;
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
+      if (k >= 2 && (k - 2) % 3 != 1 && !a.grad_tau) continue;  // k1, gamma slots: warp-uniform skip
       const float v = lane_sum<L>(gv[k]);
       if (f9 && (k % L) == lo) atomicAdd(gw + k, (double)v);
     }

@@ -26,6 +26,7 @@ struct Adjoint2dParams {
   // then per pole k1, k2, gamma (and a zero pad)
   double* g;
   const float* probe_grad;  // (ntx, nprobe, nsteps) dLoss/dprobe
+  int grad_tau;             // also d/dk1 and d/dgamma (reads the forward J^n); else those slots stay 0
 };
 
 __host__ __device__ constexpr int adjoint2d_grad_width(int n_debye) { return (2 + 3 * n_debye + 1) & ~1; }

@@ -144,8 +144,7 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
   if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
     return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
                 (long long)(step0 + nsteps), pl->p.nsteps);
-  if (save_ez && (save_base > step0 || (pl->p.n_debye + pl->p.n_lorentz > 0 && !save_j)))
-    return fail(CEEP_ERR_INVALID, "save buffers need save_base <= step0 and a J buffer when poles exist");
+  if (save_ez && save_base > step0) return fail(CEEP_ERR_INVALID, "save buffers need save_base <= step0");
   if (nsteps == 0) return CEEP_OK;
   ceep::Fdtd2dParams q = pl->p;
   q.save_ez = reinterpret_cast<float4*>(save_ez);
@@ -380,6 +379,7 @@ extern "C" int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoi
   }
   a.g = d->grad;
   a.probe_grad = d->probe_grad;
+  a.grad_tau = d->grad_tau ? 1 : 0;
   cudaError_t e = ceep::adjoint2d_configure(a);
   if (e != cudaSuccess) {
     delete ad;
@@ -393,7 +393,7 @@ extern "C" int ceep2d_adjoint_run(ceep2d_adjoint* ad, int64_t step_hi, int64_t n
                                   const float* seg_j, int64_t seg_base, void* stream) {
   if (!ad || !seg_ez) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_run: null argument");
   const ceep::Fdtd2dParams& f = ad->a.f;
-  if (nsteps < 0 || step_hi > f.nsteps || step_hi - nsteps < seg_base || (f.n_debye && !seg_j))
+  if (nsteps < 0 || step_hi > f.nsteps || step_hi - nsteps < seg_base || (f.n_debye && ad->a.grad_tau && !seg_j))
     return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_run: steps [%lld, %lld) with segment base %lld",
                 (long long)(step_hi - nsteps), (long long)step_hi, (long long)seg_base);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -403,7 +403,7 @@ extern "C" int ceep2d_adjoint_run(ceep2d_adjoint* ad, int64_t step_hi, int64_t n
   for (int64_t n = step_hi - 1; n >= step_hi - nsteps; --n) {
     const size_t k = (size_t)(n - seg_base);
     cudaError_t e = ceep::adjoint2d_launch_step(ad->a, (int)n, ad->cur, E + k * fslot, E + (k + 1) * fslot,
-                                                J ? J + k * jslot : nullptr, s);
+                                                (J && ad->a.grad_tau) ? J + k * jslot : nullptr, s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "adjoint2d step launch");
     ad->cur ^= 1;
   }

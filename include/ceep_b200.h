@@ -117,11 +117,12 @@ int ceep2d_plan_reset(ceep2d_plan* plan);
 int64_t ceep2d_desc_size(void);
 /* Rows per block the plan launches with (chosen at creation when 0). */
 int ceep2d_plan_rows(const ceep2d_plan* plan);
-/* As ceep2d_plan_run, and also store Ez^{n+1} (and J^{n+1} when the plan has
- * Debye poles) of every step n into slot n + 1 - save_base of save_ez
+/* As ceep2d_plan_run, and also store Ez^{n+1} (and J^{n+1} when save_j is
+ * given) of every step n into slot n + 1 - save_base of save_ez
  * (slots, G, ny, nx, .) / save_j (slots, G, poles, ny, nx, .): the forward
- * values the adjoint needs.  J entries outside the interior E region are
- * never written (the caller zeroes the buffer once). */
+ * values the adjoint needs (J only for tau gradients).  J entries outside
+ * the interior E region are never written (the caller zeroes the buffer
+ * once). */
 int ceep2d_plan_run_save(ceep2d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph,
                          float* save_ez, float* save_j, int64_t save_base);
 /* Select which ping-pong buffer holds the current state (after the caller
@@ -174,6 +175,10 @@ typedef struct ceep2d_adjoint_desc {
                               then per pole d/dk1, d/dk2, d/dgamma, then a
                               zero pad; accumulated                          */
   const float* probe_grad; /* (ntx, nprobe, nsteps) dLoss/dprobe             */
+  int32_t grad_tau;        /* nonzero: also d/dk1 and d/dgamma, which depend
+                              on tau only and need the forward's saved J;
+                              0: those slots stay 0 and ceep2d_adjoint_run
+                              takes seg_j = NULL                             */
 } ceep2d_adjoint_desc;
 
 typedef struct ceep2d_adjoint ceep2d_adjoint;

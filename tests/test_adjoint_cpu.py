@@ -1,6 +1,7 @@
 """Gradient oracle pins (CPU): the PyTorch restatement equals the NumPy oracle,
 and its autograd gradient equals central finite differences (h = 1e-3) of the
-FP64 oracle on 32 random interior cells for eps_r, sigma and Debye delta_eps."""
+FP64 oracle on 32 random interior cells for eps_r, sigma, Debye delta_eps and
+tau (step 1e-3 of the value's scale)."""
 import numpy as np
 import torch
 
@@ -47,21 +48,23 @@ def test_autograd_matches_central_differences():
     e_ = torch.tensor(eps, dtype=torch.float64, requires_grad=True)
     s_ = torch.tensor(sig, dtype=torch.float64, requires_grad=True)
     d_ = torch.tensor(de, dtype=torch.float64, requires_grad=True)
-    probes = t.run(e_, s_, [(d_, torch.tensor(tau, dtype=torch.float64))])
+    t_ = torch.tensor(tau, dtype=torch.float64, requires_grad=True)
+    probes = t.run(e_, s_, [(d_, t_)])
     loss, _ = s_misfit_loss(probes, t.dt, FREQS, torch.as_tensor(target))
     loss.backward()
     rng = np.random.default_rng(3)
     cells = [tuple(c) for c in np.argwhere(m)[rng.choice(int(m.sum()), 32, replace=False)]]
-    h = 1e-3
-    for name, base, grad in (("eps_r", eps, e_.grad), ("sigma", sig, s_.grad), ("deps", de, d_.grad)):
+    for name, base, grad, h in (("eps_r", eps, e_.grad, 1e-3), ("sigma", sig, s_.grad, 1e-3),
+                                ("deps", de, d_.grad, 1e-3), ("tau", tau, t_.grad, 8e-15)):
         fd, ad = [], []
         for c in cells:
             vals = []
             for sgn in (1, -1):
                 arr = base.copy()
                 arr[c] += sgn * h
-                args = {"eps_r": (arr, sig, de), "sigma": (eps, arr, de), "deps": (eps, sig, arr)}[name]
-                vals.append(_oracle_loss(*args[:3], tau, target)[0])
+                args = {"eps_r": (arr, sig, de, tau), "sigma": (eps, arr, de, tau), "deps": (eps, sig, arr, tau),
+                        "tau": (eps, sig, de, arr)}[name]
+                vals.append(_oracle_loss(*args, target)[0])
             fd.append((vals[0] - vals[1]) / (2 * h))
             ad.append(float(grad[c]))
         fd, ad = np.array(fd), np.array(ad)

@@ -26,7 +26,7 @@ def _case(nx, ny, n, seed, debye=True, nring=4):
     return eps, sig, de, tau, m, ring
 
 
-def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp", nring=4):
+def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp", nring=4, grad_tau=False):
     """Gradient of the same scalar through the CUDA adjoint and through autograd
     of the FP64 restatement.  loss="vjp": sum(probes * G) for a fixed random G,
     which tests the transposed Jacobian alone; loss="misfit": the S-parameter
@@ -50,21 +50,25 @@ def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp", nring=4):
         (lambda p, dt: s_parameter_loss(p, dt, freqs, target)[0])
     e_, s_ = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
     d_ = f64(de).requires_grad_(True) if debye else None
-    ref = scalar(t.run(e_, s_, [(d_, f64(tau))] if debye else []), t.dt)
+    t_ = f64(tau).requires_grad_(grad_tau) if debye else None
+    ref = scalar(t.run(e_, s_, [(d_, t_)] if debye else []), t.dt)
     ref.backward()
     s = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9)
     if debye:
         s.set_dispersion(debye=[(de, tau)])
-    adj = Adjoint2D(s, checkpoint_every=K)
+    adj = Adjoint2D(s, checkpoint_every=K, grad_tau=grad_tau)
     e2, s2 = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
     d2 = f64(de).requires_grad_(True) if debye else None
-    val = scalar(probes_with_grad(e2, s2, adj, d2, f64(tau) if debye else None).double(), s.dt)
+    t2 = f64(tau).requires_grad_(grad_tau) if debye else None
+    val = scalar(probes_with_grad(e2, s2, adj, d2, t2).double(), s.dt)
     val.backward()
     inner = np.zeros((nx, ny), bool)
     inner[n + 1:nx - n, n + 1:ny - n] = True
     out = {"value": (float(val), float(ref)), "eps_r": (e2.grad, e_.grad), "sigma": (s2.grad, s_.grad)}
     if debye:
         out["deps"] = (d2.grad, d_.grad)
+    if grad_tau:
+        out["tau"] = (t2.grad, t_.grad)
     return out, inner
 
 
@@ -97,6 +101,14 @@ def test_adjoint_two_tx_groups(cuda_device):
     """37 TX: two TX groups, whose per-group gradient sums are added."""
     out, inner = _run_both(100, 92, 7, 140, 7, K=1, ntx=37, nring=37)
     _check(out, inner, ("eps_r", "sigma", "deps"), TOL)
+
+
+def test_adjoint_tau_gradient(cuda_device):
+    """grad_tau: the forward keeps J of every step and the adjoint adds the
+    k1 and gamma terms, giving d/dtau; the other gradients do not change."""
+    for K in (1, 30):
+        out, inner = _run_both(96, 88, 8, 200, 8, K=K, grad_tau=True)
+        _check(out, inner, ("eps_r", "sigma", "deps", "tau"), TOL)
 
 
 def test_adjoint_without_dispersion(cuda_device):
