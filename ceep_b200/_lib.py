@@ -75,6 +75,12 @@ _SIGS = {
     "ceep3d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
     "ceep3d_plan_destroy": (C.c_int, [P]),
     "ceep3d_desc_size": (I64, []),
+    "ceep3d_plan_run_save": (C.c_int, [P, I64, I64, P, C.c_int, P, I64]),
+    "ceep3d_adjoint_create": (C.c_int, [P, P, C.POINTER(P)]),
+    "ceep3d_adjoint_run": (C.c_int, [P, I64, I64, P, I64, P]),
+    "ceep3d_adjoint_grad_slots": (I32, [P]),
+    "ceep3d_adjoint_destroy": (C.c_int, [P]),
+    "ceep3d_adjoint_desc_size": (I64, []),
     "ceep_dft": (C.c_int, [P, P, P, I32, I32, I32, I32, P]),
     "ceep_das_workspace_bytes": (I64, [I32, I32, I32]),
     "ceep_das": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P]),

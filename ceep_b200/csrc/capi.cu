@@ -234,7 +234,7 @@ extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
 
 struct ceep3d_plan {
   ceep::Fdtd3dParams p;
-  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int64_t, int64_t, const void*, int64_t>, cudaGraphExec_t> graphs;
 };
 
 extern "C" int64_t ceep3d_desc_size(void) { return (int64_t)sizeof(ceep3d_desc); }
@@ -292,33 +292,42 @@ extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
   p.j = f4p(d->j); p.j_prev = f4p(d->j_prev);
   p.coef = d->coef; p.ade_coef = d->ade_coef; p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
   p.src_xyz = d->src_xyz; p.prb_xyz = d->prb_xyz; p.waveform = d->waveform; p.probes = d->probes;
+  p.save_e = nullptr;
+  p.save_cs = p.groups * p.gs_field;
+  p.save_base = 0;
   *out = pl;
   return CEEP_OK;
 }
 
-static int run_steps3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, cudaStream_t s) {
+static int run_steps3d(const ceep::Fdtd3dParams& q, int64_t step0, int64_t nsteps, cudaStream_t s) {
   for (int64_t k = 0; k < nsteps; ++k) {
-    cudaError_t e = ceep::fdtd3d_launch_step(pl->p, (int)(step0 + k), s);
+    cudaError_t e = ceep::fdtd3d_launch_step(q, (int)(step0 + k), s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd3d step launch");
   }
   return CEEP_OK;
 }
 
-extern "C" int ceep3d_plan_run(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+static int plan_run3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph, float* save_e,
+                      int64_t save_base) {
   if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
   if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
     return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
                 (long long)(step0 + nsteps), pl->p.nsteps);
+  if (save_e && (save_base < 0 || save_base > step0))
+    return fail(CEEP_ERR_INVALID, "save buffer needs 0 <= save_base <= step0");
   if (nsteps == 0) return CEEP_OK;
+  ceep::Fdtd3dParams q = pl->p;
+  q.save_e = reinterpret_cast<float4*>(save_e);
+  q.save_base = save_e ? (int)save_base : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!use_graph || s == nullptr) return run_steps3d(pl, step0, nsteps, s);
-  auto key = std::make_pair(step0, nsteps);
+  if (!use_graph || s == nullptr) return run_steps3d(q, step0, nsteps, s);
+  auto key = std::make_tuple(step0, nsteps, (const void*)save_e, (int64_t)q.save_base);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps3d(pl, step0, nsteps, s);
+    int rc = run_steps3d(q, step0, nsteps, s);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -330,6 +339,16 @@ extern "C" int ceep3d_plan_run(ceep3d_plan* pl, int64_t step0, int64_t nsteps, v
   }
   cudaError_t e = cudaGraphLaunch(it->second, s);
   return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "cudaGraphLaunch");
+}
+
+extern "C" int ceep3d_plan_run(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
+  return plan_run3d(pl, step0, nsteps, stream, use_graph, nullptr, 0);
+}
+
+extern "C" int ceep3d_plan_run_save(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph,
+                                    float* save_e, int64_t save_base) {
+  if (!save_e) return fail(CEEP_ERR_INVALID, "ceep3d_plan_run_save: null save buffer");
+  return plan_run3d(pl, step0, nsteps, stream, use_graph, save_e, save_base);
 }
 
 extern "C" int ceep3d_plan_destroy(ceep3d_plan* pl) {
@@ -422,6 +441,71 @@ extern "C" int ceep2d_adjoint_destroy(ceep2d_adjoint* ad) {
 }
 
 extern "C" int64_t ceep2d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep2d_adjoint_desc); }
+
+// --------------------------------------------------------------------------
+// 3D adjoint
+// --------------------------------------------------------------------------
+#include "adjoint3d.cuh"
+
+struct ceep3d_adjoint {
+  ceep::Adjoint3dParams a;
+};
+
+extern "C" int ceep3d_adjoint_create(const ceep3d_plan* plan, const ceep3d_adjoint_desc* d, ceep3d_adjoint** out) {
+  if (!plan || !d || !out) return fail(CEEP_ERR_INVALID, "ceep3d_adjoint_create: null argument");
+  *out = nullptr;
+  const ceep::Fdtd3dParams& f = plan->p;
+  if (f.n_lorentz) return fail(CEEP_ERR_UNSUPPORTED, "3D adjoint: Lorentz poles are not supported");
+  if (f.n < 1) return fail(CEEP_ERR_UNSUPPORTED, "3D adjoint: needs a CPML of at least 2 cells");
+  if (!d->mu || !d->nu || !d->grad || (f.n_debye && !d->lj))
+    return fail(CEEP_ERR_INVALID, "3D adjoint: null state/gradient buffer");
+  if (f.nprobe && !d->probe_grad) return fail(CEEP_ERR_INVALID, "3D adjoint: null probe gradient");
+  ceep3d_adjoint* ad = new (std::nothrow) ceep3d_adjoint();
+  if (!ad) return fail(CEEP_ERR_INVALID, "host allocation failed");
+  ceep::Adjoint3dParams& a = ad->a;
+  a.f = f;
+  a.f.save_e = nullptr;
+  const int eh = f.nz - 2 * f.n;  // H box [n, nz-n), E interior [n+1, nz-n)
+  a.zsegs_h = (eh + f.zrows - 1) / f.zrows;
+  a.zsegs_e = (eh - 1 + f.zrows - 1) / f.zrows;
+  a.cs = (long long)f.groups * f.gs_field;
+  a.icells = (long long)(f.nx - 2 * f.n - 1) * (f.ny - 2 * f.n - 1) * (f.nz - 2 * f.n - 1);
+  a.ks = 2 + f.n_debye;
+  a.mu = reinterpret_cast<float4*>(d->mu);
+  a.nu = reinterpret_cast<float4*>(d->nu);
+  a.lj = reinterpret_cast<float4*>(d->lj);
+  a.g = d->grad;
+  a.probe_grad = d->probe_grad;
+  *out = ad;
+  return CEEP_OK;
+}
+
+extern "C" int ceep3d_adjoint_run(ceep3d_adjoint* ad, int64_t step_hi, int64_t nsteps, const float* seg_e,
+                                  int64_t seg_base, void* stream) {
+  if (!ad || !seg_e) return fail(CEEP_ERR_INVALID, "ceep3d_adjoint_run: null argument");
+  const ceep::Adjoint3dParams& a = ad->a;
+  if (nsteps < 0 || step_hi > a.f.nsteps || step_hi - nsteps < seg_base || seg_base < 0)
+    return fail(CEEP_ERR_INVALID, "ceep3d_adjoint_run: steps [%lld, %lld) with segment base %lld",
+                (long long)(step_hi - nsteps), (long long)step_hi, (long long)seg_base);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t slot = 3 * (size_t)a.cs;
+  const float4* E = reinterpret_cast<const float4*>(seg_e);
+  for (int64_t n = step_hi - 1; n >= step_hi - nsteps; --n) {
+    const size_t k = (size_t)(n - seg_base);
+    cudaError_t e = ceep::adjoint3d_launch_step(a, (int)n, E + k * slot, E + (k + 1) * slot, n == seg_base, s);
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "adjoint3d step launch");
+  }
+  return CEEP_OK;
+}
+
+extern "C" int32_t ceep3d_adjoint_grad_slots(const ceep3d_adjoint* ad) { return ad ? ad->a.ks : 0; }
+
+extern "C" int ceep3d_adjoint_destroy(ceep3d_adjoint* ad) {
+  delete ad;
+  return CEEP_OK;
+}
+
+extern "C" int64_t ceep3d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep3d_adjoint_desc); }
 
 extern "C" int ceep2d_adjoint_rows(const ceep2d_adjoint* ad) { return ad ? ad->a.rows : 0; }
 

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kThreads3d, 6) fdtd3d_h_kernel(const Fdtd3dPar
 // component (the 3D analogue of dispersive.py:364-404 / fdtd_2d.py:163-178).
 // ---------------------------------------------------------------------------
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dParams p) {
+__global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dParams p, int step) {
   constexpr int CX = kThreads3d / L;
   constexpr int NP = ND + NL;
   const int n = p.n, nx = p.nx, ny = p.ny, nz = p.nz;
@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dPar
   const float inv = p.inv_dx;
   size_t at = (size_t)z0 * sz + (size_t)y * sy + (size_t)x * sx + lo;
   float4 hxm = ld4(hx + at - sz), hym = ld4(hy + at - sz);
+  float4* save = p.save_e ? p.save_e + (size_t)(step + 1 - p.save_base) * 3 * p.save_cs + gs : nullptr;
   for (int z = z0; z < z1; ++z, at += sz) {
     const float4 Hx = ld4(hx + at), Hy = ld4(hy + at), Hz = ld4(hz + at);
     const float4 hzy = ld4(hz + at - sy), hzx = ld4(hz + at - sx);
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dPar
         }
       }
       *E[c] = e;
+      if (save) save[c * p.save_cs + at] = e;
     }
     hxm = Hx;
     hym = Hy;
@@ -270,7 +272,7 @@ static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s) {
   const int ni = p.nx - 2 * p.n - 1, nj = p.ny - 2 * p.n - 1;
   if (ni > 0 && nj > 0 && p.zsegs_e > 0) {
     dim3 ge((ni + CX - 1) / CX, nj, p.zsegs_e * p.groups);
-    fdtd3d_e_kernel<L, ND, NL><<<ge, kThreads3d, 0, s>>>(p);
+    fdtd3d_e_kernel<L, ND, NL><<<ge, kThreads3d, 0, s>>>(p, step);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

@@ -26,6 +26,12 @@ struct Fdtd3dParams {
   const int32_t* prb_xyz;
   const float* waveform;
   float* probes;
+  // optional: the E half-step also stores each updated component (before the
+  // source) of step s into slot s + 1 - save_base of save_e, a
+  // (slots, 3, G, nz, ny, nx, L) array; save_cs = G * gs_field
+  float4* save_e;
+  long long save_cs;
+  int save_base;
 };
 
 cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s);

@@ -231,8 +231,45 @@ typedef struct ceep3d_desc {
 typedef struct ceep3d_plan ceep3d_plan;
 int ceep3d_plan_create(const ceep3d_desc* desc, ceep3d_plan** out);
 int ceep3d_plan_run(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+/* As ceep3d_plan_run, and also store the three E components of every step n,
+ * as the E half-step leaves them (before the source), into slot
+ * n + 1 - save_base of save_e, a (slots, 3, G, nz, ny, nx, .) float array;
+ * only the interior E box is written. */
+int ceep3d_plan_run_save(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph,
+                         float* save_e, int64_t save_base);
 int ceep3d_plan_destroy(ceep3d_plan* plan);
 int64_t ceep3d_desc_size(void);
+
+/* ------------------------------------------------------------------------
+ * 3D adjoint: the exact transpose of the 3D step restricted to what the
+ * probe series depends on (the E interior [n+1, N-n)^3 and the H box
+ * [n, N-n)^3, which no CPML face touches), giving per-cell gradients of a
+ * loss of the probe series with respect to ca, cb and each Debye k2.  No
+ * reference counterpart (the reference's 3D solver has no gradient); the
+ * forward it transposes is fdtd_3d_batched.py:886-985.
+ * State arrays (caller-owned, zeroed before the first run):
+ *   mu, nu: (3, G, nz, ny, nx, .) float;  lj: the forward J layout;
+ *   grad:   (G, 2 + poles, nz-2n-1, ny-2n-1, nx-2n-1) double, per interior
+ *           cell ca, cb, then k2 of each Debye pole, summed over steps/TX.
+ * ---------------------------------------------------------------------- */
+typedef struct ceep3d_adjoint_desc {
+  float* mu;                /* adjoint E plus (k2/dt) adjoint J               */
+  float* nu;                /* adjoint H (before the next step's da)          */
+  float* lj;                /* adjoint Debye currents                         */
+  double* grad;
+  const float* probe_grad;  /* (ntx, nprobe, nsteps) dLoss/dprobe             */
+} ceep3d_adjoint_desc;
+
+typedef struct ceep3d_adjoint ceep3d_adjoint;
+int ceep3d_adjoint_create(const ceep3d_plan* plan, const ceep3d_adjoint_desc* desc, ceep3d_adjoint** out);
+/* Adjoint steps step_hi-1 down to step_hi-nsteps; seg_e holds the slots that
+ * ceep3d_plan_run_save wrote with save_base = seg_base, slot 0 being a copy of
+ * the E state at step seg_base (source included). */
+int ceep3d_adjoint_run(ceep3d_adjoint* adj, int64_t step_hi, int64_t nsteps, const float* seg_e,
+                       int64_t seg_base, void* stream);
+int32_t ceep3d_adjoint_grad_slots(const ceep3d_adjoint* adj);
+int ceep3d_adjoint_destroy(ceep3d_adjoint* adj);
+int64_t ceep3d_adjoint_desc_size(void);
 
 /* ------------------------------------------------------------------------
  * On-device DFT of the probe series into the S-matrix.
