@@ -533,6 +533,94 @@ def run_adjoint_bench(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint3d_bench(args):
+    """Config 5's gradient: 192^3, 1 mm, 1000 steps, CPML 10, 8 z-directed
+    TX/RX on a mid-plane ring, 101 frequencies, Debye ellipsoid-shell head;
+    target S from the head with its inclusion, parameters from the same head
+    without it; d(S-misfit)/d(eps_r, sigma, delta_eps) through the
+    checkpointed 3D adjoint, timed against one plain forward."""
+    import torch
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200.adjoint import s_parameter_loss
+    from ceep_b200.adjoint3d import Adjoint3D, probes_with_grad_3d
+    from ceep_b200.phantoms import HeadPhantom3D, ring_positions
+    dev = torch.device("cuda", 0)
+    w = WORKLOADS["head192"]
+    nx, ny, nz, T, n = w["nx"], w["ny"], w["nz"], w["steps"], w["cpml"]
+    if args.small:
+        nx = ny = nz = 96
+        T = 300
+    c = nx // 2
+    pos = [(x, y, nz // 2) for x, y in ring_positions(w["ntx"], (c, ny // 2), w["ring"] * nx // 192)]
+    freqs = np.linspace(0.5e9, 3.5e9, w["nfreq"])
+    sc = nx / 192.0
+    kw = dict(nx=nx, ny=ny, nz=nz, dx=w["dx"], seed=7, semi_axes=(0.070 * sc, 0.056 * sc, 0.060 * sc))
+    truth, guess = HeadPhantom3D(**kw), HeadPhantom3D(with_inclusion=False, **kw)
+    mk = lambda: BatchedFDTD3D(nx, ny, nz, w["dx"], T, n, pos, pos, 2e9, frequencies=freqs, device=str(dev))
+    s = mk()
+    s.set_phantom(truth)
+    s.run()
+    target = torch.as_tensor(s.s_matrix(), device=dev)
+    del s
+    eps, sig = guess.get_eps_map_3d()
+    de, tau = guess.get_dispersion()["debye"][0]
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    s2 = mk()
+    s2.set_phantom(guess)
+    s2._build()
+
+    def fwd():
+        s2.reset()
+        s2.advance(0, T, stream=stream)
+    t_fwd = timed(fwd, 3)
+    del s2
+    torch.cuda.empty_cache()
+    ratios, mem, split = {}, {}, {}
+    for K in (25, 50, 100):
+        torch.cuda.reset_peak_memory_stats(dev)
+        sk = mk()
+        sk.set_phantom(guess)
+        adj = Adjoint3D(sk, checkpoint_every=K)
+        e, g, d = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True), f64(de).requires_grad_(True)
+
+        def grad_step():
+            e.grad = g.grad = d.grad = None
+            p = probes_with_grad_3d(e, g, adj, d, f64(tau))
+            loss, _ = s_parameter_loss(p.double(), sk.dt, freqs, target)
+            loss.backward()
+        ratios[K] = timed(grad_step, 1) / t_fwd
+        mem[K] = torch.cuda.max_memory_allocated(dev) / 2 ** 30
+        if K == 50:
+            gprobe = torch.randn((len(pos), len(pos), T), dtype=torch.float32, device=dev)
+            adj.set_parameters(e.detach(), g.detach(), d.detach(), f64(tau))
+            split = {"forward_ms": timed(adj.forward, 1), "backward_ms": timed(lambda: adj.backward(gprobe), 1)}
+        del adj, sk, e, g, d
+        torch.cuda.empty_cache()
+    line = {"metric": "adjoint gradient cost vs forward", "value": round(ratios[50], 3), "unit": "x forward",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded phantom)",
+            "config": {"workload": "adjoint192", "nx": nx, "ny": ny, "nz": nz, "time_steps": T,
+                       "tx": len(pos), "cpml": n, "debye_poles": 1, "dft_freqs": len(freqs),
+                       "loss": "sum |S - S*|^2", "grad": "eps_r, sigma, debye delta_eps"},
+            "forward_ms": round(t_fwd, 3),
+            "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()},
+            "peak_device_gib_by_checkpoint_interval": {str(k): round(v, 1) for k, v in mem.items()},
+            "checkpoint50_split_ms": {k: round(v, 3) for k, v in split.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def _pack_solvers(count, device, seed=2024):
     """Config-3 phantoms: nx, ny in {256..768 step 32}, steps in [600, 1200],
     8-16 TX, one third with a two-pole Lorentz model instead of Debye."""
@@ -677,7 +765,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="head600", choices=list(WORKLOADS) + ["adjoint400", "pack256"])
+    ap.add_argument("--workload", default="head600",
+                    choices=list(WORKLOADS) + ["adjoint400", "adjoint192", "pack256"])
     ap.add_argument("--pack-count", type=int, default=256)
     ap.add_argument("--pack-sample", type=int, default=32)
     ap.add_argument("--small", action="store_true", help="with --profile: a smaller 3D grid")
@@ -696,6 +785,9 @@ def main():
             run_profile_adjoint(args)
         else:
             run_adjoint_bench(args)
+        return
+    if args.workload == "adjoint192":
+        run_adjoint3d_bench(args)
         return
     if args.workload == "pack256":
         run_pack_bench(args)

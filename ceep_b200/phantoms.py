@@ -131,7 +131,8 @@ class HeadPhantom3D:
     """Concentric ellipsoid shells (the 2D layer sequence, thicknesses from
     head_models.py:541-545) with one seeded Debye pole per shell and a seeded
     ellipsoidal inclusion of 0.8-1.5 cm; ``get_eps_map_3d`` feeds
-    ``BatchedFDTD3D.set_phantom``."""
+    ``BatchedFDTD3D.set_phantom``.  ``with_inclusion=False`` gives the same
+    head without the inclusion (the same draws, so the shells are identical)."""
     nx: int = 192
     ny: int = 192
     nz: int = 192
@@ -146,6 +147,7 @@ class HeadPhantom3D:
     inclusion_radius: tuple = (0.8e-2, 1.5e-2)
     inclusion_eps: tuple = (55.0, 65.0)
     inclusion_sigma: tuple = (1.4, 1.8)
+    with_inclusion: bool = True
 
     def __post_init__(self):
         rng = np.random.default_rng(self.seed)
@@ -178,7 +180,8 @@ class HeadPhantom3D:
         inc = self.inclusion
         (cx, cy, cz), (rx, ry, rz) = inc["center"], inc["radii"]
         m = ((x - cx) / rx) ** 2 + ((y - cy) / ry) ** 2 + ((z - cz) / rz) ** 2 <= 1.0
-        eps[m], sig[m], de[m], tau[m] = inc["eps"], inc["sigma"], 0.0, 0.0
+        if self.with_inclusion:
+            eps[m], sig[m], de[m], tau[m] = inc["eps"], inc["sigma"], 0.0, 0.0
         self._maps = (eps, sig, de, tau)
         return self._maps
 
