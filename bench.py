@@ -734,6 +734,30 @@ def run_profile_adjoint(args):
     print("profile run done", flush=True)
 
 
+def run_profile_adjoint3d(args):
+    """One gradient of a 128^3, 8-TX Debye head over --profile steps (one
+    checkpoint segment, so no recompute), launched without graphs."""
+    import torch
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200.adjoint3d import Adjoint3D, probes_with_grad_3d
+    from ceep_b200.phantoms import HeadPhantom3D, ring_positions
+    dev = torch.device("cuda", 0)
+    T, nx = args.profile, 128
+    pos = [(x, y, nx // 2) for x, y in ring_positions(8, (nx // 2, nx // 2), 50)]
+    sc = nx / 192.0
+    ph = HeadPhantom3D(nx=nx, ny=nx, nz=nx, dx=1e-3, seed=7, semi_axes=(0.070 * sc, 0.056 * sc, 0.060 * sc))
+    s = BatchedFDTD3D(nx, nx, nx, 1e-3, T, 10, pos, pos, 2e9, device=str(dev), use_graph=False)
+    s.set_phantom(ph)
+    eps, sig = ph.get_eps_map_3d()
+    de, tau = ph.get_dispersion()["debye"][0]
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    e = f64(eps).requires_grad_(True)
+    p = probes_with_grad_3d(e, f64(sig), Adjoint3D(s, checkpoint_every=T), f64(de), f64(tau))
+    (p.double() ** 2).sum().backward()
+    torch.cuda.synchronize()
+    print("profile run done", flush=True)
+
+
 def run_profile(args, w):
     """A few fused steps of one sample, launched without a graph, then the DFT
     and DAS once: the small command that ncu captures.  With --small the 3D
@@ -787,7 +811,10 @@ def main():
             run_adjoint_bench(args)
         return
     if args.workload == "adjoint192":
-        run_adjoint3d_bench(args)
+        if args.profile:
+            run_profile_adjoint3d(args)
+        else:
+            run_adjoint3d_bench(args)
         return
     if args.workload == "pack256":
         run_pack_bench(args)

@@ -8,7 +8,8 @@ adjoint of its step (``csrc/adjoint3d.cu``) run backwards in time:
   segment is run with the E save on, so it is never recomputed);
 * for each segment, last first, the state is restored, the segment is
   recomputed while the E half-step stores the three E components of every
-  step, and the transposed steps run back over it, accumulating d(loss)/d of
+  step (the recompute skips the CPML shell, which no stored value depends
+  on), and the transposed steps run back over it, accumulating d(loss)/d of
   the interior update coefficients (ca, cb, k2) in FP64;
 * the chain rule from those coefficients to (eps_r, sigma, delta_eps) runs in
   torch FP64 through the same formulas as the forward
@@ -97,13 +98,13 @@ class Adjoint3D:
                                     device=s.device)
         return self._seg
 
-    def _run_save(self, a, b, stream):
+    def _run_save(self, a, b, stream, interior_only):
         s = self.s
         seg = self._segment_buffer()
         for c, k in enumerate(("ex", "ey", "ez")):
             seg[0, c].copy_(s._f[k])
         check(lib().ceep3d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
-                                         seg.data_ptr(), a), "ceep3d_plan_run_save")
+                                         seg.data_ptr(), a, int(interior_only)), "ceep3d_plan_run_save")
         return seg
 
     def forward(self) -> torch.Tensor:
@@ -119,7 +120,7 @@ class Adjoint3D:
             b = min(a + K, T)
             self._ckpt[a] = None if a == 0 else [t.clone() for t in self._state_tensors()]
             if a == starts[-1]:
-                self._run_save(a, b, stream)
+                self._run_save(a, b, stream, interior_only=False)
                 self._seg_ready = a
             else:
                 s.advance(a, b - a, stream=stream)
@@ -159,7 +160,8 @@ class Adjoint3D:
                     self._seg_ready = None
                 else:
                     self._restore(a)
-                    seg = self._run_save(a, b, stream)
+                    # the recompute skips the CPML shell, which no saved value depends on
+                    seg = self._run_save(a, b, stream, interior_only=True)
                 check(lib().ceep3d_adjoint_run(h, b, b - a, seg.data_ptr(), a, C.c_void_p(stream.cuda_stream)),
                       "ceep3d_adjoint_run")
         finally:

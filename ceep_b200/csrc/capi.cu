@@ -234,7 +234,7 @@ extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
 
 struct ceep3d_plan {
   ceep::Fdtd3dParams p;
-  std::map<std::tuple<int64_t, int64_t, const void*, int64_t>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int64_t, int64_t, const void*, int64_t, int>, cudaGraphExec_t> graphs;
 };
 
 extern "C" int64_t ceep3d_desc_size(void) { return (int64_t)sizeof(ceep3d_desc); }
@@ -295,6 +295,7 @@ extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
   p.save_e = nullptr;
   p.save_cs = p.groups * p.gs_field;
   p.save_base = 0;
+  p.interior_only = 0;
   *out = pl;
   return CEEP_OK;
 }
@@ -308,7 +309,7 @@ static int run_steps3d(const ceep::Fdtd3dParams& q, int64_t step0, int64_t nstep
 }
 
 static int plan_run3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph, float* save_e,
-                      int64_t save_base) {
+                      int64_t save_base, int interior_only) {
   if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
   if (step0 < 0 || nsteps < 0 || step0 + nsteps > pl->p.nsteps)
     return fail(CEEP_ERR_INVALID, "steps [%lld, %lld) outside [0, %d)", (long long)step0,
@@ -319,9 +320,10 @@ static int plan_run3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stre
   ceep::Fdtd3dParams q = pl->p;
   q.save_e = reinterpret_cast<float4*>(save_e);
   q.save_base = save_e ? (int)save_base : 0;
+  q.interior_only = interior_only && pl->p.n > 0 ? 1 : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (!use_graph || s == nullptr) return run_steps3d(q, step0, nsteps, s);
-  auto key = std::make_tuple(step0, nsteps, (const void*)save_e, (int64_t)q.save_base);
+  auto key = std::make_tuple(step0, nsteps, (const void*)save_e, (int64_t)q.save_base, q.interior_only);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
@@ -342,13 +344,13 @@ static int plan_run3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stre
 }
 
 extern "C" int ceep3d_plan_run(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
-  return plan_run3d(pl, step0, nsteps, stream, use_graph, nullptr, 0);
+  return plan_run3d(pl, step0, nsteps, stream, use_graph, nullptr, 0, 0);
 }
 
 extern "C" int ceep3d_plan_run_save(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph,
-                                    float* save_e, int64_t save_base) {
+                                    float* save_e, int64_t save_base, int interior_only) {
   if (!save_e) return fail(CEEP_ERR_INVALID, "ceep3d_plan_run_save: null save buffer");
-  return plan_run3d(pl, step0, nsteps, stream, use_graph, save_e, save_base);
+  return plan_run3d(pl, step0, nsteps, stream, use_graph, save_e, save_base, interior_only);
 }
 
 extern "C" int ceep3d_plan_destroy(ceep3d_plan* pl) {

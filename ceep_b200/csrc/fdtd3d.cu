@@ -150,10 +150,15 @@ __global__ void __launch_bounds__(kThreads3d, 6) fdtd3d_h_kernel(const Fdtd3dPar
   // x in [n, nx-n), y in [n, ny-n), z in [n, nz-n) with n >= 1 (nx-n <= nx-1)
   const int m = n > 1 ? n : 1;
   const bool interior = x0 >= n && x0 + CX <= nx - m && y >= n && y < ny - m && z0 >= n && z1 <= nz - m;
-  if (interior)
+  if (interior) {
     h_segment<L, false>(p, x, lo, y, g, z0, z1);
-  else
+  } else if (!p.interior_only) {
     h_segment<L, true>(p, x, lo, y, g, z0, z1);
+  } else if (n > 0 && x >= n && x < nx - n && y >= n && y < ny - n) {
+    // the cells of [n, N-n)^3 take the same code path as in a full step
+    const int za = max(z0, n), zb = min(z1, nz - n);
+    if (za < zb) h_segment<L, true>(p, x, lo, y, g, za, zb);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,9 @@ struct Fdtd3dParams {
   float4* save_e;
   long long save_cs;
   int save_base;
+  // nonzero: the H half-step skips every cell outside [n, N-n)^3 (the CPML
+  // shell and its psi), which no interior E or probe value depends on
+  int interior_only;
 };
 
 cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s);

@@ -234,9 +234,12 @@ int ceep3d_plan_run(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stre
 /* As ceep3d_plan_run, and also store the three E components of every step n,
  * as the E half-step leaves them (before the source), into slot
  * n + 1 - save_base of save_e, a (slots, 3, G, nz, ny, nx, .) float array;
- * only the interior E box is written. */
+ * only the interior E box is written.  With interior_only the H half-step
+ * skips the CPML shell (H outside [n, N-n)^3 and the psi arrays stay as they
+ * were): E, the H box, the currents and the probes come out bit-identical,
+ * since nothing in the shell reaches them, for a fraction of the traffic. */
 int ceep3d_plan_run_save(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph,
-                         float* save_e, int64_t save_base);
+                         float* save_e, int64_t save_base, int interior_only);
 int ceep3d_plan_destroy(ceep3d_plan* plan);
 int64_t ceep3d_desc_size(void);
 

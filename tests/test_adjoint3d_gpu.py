@@ -126,3 +126,32 @@ def test_adjoint3d_checkpoint_interval_does_not_change_the_gradient(cuda_device)
         (p.double() ** 2).sum().backward()
         res.append(e.grad.clone())
     assert torch.equal(res[0], res[1]) and torch.equal(res[0], res[2])
+
+
+def test_interior_only_save_pass_is_bit_identical(cuda_device):
+    """The recompute mode (CPML shell skipped) stores the same E slots and
+    leaves the same E, H box, currents and probes as a full save pass."""
+    import ctypes as C
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200._lib import check, lib
+    eps, sig, de, tau, m, ring = _case(30, 28, 26, 9)
+    out = []
+    for interior_only in (0, 1):
+        s = BatchedFDTD3D(30, 28, 26, 1e-3, 60, 3, ring[:3], ring, 2e9)
+        s._eps_r[:], s._sigma_e[:] = eps, sig
+        s.set_dispersion(debye=[(de, tau)])
+        s.advance(0, 20)
+        seg = torch.zeros((41, 3) + tuple(s._f["ex"].shape), dtype=torch.float32, device="cuda")
+        st = torch.cuda.current_stream()
+        check(lib().ceep3d_plan_run_save(s._plan, 20, 40, C.c_void_p(st.cuda_stream), 1, seg.data_ptr(), 20,
+                                         interior_only), "ceep3d_plan_run_save")
+        torch.cuda.synchronize()
+        out.append((seg, {k: v.clone() for k, v in s._f.items()}, s._j.clone(), s.probe_data.clone()))
+    (sa, fa, ja, pa), (sb, fb, jb, pb) = out
+    n = 3
+    box = (slice(None), slice(n, 26 - n), slice(n, 28 - n), slice(n, 30 - n))
+    assert torch.equal(sa, sb) and torch.equal(ja, jb) and torch.equal(pa, pb)
+    for k in ("ex", "ey", "ez"):
+        assert torch.equal(fa[k], fb[k])
+    for k in ("hx", "hy", "hz"):
+        assert torch.equal(fa[k][box], fb[k][box])
