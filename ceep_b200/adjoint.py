@@ -6,11 +6,15 @@ probe series with respect to the per-cell eps_r, sigma and Debye delta_eps
 maps comes from the exact discrete adjoint of the fused forward step
 (``csrc/adjoint2d.cu``), run backwards in time:
 
-* the forward pass stores the full state every ``checkpoint_every`` steps;
-* for each segment, last first, the state is restored, the segment is
-  recomputed while the step kernel saves Ez and the Debye currents of every
-  step, and the transposed steps run back over it, accumulating d(loss)/d of
-  the per-cell update coefficients (ca, cb, k1, k2, gamma) in FP64;
+* the forward pass stores the full state every ``checkpoint_every`` steps
+  and runs its last segment with the save on;
+* for each other segment, last first, the state is restored and the segment
+  recomputed while the step kernel saves Ez (and, for tau gradients, the
+  Debye currents) of every step; the transposed steps run back over each
+  segment, accumulating d(loss)/d of the per-cell update coefficients
+  (ca, cb, k2, and k1, gamma with ``grad_tau``) in FP64.  The recompute of
+  the next segment overlaps the adjoint of the current one on a second
+  stream (``overlap``, two segment buffers);
 * the chain rule from those coefficients to (eps_r, sigma, delta_eps) runs in
   torch FP64 through the same coefficient formulas as the forward
   (src/ceep/solvers/fdtd_2d_batched.py:151-167, src/ceep/materials/dispersive.py:253-261).
@@ -59,6 +63,54 @@ def coefficient_maps(eps_r, sigma, debye, dt):
     return (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s), dt / (eps_r * EPS_0), poles
 
 
+def run_segments_backward(starts, seg_ready, recompute, adjoint, device, overlap):
+    """Drive the segments of a checkpointed adjoint, last first.
+
+    ``recompute(a, buf)`` enqueues, on the current stream, the restore of
+    checkpoint ``a`` and the saving recompute of its segment into segment
+    buffer ``buf``; ``adjoint(a, buf)`` enqueues the transposed steps of that
+    segment reading buffer ``buf``.  ``seg_ready`` is the segment whose slots
+    the forward pass already left in buffer 0.  With ``overlap`` (two
+    buffers) the recompute of the next segment runs on a second stream while
+    the adjoint of the current one runs on a high-priority stream: the two
+    are independent (different state, different buffers), and neither
+    saturates the GPU alone at these sizes.  Events order each buffer's
+    reuse; the caller's stream waits for both at the end."""
+    main = torch.cuda.current_stream(device)
+    if not overlap:
+        for a in starts:
+            if a != seg_ready:
+                recompute(a, 0)
+            adjoint(a, 0)
+        return
+    adj_s = torch.cuda.Stream(device, priority=-1)
+    rec_s = torch.cuda.Stream(device)
+    adj_s.wait_stream(main)
+    rec_s.wait_stream(main)
+    freed = [None, None]
+    ready = {}
+    if starts[0] != seg_ready:
+        with torch.cuda.stream(rec_s):
+            recompute(starts[0], 0)
+        ready[0] = rec_s.record_event()
+    for i, a in enumerate(starts):
+        buf = i % 2
+        if i + 1 < len(starts):
+            nb = (i + 1) % 2
+            if freed[nb] is not None:
+                rec_s.wait_event(freed[nb])
+            with torch.cuda.stream(rec_s):
+                recompute(starts[i + 1], nb)
+            ready[i + 1] = rec_s.record_event()
+        if i in ready:
+            adj_s.wait_event(ready[i])
+        with torch.cuda.stream(adj_s):
+            adjoint(a, buf)
+        freed[buf] = adj_s.record_event()
+    main.wait_stream(adj_s)
+    main.wait_stream(rec_s)
+
+
 class Adjoint2D:
     """Gradient driver for one ``BatchedFDTD2D`` (Debye poles only).
 
@@ -67,12 +119,15 @@ class Adjoint2D:
     so their gradients are never formed and the forward pass does not keep
     the Debye currents of every step (one field less to write and read)."""
 
-    def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False):
+    def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False,
+                 overlap: bool = True):
         if solver._lorentz:
             raise ValueError("the adjoint supports Debye poles only")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
         self.grad_tau = bool(grad_tau)
+        self.overlap = bool(overlap)
+        self._seg_ready = None
         self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
         self._ckpt = {}
@@ -109,24 +164,43 @@ class Adjoint2D:
             st["j"] = s._j[cur]
         return st
 
+    def _seglen(self):
+        return self.s.total_steps if self.K == 1 else min(self.K, self.s.total_steps)
+
+    def _buffers(self, count):
+        """`count` segment buffers (Ez slots, J slots or None), allocated once:
+        the saving graphs are keyed on their addresses."""
+        s = self.s
+        G, W = s._groups, s._gwidth
+        slots = self._seglen() + 1
+        segs = getattr(self, "_segs", [])
+        while len(segs) < count:
+            seg_ez = torch.empty((slots, G, s.ny, s.nx, W), dtype=torch.float32, device=s.device)
+            seg_j = (torch.zeros((slots,) + tuple(s._j[0].shape), dtype=torch.float32, device=s.device)
+                     if s._j is not None and self.grad_tau else None)
+            segs.append((seg_ez, seg_j))
+        self._segs = segs
+        return segs
+
     def forward(self) -> torch.Tensor:
         """Run all steps from a zero state, keeping checkpoints; returns the probe
-        series (ntx, nprobe, T) float32 on the device."""
+        series (ntx, nprobe, T) float32 on the device.  The last segment runs
+        with the save on, so the backward pass never recomputes it."""
         s = self.s
         s.reset()
-        T, K = s.total_steps, self.K
+        T, L = s.total_steps, self._seglen()
         self._ckpt = {}
+        self._buffers(1)
         stream = torch.cuda.current_stream(s.device)
-        for a in range(0, T, K):
-            if K > 1 or a == 0:
-                self._ckpt[a] = {k: v.clone() for k, v in self._state().items()}
-            nst = min(K, T - a)
-            if K == 1:
-                break
-            s.advance(a, nst, stream=stream)
-        if K == 1:
-            # keep every step: one saving forward pass serves the whole adjoint
-            self._full = self._save_segment(0, T)
+        starts = list(range(0, T, L))
+        for a in starts:
+            b = min(a + L, T)
+            self._ckpt[a] = {k: v.clone() for k, v in self._state().items()}
+            if a == starts[-1]:
+                self._run_save(a, b, 0)
+            else:
+                s.advance(a, b - a, stream=stream)
+        self._seg_ready = starts[-1]
         return s.probe_data[:, :len(s.probe_positions)].clone()
 
     def _restore(self, a):
@@ -139,34 +213,25 @@ class Adjoint2D:
             s._j[0].copy_(ck["j"])
         check(lib().ceep2d_plan_set_current_buffer(s._plan, 0), "ceep2d_plan_set_current_buffer")
 
-    def _save_segment(self, a, b):
-        """Restore step a, recompute [a, b) saving Ez (and, for tau gradients,
-        J) of every step."""
+    def _run_save(self, a, b, buf):
+        """Run [a, b) from the current state on the current stream, saving Ez
+        (and, for tau gradients, J) of every step into buffer `buf`."""
         s = self.s
-        self._restore(a)
-        G, W = s._groups, s._gwidth
-        slots = (s.total_steps if self.K == 1 else self.K) + 1
-        if getattr(self, "_seg", None) is None:
-            # allocated once: the recompute graphs are keyed on these addresses
-            seg_ez = torch.empty((slots, G, s.ny, s.nx, W), dtype=torch.float32, device=s.device)
-            seg_j = (torch.zeros((slots,) + tuple(s._j[0].shape), dtype=torch.float32, device=s.device)
-                     if s._j is not None and self.grad_tau else None)
-            self._seg = (seg_ez, seg_j)
-        seg_ez, seg_j = self._seg
-        seg_ez[0].copy_(s._ez[0])
+        seg_ez, seg_j = self._segs[buf]
+        cur = s._cur()
+        seg_ez[0].copy_(s._ez[cur])
         if seg_j is not None:
-            seg_j[0].copy_(s._j[0])
+            seg_j[0].copy_(s._j[cur])
         stream = torch.cuda.current_stream(s.device)
         check(lib().ceep2d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
                                          seg_ez.data_ptr(), _ptr(seg_j), a), "ceep2d_plan_run_save")
-        return seg_ez, seg_j
 
     # -- backward ------------------------------------------------------------------
     def backward(self, grad_probes: torch.Tensor):
         """d(loss)/d(eps_r, sigma, delta_eps) given d(loss)/d(probe series)."""
         s = self.s
         dev = s.device
-        T, K = s.total_steps, self.K
+        T, L = s.total_steps, self._seglen()
         G, W = s._groups, s._gwidth
         f32 = dict(dtype=torch.float32, device=dev)
         pair = lambda t: [torch.zeros_like(t), torch.zeros_like(t)] if t is not None else [None, None]
@@ -184,22 +249,26 @@ class Adjoint2D:
             arr[0], arr[1] = _ptr(bufs[0]), _ptr(bufs[1])
         d.grad, d.probe_grad = grad.data_ptr(), gp.data_ptr()
         d.grad_tau = int(self.grad_tau)
+        starts = sorted(self._ckpt, reverse=True)
+        two = self.overlap and len(starts) > 1
+        self._buffers(2 if two else 1)
         h = C.c_void_p()
         check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
         self.launch_rows = lib().ceep2d_adjoint_rows(h)
-        stream = torch.cuda.current_stream(dev)
+
+        def recompute(a, buf):
+            self._restore(a)
+            self._run_save(a, min(a + L, T), buf)
+
+        def adjoint(a, buf):
+            seg_ez, seg_j = self._segs[buf]
+            st = torch.cuda.current_stream(dev)
+            check(lib().ceep2d_adjoint_run(h, min(a + L, T), min(a + L, T) - a, seg_ez.data_ptr(), _ptr(seg_j), a,
+                                           C.c_void_p(st.cuda_stream)), "ceep2d_adjoint_run")
         try:
-            if K == 1:
-                seg_ez, seg_j = self._full
-                check(lib().ceep2d_adjoint_run(h, T, T, seg_ez.data_ptr(), _ptr(seg_j), 0,
-                                               C.c_void_p(stream.cuda_stream)), "ceep2d_adjoint_run")
-            else:
-                for a in sorted(self._ckpt, reverse=True):
-                    b = min(a + K, T)
-                    seg_ez, seg_j = self._save_segment(a, b)
-                    check(lib().ceep2d_adjoint_run(h, b, b - a, seg_ez.data_ptr(), _ptr(seg_j), a,
-                                                   C.c_void_p(stream.cuda_stream)), "ceep2d_adjoint_run")
+            run_segments_backward(starts, self._seg_ready, recompute, adjoint, dev, two)
         finally:
+            self._seg_ready = None
             lib().ceep2d_adjoint_destroy(h)
         # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
         return self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])

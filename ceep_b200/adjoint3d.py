@@ -6,6 +6,9 @@ adjoint of its step (``csrc/adjoint3d.cu``) run backwards in time:
 
 * the forward pass keeps the state every ``checkpoint_every`` steps (the last
   segment is run with the E save on, so it is never recomputed);
+* the recompute of the next segment overlaps the adjoint of the current one
+  on a second stream when a second segment buffer fits in free memory
+  (``overlap=None``; True/False force it);
 * for each segment, last first, the state is restored, the segment is
   recomputed while the E half-step stores the three E components of every
   step (the recompute skips the CPML shell, which no stored value depends
@@ -24,11 +27,12 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import physics
 from ._lib import check, lib
-from .adjoint import coefficient_maps
+from .adjoint import coefficient_maps, run_segments_backward
 from .solvers import _ptr
 from .solvers3d import BatchedFDTD3D
 
@@ -41,16 +45,17 @@ class _AdjDesc3D(C.Structure):
 class Adjoint3D:
     """Gradient driver for one ``BatchedFDTD3D`` (Debye poles only, CPML >= 2)."""
 
-    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50):
+    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50, overlap=None):
         if solver._lorentz:
             raise ValueError("the 3D adjoint supports Debye poles only")
         if solver.cpml_thickness < 1:
             raise ValueError("the 3D adjoint needs a CPML (cpml_thickness >= 2)")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
+        self.overlap = overlap          # None: when a second segment buffer fits in free memory
         self._params = None
         self._ckpt = {}
-        self._seg = None
+        self._segs = []
         self._seg_ready = None          # segment start whose E slots the forward already stored
 
     # -- parameters -------------------------------------------------------------
@@ -89,23 +94,25 @@ class Adjoint3D:
             for t, c in zip(self._state_tensors(), ck):
                 t.copy_(c)
 
-    def _segment_buffer(self):
+    def _segment_shape(self):
         s = self.s
-        if self._seg is None:
-            # allocated once: the save graphs are keyed on this address
-            slots = min(self.K, s.total_steps) + 1
-            self._seg = torch.empty((slots, 3) + tuple(s._f["ex"].shape), dtype=torch.float32,
-                                    device=s.device)
-        return self._seg
+        return (min(self.K, s.total_steps) + 1, 3) + tuple(s._f["ex"].shape)
 
-    def _run_save(self, a, b, stream, interior_only):
+    def _buffers(self, count):
+        """`count` segment buffers, allocated once: the save graphs are keyed
+        on their addresses."""
+        while len(self._segs) < count:
+            self._segs.append(torch.empty(self._segment_shape(), dtype=torch.float32, device=self.s.device))
+        return self._segs
+
+    def _run_save(self, a, b, buf, interior_only):
         s = self.s
-        seg = self._segment_buffer()
+        seg = self._segs[buf]
+        stream = torch.cuda.current_stream(s.device)
         for c, k in enumerate(("ex", "ey", "ez")):
             seg[0, c].copy_(s._f[k])
         check(lib().ceep3d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
                                          seg.data_ptr(), a, int(interior_only)), "ceep3d_plan_run_save")
-        return seg
 
     def forward(self) -> torch.Tensor:
         """Run all steps from a zero state, keeping checkpoints; returns the
@@ -114,13 +121,14 @@ class Adjoint3D:
         s.reset()
         T, K = s.total_steps, self.K
         self._ckpt, self._seg_ready = {}, None
+        self._buffers(1)
         stream = torch.cuda.current_stream(s.device)
         starts = list(range(0, T, K))
         for a in starts:
             b = min(a + K, T)
             self._ckpt[a] = None if a == 0 else [t.clone() for t in self._state_tensors()]
             if a == starts[-1]:
-                self._run_save(a, b, stream, interior_only=False)
+                self._run_save(a, b, 0, interior_only=False)
                 self._seg_ready = a
             else:
                 s.advance(a, b - a, stream=stream)
@@ -151,20 +159,28 @@ class Adjoint3D:
             gp.data_ptr()
         h = C.c_void_p()
         check(lib().ceep3d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep3d_adjoint_create")
-        stream = torch.cuda.current_stream(dev)
+        starts = sorted(self._ckpt, reverse=True)
+        overlap = self.overlap
+        if overlap is None:
+            seg_bytes = 4 * int(np.prod(self._segment_shape()))
+            overlap = len(self._segs) >= 2 or torch.cuda.mem_get_info(dev)[0] > 2 * seg_bytes
+        two = bool(overlap) and len(starts) > 1
+        self._buffers(2 if two else 1)
+
+        def recompute(a, buf):
+            self._restore(a)
+            # the recompute skips the CPML shell, which no saved value depends on
+            self._run_save(a, min(a + K, T), buf, interior_only=True)
+
+        def adjoint(a, buf):
+            st = torch.cuda.current_stream(dev)
+            b = min(a + K, T)
+            check(lib().ceep3d_adjoint_run(h, b, b - a, self._segs[buf].data_ptr(), a, C.c_void_p(st.cuda_stream)),
+                  "ceep3d_adjoint_run")
         try:
-            for a in sorted(self._ckpt, reverse=True):
-                b = min(a + K, T)
-                if a == self._seg_ready:
-                    seg = self._segment_buffer()
-                    self._seg_ready = None
-                else:
-                    self._restore(a)
-                    # the recompute skips the CPML shell, which no saved value depends on
-                    seg = self._run_save(a, b, stream, interior_only=True)
-                check(lib().ceep3d_adjoint_run(h, b, b - a, seg.data_ptr(), a, C.c_void_p(stream.cuda_stream)),
-                      "ceep3d_adjoint_run")
+            run_segments_backward(starts, self._seg_ready, recompute, adjoint, dev, two)
         finally:
+            self._seg_ready = None
             lib().ceep3d_adjoint_destroy(h)
         full = torch.zeros((ks, s.nz, s.ny, s.nx), dtype=torch.float64, device=dev)
         full[:, n + 1:s.nz - n, n + 1:s.ny - n, n + 1:s.nx - n] = grad.sum(0)

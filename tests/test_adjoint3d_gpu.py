@@ -155,3 +155,20 @@ def test_interior_only_save_pass_is_bit_identical(cuda_device):
         assert torch.equal(fa[k], fb[k])
     for k in ("hx", "hy", "hz"):
         assert torch.equal(fa[k][box], fb[k][box])
+
+
+def test_adjoint3d_overlapped_recompute_gives_the_same_gradient(cuda_device):
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200.adjoint3d import Adjoint3D, probes_with_grad_3d
+    eps, sig, de, tau, m, ring = _case(30, 28, 26, 10)
+    res = []
+    for overlap in (False, True):
+        s = BatchedFDTD3D(30, 28, 26, 1e-3, 75, 3, ring[:3], ring, 2e9)
+        s.set_dispersion(debye=[(de, tau)])
+        adj = Adjoint3D(s, checkpoint_every=9, overlap=overlap)
+        e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+        p = probes_with_grad_3d(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                                torch.tensor(tau, device="cuda"))
+        (p.double() ** 2).sum().backward()
+        res.append(e.grad.clone())
+    assert torch.equal(res[0], res[1])

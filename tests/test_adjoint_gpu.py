@@ -140,3 +140,22 @@ def test_checkpoint_interval_does_not_change_the_gradient(cuda_device):
         (p.double() ** 2).sum().backward()
         res.append(e.grad.clone())
     assert torch.equal(res[0], res[1]) and torch.equal(res[0], res[2])
+
+
+def test_overlapped_recompute_gives_the_same_gradient(cuda_device):
+    """The two-stream backward (recompute of the next segment beside the
+    adjoint of the current one) gives the sequential backward's bits."""
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    eps, sig, de, tau, m, ring = _case(72, 64, 6, 8)
+    res = []
+    for overlap in (False, True):
+        s = BatchedFDTD2D(72, 64, 0.5e-3, 130, 6, ring[:3], ring, 2e9)
+        s.set_dispersion(debye=[(de, tau)])
+        adj = Adjoint2D(s, checkpoint_every=11, overlap=overlap)
+        e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+        p = probes_with_grad(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                             torch.tensor(tau, device="cuda"))
+        (p.double() ** 2).sum().backward()
+        res.append(e.grad.clone())
+    assert torch.equal(res[0], res[1])
