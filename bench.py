@@ -251,8 +251,11 @@ def run_ours(args, w):
     value = world * K * cell_steps / (total_ms * 1e-3) / 1e9
 
     # -- dominant kernel alone: the fused step kernel (one or two steps per
-    # launch), per-launch time over full loops; each launch reads and writes
-    # every state word once, so its algorithmic bytes are one step's formula
+    # launch), per-launch time over full loops.  Algorithmic bytes per launch
+    # = the unblocked per-cell-step formula x the cell-steps one launch
+    # advances (two steps for the temporally blocked kernel, which reads and
+    # writes the state once for both: its DRAM traffic is below that figure,
+    # reported separately as dram_gbs)
     launches = solver.launches(w["steps"]) if w.get("dim", 2) == 2 else w["steps"]
     per_launch = []
     for k in range(3):
@@ -267,7 +270,9 @@ def run_ours(args, w):
     launch_ms = float(np.median(per_launch))
     bytes_step = algorithmic_bytes_per_step(w, n_debye)
     peak, peak_src = hbm_peak()
-    achieved = bytes_step / (launch_ms * 1e-3) / 1e9
+    steps_per_launch = tblock if w.get("dim", 2) == 2 else 1
+    bytes_launch = bytes_step * steps_per_launch
+    achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
     traffic = None
     kname = "fdtd2d_step2" if tblock == 2 else "fdtd2d_step"
     tpath = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}.md")
@@ -307,9 +312,11 @@ def run_ours(args, w):
                      "kernel": (("fdtd2d_step2_kernel (two steps per launch)" if tblock == 2 else
                                  "fdtd2d_step_kernel") if w.get("dim", 2) == 2 else
                                 "fdtd3d step: h + e + source/probe launches"),
-                     "steps_per_launch": tblock,
+                     "steps_per_launch": steps_per_launch,
                      "launch_ms": round(launch_ms, 5),
-                     "algorithmic_bytes_per_launch": bytes_step},
+                     "algorithmic_bytes_per_step": bytes_step,
+                     "algorithmic_bytes_per_launch": bytes_launch,
+                     "dram_gbs": (round(traffic / (launch_ms * 1e-3) / 1e9, 1) if traffic else None)},
         "gpu_launches": K * ((launches if w.get("dim", 2) == 2 else 3 * w["steps"]) + 3),
         "clocks": clk.summary(),
     }
@@ -789,7 +796,7 @@ def run_profile(args, w):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="head600",
