@@ -26,6 +26,10 @@ das_small         DelayAndSumBeamformer DAS and DMAS on a 6-antenna S-matrix
 das_time_small    das_imaging (scripts/verify_dataset_with_das.py)
 ade2d_small       batched step composed with DispersiveManager (Debye pole 0,
                   Lorentz pole 1), 44x40, CPML 5, 2 TX, 220 steps
+single2d          the non-batched FDTD2D (TMz and TEz) with CFS-CPML, PEC and
+                  Mur boundaries, Gaussian / modulated / CW sources on every
+                  component, circle and region materials (sigma_m too);
+                  probes, snapshots, final fields, coefficient maps, waveforms
 brain_phantom     BrainPhantom2D.get_eps_map (fixed tissue table) for a
                   head-sized 400x380 grid with and without hemorrhage, and
                   the 64x64 dataset-generator grid; hemorrhage masks as
@@ -285,7 +289,101 @@ def gen_brain_phantom():
     _save("brain_phantom", **out)
 
 
+# non-batched FDTD2D cases: (name, mode, nx, ny, steps, boundaries, sources, probes,
+# record_field, record_interval, materials)
+SINGLE2D = [
+    ("tmz_cpml", "TMZ", 64, 56, 320,
+     [("cpml", 8, 4, 2.0, 0.05, 1.0)],
+     [("gauss", 30, 24, 20e9, 1.0, 6.0, "Ez"), ("modgauss", 4, 30, 8e9, 20e9, 0.5, 5.0, "Ez"),
+      ("gauss", 40, 40, 20e9, 1.0, 6.0, "Hz")],
+     [(30, 24), (50, 44), (3, 10), (62, 54)], "Ez", 40,
+     [("circle", 34, 28, 7, 4.0, 1.0, 0.2, 0.0), ("region", 10, 20, 36, 48, 2.5, 1.0, 0.05, 0.0)]),
+    ("tez_cpml", "TEZ", 60, 52, 300,
+     [("cpml", 6, 3, 1.5, 0.1, 2.0)],
+     [("gauss", 28, 26, 20e9, 1.0, 6.0, "Hz"), ("gauss", 20, 30, 15e9, 0.7, 5.0, "Ex"),
+      ("sin", 36, 18, 12e9, 0.3, "Ey"), ("gauss", 33, 33, 20e9, 1.0, 6.0, "Ez")],
+     [(28, 26), (45, 40), (2, 2), (58, 25)], "Hz", 50,
+     [("circle", 30, 26, 6, 5.0, 1.0, 0.3, 0.0), ("region", 40, 50, 10, 20, 1.0, 2.0, 0.0, 300.0)]),
+    ("tmz_pec", "TMZ", 40, 36, 220, [("pec",)],
+     [("gauss", 12, 20, 20e9, 1.0, 6.0, "Ez")], [(12, 20), (30, 10), (0, 5)], "Ez", 55,
+     [("circle", 22, 18, 5, 6.0, 1.0, 0.1, 0.0)]),
+    ("tmz_mur", "TMZ", 42, 38, 240, [("mur",)],
+     [("gauss", 20, 19, 20e9, 1.0, 6.0, "Ez")], [(20, 19), (35, 30), (0, 0), (41, 10)], None, 1,
+     [("region", 5, 15, 5, 15, 3.0, 1.0, 0.0, 0.0)]),
+    ("tez_pec_cpml", "TEZ", 48, 44, 260, [("pec",), ("cpml", 7, 4, 2.0, 0.05, 1.0)],
+     [("gauss", 24, 22, 20e9, 1.0, 6.0, "Hz")], [(24, 22), (10, 35), (47, 43)], "Ey", 65,
+     [("circle", 24, 22, 5, 3.0, 1.0, 0.0, 0.0)]),
+    ("tez_mur", "TEZ", 40, 40, 200, [("mur",)],
+     [("gauss", 18, 21, 20e9, 1.0, 6.0, "Hz")], [(18, 21), (39, 39), (1, 20)], "Hz", 40, []),
+]
+
+
+def gen_single2d():
+    """The reference's own non-batched FDTD2D (TMz/TEz) with CPML, PEC and Mur
+    boundaries, mixed sources and materials; probes, snapshots, final fields."""
+    import_reference(np.float64)
+    from ceep.boundaries.absorbing import CPML, PEC, MurABC
+    from ceep.core.config import GridConfig, SimulationConfig, SimulationMode
+    from ceep.solvers.fdtd_2d import FDTD2D
+    from ceep.sources.waveforms import GaussianSource, ModulatedGaussianSource, SinusoidalSource
+    out = {}
+    for name, mode, nx, ny, steps, bcs, srcs, prbs, rec, interval, mats in SINGLE2D:
+        cfg = SimulationConfig(grid=GridConfig(nx=nx, ny=ny, dx=1e-3, dy=0.8e-3),
+                               mode=getattr(SimulationMode, mode), total_steps=steps)
+        boundaries = []
+        for b in bcs:
+            if b[0] == "cpml":
+                boundaries.append(CPML(thickness=b[1], order=b[2], sigma_factor=b[3], alpha_max=b[4],
+                                       kappa_max=b[5]))
+            elif b[0] == "mur":
+                boundaries.append(MurABC())
+            else:
+                boundaries.append(PEC())
+        sources = []
+        for sp in srcs:
+            if sp[0] == "gauss":
+                sources.append(GaussianSource(x=sp[1], y=sp[2], frequency_max=sp[3], amplitude=sp[4],
+                                              delay_factor=sp[5], field_component=sp[6]))
+            elif sp[0] == "modgauss":
+                sources.append(ModulatedGaussianSource(x=sp[1], y=sp[2], frequency=sp[3], bandwidth=sp[4],
+                                                       amplitude=sp[5], delay_factor=sp[6],
+                                                       field_component=sp[7]))
+            else:
+                sources.append(SinusoidalSource(x=sp[1], y=sp[2], frequency=sp[3], amplitude=sp[4],
+                                                field_component=sp[5]))
+        s = FDTD2D(cfg, sources=sources, boundaries=boundaries, record_field=rec, record_interval=interval,
+                   probe_points=[tuple(p) for p in prbs])
+        for m in mats:
+            if m[0] == "circle":
+                s.grid.set_material_circle(m[1], m[2], m[3], eps_r=m[4], mu_r=m[5], sigma_e=m[6], sigma_m=m[7])
+            else:
+                s.grid.set_material_region(m[1], m[2], m[3], m[4], eps_r=m[5], mu_r=m[6], sigma_e=m[7],
+                                           sigma_m=m[8])
+        s.grid._precompute_coefficients()
+        # on the NumPy array module the reference's snapshots alias the live
+        # field (to_numpy returns the array itself), so every entry ends up as
+        # the final state; the snapshots kept here are copies taken after the
+        # reference's own step() at the steps its _record() would use
+        snaps = []
+        for n in range(steps):
+            s.step()
+            if rec and n % interval == 0:
+                snaps.append(np.array(s.get_field(rec)))
+        g = s.grid
+        fields = ("ez", "hx", "hy") if mode == "TMZ" else ("hz", "ex", "ey")
+        out[name + "_probes"] = np.array([s.probe_data[tuple(p)] for p in prbs])
+        out[name + "_snapshots"] = np.array(snaps) if snaps else np.zeros((0, nx, ny))
+        for f in fields:
+            out[f"{name}_{f}"] = np.asarray(getattr(g, f))
+        for k in ("_ca", "_cb", "_da", "_db"):
+            out[name + k] = np.asarray(getattr(g, k))
+        out[name + "_dt"] = np.float64(cfg.dt)
+        out[name + "_waveforms"] = np.array([[src.value_at(n, cfg.dt) for n in range(steps)] for src in sources])
+    _save("single2d", **out)
+
+
 JOBS = {
+    "single2d": gen_single2d,
     "ceep_results": gen_ceep_results,
     "brain_phantom": gen_brain_phantom,
     "small": lambda: (gen_small(np.float64), gen_small(np.float32)),
