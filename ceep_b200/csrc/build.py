@@ -18,7 +18,8 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libceep_b200.so")
-SOURCES = ["capi.cu", "fdtd2d.cu", "fdtd3d.cu", "adjoint2d.cu", "adjoint3d.cu", "spectral.cu", "phantom.cu"]
+SOURCES = ["capi.cu", "fdtd2d.cu", "fdtd3d.cu", "adjoint2d.cu", "adjoint3d.cu", "spectral.cu", "phantom.cu",
+           "single2d.cu"]
 HEADERS = ["common.cuh", "fdtd2d.cuh", "fdtd3d.cuh", "adjoint2d.cuh", "adjoint3d.cuh", "tma.cuh",
            "capi_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

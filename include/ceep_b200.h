@@ -244,6 +244,53 @@ int ceep3d_plan_destroy(ceep3d_plan* plan);
 int64_t ceep3d_desc_size(void);
 
 /* ------------------------------------------------------------------------
+ * Non-batched 2D FDTD, TMz or TEz, one field set.
+ * Replaces FDTD2D.step()/run() (src/ceep/solvers/fdtd_2d.py:111-260 through
+ * src/ceep/solvers/fdtd_base.py:158-210) with the boundaries PEC
+ * (src/ceep/boundaries/absorbing.py:48-78), MurABC (:80-172, last in the
+ * list only) and CFS-CPML (:174-561, one per plan), soft sources and the
+ * probe / monitor recording of FDTD2D._record (fdtd_2d.py:277-291).
+ * Fields are (nx, ny) float with y fastest (the reference's arrays).
+ * ---------------------------------------------------------------------- */
+typedef struct ceep2s_desc {
+  int32_t nx, ny;
+  int32_t mode;             /* 0 TMz: f0 Ez, f1 Hx, f2 Hy; 1 TEz: f0 Hz, f1 Ex, f2 Ey */
+  int32_t nsteps;
+  float inv_dx, inv_dy;
+  float dt_mu0, dt_eps0;    /* scale of the CPML H and E corrections          */
+  float mur_kx, mur_ky;     /* (c dt - d) / (c dt + d)                         */
+  float *f0, *f1, *f2;
+  const float* coef_e;      /* (nx, ny, 2): ca, cb                             */
+  const float* coef_h;      /* (nx, ny, 2): da, db                             */
+  int32_t n_ops;            /* boundary operations in list order (<= 4):      */
+  int32_t ops[4];           /* 1 CPML, 2 PEC, 3 Mur (Mur last)                 */
+  int32_t cpml_t;           /* CPML thickness                                  */
+  const float* cpml;        /* (8, t): be_x ce_x bh_x ch_x be_y ce_y bh_y ch_y */
+  float* psi;               /* 4 x (t, ny) E/E/H/H x-lo/x-hi, then 4 x (nx, t)
+                               E/E/H/H y-lo/y-hi, zeroed by the caller         */
+  float* mur_prev;          /* 2 x (2 ny + 2 nx), zeroed by the caller         */
+  int32_t nsrc;
+  int32_t hz_sources;       /* nonzero: TEz sources on Hz (field 0) exist      */
+  const int32_t* src;       /* (nsrc, 3) x, y, field; stable-sorted by x       */
+  const int32_t* src_row;   /* (nx + 1) offsets of each x in src               */
+  const float* waveform;    /* (nsrc, nsteps) in the order of src              */
+  int32_t nrec;
+  const int32_t* rec;       /* (nrec, 2) flat cell index, field                */
+  float* rec_out;           /* (nrec, nsteps)                                  */
+  int32_t snap_field, snap_interval;
+  float* snapshots;         /* (ceil(nsteps / interval), nx, ny) or NULL       */
+} ceep2s_desc;
+
+typedef struct ceep2s_plan ceep2s_plan;
+int ceep2s_plan_create(const ceep2s_desc* desc, ceep2s_plan** out);
+/* Steps step0 .. step0+nsteps-1 (the step index selects the waveform column,
+ * the record column and the Mur state half); graph-captured per
+ * (step0, nsteps) when use_graph and a stream are given. */
+int ceep2s_plan_run(ceep2s_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+int ceep2s_plan_destroy(ceep2s_plan* plan);
+int64_t ceep2s_desc_size(void);
+
+/* ------------------------------------------------------------------------
  * 3D adjoint: the exact transpose of the 3D step restricted to what the
  * probe series depends on (the E interior [n+1, N-n)^3 and the H box
  * [n, N-n)^3, which no CPML face touches), giving per-cell gradients of a

@@ -1,0 +1,133 @@
+"""The non-batched FDTD2D on the GPU against the reference's own run
+(tests/golden/single2d.npz: TMz / TEz, CFS-CPML, PEC, Mur, every source
+component) and against the oracle, at the 1e-4 relative L2 bar."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+from make_golden import SINGLE2D  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+GOLD = np.load(os.path.join(HERE, "golden", "single2d.npz"))
+FIELDS = {"TMZ": ("ez", "hx", "hy"), "TEZ": ("hz", "ex", "ey")}
+
+
+def build(case, **kw):
+    from ceep_b200 import fdtd2d as F
+    name, mode, nx, ny, steps, bcs, srcs, prbs, rec, interval, mats = case
+    cfg = F.SimulationConfig(grid=F.GridConfig(nx=nx, ny=ny, dx=1e-3, dy=0.8e-3),
+                             mode=getattr(F.SimulationMode, mode), total_steps=steps)
+    boundaries = []
+    for b in bcs:
+        if b[0] == "cpml":
+            boundaries.append(F.CPML(thickness=b[1], order=b[2], sigma_factor=b[3], alpha_max=b[4], kappa_max=b[5]))
+        else:
+            boundaries.append(F.MurABC() if b[0] == "mur" else F.PEC())
+    sources = []
+    for sp in srcs:
+        if sp[0] == "gauss":
+            sources.append(F.GaussianSource(x=sp[1], y=sp[2], frequency_max=sp[3], amplitude=sp[4],
+                                            delay_factor=sp[5], field_component=sp[6]))
+        elif sp[0] == "modgauss":
+            sources.append(F.ModulatedGaussianSource(x=sp[1], y=sp[2], frequency=sp[3], bandwidth=sp[4],
+                                                     amplitude=sp[5], delay_factor=sp[6], field_component=sp[7]))
+        else:
+            sources.append(F.SinusoidalSource(x=sp[1], y=sp[2], frequency=sp[3], amplitude=sp[4],
+                                              field_component=sp[5]))
+    s = F.FDTD2D(cfg, sources=sources, boundaries=boundaries, record_field=rec, record_interval=interval,
+                 probe_points=[tuple(p) for p in prbs], **kw)
+    for m in mats:
+        if m[0] == "circle":
+            s.grid.set_material_circle(m[1], m[2], m[3], eps_r=m[4], mu_r=m[5], sigma_e=m[6], sigma_m=m[7])
+        else:
+            s.grid.set_material_region(m[1], m[2], m[3], m[4], eps_r=m[5], mu_r=m[6], sigma_e=m[7], sigma_m=m[8])
+    return s
+
+
+@pytest.mark.parametrize("case", SINGLE2D, ids=[c[0] for c in SINGLE2D])
+def test_fdtd2d_matches_reference(cuda_device, case):
+    name, mode, nx, ny, steps, bcs, srcs, prbs, rec, interval, mats = case
+    s = build(case)
+    s.run()
+    assert s.current_step == steps
+    got = np.array([s.probe_data[tuple(p)] for p in prbs])
+    ref = GOLD[f"{name}_probes"]
+    err = rel_l2(got, ref)
+    print(f"{name}: probes rel L2 {err:.2e}")
+    assert err < TOL
+    for f in FIELDS[mode]:
+        e = rel_l2(getattr(s.grid, f).double().cpu().numpy(), GOLD[f"{name}_{f}"])
+        assert e < TOL, (f, e)
+    snaps = GOLD[f"{name}_snapshots"]
+    assert len(s.field_snapshots) == len(snaps)
+    if len(snaps):
+        assert rel_l2(np.array(s.field_snapshots), snaps) < TOL
+
+
+def test_step_by_step_equals_run_and_graph_equals_stream(cuda_device):
+    case = SINGLE2D[1]
+    a = build(case)
+    a.run()
+    b = build(case, use_graph=False)
+    for _ in range(case[4]):
+        b.step()
+    c = build(case)
+    c.run(100)
+    c.run(case[4] - 100)   # grows past nothing, second graph
+    for other in (b, c):
+        for f in FIELDS[case[1]]:
+            assert torch.equal(getattr(a.grid, f), getattr(other.grid, f))
+        assert a.probe_data == other.probe_data
+        assert all(np.array_equal(x, y) for x, y in zip(a.field_snapshots, other.field_snapshots))
+
+
+def test_run_past_the_configured_steps(cuda_device):
+    """Running more steps than config.num_steps regrows the waveform and
+    record buffers and keeps what was recorded."""
+    case = SINGLE2D[2]
+    a = build(case)
+    a.run(case[4] + 60)
+    b = build(case)
+    b.run()
+    b.run(60)
+    assert a.probe_data == b.probe_data
+    assert torch.equal(a.grid.ez, b.grid.ez)
+
+
+def test_dft_monitor_matches_oracle_series(cuda_device):
+    from ceep_b200 import fdtd2d as F
+    from oracle.fdtd2d_single import Single2DOracle
+    case = SINGLE2D[0]
+    name, mode, nx, ny, steps, bcs, srcs, prbs, rec, interval, mats = case
+    freqs = np.array([3e9, 6e9, 9e9])
+    mon = F.DFTMonitor(freqs, (slice(20, 26), slice(30, 33)), component="Ez")
+    pt = F.DFTMonitor(freqs, (40, 12), component="Ez")
+    s = build(case)
+    s.dft_monitors = [mon, pt]
+    s.initialize(s.config)
+    for m in mats:
+        if m[0] == "circle":
+            s.grid.set_material_circle(m[1], m[2], m[3], eps_r=m[4], mu_r=m[5], sigma_e=m[6], sigma_m=m[7])
+        else:
+            s.grid.set_material_region(m[1], m[2], m[3], m[4], eps_r=m[5], mu_r=m[6], sigma_e=m[7], sigma_m=m[8])
+    s.run()
+    cells = [(i, j) for i in range(20, 26) for j in range(30, 33)] + [(40, 12)]
+    w = GOLD[f"{name}_waveforms"]
+    g = lambda k: GOLD[f"{name}_{k}"]
+    o = Single2DOracle(nx, ny, 1e-3, 0.8e-3, float(g("dt")), mode, g("ca"), g("cb"), g("da"), g("db"),
+                       [(sp[1], sp[2], sp[-1], w[k]) for k, sp in enumerate(srcs)], bcs, cells, "Ez", 10 ** 9)
+    o.run(steps)
+    ser = np.array([o.probe_data[c] for c in cells])                      # (cells, T)
+    t = np.arange(steps) * float(g("dt"))
+    ph = 2 * np.pi * freqs[:, None] * t[None, :]
+    ref = (np.cos(ph) - 1j * np.sin(ph)) @ ser.T * float(g("dt"))         # (F, cells)
+    got = np.concatenate([mon.get_complex_field().reshape(3, -1), pt.get_complex_field().reshape(3, 1)], 1)
+    assert rel_l2(np.concatenate([got.real, got.imag]), np.concatenate([ref.real, ref.imag])) < TOL
