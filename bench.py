@@ -631,6 +631,110 @@ def run_adjoint3d_bench(args):
     print(json.dumps(line), flush=True)
 
 
+def single_bytes_per_cell_step(mode, n, nx, ny):
+    """Unblocked compulsory bytes of one step of the non-batched solver: the
+    three fields read and written (24 B per cell) and the four update
+    coefficients (16 B per cell), plus psi read+write (8 B) per CPML strip
+    cell and field: 2 for TMz cells on the x strips (Hy, Ez) and the y strips
+    (Hx, Ez), same count for TEz."""
+    strip_x = 2 * n * ny
+    strip_y = 2 * n * nx
+    return 40 * nx * ny + 2 * 8 * (strip_x + strip_y)
+
+
+def run_single_bench(args):
+    """The non-batched FDTD2D (fdtd_2d.py) on a grid well above L2: TMz,
+    4096 x 4096, 1 mm, CFS-CPML 20 cells, a Gaussian Ez source at the centre,
+    eight probes, 1000 steps per bench step; GCell-steps/s (cells x steps)."""
+    import torch
+    from ceep_b200 import fdtd2d as F
+    dev = torch.device("cuda", 0)
+    nx = ny = 1024 if args.small else 4096
+    T, n = 1000, 20
+    cfg = F.SimulationConfig(grid=F.GridConfig(nx=nx, ny=ny, dx=1e-3, dy=1e-3), mode=F.SimulationMode.TMZ,
+                             total_steps=T)
+    src = [F.GaussianSource(x=nx // 2, y=ny // 2, frequency_max=20e9)]
+    prb = [(nx // 2 + int(0.3 * nx * np.cos(a)), ny // 2 + int(0.3 * ny * np.sin(a)))
+           for a in np.linspace(0, 2 * np.pi, 8, endpoint=False)]
+    s = F.FDTD2D(cfg, sources=src, boundaries=[F.CPML(thickness=n)], probe_points=prb)
+    s.grid.set_material_circle(nx // 2, ny // 2, nx // 5, eps_r=4.0, sigma_e=0.2)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device=dev)   # 256 MB
+
+    def one():
+        s.grid.reset_fields()
+        s._psi.zero_()
+        s._step = 0
+        s._pending = 0
+        s.advance(T, stream=stream)
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            one()
+            b.record(stream)
+        torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total = float(np.sum(ms))
+    value = len(ms) * nx * ny * T / (total * 1e-3) / 1e9
+    step_ms = float(np.median(ms)) / T
+    peak, src_peak = hbm_peak()
+    bytes_step = single_bytes_per_cell_step("TMZ", n, nx, ny)
+    achieved = bytes_step / (step_ms * 1e-3) / 1e9
+    # e2e through the public API: maps and sources in from the host, run(),
+    # probe series back as host lists
+    host_eps = s.grid.eps_r.copy()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    s2 = F.FDTD2D(cfg, sources=src, boundaries=[F.CPML(thickness=n)], probe_points=prb)
+    s2.grid.eps_r[:] = host_eps
+    s2.grid.eps_inf[:] = host_eps
+    s2.grid.sigma_e[:] = s.grid.sigma_e
+    s2.grid._precompute_coefficients()
+    s2.run()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = t0.elapsed_time(t1)
+    cpu = None
+    if not args.no_cpu:
+        from oracle.fdtd2d_single import Single2DOracle
+        import time
+        g = s.grid
+        w = [np.array([src[0].value_at(k, cfg.dt) for k in range(T)])]
+        o = Single2DOracle(nx, ny, 1e-3, 1e-3, cfg.dt, "TMZ", g._ca, g._cb, g._da, g._db,
+                           [(nx // 2, ny // 2, "Ez", w[0])], [("cpml", n, 4, 2.0, 0.05, 1.0)], prb)
+        k = 6
+        t = time.perf_counter()
+        o.run(k)
+        el = time.perf_counter() - t
+        cpu = {"value": round(nx * ny * k / el / 1e9, 5), "unit": "GCell-steps/s", "cores": 1, "kind": "port",
+               "sample": f"{k} of {T} time steps, FP64 NumPy oracle, {el:.1f} s"}
+    line = {"metric": "FDTD2D (non-batched) GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
+            "n_gpus": 1, "steps": len(ms), "warmup": args.warmup, "ms_per_step": round(total / len(ms), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (dielectric disk)",
+            "config": {"workload": "single4096" if not args.small else "single1024", "nx": nx, "ny": ny,
+                       "mode": "TMz", "time_steps": T, "cpml": n, "boundary": "CFS-CPML",
+                       "l2": "256 MB flush before every bench step; state 335 MB > L2"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 3), "traffic": None, "peak_source": src_peak,
+                         "kernel": "single2d_h_kernel + single2d_e_kernel (+ record) per step",
+                         "algorithmic_bytes_per_step": bytes_step, "step_ms": round(step_ms, 5)},
+            "e2e": {"value": round(nx * ny * T / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GCell-steps/s",
+                    "h2d_bytes_per_step": 4 * 4 * nx * ny, "d2h_bytes_per_step": 4 * len(prb) * T,
+                    "path": "FDTD2D(...) + set materials + run(), probe lists back on the host"},
+            "gpu_launches": len(ms) * 3 * T,
+            "clocks": clk.summary()}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def _pack_solvers(count, device, seed=2024):
     """Config-3 phantoms: nx, ny in {256..768 step 32}, steps in [600, 1200],
     8-16 TX, one third with a two-pole Lorentz model instead of Debye."""
@@ -800,7 +904,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="head600",
-                    choices=list(WORKLOADS) + ["adjoint400", "adjoint192", "pack256"])
+                    choices=list(WORKLOADS) + ["adjoint400", "adjoint192", "pack256", "single4096"])
     ap.add_argument("--pack-count", type=int, default=256)
     ap.add_argument("--pack-sample", type=int, default=32)
     ap.add_argument("--small", action="store_true", help="with --profile: a smaller 3D grid")
@@ -825,6 +929,9 @@ def main():
             run_profile_adjoint3d(args)
         else:
             run_adjoint3d_bench(args)
+        return
+    if args.workload == "single4096":
+        run_single_bench(args)
         return
     if args.workload == "pack256":
         run_pack_bench(args)
