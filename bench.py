@@ -662,10 +662,7 @@ def run_single_bench(args):
     flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device=dev)   # 256 MB
 
     def one():
-        s.grid.reset_fields()
-        s._psi.zero_()
-        s._step = 0
-        s._pending = 0
+        s.reset()
         s.advance(T, stream=stream)
     for _ in range(args.warmup):
         one()
@@ -723,7 +720,7 @@ def run_single_bench(args):
                        "l2": "256 MB flush before every bench step; state 335 MB > L2"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 3), "traffic": None, "peak_source": src_peak,
-                         "kernel": "single2d_h_kernel + single2d_e_kernel (+ record) per step",
+                         "kernel": "single2d_step_kernel interior + frame launches (+ record) per step",
                          "algorithmic_bytes_per_step": bytes_step, "step_ms": round(step_ms, 5)},
             "e2e": {"value": round(nx * ny * T / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GCell-steps/s",
                     "h2d_bytes_per_step": 4 * 4 * nx * ny, "d2h_bytes_per_step": 4 * len(prb) * T,

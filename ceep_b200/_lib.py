@@ -79,6 +79,8 @@ _SIGS = {
     "ceep2s_plan_create": (C.c_int, [P, C.POINTER(P)]),
     "ceep2s_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),
     "ceep2s_plan_destroy": (C.c_int, [P]),
+    "ceep2s_plan_current_buffer": (C.c_int, [P]),
+    "ceep2s_plan_set_current_buffer": (C.c_int, [P, C.c_int]),
     "ceep2s_desc_size": (I64, []),
     "ceep3d_adjoint_create": (C.c_int, [P, P, C.POINTER(P)]),
     "ceep3d_adjoint_run": (C.c_int, [P, I64, I64, P, I64, P]),

@@ -3,13 +3,17 @@
 // src/ceep/solvers/fdtd_2d.py:111-260, src/ceep/boundaries/absorbing.py).
 //
 // One step is
-//   H kernel   plain H update of every cell plus the CPML H corrections of
-//              the strip cells (they read only E, so each cell finishes its
-//              H values alone; absorbing.py:332-451)
-//   E kernel   plain E update, the soft sources of E components at the cell
-//              (list order), then the boundary operations in list order:
-//              CPML E corrections (absorbing.py:453-561) and PEC zeroing
-//              (absorbing.py:58-72).  E corrections read only H.
+//   step kernel  two launches, the interior blocks (no CPML code) and the
+//                frame of blocks around them; warps walk 31-column strips
+//                row by row: the H update of
+//                every cell with its CPML H corrections (absorbing.py:332-451;
+//                they read only E), then the E update of the cell from H in
+//                registers (neighbours by shuffle), the soft sources of E
+//                components at the cell (list order) and the boundary
+//                operations in list order: CPML E corrections
+//                (absorbing.py:453-561) and PEC zeroing (absorbing.py:58-72).
+//                Fields and the H psi are ping-pong buffered (read [cur],
+//                write [cur ^ 1]); the E psi is updated in place.
 //   Hz-source  one thread adds TEz Hz sources in list order (Hz is read by
 //              the neighbours' E updates, so it cannot be added inside the
 //              E kernel)
@@ -18,7 +22,8 @@
 //              faces (absorbing.py:126-166); last boundary operation only
 //   record     probe / monitor cells into (nrec, nsteps), and a copy of the
 //              snapshot field every snap_interval steps
-// Fields are (nx, ny) FP32 with y fastest, the reference's layout.  All
+// Fields are (nx, ny) FP32 with y fastest, the reference's layout; a step
+// reads and writes each field and reads each coefficient pair once.  All
 // launches of a run are captured once into a CUDA graph and replayed.
 #include <map>
 #include <tuple>
@@ -29,18 +34,17 @@
 
 namespace ceep {
 
-constexpr int kS2x = 32, kS2y = 8;  // threads per block along y (fastest) and x
-
 struct Single2dParams {
   int nx, ny, mode, nsteps;
   float inv_dx, inv_dy, dt_mu0, dt_eps0, mur_kx, mur_ky;
-  float* f[3];
-  const float2* ce;  // ca, cb
-  const float2* ch;  // da, db
+  float* f[3][2];     // ping-pong fields: read [cur], write [cur ^ 1]
+  const float2* ce;   // ca, cb
+  const float2* ch;   // da, db
   int n_ops, ops[4];
   int t;
   const float* cpml;  // be_x, ce_x, bh_x, ch_x, be_y, ce_y, bh_y, ch_y: t each
-  float* psi;         // 4 x (t, ny): E x-lo, E x-hi, H x-lo, H x-hi; 4 x (nx, t): E/H y-lo/hi
+  float* psi_e;       // x-lo, x-hi (t, ny) each, then y-lo, y-hi (nx, t) each; updated in place
+  float* psi_h[2];    // same layout, ping-pong (neighbour tiles recompute from the read half)
   float* mur_prev;    // two sets of (ny, ny, nx, nx)
   int nsrc;
   const int* src;      // (nsrc, 3) x, y, field, sorted by x (stable)
@@ -72,209 +76,349 @@ CEEP_D Strips strips(int i, int n, int t, bool h_rule) {
   return s;
 }
 
-template <int MODE, bool CPML>
-__global__ void __launch_bounds__(kS2x * kS2y) single2d_h_kernel(const Single2dParams p) {
-  const int j = blockIdx.x * kS2x + threadIdx.x;
-  const int i = blockIdx.y * kS2y + threadIdx.y;
-  const int nx = p.nx, ny = p.ny;
-  if (i >= nx || j >= ny) return;
-  const size_t c = (size_t)i * ny + j;
-  const float2 d = __ldg(p.ch + c);
-  const float* bhx = p.cpml + 2 * p.t;
-  const float* chx = p.cpml + 3 * p.t;
-  const float* bhy = p.cpml + 6 * p.t;
-  const float* chy = p.cpml + 7 * p.t;
-  float* psi_hx = p.psi + 2 * (size_t)p.t * ny;      // H x-lo, then H x-hi
-  float* psi_hy = p.psi + 4 * (size_t)p.t * ny + 2 * (size_t)nx * p.t;  // H y-lo, then H y-hi
-  if (MODE == 0) {
-    // TMz: Hx (fdtd_2d.py:132-136), Hy (:139-142); CPML x strips act on Hy,
-    // y strips on Hx (absorbing.py:413-451)
-    const float* ez = p.f[0];
-    float* hx = p.f[1];
-    float* hy = p.f[2];
-    const float e0 = __ldg(ez + c);
-    const float dy = j + 1 < ny ? __ldg(ez + c + 1) - e0 : 0.f;
-    const float dx = i + 1 < nx ? __ldg(ez + c + ny) - e0 : 0.f;
-    float vx = hx[c], vy = hy[c];
-    if (j < ny - 1) vx = d.x * vx - (d.y * p.inv_dy) * dy;
-    if (i < nx - 1) vy = d.x * vy + (d.y * p.inv_dx) * dx;
-    if (CPML) {
-      const int t = p.t;
-      const Strips sx = strips(i, nx, t, true);
-      if (sx.lo >= 0) {
-        float* q = psi_hx + (size_t)sx.lo * ny + j;
-        const float v = bhx[sx.lo_k] * *q + chx[sx.lo_k] * dx * p.inv_dx;
-        *q = v;
-        vy += p.dt_mu0 * v;
-      }
-      if (sx.hi >= 0) {
-        float* q = psi_hx + (size_t)(t + sx.hi) * ny + j;
-        const float v = bhx[sx.hi] * *q + chx[sx.hi] * dx * p.inv_dx;
-        *q = v;
-        vy += p.dt_mu0 * v;
-      }
-      const Strips sy = strips(j, ny, t, true);
-      if (sy.lo >= 0) {
-        float* q = psi_hy + (size_t)i * t + sy.lo;
-        const float v = bhy[sy.lo_k] * *q + chy[sy.lo_k] * dy * p.inv_dy;
-        *q = v;
-        vx -= p.dt_mu0 * v;
-      }
-      if (sy.hi >= 0) {
-        float* q = psi_hy + (size_t)nx * t + (size_t)i * t + sy.hi;
-        const float v = bhy[sy.hi] * *q + chy[sy.hi] * dy * p.inv_dy;
-        *q = v;
-        vx -= p.dt_mu0 * v;
-      }
-    }
-    hx[c] = vx;
-    hy[c] = vy;
-  } else {
-    // TEz: Hz (fdtd_2d.py:169-183); CPML x strips subtract, y strips add
-    // (absorbing.py:355-405)
-    float* hz = p.f[0];
-    const float* ex = p.f[1];
-    const float* ey = p.f[2];
-    const float x0 = __ldg(ex + c), y0 = __ldg(ey + c);
-    const float dex = j + 1 < ny ? __ldg(ex + c + 1) - x0 : 0.f;
-    const float dey = i + 1 < nx ? __ldg(ey + c + ny) - y0 : 0.f;
-    float v = hz[c];
-    if (i < nx - 1 && j < ny - 1) v = d.x * v + d.y * (dex * p.inv_dy - dey * p.inv_dx);
-    if (CPML) {
-      const int t = p.t;
-      const Strips sx = strips(i, nx, t, true);
-      if (sx.lo >= 0) {
-        float* q = psi_hx + (size_t)sx.lo * ny + j;
-        const float w = bhx[sx.lo_k] * *q + chx[sx.lo_k] * dey * p.inv_dx;
-        *q = w;
-        v -= p.dt_mu0 * w;
-      }
-      if (sx.hi >= 0) {
-        float* q = psi_hx + (size_t)(t + sx.hi) * ny + j;
-        const float w = bhx[sx.hi] * *q + chx[sx.hi] * dey * p.inv_dx;
-        *q = w;
-        v -= p.dt_mu0 * w;
-      }
-      const Strips sy = strips(j, ny, t, true);
-      if (sy.lo >= 0) {
-        float* q = psi_hy + (size_t)i * t + sy.lo;
-        const float w = bhy[sy.lo_k] * *q + chy[sy.lo_k] * dex * p.inv_dy;
-        *q = w;
-        v += p.dt_mu0 * w;
-      }
-      if (sy.hi >= 0) {
-        float* q = psi_hy + (size_t)nx * t + (size_t)i * t + sy.hi;
-        const float w = bhy[sy.hi] * *q + chy[sy.hi] * dex * p.inv_dy;
-        *q = w;
-        v += p.dt_mu0 * w;
-      }
-    }
-    hz[c] = v;
-  }
-}
-
-// CPML E correction of one strip side: psi' = b psi + c diff/d, returns psi'.
-CEEP_D float psi_e(float* q, float b, float cc, float diff, float inv) {
-  const float v = b * *q + cc * diff * inv;
-  *q = v;
+// One CPML psi recurrence psi' = b psi + c diff / d, reading `q`; written to
+// `out` when given (the owning cell), returned.
+CEEP_D float psi_step(const float* q, float* out, float b, float c, float diff, float inv) {
+  const float v = b * *q + c * diff * inv;
+  if (out) *out = v;
   return v;
 }
 
-template <int MODE, bool CPML>
-__global__ void __launch_bounds__(kS2x * kS2y) single2d_e_kernel(const Single2dParams p, int step) {
-  const int j = blockIdx.x * kS2x + threadIdx.x;
-  const int i = blockIdx.y * kS2y + threadIdx.y;
-  const int nx = p.nx, ny = p.ny;
-  if (i >= nx || j >= ny) return;
-  const size_t c = (size_t)i * ny + j;
-  const float2 k = __ldg(p.ce + c);
+// The x-strip (t, ny) and y-strip (nx, t) psi slots of cell (i, j) in a
+// psi array of the layout above; -1 when the cell is not on that side.
+struct PsiSlots {
+  long long xlo, xhi, ylo, yhi;
+  int kxlo, kylo;
+};
+CEEP_D PsiSlots psi_slots(int i, int j, int nx, int ny, int t, bool h_rule) {
+  PsiSlots s{-1, -1, -1, -1, 0, 0};
+  const Strips sx = strips(i, nx, t, h_rule), sy = strips(j, ny, t, h_rule);
+  if (sx.lo >= 0) { s.xlo = (long long)sx.lo * ny + j; s.kxlo = sx.lo_k; }
+  if (sx.hi >= 0) s.xhi = (long long)(t + sx.hi) * ny + j;
+  const long long yb = 2LL * t * ny;
+  if (sy.lo >= 0) { s.ylo = yb + (long long)i * t + sy.lo; s.kylo = sy.lo_k; }
+  if (sy.hi >= 0) s.yhi = yb + (long long)nx * t + (long long)i * t + sy.hi;
+  return s;
+}
+
+// -- CPML H corrections of one cell (absorbing.py:332-451), given the E
+// differences the cell's plain update used; psi is read from half r and, for
+// the owning cell, written to half r^1.  Each returns the signed sum to add.
+template <bool CPML>
+CEEP_D float cpml_h_x(const Single2dParams& p, int r, int i, int c, float diff, bool own) {
+  if (!CPML) return 0.f;
   const int t = p.t;
-  const float* bex = p.cpml;
-  const float* cex = p.cpml + t;
-  const float* bey = p.cpml + 4 * t;
-  const float* cey = p.cpml + 5 * t;
-  float* psi_ex = p.psi;                                  // E x-lo, then E x-hi: (t, ny)
-  float* psi_ey = p.psi + 4 * (size_t)t * ny;             // E y-lo, then E y-hi: (nx, t)
-  const bool edge = i == 0 || i == nx - 1 || j == 0 || j == ny - 1;
+  const Strips sx = strips(i, p.nx, t, true);
+  const float* bh = p.cpml + 2 * t;
+  const float* chh = p.cpml + 3 * t;
+  float acc = 0.f;
+  if (sx.lo >= 0) {
+    const long long q = (long long)sx.lo * p.ny + c;
+    acc += p.dt_mu0 * psi_step(p.psi_h[r] + q, own ? p.psi_h[r ^ 1] + q : nullptr, bh[sx.lo_k], chh[sx.lo_k], diff,
+                               p.inv_dx);
+  }
+  if (sx.hi >= 0) {
+    const long long q = (long long)(t + sx.hi) * p.ny + c;
+    acc += p.dt_mu0 * psi_step(p.psi_h[r] + q, own ? p.psi_h[r ^ 1] + q : nullptr, bh[sx.hi], chh[sx.hi], diff,
+                               p.inv_dx);
+  }
+  return acc;
+}
+
+template <bool CPML>
+CEEP_D float cpml_h_y(const Single2dParams& p, int r, int i, int c, float diff, bool own) {
+  if (!CPML) return 0.f;
+  const int t = p.t;
+  const Strips sy = strips(c, p.ny, t, true);
+  const float* bh = p.cpml + 6 * t;
+  const float* chh = p.cpml + 7 * t;
+  const long long yb = 2LL * t * p.ny;
+  float acc = 0.f;
+  if (sy.lo >= 0) {
+    const long long q = yb + (long long)i * t + sy.lo;
+    acc += p.dt_mu0 * psi_step(p.psi_h[r] + q, own ? p.psi_h[r ^ 1] + q : nullptr, bh[sy.lo_k], chh[sy.lo_k], diff,
+                               p.inv_dy);
+  }
+  if (sy.hi >= 0) {
+    const long long q = yb + (long long)p.nx * t + (long long)i * t + sy.hi;
+    acc += p.dt_mu0 * psi_step(p.psi_h[r] + q, own ? p.psi_h[r ^ 1] + q : nullptr, bh[sy.hi], chh[sy.hi], diff,
+                               p.inv_dy);
+  }
+  return acc;
+}
+
+// Plain + CPML H of one component at (i, c), everything loaded here: used
+// for the row just below a segment, which the walk does not otherwise visit.
+template <bool CPML>
+CEEP_D float tmz_hy_at(const Single2dParams& p, int r, int i, int c) {
+  const size_t k = (size_t)i * p.ny + c;
+  const float* ez = p.f[0][r];
+  const float dx = i + 1 < p.nx ? __ldg(ez + k + p.ny) - __ldg(ez + k) : 0.f;
+  const float2 d = __ldg(p.ch + k);
+  float v = __ldg(p.f[2][r] + k);
+  if (i < p.nx - 1) v = d.x * v + (d.y * p.inv_dx) * dx;
+  return v + cpml_h_x<CPML>(p, r, i, c, dx, false);
+}
+
+template <bool CPML>
+CEEP_D float tez_hz_at(const Single2dParams& p, int r, int i, int c) {
+  const size_t k = (size_t)i * p.ny + c;
+  const float* ex = p.f[1][r];
+  const float* ey = p.f[2][r];
+  const float dex = c + 1 < p.ny ? __ldg(ex + k + 1) - __ldg(ex + k) : 0.f;
+  const float dey = i + 1 < p.nx ? __ldg(ey + k + p.ny) - __ldg(ey + k) : 0.f;
+  const float2 d = __ldg(p.ch + k);
+  float v = __ldg(p.f[0][r] + k);
+  if (i < p.nx - 1 && c < p.ny - 1) v = d.x * v + d.y * (dex * p.inv_dy - dey * p.inv_dx);
+  return v - cpml_h_x<CPML>(p, r, i, c, dey, false) + cpml_h_y<CPML>(p, r, i, c, dex, false);
+}
+
+// CPML E corrections of the owning cell (absorbing.py:453-561), psi in place.
+template <bool CPML>
+CEEP_D float cpml_e_x(const Single2dParams& p, int i, int c, float diff) {
+  if (!CPML) return 0.f;
+  const int t = p.t;
+  const Strips sx = strips(i, p.nx, t, false);
+  float* q = p.psi_e;
+  float acc = 0.f;
+  if (sx.lo >= 0) {
+    const long long o = (long long)sx.lo * p.ny + c;
+    acc += p.dt_eps0 * psi_step(q + o, q + o, p.cpml[sx.lo_k], p.cpml[t + sx.lo_k], diff, p.inv_dx);
+  }
+  if (sx.hi >= 0) {
+    const long long o = (long long)(t + sx.hi) * p.ny + c;
+    acc += p.dt_eps0 * psi_step(q + o, q + o, p.cpml[sx.hi], p.cpml[t + sx.hi], diff, p.inv_dx);
+  }
+  return acc;
+}
+
+template <bool CPML>
+CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
+  if (!CPML) return 0.f;
+  const int t = p.t;
+  const Strips sy = strips(c, p.ny, t, false);
+  const long long yb = 2LL * t * p.ny;
+  float* q = p.psi_e;
+  float acc = 0.f;
+  if (sy.lo >= 0) {
+    const long long o = yb + (long long)i * t + sy.lo;
+    acc += p.dt_eps0 * psi_step(q + o, q + o, p.cpml[4 * t + sy.lo_k], p.cpml[5 * t + sy.lo_k], diff, p.inv_dy);
+  }
+  if (sy.hi >= 0) {
+    const long long o = yb + (long long)p.nx * t + (long long)i * t + sy.hi;
+    acc += p.dt_eps0 * psi_step(q + o, q + o, p.cpml[4 * t + sy.hi], p.cpml[5 * t + sy.hi], diff, p.inv_dy);
+  }
+  return acc;
+}
+
+// One step as a warp row-walk.  A warp covers columns j0-1 .. j0+30 (lane l
+// at column j0-1+l) and owns j0 .. j0+30 (lanes 1..31); it walks its segment
+// of kRows rows upward.  At row i each lane forms the new H of its column;
+// the E update of (i, c) then takes H(i, c-1) from the lane on its left by
+// shuffle (lane 0 computes the column left of the strip for that purpose
+// only and writes nothing), H(i-1, c) from the previous iteration's
+// register, and E(i, c+1) / E(i+1, c) of the read half by shuffle and by
+// carrying the next row.  The row below a segment is recomputed before the
+// walk.  Fields and the H psi are ping-pong buffered, so those recomputes
+// read values that no warp is writing; the E psi is touched by its own cell
+// only.  No shared memory and no barriers: every field is read and written
+// once and each coefficient pair read once per step.
+constexpr int kRows = 32, kWarps = 4;
+
+// Blocks (31 columns x kWarps*kRows rows) split into an interior rectangle,
+// whose cells and halo touch no CPML strip and no grid edge, and the frame
+// around it.  The interior launch runs the code without CPML (half the
+// registers, twice the resident warps); the frame launch maps its linear
+// block index onto the frame.
+struct BlockMap {
+  int gx, gy;                   // blocks along y (columns) and x (rows)
+  int bx_lo, bx_hi, by_lo, by_hi;  // interior rectangle [lo, hi)
+  int frame;                    // 0: interior launch (2D grid), 1: frame launch (1D grid)
+};
+
+CEEP_D void block_of(const BlockMap& m, int& bx, int& by) {
+  if (!m.frame) {
+    bx = m.bx_lo + blockIdx.x;
+    by = m.by_lo + blockIdx.y;
+    return;
+  }
+  int f = blockIdx.x;
+  const int top = m.by_lo * m.gx;
+  if (f < top) { bx = f % m.gx; by = f / m.gx; return; }
+  f -= top;
+  const int bottom = (m.gy - m.by_hi) * m.gx;
+  if (f < bottom) { bx = f % m.gx; by = m.by_hi + f / m.gx; return; }
+  f -= bottom;
+  const int side = m.bx_lo + (m.gx - m.bx_hi);
+  by = m.by_lo + f / side;
+  const int q = f % side;
+  bx = q < m.bx_lo ? q : m.bx_hi + (q - m.bx_lo);
+}
+
+template <int MODE, bool CPML>
+__global__ void __launch_bounds__(32 * kWarps) single2d_step_kernel(const Single2dParams p, int step, int r,
+                                                                      const BlockMap bm) {
+  const int w = r ^ 1;
+  const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
+  int bx, by;
+  block_of(bm, bx, by);
+  const int j0 = bx * 31;
+  const int c = j0 - 1 + lane;
+  const int i0 = (by * kWarps + threadIdx.y) * kRows;
+  if (i0 >= nx) return;  // whole warp
+  const int i1 = min(i0 + kRows, nx);
+  const bool live = c >= 0 && c < ny;
+  const bool own = live && lane > 0;
+  const int cl = live ? c : max(min(c, ny - 1), 0);  // a valid column for the non-live lanes' loads
   if (MODE == 0) {
-    // TMz: Ez on [1, nx) x [1, ny) (fdtd_2d.py:165-171)
-    float* ez = p.f[0];
-    const float* hx = p.f[1];
-    const float* hy = p.f[2];
-    const float hxc = __ldg(hx + c), hyc = __ldg(hy + c);
-    const float dhy = i > 0 ? hyc - __ldg(hy + c - ny) : 0.f;
-    const float dhx = j > 0 ? hxc - __ldg(hx + c - 1) : 0.f;
-    float e = ez[c];
-    if (i > 0 && j > 0) e = k.x * e + k.y * (dhy * p.inv_dx - dhx * p.inv_dy);
-    for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s)  // fdtd_2d.py:245-260
-      if (__ldg(p.src + 3 * s + 1) == j && __ldg(p.src + 3 * s + 2) == 0)
-        e += __ldg(p.waveform + (size_t)s * p.nsteps + step);
-    for (int o = 0; o < p.n_ops; ++o) {
-      if (CPML && p.ops[o] == kOpCpml) {
-        const Strips sx = strips(i, nx, t, false);
-        if (sx.lo >= 0) e += p.dt_eps0 * psi_e(psi_ex + (size_t)sx.lo * ny + j, bex[sx.lo_k], cex[sx.lo_k], dhy, p.inv_dx);
-        if (sx.hi >= 0) e += p.dt_eps0 * psi_e(psi_ex + (size_t)(t + sx.hi) * ny + j, bex[sx.hi], cex[sx.hi], dhy, p.inv_dx);
-        const Strips sy = strips(j, ny, t, false);
-        if (sy.lo >= 0) e -= p.dt_eps0 * psi_e(psi_ey + (size_t)i * t + sy.lo, bey[sy.lo_k], cey[sy.lo_k], dhx, p.inv_dy);
-        if (sy.hi >= 0)
-          e -= p.dt_eps0 * psi_e(psi_ey + (size_t)nx * t + (size_t)i * t + sy.hi, bey[sy.hi], cey[sy.hi], dhx, p.inv_dy);
-      } else if (p.ops[o] == kOpPec && edge) {
-        e = 0.f;
+    const float* ez_r = p.f[0][r];
+    const float* hx_r = p.f[1][r];
+    const float* hy_r = p.f[2][r];
+    float hy_prev = 0.f;
+    if (i0 > 0) hy_prev = tmz_hy_at<CPML>(p, r, i0 - 1, cl);
+    // the read-half operands of the current row are loaded one iteration
+    // ahead, before the current row's stores, so each warp keeps two rows of
+    // loads in flight
+    size_t k = (size_t)i0 * ny + cl;
+    float ez_c = __ldg(ez_r + k);
+    float ez_n = i0 + 1 < nx ? __ldg(ez_r + k + ny) : 0.f;
+    float hx_c = __ldg(hx_r + k), hy_c = __ldg(hy_r + k);
+    float2 d_c = __ldg(p.ch + k), e_c = __ldg(p.ce + k);
+    for (int i = i0; i < i1; ++i, k += ny) {
+      const bool more = i + 1 < i1;
+      const float ez_nn = more && i + 2 < nx ? __ldg(ez_r + k + 2 * (size_t)ny) : 0.f;
+      const float hx_n = more ? __ldg(hx_r + k + ny) : 0.f;
+      const float hy_n = more ? __ldg(hy_r + k + ny) : 0.f;
+      const float2 d_n = more ? __ldg(p.ch + k + ny) : make_float2(0.f, 0.f);
+      const float2 e_n = more ? __ldg(p.ce + k + ny) : make_float2(0.f, 0.f);
+      float ez_rt = __shfl_down_sync(0xffffffffu, ez_c, 1);
+      if (lane == 31) ez_rt = c + 1 < ny ? __ldg(ez_r + k + 1) : 0.f;
+      const float2 d = d_c;
+      const float dy = c + 1 < ny ? ez_rt - ez_c : 0.f;
+      const float dx = i + 1 < nx ? ez_n - ez_c : 0.f;
+      float hx = hx_c, hy = hy_c;
+      if (c < ny - 1) hx = d.x * hx - (d.y * p.inv_dy) * dy;
+      if (i < nx - 1) hy = d.x * hy + (d.y * p.inv_dx) * dx;
+      if (CPML) {
+        hx -= cpml_h_y<CPML>(p, r, i, cl, dy, own);
+        hy += cpml_h_x<CPML>(p, r, i, cl, dx, own);
       }
+      const float hx_l = __shfl_up_sync(0xffffffffu, hx, 1);
+      if (own) {
+        p.f[1][w][k] = hx;
+        p.f[2][w][k] = hy;
+        // Ez on [1, nx) x [1, ny) (fdtd_2d.py:165-171)
+        const float dhy = i > 0 ? hy - hy_prev : 0.f;
+        const float dhx = c > 0 ? hx - hx_l : 0.f;
+        const float2 kk = e_c;
+        float e = ez_c;
+        if (i > 0 && c > 0) e = kk.x * e + kk.y * (dhy * p.inv_dx - dhx * p.inv_dy);
+        for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s)  // fdtd_2d.py:245-260
+          if (__ldg(p.src + 3 * s + 1) == c && __ldg(p.src + 3 * s + 2) == 0)
+            e += __ldg(p.waveform + (size_t)s * p.nsteps + step);
+        for (int o = 0; o < p.n_ops; ++o) {
+          if (CPML && p.ops[o] == kOpCpml) {
+            e += cpml_e_x<CPML>(p, i, c, dhy);
+            e -= cpml_e_y<CPML>(p, i, c, dhx);
+          } else if (p.ops[o] == kOpPec && (i == 0 || i == nx - 1 || c == 0 || c == ny - 1)) {
+            e = 0.f;  // absorbing.py:58-66
+          }
+        }
+        p.f[0][w][k] = e;
+      }
+      hy_prev = hy;
+      ez_c = ez_n;
+      ez_n = ez_nn;
+      hx_c = hx_n;
+      hy_c = hy_n;
+      d_c = d_n;
+      e_c = e_n;
     }
-    ez[c] = e;
   } else {
-    // TEz: Ex on j >= 1, Ey on i >= 1 (fdtd_2d.py:205-217)
-    const float* hz = p.f[0];
-    float* ex = p.f[1];
-    float* ey = p.f[2];
-    const float hc = __ldg(hz + c);
-    const float dy = j > 0 ? hc - __ldg(hz + c - 1) : 0.f;
-    const float dx = i > 0 ? hc - __ldg(hz + c - ny) : 0.f;
-    float vx = ex[c], vy = ey[c];
-    if (j > 0) vx = k.x * vx + (k.y * p.inv_dy) * dy;
-    if (i > 0) vy = k.x * vy - (k.y * p.inv_dx) * dx;
-    for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s) {
-      if (__ldg(p.src + 3 * s + 1) != j) continue;
-      const int fld = __ldg(p.src + 3 * s + 2);
-      const float w = __ldg(p.waveform + (size_t)s * p.nsteps + step);
-      if (fld == 1) vx += w;
-      else if (fld == 2) vy += w;
-    }
-    for (int o = 0; o < p.n_ops; ++o) {
-      if (CPML && p.ops[o] == kOpCpml) {
-        // y strips on Ex first, then x strips on Ey (absorbing.py:467-511)
-        const Strips sy = strips(j, ny, t, false);
-        if (sy.lo >= 0) vx += p.dt_eps0 * psi_e(psi_ey + (size_t)i * t + sy.lo, bey[sy.lo_k], cey[sy.lo_k], dy, p.inv_dy);
-        if (sy.hi >= 0)
-          vx += p.dt_eps0 * psi_e(psi_ey + (size_t)nx * t + (size_t)i * t + sy.hi, bey[sy.hi], cey[sy.hi], dy, p.inv_dy);
-        const Strips sx = strips(i, nx, t, false);
-        if (sx.lo >= 0) vy -= p.dt_eps0 * psi_e(psi_ex + (size_t)sx.lo * ny + j, bex[sx.lo_k], cex[sx.lo_k], dx, p.inv_dx);
-        if (sx.hi >= 0) vy -= p.dt_eps0 * psi_e(psi_ex + (size_t)(t + sx.hi) * ny + j, bex[sx.hi], cex[sx.hi], dx, p.inv_dx);
-      } else if (p.ops[o] == kOpPec) {
-        if (i == 0 || i == nx - 1) vx = 0.f;  // absorbing.py:68-72
-        if (j == 0 || j == ny - 1) vy = 0.f;
+    const float* hz_r = p.f[0][r];
+    const float* ex_r = p.f[1][r];
+    const float* ey_r = p.f[2][r];
+    float hz_prev = 0.f;
+    if (i0 > 0) hz_prev = tez_hz_at<CPML>(p, r, i0 - 1, cl);
+    size_t k = (size_t)i0 * ny + cl;
+    float ey_c = __ldg(ey_r + k);
+    float ey_n = i0 + 1 < nx ? __ldg(ey_r + k + ny) : 0.f;
+    float ex_c = __ldg(ex_r + k), hz_c = __ldg(hz_r + k);
+    float2 d_c = __ldg(p.ch + k), e_c = __ldg(p.ce + k);
+    for (int i = i0; i < i1; ++i, k += ny) {
+      const bool more = i + 1 < i1;
+      const float ey_nn = more && i + 2 < nx ? __ldg(ey_r + k + 2 * (size_t)ny) : 0.f;
+      const float ex_n = more ? __ldg(ex_r + k + ny) : 0.f;
+      const float hz_n = more ? __ldg(hz_r + k + ny) : 0.f;
+      const float2 d_n = more ? __ldg(p.ch + k + ny) : make_float2(0.f, 0.f);
+      const float2 e_n = more ? __ldg(p.ce + k + ny) : make_float2(0.f, 0.f);
+      float ex_rt = __shfl_down_sync(0xffffffffu, ex_c, 1);
+      if (lane == 31) ex_rt = c + 1 < ny ? __ldg(ex_r + k + 1) : 0.f;
+      const float2 d = d_c;
+      const float dex = c + 1 < ny ? ex_rt - ex_c : 0.f;
+      const float dey = i + 1 < nx ? ey_n - ey_c : 0.f;
+      float hz = hz_c;
+      if (i < nx - 1 && c < ny - 1) hz = d.x * hz + d.y * (dex * p.inv_dy - dey * p.inv_dx);
+      if (CPML) {
+        // x strips subtract, y strips add (absorbing.py:355-405)
+        hz -= cpml_h_x<CPML>(p, r, i, cl, dey, own);
+        hz += cpml_h_y<CPML>(p, r, i, cl, dex, own);
       }
+      const float hz_l = __shfl_up_sync(0xffffffffu, hz, 1);
+      if (own) {
+        p.f[0][w][k] = hz;
+        // Ex on c >= 1, Ey on i >= 1 (fdtd_2d.py:205-217)
+        const float dy = c > 0 ? hz - hz_l : 0.f;
+        const float dx = i > 0 ? hz - hz_prev : 0.f;
+        const float2 kk = e_c;
+        float vx = ex_c, vy = ey_c;
+        if (c > 0) vx = kk.x * vx + (kk.y * p.inv_dy) * dy;
+        if (i > 0) vy = kk.x * vy - (kk.y * p.inv_dx) * dx;
+        for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s) {
+          if (__ldg(p.src + 3 * s + 1) != c) continue;
+          const int fld = __ldg(p.src + 3 * s + 2);
+          const float wv = __ldg(p.waveform + (size_t)s * p.nsteps + step);
+          if (fld == 1) vx += wv;
+          else if (fld == 2) vy += wv;
+        }
+        for (int o = 0; o < p.n_ops; ++o) {
+          if (CPML && p.ops[o] == kOpCpml) {
+            // y strips on Ex first, then x strips on Ey (absorbing.py:467-511)
+            vx += cpml_e_y<CPML>(p, i, c, dy);
+            vy -= cpml_e_x<CPML>(p, i, c, dx);
+          } else if (p.ops[o] == kOpPec) {
+            if (i == 0 || i == nx - 1) vx = 0.f;  // absorbing.py:68-72
+            if (c == 0 || c == ny - 1) vy = 0.f;
+          }
+        }
+        p.f[1][w][k] = vx;
+        p.f[2][w][k] = vy;
+      }
+      hz_prev = hz;
+      ey_c = ey_n;
+      ey_n = ey_nn;
+      ex_c = ex_n;
+      hz_c = hz_n;
+      d_c = d_n;
+      e_c = e_n;
     }
-    ex[c] = vx;
-    ey[c] = vy;
   }
 }
 
 // TEz Hz sources, in list order (fdtd_2d.py:253-254).
-__global__ void single2d_src_h_kernel(const Single2dParams p, int step) {
+__global__ void single2d_src_h_kernel(const Single2dParams p, int step, int cur) {
   if (threadIdx.x != 0) return;
   for (int s = 0; s < p.nsrc; ++s)
     if (p.src[3 * s + 2] == 0)
-      p.f[0][(size_t)p.src[3 * s] * p.ny + p.src[3 * s + 1]] += p.waveform[(size_t)s * p.nsteps + step];
+      p.f[0][cur][(size_t)p.src[3 * s] * p.ny + p.src[3 * s + 1]] += p.waveform[(size_t)s * p.nsteps + step];
 }
 
 // First-order Mur on the edges of field 0 (absorbing.py:126-166).  prev holds
 // the previous step's lines next to the edges (x0, xn: ny each; y0, yn: nx
 // each); this step's lines go to the other half of the pair.
-__global__ void single2d_mur_kernel(const Single2dParams p, int step) {
+__global__ void single2d_mur_kernel(const Single2dParams p, int step, int cur) {
   const int nx = p.nx, ny = p.ny;
-  float* e = p.f[0];
+  float* e = p.f[0][cur];
   const int len = 2 * ny + 2 * nx;
   const float* prev = p.mur_prev + (size_t)(step & 1) * len;
   float* next = p.mur_prev + (size_t)((step + 1) & 1) * len;
@@ -302,17 +446,44 @@ __global__ void single2d_mur_kernel(const Single2dParams p, int step) {
   }
 }
 
-__global__ void single2d_record_kernel(const Single2dParams p, int step) {
+__global__ void single2d_record_kernel(const Single2dParams p, int step, int cur) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.nrec) return;
-  p.rec_out[(size_t)r * p.nsteps + step] = p.f[p.rec[2 * r + 1]][p.rec[2 * r]];
+  p.rec_out[(size_t)r * p.nsteps + step] = p.f[p.rec[2 * r + 1]][cur][p.rec[2 * r]];
+}
+
+BlockMap block_map(const Single2dParams& p) {
+  BlockMap m;
+  const int rows = kRows * kWarps;
+  m.gx = (p.ny + 30) / 31;
+  m.gy = (p.nx + rows - 1) / rows;
+  // interior: columns bx*31-1 .. bx*31+30 and rows by*rows-1 .. by*rows+rows-1
+  // inside [e, n-e) with e = max(t, 1) (strips and edges excluded)
+  const int e = p.t > 1 ? p.t : 1;
+  m.bx_lo = (e + 1 + 30) / 31;
+  m.bx_hi = (p.ny - e - 31) >= 0 ? (p.ny - e - 31) / 31 + 1 : 0;
+  m.by_lo = (e + 1 + rows - 1) / rows;
+  m.by_hi = (p.nx - e - rows) >= 0 ? (p.nx - e - rows) / rows + 1 : 0;
+  if (m.bx_hi <= m.bx_lo || m.by_hi <= m.by_lo) m.bx_lo = m.bx_hi = m.by_lo = m.by_hi = 0;
+  m.frame = 0;
+  return m;
 }
 
 template <int MODE, bool CPML>
-static cudaError_t step_t(const Single2dParams& p, int step, cudaStream_t s) {
-  const dim3 blk(kS2x, kS2y), grd((p.ny + kS2x - 1) / kS2x, (p.nx + kS2y - 1) / kS2y);
-  single2d_h_kernel<MODE, CPML><<<grd, blk, 0, s>>>(p);
-  single2d_e_kernel<MODE, CPML><<<grd, blk, 0, s>>>(p, step);
+static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s) {
+  const dim3 blk(32, kWarps);
+  BlockMap m = block_map(p);
+  const int interior = (m.bx_hi - m.bx_lo) * (m.by_hi - m.by_lo);
+  if (interior > 0) {
+    single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), blk, 0, s>>>(p, step, r, m);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const int rest = m.gx * m.gy - interior;
+  if (rest > 0) {
+    m.frame = 1;
+    single2d_step_kernel<MODE, CPML><<<rest, blk, 0, s>>>(p, step, r, m);
+  }
   return cudaGetLastError();
 }
 
@@ -321,28 +492,30 @@ static cudaError_t step_t(const Single2dParams& p, int step, cudaStream_t s) {
 struct ceep2s_plan {
   ceep::Single2dParams p;
   bool hz_src = false, mur = false, cpml = false;
-  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+  int cur = 0;  // the half of every ping-pong array holding the current state
+  std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
 };
 
-static int run_steps2s(const ceep2s_plan* pl, int64_t step0, int64_t nsteps, cudaStream_t s) {
+static int run_steps2s(const ceep2s_plan* pl, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
   const ceep::Single2dParams& p = pl->p;
-  for (int64_t k = 0; k < nsteps; ++k) {
+  for (int64_t k = 0; k < nsteps; ++k, cur ^= 1) {
     const int step = (int)(step0 + k);
     cudaError_t e;
     if (p.mode == 0)
-      e = pl->cpml ? ceep::step_t<0, true>(p, step, s) : ceep::step_t<0, false>(p, step, s);
+      e = pl->cpml ? ceep::step_t<0, true>(p, step, cur, s) : ceep::step_t<0, false>(p, step, cur, s);
     else
-      e = pl->cpml ? ceep::step_t<1, true>(p, step, s) : ceep::step_t<1, false>(p, step, s);
+      e = pl->cpml ? ceep::step_t<1, true>(p, step, cur, s) : ceep::step_t<1, false>(p, step, cur, s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "single2d step launch");
-    if (pl->hz_src) ceep::single2d_src_h_kernel<<<1, 32, 0, s>>>(p, step);
-    if (pl->mur) ceep::single2d_mur_kernel<<<1, 1024, 0, s>>>(p, step);
-    if (p.nrec) ceep::single2d_record_kernel<<<(p.nrec + 255) / 256, 256, 0, s>>>(p, step);
+    const int nw = cur ^ 1;
+    if (pl->hz_src) ceep::single2d_src_h_kernel<<<1, 32, 0, s>>>(p, step, nw);
+    if (pl->mur) ceep::single2d_mur_kernel<<<1, 1024, 0, s>>>(p, step, nw);
+    if (p.nrec) ceep::single2d_record_kernel<<<(p.nrec + 255) / 256, 256, 0, s>>>(p, step, nw);
     e = cudaGetLastError();
     if (e != cudaSuccess) return ceep::cuda_fail(e, "single2d epilogue launch");
     if (p.snapshots && step % p.snap_interval == 0) {
       const size_t n = (size_t)p.nx * p.ny;
-      e = cudaMemcpyAsync(p.snapshots + (size_t)(step / p.snap_interval) * n, p.f[p.snap_field], n * sizeof(float),
-                          cudaMemcpyDeviceToDevice, s);
+      e = cudaMemcpyAsync(p.snapshots + (size_t)(step / p.snap_interval) * n, p.f[p.snap_field][nw],
+                          n * sizeof(float), cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) return ceep::cuda_fail(e, "single2d snapshot copy");
     }
   }
@@ -358,8 +531,9 @@ extern "C" int ceep2s_plan_create(const ceep2s_desc* d, ceep2s_plan** out) {
   if (d->nx < 3 || d->ny < 3) return fail(CEEP_ERR_INVALID, "grid %dx%d: at least 3x3", d->nx, d->ny);
   if (d->mode != 0 && d->mode != 1) return fail(CEEP_ERR_INVALID, "mode %d (0 TMz, 1 TEz)", d->mode);
   if (d->nsteps < 1) return fail(CEEP_ERR_INVALID, "nsteps %d", d->nsteps);
-  if (!d->f0 || !d->f1 || !d->f2 || !d->coef_e || !d->coef_h)
-    return fail(CEEP_ERR_INVALID, "null field or coefficient buffer");
+  for (int k = 0; k < 2; ++k)
+    if (!d->f0[k] || !d->f1[k] || !d->f2[k]) return fail(CEEP_ERR_INVALID, "null field buffer");
+  if (!d->coef_e || !d->coef_h) return fail(CEEP_ERR_INVALID, "null coefficient buffer");
   if (d->n_ops < 0 || d->n_ops > 4) return fail(CEEP_ERR_INVALID, "n_ops %d (at most 4)", d->n_ops);
   bool cpml = false, mur = false;
   for (int o = 0; o < d->n_ops; ++o) {
@@ -375,7 +549,8 @@ extern "C" int ceep2s_plan_create(const ceep2s_desc* d, ceep2s_plan** out) {
       mur = true;
     }
   }
-  if (cpml && (d->cpml_t < 1 || !d->cpml || !d->psi)) return fail(CEEP_ERR_INVALID, "CPML: thickness/buffers");
+  if (cpml && (d->cpml_t < 1 || !d->cpml || !d->psi_e || !d->psi_h[0] || !d->psi_h[1]))
+    return fail(CEEP_ERR_INVALID, "CPML: thickness/buffers");
   if (mur && !d->mur_prev) return fail(CEEP_ERR_INVALID, "Mur: null state buffer");
   if (d->nsrc < 0 || (d->nsrc && (!d->src || !d->src_row || !d->waveform)))
     return fail(CEEP_ERR_INVALID, "sources");
@@ -389,13 +564,18 @@ extern "C" int ceep2s_plan_create(const ceep2s_desc* d, ceep2s_plan** out) {
   p.nx = d->nx; p.ny = d->ny; p.mode = d->mode; p.nsteps = d->nsteps;
   p.inv_dx = d->inv_dx; p.inv_dy = d->inv_dy; p.dt_mu0 = d->dt_mu0; p.dt_eps0 = d->dt_eps0;
   p.mur_kx = d->mur_kx; p.mur_ky = d->mur_ky;
-  p.f[0] = d->f0; p.f[1] = d->f1; p.f[2] = d->f2;
+  for (int k = 0; k < 2; ++k) {
+    p.f[0][k] = d->f0[k];
+    p.f[1][k] = d->f1[k];
+    p.f[2][k] = d->f2[k];
+    p.psi_h[k] = d->psi_h[k];
+  }
   p.ce = reinterpret_cast<const float2*>(d->coef_e);
   p.ch = reinterpret_cast<const float2*>(d->coef_h);
   p.n_ops = d->n_ops;
   for (int o = 0; o < 4; ++o) p.ops[o] = o < d->n_ops ? d->ops[o] : 0;
   p.t = cpml ? d->cpml_t : 0;
-  p.cpml = d->cpml; p.psi = d->psi; p.mur_prev = d->mur_prev;
+  p.cpml = d->cpml; p.psi_e = d->psi_e; p.mur_prev = d->mur_prev;
   p.nsrc = d->nsrc; p.src = d->src; p.src_row = d->src_row; p.waveform = d->waveform;
   p.nrec = d->nrec; p.rec = d->rec; p.rec_out = d->rec_out;
   p.snap_field = d->snap_field; p.snap_interval = d->snap_interval > 0 ? d->snap_interval : 1;
@@ -415,14 +595,20 @@ extern "C" int ceep2s_plan_run(ceep2s_plan* pl, int64_t step0, int64_t nsteps, v
                 (long long)(step0 + nsteps), pl->p.nsteps);
   if (nsteps == 0) return CEEP_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!use_graph || s == nullptr) return run_steps2s(pl, step0, nsteps, s);
-  auto key = std::make_pair(step0, nsteps);
+  const int cur = pl->cur;
+  const int cur_after = cur ^ (int)(nsteps & 1);
+  if (!use_graph || s == nullptr) {
+    const int rc = run_steps2s(pl, step0, nsteps, cur, s);
+    if (rc == CEEP_OK) pl->cur = cur_after;
+    return rc;
+  }
+  auto key = std::make_tuple(step0, nsteps, cur);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps2s(pl, step0, nsteps, s);
+    int rc = run_steps2s(pl, step0, nsteps, cur, s);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) {
       if (e == cudaSuccess) cudaGraphDestroy(g);
@@ -436,7 +622,17 @@ extern "C" int ceep2s_plan_run(ceep2s_plan* pl, int64_t step0, int64_t nsteps, v
     it = pl->graphs.emplace(key, ex).first;
   }
   cudaError_t e = cudaGraphLaunch(it->second, s);
-  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "cudaGraphLaunch");
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
+  pl->cur = cur_after;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2s_plan_current_buffer(const ceep2s_plan* pl) { return pl ? pl->cur : -1; }
+
+extern "C" int ceep2s_plan_set_current_buffer(ceep2s_plan* pl, int cur) {
+  if (!pl || (cur != 0 && cur != 1)) return ceep::fail(CEEP_ERR_INVALID, "bad plan or buffer index");
+  pl->cur = cur;
+  return CEEP_OK;
 }
 
 extern "C" int ceep2s_plan_destroy(ceep2s_plan* pl) {

@@ -301,9 +301,11 @@ class Grid2D:
             raise ValueError(f"Grid2D does not support mode: {config.mode}")
         nx, ny = config.grid.nx, config.grid.ny
         dev = torch.device(device)
-        empty = torch.empty(0, dtype=torch.float32, device=dev)
-        for f in ("ez", "hx", "hy", "hz", "ex", "ey"):
-            setattr(self, f, torch.zeros((nx, ny), dtype=torch.float32, device=dev) if f in _FIELDS[mode] else empty)
+        self._empty = torch.empty(0, dtype=torch.float32, device=dev)
+        # ping-pong halves; _cur selects the one holding the current state
+        self._pairs = {f: [torch.zeros((nx, ny), dtype=torch.float32, device=dev) for _ in range(2)]
+                       for f in _FIELDS[mode]}
+        self._cur = 0
         shp = (nx, ny)
         self.eps_r, self.eps_inf, self.mu_r = np.ones(shp), np.ones(shp), np.ones(shp)
         self.sigma_e, self.sigma_m = np.zeros(shp), np.zeros(shp)
@@ -349,9 +351,21 @@ class Grid2D:
         self.mu_r[m], self.sigma_e[m], self.sigma_m[m] = mu_r, sigma_e, sigma_m
         self._precompute_coefficients()
 
+    def _field(self, name):
+        pair = self._pairs.get(name)
+        return self._empty if pair is None else pair[self._cur]
+
+    ez = property(lambda self: self._field("ez"))
+    hx = property(lambda self: self._field("hx"))
+    hy = property(lambda self: self._field("hy"))
+    hz = property(lambda self: self._field("hz"))
+    ex = property(lambda self: self._field("ex"))
+    ey = property(lambda self: self._field("ey"))
+
     def reset_fields(self) -> None:
-        for f in _FIELDS[_mode_name(self.config)]:
-            getattr(self, f).zero_()
+        for pair in self._pairs.values():
+            for t in pair:
+                t.zero_()
 
     @property
     def memory_usage_bytes(self) -> int:
@@ -364,8 +378,9 @@ class _Desc2S(C.Structure):
     F = C.c_float
     _fields_ = [("nx", I), ("ny", I), ("mode", I), ("nsteps", I), ("inv_dx", F), ("inv_dy", F),
                 ("dt_mu0", F), ("dt_eps0", F), ("mur_kx", F), ("mur_ky", F),
-                ("f0", P), ("f1", P), ("f2", P), ("coef_e", P), ("coef_h", P),
-                ("n_ops", I), ("ops", I * 4), ("cpml_t", I), ("cpml", P), ("psi", P), ("mur_prev", P),
+                ("f0", P * 2), ("f1", P * 2), ("f2", P * 2), ("coef_e", P), ("coef_h", P),
+                ("n_ops", I), ("ops", I * 4), ("cpml_t", I), ("cpml", P), ("psi_e", P), ("psi_h", P * 2),
+                ("mur_prev", P),
                 ("nsrc", I), ("hz_sources", I), ("src", P), ("src_row", P), ("waveform", P),
                 ("nrec", I), ("rec", P), ("rec_out", P), ("snap_field", I), ("snap_interval", I),
                 ("snapshots", P)]
@@ -445,7 +460,8 @@ class FDTD2D:
         cp = next((b for b in self.boundaries if type(b).__name__ == "CPML"), None)
         self._cpml_t = int(cp.thickness) if cp is not None else 0
         t = max(self._cpml_t, 1)
-        self._psi = torch.zeros(4 * t * ny + 4 * nx * t, **f32)
+        self._psi_e = torch.zeros(2 * t * ny + 2 * nx * t, **f32)
+        self._psi_h = [torch.zeros(2 * t * ny + 2 * nx * t, **f32) for _ in range(2)]
         if cp is not None:
             kw = (cp.order, cp.sigma_factor, cp.alpha_max, cp.kappa_max)
             ax = cpml_coefficients(t, g.dx, config.dt, *kw)
@@ -479,7 +495,7 @@ class FDTD2D:
         self._ops = [{"CPML": 1, "PEC": 2, "MurABC": 3}[type(b).__name__] for b in self.boundaries]
 
     def _fields(self):
-        return [getattr(self.grid, f) for f in _FIELDS[self._mode]]
+        return [self.grid._pairs[f] for f in _FIELDS[self._mode]]
 
     def _ensure(self, end: int) -> None:
         """Plan covering steps [0, end): waveform table, record and snapshot
@@ -513,12 +529,14 @@ class FDTD2D:
         cdt = C_0 * dt
         d.mur_kx, d.mur_ky = (cdt - g.dx) / (cdt + g.dx), (cdt - g.dy) / (cdt + g.dy)
         f = self._fields()
-        d.f0, d.f1, d.f2 = f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr()
+        for k in range(2):
+            d.f0[k], d.f1[k], d.f2[k] = f[0][k].data_ptr(), f[1][k].data_ptr(), f[2][k].data_ptr()
+            d.psi_h[k] = self._psi_h[k].data_ptr()
         d.coef_e, d.coef_h = self._coef_e.data_ptr(), self._coef_h.data_ptr()
         d.n_ops = len(self._ops)
         for k, op in enumerate(self._ops):
             d.ops[k] = op
-        d.cpml_t, d.cpml, d.psi, d.mur_prev = self._cpml_t, self._cpml.data_ptr(), self._psi.data_ptr(), \
+        d.cpml_t, d.cpml, d.psi_e, d.mur_prev = self._cpml_t, self._cpml.data_ptr(), self._psi_e.data_ptr(), \
             self._mur.data_ptr()
         d.nsrc, d.hz_sources = len(self._src_objs), self._hz_src
         if self._src_objs:
@@ -531,6 +549,7 @@ class FDTD2D:
             d.snapshots = self._snaps.data_ptr()
         plan = C.c_void_p()
         check(lib().ceep2s_plan_create(C.addressof(d), C.byref(plan)), "ceep2s_plan_create")
+        check(lib().ceep2s_plan_set_current_buffer(plan, self.grid._cur), "ceep2s_plan_set_current_buffer")
         self._plan, self._cap = plan, cap
 
     def _upload_coefficients(self) -> None:
@@ -563,6 +582,7 @@ class FDTD2D:
         s = torch.cuda.current_stream(self.device) if stream is None else stream
         check(lib().ceep2s_plan_run(self._plan, a, num_steps, C.c_void_p(s.cuda_stream), int(self.use_graph)),
               "ceep2s_plan_run")
+        self.grid._cur = lib().ceep2s_plan_current_buffer(self._plan)
         self._step += num_steps
         self._pending = getattr(self, "_pending", 0) + num_steps
 
@@ -599,6 +619,22 @@ class FDTD2D:
             for k in range(first, last + 1):
                 self.field_snapshots.append(self._snaps[k].cpu().numpy().astype(np.float64))
         self._pending = 0
+
+    def reset(self) -> None:
+        """Zero every field, psi and Mur state and start again at step 0 with
+        empty probe lists and snapshots (not in the reference; reuses buffers
+        and captured graphs)."""
+        self.grid.reset_fields()
+        self._psi_e.zero_()
+        for t in self._psi_h:
+            t.zero_()
+        self._mur.zero_()
+        self._step, self._pending = 0, 0
+        self.field_snapshots = []
+        self.probe_data = {pt: [] for pt in self.probe_points}
+        for m in self.dft_monitors:
+            m.dft_real = m.dft_imag = None
+            m._initialized = False
 
     def step(self) -> None:
         """One step (H, H boundaries, E, sources, E boundaries, record)."""

@@ -259,15 +259,17 @@ typedef struct ceep2s_desc {
   float inv_dx, inv_dy;
   float dt_mu0, dt_eps0;    /* scale of the CPML H and E corrections          */
   float mur_kx, mur_ky;     /* (c dt - d) / (c dt + d)                         */
-  float *f0, *f1, *f2;
+  float *f0[2], *f1[2], *f2[2];  /* ping-pong: the plan's current half holds
+                               the state (starts at 0)                         */
   const float* coef_e;      /* (nx, ny, 2): ca, cb                             */
   const float* coef_h;      /* (nx, ny, 2): da, db                             */
   int32_t n_ops;            /* boundary operations in list order (<= 4):      */
   int32_t ops[4];           /* 1 CPML, 2 PEC, 3 Mur (Mur last)                 */
   int32_t cpml_t;           /* CPML thickness                                  */
   const float* cpml;        /* (8, t): be_x ce_x bh_x ch_x be_y ce_y bh_y ch_y */
-  float* psi;               /* 4 x (t, ny) E/E/H/H x-lo/x-hi, then 4 x (nx, t)
-                               E/E/H/H y-lo/y-hi, zeroed by the caller         */
+  float* psi_e;             /* E psi: x-lo, x-hi (t, ny) each, then y-lo, y-hi
+                               (nx, t) each; zeroed by the caller              */
+  float* psi_h[2];          /* H psi, same layout, ping-pong like the fields   */
   float* mur_prev;          /* 2 x (2 ny + 2 nx), zeroed by the caller         */
   int32_t nsrc;
   int32_t hz_sources;       /* nonzero: TEz sources on Hz (field 0) exist      */
@@ -287,6 +289,10 @@ int ceep2s_plan_create(const ceep2s_desc* desc, ceep2s_plan** out);
  * the record column and the Mur state half); graph-captured per
  * (step0, nsteps) when use_graph and a stream are given. */
 int ceep2s_plan_run(ceep2s_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
+/* The half (0 or 1) of the ping-pong arrays that holds the current state;
+ * each step flips it. */
+int ceep2s_plan_current_buffer(const ceep2s_plan* plan);
+int ceep2s_plan_set_current_buffer(ceep2s_plan* plan, int cur);
 int ceep2s_plan_destroy(ceep2s_plan* plan);
 int64_t ceep2s_desc_size(void);
 
