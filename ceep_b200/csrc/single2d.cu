@@ -213,7 +213,7 @@ CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
 
 // One step as a warp row-walk.  A warp covers columns j0-1 .. j0+30 (lane l
 // at column j0-1+l) and owns j0 .. j0+30 (lanes 1..31); it walks its segment
-// of kRows rows upward.  At row i each lane forms the new H of its column;
+// of rows upward.  At row i each lane forms the new H of its column;
 // the E update of (i, c) then takes H(i, c-1) from the lane on its left by
 // shuffle (lane 0 computes the column left of the strip for that purpose
 // only and writes nothing), H(i-1, c) from the previous iteration's
@@ -223,9 +223,12 @@ CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
 // read values that no warp is writing; the E psi is touched by its own cell
 // only.  No shared memory and no barriers: every field is read and written
 // once and each coefficient pair read once per step.
-constexpr int kRows = 32, kWarps = 4;
+// A block covers kBlockRows rows of a 31-column strip; its warps split them:
+// 4 warps of 32 rows in the interior launch, 16 warps of 8 rows in the frame
+// launch (few blocks, so shorter walks keep its duration down).
+constexpr int kBlockRows = 128, kWarpsInterior = 4, kWarpsFrame = 16;
 
-// Blocks (31 columns x kWarps*kRows rows) split into an interior rectangle,
+// Blocks (31 columns x kBlockRows rows) split into an interior rectangle,
 // whose cells and halo touch no CPML strip and no grid edge, and the frame
 // around it.  The interior launch runs the code without CPML (half the
 // registers, twice the resident warps); the frame launch maps its linear
@@ -256,17 +259,18 @@ CEEP_D void block_of(const BlockMap& m, int& bx, int& by) {
 }
 
 template <int MODE, bool CPML>
-__global__ void __launch_bounds__(32 * kWarps) single2d_step_kernel(const Single2dParams p, int step, int r,
-                                                                      const BlockMap bm) {
+__global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const Single2dParams p, int step, int r,
+                                                                           const BlockMap bm) {
   const int w = r ^ 1;
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
   int bx, by;
   block_of(bm, bx, by);
   const int j0 = bx * 31;
   const int c = j0 - 1 + lane;
-  const int i0 = (by * kWarps + threadIdx.y) * kRows;
+  const int rows = kBlockRows / blockDim.y;
+  const int i0 = by * kBlockRows + threadIdx.y * rows;
   if (i0 >= nx) return;  // whole warp
-  const int i1 = min(i0 + kRows, nx);
+  const int i1 = min(i0 + rows, nx);
   const bool live = c >= 0 && c < ny;
   const bool own = live && lane > 0;
   const int cl = live ? c : max(min(c, ny - 1), 0);  // a valid column for the non-live lanes' loads
@@ -454,7 +458,7 @@ __global__ void single2d_record_kernel(const Single2dParams p, int step, int cur
 
 BlockMap block_map(const Single2dParams& p) {
   BlockMap m;
-  const int rows = kRows * kWarps;
+  const int rows = kBlockRows;
   m.gx = (p.ny + 30) / 31;
   m.gy = (p.nx + rows - 1) / rows;
   // interior: columns bx*31-1 .. bx*31+30 and rows by*rows-1 .. by*rows+rows-1
@@ -469,22 +473,37 @@ BlockMap block_map(const Single2dParams& p) {
   return m;
 }
 
+// The frame launch (few blocks, latency-bound walks) runs on a second stream
+// beside the interior launch; both read only the read half and write
+// disjoint cells of the write half.
 template <int MODE, bool CPML>
-static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s) {
-  const dim3 blk(32, kWarps);
+static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s, cudaStream_t s2,
+                          cudaEvent_t fork, cudaEvent_t join) {
   BlockMap m = block_map(p);
   const int interior = (m.bx_hi - m.bx_lo) * (m.by_hi - m.by_lo);
-  if (interior > 0) {
-    single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), blk, 0, s>>>(p, step, r, m);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
   const int rest = m.gx * m.gy - interior;
-  if (rest > 0) {
-    m.frame = 1;
-    single2d_step_kernel<MODE, CPML><<<rest, blk, 0, s>>>(p, step, r, m);
+  const bool two = interior > 0 && rest > 0;
+  cudaError_t e;
+  if (two) {
+    if ((e = cudaEventRecord(fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s2, fork, 0)) != cudaSuccess) return e;
   }
-  return cudaGetLastError();
+  if (rest > 0) {
+    BlockMap f = m;
+    f.frame = 1;
+    single2d_step_kernel<MODE, CPML><<<rest, dim3(32, kWarpsFrame), 0, two ? s2 : s>>>(p, step, r, f);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (interior > 0) {
+    single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0, s>>>(
+        p, step, r, m);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (two) {
+    if ((e = cudaEventRecord(join, s2)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, join, 0)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace ceep
@@ -493,6 +512,8 @@ struct ceep2s_plan {
   ceep::Single2dParams p;
   bool hz_src = false, mur = false, cpml = false;
   int cur = 0;  // the half of every ping-pong array holding the current state
+  cudaStream_t side = nullptr;  // the frame launch's stream
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
 };
 
@@ -502,9 +523,11 @@ static int run_steps2s(const ceep2s_plan* pl, int64_t step0, int64_t nsteps, int
     const int step = (int)(step0 + k);
     cudaError_t e;
     if (p.mode == 0)
-      e = pl->cpml ? ceep::step_t<0, true>(p, step, cur, s) : ceep::step_t<0, false>(p, step, cur, s);
+      e = pl->cpml ? ceep::step_t<0, true>(p, step, cur, s, pl->side, pl->fork, pl->join)
+                   : ceep::step_t<0, false>(p, step, cur, s, pl->side, pl->fork, pl->join);
     else
-      e = pl->cpml ? ceep::step_t<1, true>(p, step, cur, s) : ceep::step_t<1, false>(p, step, cur, s);
+      e = pl->cpml ? ceep::step_t<1, true>(p, step, cur, s, pl->side, pl->fork, pl->join)
+                   : ceep::step_t<1, false>(p, step, cur, s, pl->side, pl->fork, pl->join);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "single2d step launch");
     const int nw = cur ^ 1;
     if (pl->hz_src) ceep::single2d_src_h_kernel<<<1, 32, 0, s>>>(p, step, nw);
@@ -583,6 +606,15 @@ extern "C" int ceep2s_plan_create(const ceep2s_desc* d, ceep2s_plan** out) {
   pl->cpml = cpml;
   pl->mur = mur;
   pl->hz_src = hz_src;
+  cudaError_t e = cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->join, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    if (pl->fork) cudaEventDestroy(pl->fork);
+    if (pl->side) cudaStreamDestroy(pl->side);
+    delete pl;
+    return ceep::cuda_fail(e, "ceep2s_plan_create stream/events");
+  }
   *out = pl;
   return CEEP_OK;
 }
@@ -638,6 +670,10 @@ extern "C" int ceep2s_plan_set_current_buffer(ceep2s_plan* pl, int cur) {
 extern "C" int ceep2s_plan_destroy(ceep2s_plan* pl) {
   if (!pl) return CEEP_OK;
   for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  if (pl->side) cudaStreamSynchronize(pl->side);
+  if (pl->join) cudaEventDestroy(pl->join);
+  if (pl->fork) cudaEventDestroy(pl->fork);
+  if (pl->side) cudaStreamDestroy(pl->side);
   delete pl;
   return CEEP_OK;
 }
