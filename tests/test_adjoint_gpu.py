@@ -64,7 +64,7 @@ def _run_both(nx, ny, n, T, seed, K, debye=True, ntx=3, loss="vjp", nring=4, gra
     val.backward()
     inner = np.zeros((nx, ny), bool)
     inner[n + 1:nx - n, n + 1:ny - n] = True
-    out = {"value": (float(val), float(ref)), "eps_r": (e2.grad, e_.grad), "sigma": (s2.grad, s_.grad)}
+    out = {"value": (float(val.detach()), float(ref.detach())), "eps_r": (e2.grad, e_.grad), "sigma": (s2.grad, s_.grad)}
     if debye:
         out["deps"] = (d2.grad, d_.grad)
     if grad_tau:
