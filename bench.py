@@ -814,7 +814,7 @@ def run_pack_bench(args):
                        "cell_steps": pk.cell_steps},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 3), "peak_source": peak_src,
-                         "algorithmic_bytes": int(alg), "kernel": "fdtd2d_packed_kernel (whole run)"},
+                         "algorithmic_bytes": int(alg), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block},
             "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
             "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
             "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),

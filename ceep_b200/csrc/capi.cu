@@ -522,6 +522,11 @@ struct PackClass {
   int L, nd, nl;
   ceep::PackTile* tiles;            // device (inside the caller's workspace)
   std::vector<int> active_by_step;  // tiles active at each step (a prefix)
+  // two steps per launch: tiles of the two-step geometry; at pair t (steps
+  // 2t, 2t+1) the phantoms with >= 2t+2 steps run two-step tiles (a prefix)
+  // and those with exactly 2t+1 steps run one-step tiles [tail_lo, tail_hi)
+  ceep::PackTile* tiles2;
+  std::vector<int> active2_by_pair, tail_lo_by_pair, tail_hi_by_pair;
 };
 size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 }  // namespace
@@ -531,8 +536,13 @@ struct ceep2d_pack {
   ceep::Fdtd2dParams* params = nullptr;  // device
   std::vector<PackClass> classes;
   int max_steps = 0;
-  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+  int tblock = 1;  // steps per launch (1 or 2)
+  std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
 };
+
+// Launches a phantom has taken after `steps` steps in the pack's mode; its
+// ping-pong parity is their count & 1.
+static int pack_launches(int64_t steps, int tblock) { return (int)(tblock == 2 ? (steps + 1) / 2 : steps); }
 
 static int pack_layout(ceep2d_plan* const* plans, int32_t count, size_t* bytes,
                        std::vector<std::vector<std::pair<int, int>>>* cls_out,
@@ -561,6 +571,14 @@ static int pack_layout(ceep2d_plan* const* plans, int32_t count, size_t* bytes,
       tiles += (size_t)((p.nx + cx - 1) / cx) * ((p.ny + p.rows - 1) / p.rows) * p.groups;
     }
     b += align16(tiles * sizeof(ceep::PackTile));
+    size_t tiles2 = 0;
+    for (auto& e : c) {
+      const ceep::Fdtd2dParams& p = plans[e.second]->p;
+      const int cx = ceep::fdtd2d_cells_per_block(p.L) - 2;
+      if (p.rows2 < 1) return fail(CEEP_ERR_INVALID, "pack: plan %d has no two-step tile height", e.second);
+      tiles2 += (size_t)((p.nx + cx - 1) / cx) * ((p.ny + p.rows2 - 1) / p.rows2) * p.groups;
+    }
+    b += align16(tiles2 * sizeof(ceep::PackTile));
   }
   *bytes = b;
   if (cls_out) *cls_out = cls;
@@ -595,7 +613,7 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
     pk->max_steps = std::max(pk->max_steps, hp[i].nsteps);
   }
   // host staging vectors must outlive the asynchronous copies: synchronise below
-  std::vector<std::vector<ceep::PackTile>> host_tiles(cls.size());
+  std::vector<std::vector<ceep::PackTile>> host_tiles(cls.size()), host_tiles2(cls.size());
   size_t off = align16(sizeof(ceep::Fdtd2dParams) * count);
   for (size_t c = 0; c < cls.size(); ++c) {
     auto& v = cls[c];
@@ -625,13 +643,47 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
     }
     pc.tiles = reinterpret_cast<ceep::PackTile*>(ws + off);
     off += align16(tl.size() * sizeof(ceep::PackTile));
+    // the two-step tables (same phantom order)
+    std::vector<ceep::PackTile>& t2 = host_tiles2[c];
+    std::vector<std::pair<int, size_t>> ends2;
+    for (auto& e : v) {
+      const ceep::Fdtd2dParams& p = hp[e.second];
+      const int cx = ceep::fdtd2d_cells_per_block(p.L) - 2;
+      for (int g = 0; g < p.groups; ++g)
+        for (int y0 = 0; y0 < p.ny; y0 += p.rows2)
+          for (int x = 0; x < p.nx; x += cx) t2.push_back({e.second, x - 1, y0, g});
+      ends2.push_back({p.nsteps, t2.size()});
+    }
+    const int pairs = (pk->max_steps + 1) / 2;
+    pc.active2_by_pair.assign(pairs, 0);
+    pc.tail_lo_by_pair.assign(pairs, 0);
+    pc.tail_hi_by_pair.assign(pairs, 0);
+    for (int t = 0; t < pairs; ++t) {
+      size_t a2 = 0, lo = 0, hi = 0;
+      for (size_t k = 0; k < ends2.size(); ++k) {
+        if (ends2[k].first >= 2 * t + 2) {
+          a2 = ends2[k].second;
+          lo = ends[k].second;
+        }
+        if (ends2[k].first >= 2 * t + 1) hi = ends[k].second;
+      }
+      pc.active2_by_pair[t] = (int)a2;
+      pc.tail_lo_by_pair[t] = (int)lo;
+      pc.tail_hi_by_pair[t] = (int)hi;
+    }
+    pc.tiles2 = reinterpret_cast<ceep::PackTile*>(ws + off);
+    off += align16(t2.size() * sizeof(ceep::PackTile));
     pk->classes.push_back(pc);
   }
   cudaError_t e = cudaMemcpyAsync(pk->params, hp.data(), sizeof(ceep::Fdtd2dParams) * count,
                                   cudaMemcpyHostToDevice, s);
-  for (size_t c = 0; c < cls.size() && e == cudaSuccess; ++c)
+  for (size_t c = 0; c < cls.size() && e == cudaSuccess; ++c) {
     e = cudaMemcpyAsync(pk->classes[c].tiles, host_tiles[c].data(), host_tiles[c].size() * sizeof(ceep::PackTile),
                         cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(pk->classes[c].tiles2, host_tiles2[c].data(),
+                          host_tiles2[c].size() * sizeof(ceep::PackTile), cudaMemcpyHostToDevice, s);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     delete pk;
@@ -643,23 +695,50 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
 }
 
 static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream_t s) {
+  if (pk->tblock == 2) {
+    // pairs of steps: par is the pair index & 1 for every phantom still running
+    for (int64_t t = step0 / 2; 2 * t < step0 + nsteps; ++t)
+      for (auto& c : pk->classes) {
+        const int a2 = c.active2_by_pair[t], lo = c.tail_lo_by_pair[t], hi = c.tail_hi_by_pair[t];
+        cudaError_t e = cudaSuccess;
+        if (a2 > 0)
+          e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles2, a2, pk->params, (int)(2 * t), (int)(t & 1), true,
+                                         s);
+        if (e == cudaSuccess && hi > lo)
+          e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles + lo, hi - lo, pk->params, (int)(2 * t),
+                                         (int)(t & 1), false, s);
+        if (e != cudaSuccess) return ceep::cuda_fail(e, "packed step launch");
+      }
+    return CEEP_OK;
+  }
   for (int64_t t = step0; t < step0 + nsteps; ++t)
     for (auto& c : pk->classes) {
       const int act = c.active_by_step[t];
       if (act == 0) continue;
-      cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, act, pk->params, (int)t, s);
+      cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, act, pk->params, (int)t, (int)(t & 1),
+                                                 false, s);
       if (e != cudaSuccess) return ceep::cuda_fail(e, "packed step launch");
     }
   return CEEP_OK;
 }
+
+extern "C" int ceep2d_pack_set_temporal_block(ceep2d_pack* pk, int steps) {
+  if (!pk || (steps != 1 && steps != 2)) return fail(CEEP_ERR_INVALID, "pack: temporal block %d (1 or 2)", steps);
+  pk->tblock = steps;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_pack_temporal_block(const ceep2d_pack* pk) { return pk ? pk->tblock : 0; }
 
 extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, void* stream, int use_graph) {
   if (!pk) return fail(CEEP_ERR_INVALID, "null pack");
   if (step0 < 0 || nsteps < 0 || step0 + nsteps > pk->max_steps)
     return fail(CEEP_ERR_INVALID, "pack: steps [%lld, %lld) outside [0, %d)", (long long)step0,
                 (long long)(step0 + nsteps), pk->max_steps);
+  if (pk->tblock == 2 && (step0 % 2 || ((step0 + nsteps) % 2 && step0 + nsteps != pk->max_steps)))
+    return fail(CEEP_ERR_INVALID, "pack: two steps per launch need even step bounds (or the last step)");
   for (auto* pl : pk->plans)
-    if ((pl->cur != (int)(std::min<int64_t>(step0, pl->p.nsteps) & 1)))
+    if (pl->cur != (pack_launches(std::min<int64_t>(step0, pl->p.nsteps), pk->tblock) & 1))
       return fail(CEEP_ERR_INVALID, "pack: a plan's state is not at step %lld", (long long)step0);
   if (nsteps == 0) return CEEP_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -667,7 +746,7 @@ extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, v
   if (!use_graph || s == nullptr) {
     rc = pack_steps(pk, step0, nsteps, s);
   } else {
-    auto key = std::make_pair(step0, nsteps);
+    auto key = std::make_tuple(step0, nsteps, pk->tblock);
     auto it = pk->graphs.find(key);
     if (it == pk->graphs.end()) {
       cudaGraph_t g;
@@ -687,7 +766,7 @@ extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, v
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaGraphLaunch");
   }
   if (rc == CEEP_OK)
-    for (auto* pl : pk->plans) pl->cur = (int)(std::min<int64_t>(step0 + nsteps, pl->p.nsteps) & 1);
+    for (auto* pl : pk->plans) pl->cur = pack_launches(std::min<int64_t>(step0 + nsteps, pl->p.nsteps), pk->tblock) & 1;
   return rc;
 }
 

@@ -787,9 +787,10 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
   if (own && !aborted && ya1 == y1 && y1 - 1 >= y0) b_row(y1 - 1, f4(0.f));
 }
 
+// One block of the two-step kernel: thread columns x0 .. x0+CX-1 (outputs
+// x0+1 .. x0+CX-2), own rows y0 .. y0+rows2-1, TX group g.
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step2_kernel(const Fdtd2dParams p, int step, int par) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
   using St = Stage2d<L, ND + NL, NL>;
   constexpr int CX = kConsumers / L;
   St* st = reinterpret_cast<St*>(smem_raw);
@@ -798,10 +799,6 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   Exch2<L>* xr = reinterpret_cast<Exch2<L>*>(empty + kStages2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(xr + 2);
   const int ny = p.ny, n = p.n;
-  // row-major tile order: neighbouring tiles, which share halo rows and
-  // columns, run close together in time (their halos hit in L2)
-  const int x0 = (int)blockIdx.x * (CX - 2) - 1;  // first thread column; outputs x0+1 .. x0+CX-2
-  const int y0 = blockIdx.y * p.rows2, g = blockIdx.z;
   const int y1 = min(y0 + p.rows2, ny);
   const int ya0 = y0 > 0 ? y0 - 1 : 0, ya1 = y1 < ny ? y1 + 1 : ny;  // step A's rows
   const int rs = ya0 > 0 ? ya0 - 1 : 0;
@@ -832,12 +829,22 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
     consume2<L, true, ND, NL>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
 }
 
-// Many phantoms in one launch: block b runs tile tiles[b] of phantom
-// tiles[b].phantom, whose parameters are staged into shared memory first
-// (they are constant, so this happens before the dependency wait).
 template <int L, int ND, int NL>
-__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
-    fdtd2d_packed_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step) {
+__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step2_kernel(const Fdtd2dParams p, int step, int par) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int CX = kConsumers / L;
+  // row-major tile order: neighbouring tiles, which share halo rows and
+  // columns, run close together in time (their halos hit in L2)
+  step2_block<L, ND, NL>(p, step, par, (int)blockIdx.x * (CX - 2) - 1, (int)blockIdx.y * p.rows2, (int)blockIdx.z,
+                         smem_raw);
+}
+
+// Many phantoms, two steps per launch: block b runs two-step tile tiles[b]
+// (x0 = its first thread column) of phantom tiles[b].phantom.
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
+    fdtd2d_packed2_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step,
+                          int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(16) Fdtd2dParams sp;
   const PackTile t = tiles[blockIdx.x];
@@ -845,7 +852,24 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  step_block<L, ND, NL>(sp, step, step & 1, t.x0, t.y0, t.g, smem_raw);
+  step2_block<L, ND, NL>(sp, step, par, t.x0, t.y0, t.g, smem_raw);
+}
+
+// Many phantoms in one launch: block b runs tile tiles[b] of phantom
+// tiles[b].phantom, whose parameters are staged into shared memory first
+// (they are constant, so this happens before the dependency wait).
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
+    fdtd2d_packed_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step,
+                         int par) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(16) Fdtd2dParams sp;
+  const PackTile t = tiles[blockIdx.x];
+  const int* src = reinterpret_cast<const int*>(params + t.phantom);
+  int* dst = reinterpret_cast<int*>(&sp);
+  for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  step_block<L, ND, NL>(sp, step, par, t.x0, t.y0, t.g, smem_raw);
 }
 
 // ------------------------------------------------------------------------
@@ -939,15 +963,17 @@ static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream
 }
 
 template <int L, int ND, int NL>
-static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step,
-                                   cudaStream_t s) {
-  constexpr size_t smem = stage_smem_bytes<L, ND + NL, NL>();
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(fdtd2d_packed_kernel<L, ND, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step, int par,
+                                   bool two, cudaStream_t s) {
+  const size_t smem = two ? step2_smem_bytes<L, ND, NL>() : stage_smem_bytes<L, ND + NL, NL>();
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[two]) {
+    cudaError_t e = two ? cudaFuncSetAttribute(fdtd2d_packed2_kernel<L, ND, NL>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(fdtd2d_packed_kernel<L, ND, NL>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_set[two] = true;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ntiles);
@@ -959,29 +985,30 @@ static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, fdtd2d_packed_kernel<L, ND, NL>, tiles, params, step);
+  if (two) return cudaLaunchKernelEx(&cfg, fdtd2d_packed2_kernel<L, ND, NL>, tiles, params, step, par);
+  return cudaLaunchKernelEx(&cfg, fdtd2d_packed_kernel<L, ND, NL>, tiles, params, step, par);
 }
 
 template <int ND, int NL>
-static cudaError_t packed_l(int L, const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step,
-                            cudaStream_t s) {
+static cudaError_t packed_l(int L, const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step, int par,
+                            bool two, cudaStream_t s) {
   switch (L) {
-    case 1: return launch_packed_l<1, ND, NL>(tiles, ntiles, params, step, s);
-    case 2: return launch_packed_l<2, ND, NL>(tiles, ntiles, params, step, s);
-    case 4: return launch_packed_l<4, ND, NL>(tiles, ntiles, params, step, s);
-    default: return launch_packed_l<8, ND, NL>(tiles, ntiles, params, step, s);
+    case 1: return launch_packed_l<1, ND, NL>(tiles, ntiles, params, step, par, two, s);
+    case 2: return launch_packed_l<2, ND, NL>(tiles, ntiles, params, step, par, two, s);
+    case 4: return launch_packed_l<4, ND, NL>(tiles, ntiles, params, step, par, two, s);
+    default: return launch_packed_l<8, ND, NL>(tiles, ntiles, params, step, par, two, s);
   }
 }
 
 cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
-                                 const Fdtd2dParams* params, int step, cudaStream_t s) {
+                                 const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s) {
   switch (n_debye * 3 + n_lorentz) {
-    case 0: return packed_l<0, 0>(L, tiles, ntiles, params, step, s);
-    case 1: return packed_l<0, 1>(L, tiles, ntiles, params, step, s);
-    case 2: return packed_l<0, 2>(L, tiles, ntiles, params, step, s);
-    case 3: return packed_l<1, 0>(L, tiles, ntiles, params, step, s);
-    case 4: return packed_l<1, 1>(L, tiles, ntiles, params, step, s);
-    case 6: return packed_l<2, 0>(L, tiles, ntiles, params, step, s);
+    case 0: return packed_l<0, 0>(L, tiles, ntiles, params, step, par, two, s);
+    case 1: return packed_l<0, 1>(L, tiles, ntiles, params, step, par, two, s);
+    case 2: return packed_l<0, 2>(L, tiles, ntiles, params, step, par, two, s);
+    case 3: return packed_l<1, 0>(L, tiles, ntiles, params, step, par, two, s);
+    case 4: return packed_l<1, 1>(L, tiles, ntiles, params, step, par, two, s);
+    case 6: return packed_l<2, 0>(L, tiles, ntiles, params, step, par, two, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -52,10 +52,12 @@ struct PackTile {
   int g;        // TX group
 };
 
-// Launch one step of every tile in `tiles` (all of one lane width L and one
-// ADE shape), each block reading its phantom's parameters from `params`.
+// Launch one step (two steps when `two`: tiles of the two-step geometry,
+// x0 = the first thread column) of every tile in `tiles` (all of one lane
+// width L and one ADE shape), each block reading its phantom's parameters
+// from `params`; `par` is the read half of every ping-pong array.
 cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
-                                 const Fdtd2dParams* params, int step, cudaStream_t s);
+                                 const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s);
 int fdtd2d_cells_per_block(int L);
 // Rows per block for a column-strip x row-segment grid of `slots` resident blocks.
 int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int max_rows);

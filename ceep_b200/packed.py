@@ -10,13 +10,16 @@ sorted by decreasing step count so the running tiles form a prefix) and
 advances all of them together (``ceep2d_pack_*`` in include/ceep_b200.h).
 Each solver's ``probe_data``, ``ez`` ... hold its own results afterwards.
 
-``autotune`` picks the tile height (rows per block) by timing a short prefix of
-the packed run for each candidate.
+``temporal_block=2`` advances every running phantom two steps per launch with
+the temporal-block kernel (a phantom with an odd step count takes its last
+step alone).  ``autotune`` picks the temporal-block depth and the tile height
+(rows per block) by timing a short prefix of the packed run for each
+candidate pair.
 """
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, List, Sequence
+from typing import Dict, List, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -26,7 +29,8 @@ from .solvers import BatchedFDTD2D
 
 
 class PackedBatch2D:
-    def __init__(self, solvers: Sequence[BatchedFDTD2D], rows: int = 16, use_graph: bool = True):
+    def __init__(self, solvers: Sequence[BatchedFDTD2D], rows: int = 16, use_graph: bool = True,
+                 temporal_block: int = 1):
         if not solvers:
             raise ValueError("no solvers")
         self.solvers: List[BatchedFDTD2D] = list(solvers)
@@ -35,6 +39,9 @@ class PackedBatch2D:
         self._pack = None
         self._ws = None
         self.rows = int(rows)
+        self.temporal_block = int(temporal_block)
+        if self.temporal_block not in (1, 2):
+            raise ValueError("temporal_block must be 1 or 2")
         for s in self.solvers:
             if s.device != self.device:
                 raise ValueError("all solvers must live on one device")
@@ -76,6 +83,7 @@ class PackedBatch2D:
                                        C.c_void_p(stream.cuda_stream), C.byref(h)), "ceep2d_pack_create")
         self._pack = h
         self.rows = rows
+        check(lib().ceep2d_pack_set_temporal_block(h, self.temporal_block), "ceep2d_pack_set_temporal_block")
 
     def reset(self):
         for s in self.solvers:
@@ -101,23 +109,28 @@ class PackedBatch2D:
     def tiles_at(self, step: int) -> int:
         return lib().ceep2d_pack_tiles(self._pack, step)
 
-    def autotune(self, candidates=(8, 12, 16, 20, 24, 32, 48), probe_steps: int = 40) -> Dict[int, float]:
-        """Time ``probe_steps`` packed steps per candidate tile height; keep the
-        fastest.  Returns ms per step for each candidate."""
+    def autotune(self, candidates=(8, 12, 16, 20, 24, 32, 48), probe_steps: int = 40,
+                 temporal_blocks=(1, 2)) -> Dict[Tuple[int, int], float]:
+        """Time ``probe_steps`` packed steps for each (temporal-block depth,
+        tile height) pair; keep the fastest.  Returns ms per step for each."""
         stream = torch.cuda.current_stream(self.device)
         timings = {}
         nst = min(probe_steps, self.max_steps)
-        for rows in candidates:
-            self._replan(rows)
-            self.advance(0, nst, stream)           # capture + warm
-            self.reset()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            self.advance(0, nst, stream)
-            b.record(stream)
-            torch.cuda.synchronize(self.device)
-            timings[rows] = a.elapsed_time(b) / nst
-            self.reset()
+        nst -= nst % 2 if nst < self.max_steps else 0    # even, unless the whole run
+        for tb in temporal_blocks:
+            for rows in candidates:
+                self.temporal_block = tb
+                self._replan(rows)
+                self.advance(0, nst, stream)           # capture + warm
+                self.reset()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                self.advance(0, nst, stream)
+                b.record(stream)
+                torch.cuda.synchronize(self.device)
+                timings[(tb, rows)] = a.elapsed_time(b) / nst
+                self.reset()
         best = min(timings, key=timings.get)
-        self._replan(best)
+        self.temporal_block = best[0]
+        self._replan(best[1])
         return timings

@@ -149,6 +149,13 @@ int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void* workspace
 int ceep2d_pack_run(ceep2d_pack* pack, int64_t step0, int64_t nsteps, void* stream, int use_graph);
 /* Number of tiles (blocks) launched at `step`, over all classes. */
 int ceep2d_pack_tiles(const ceep2d_pack* pack, int32_t step);
+/* Steps per launch, 1 or 2 (default 1).  With 2 every launch advances each
+ * running plan two steps with the temporal-block kernel (its own tile
+ * table: tile height = each plan's two-step rows); a plan with an odd step
+ * count takes its last step alone.  Runs then start at an even step and end
+ * at an even step or the last one.  Set before the first run. */
+int ceep2d_pack_set_temporal_block(ceep2d_pack* pack, int steps);
+int ceep2d_pack_temporal_block(const ceep2d_pack* pack);
 int ceep2d_pack_destroy(ceep2d_pack* pack);
 
 /* ------------------------------------------------------------------------

@@ -63,7 +63,8 @@ def test_packed_against_oracle_and_autotune(cuda_device):
     made = [_make(spec, 10 + k) for k, spec in enumerate(SPECS[:4])]
     pk = PackedBatch2D([m[0] for m in made])
     timings = pk.autotune(candidates=(8, 16, 24), probe_steps=20)
-    assert set(timings) == {8, 16, 24} and pk.rows in timings
+    assert set(timings) == {(tb, r) for tb in (1, 2) for r in (8, 16, 24)}
+    assert (pk.temporal_block, pk.rows) in timings
     results = pk.run()
     for (s, (eps, sig, disp)), res, spec in zip(made, results, SPECS):
         o = Fdtd2DOracle(s.nx, s.ny, 0.5e-3, s.total_steps, s.cpml_n, s.source_positions, s.probe_positions,
@@ -71,3 +72,28 @@ def test_packed_against_oracle_and_autotune(cuda_device):
         o.run()
         got = np.array([[res[b][p] for p in range(len(s.probe_positions))] for b in range(s.batch)])
         assert rel_l2(got, o.probe_data) < 1e-4, spec
+
+
+def test_packed_two_steps_per_launch_equals_individual_runs(cuda_device):
+    """temporal_block=2: every running phantom advances two steps per launch
+    (the 75-step phantom takes its last step alone); probe series and final
+    fields equal each phantom's own run bit for bit."""
+    from ceep_b200.packed import PackedBatch2D
+    solo = []
+    for k, spec in enumerate(SPECS):
+        s, _ = _make(spec, 20 + k)
+        s.set_rows_per_block(12)
+        s.run()
+        solo.append((s.probe_data.clone(), s.ez.clone(), s.hx.clone()))
+    packed = [_make(spec, 20 + k)[0] for k, spec in enumerate(SPECS)]
+    pk = PackedBatch2D(packed, rows=12, temporal_block=2)
+    pk.run()
+    for (pd, ez, hx), s in zip(solo, packed):
+        assert torch.equal(pd, s.probe_data)
+        assert torch.equal(ez, s.ez) and torch.equal(hx, s.hx)
+    # a run in two halves (even bounds) gives the same
+    pk.reset()
+    pk.advance(0, 40)
+    pk.advance(40)
+    for (pd, ez, hx), s in zip(solo, packed):
+        assert torch.equal(pd, s.probe_data) and torch.equal(ez, s.ez)
