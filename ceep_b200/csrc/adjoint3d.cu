@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kAdj3dThreads, 6) adjoint3d_h_kernel(const Adj
 // (the last interior column) so that every lane joins the lane sums; they
 // store nothing.
 template <int L, int ND>
-__global__ void __launch_bounds__(kAdj3dThreads, 5)
+__global__ void __launch_bounds__(kAdj3dThreads, 4)
     adjoint3d_e_kernel(const Adjoint3dParams a, int step, const float4* __restrict__ e_n,
                        const float4* __restrict__ e_np1, int e_n_post) {
   constexpr int CX = kAdj3dThreads / L;
