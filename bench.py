@@ -283,12 +283,12 @@ def run_ours(args, w):
 
     # -- end to end through the public API with host buffers
     e2e = None
-    if not args.no_e2e and w.get("dim", 2) == 2:
+    if not args.no_e2e:
         e2e = run_e2e(w, phantoms[:min(K, 3)], pos, freqs, device, tblock)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and w.get("dim", 2) == 2:
-        cpu = cpu_baseline(w, sample_steps=args.cpu_steps)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w, sample_steps=args.cpu_steps if w.get("dim", 2) == 2 else 2)
 
     if world > 1:
         dist.barrier()
@@ -332,8 +332,11 @@ class _HostMaps:
     arrays (generating the phantom is not part of the measured path)."""
 
     def __init__(self, ph):
-        self.eps_r, self.sigma = ph.get_eps_map()
+        three = hasattr(ph, "get_eps_map_3d")
+        self.eps_r, self.sigma = ph.get_eps_map_3d() if three else ph.get_eps_map()
         self.dispersion = ph.get_dispersion()
+        if three:
+            self.get_eps_map_3d = self.get_eps_map
 
     def get_eps_map(self, frequency=None):
         return self.eps_r, self.sigma
@@ -347,10 +350,16 @@ def run_e2e(w, phantoms, pos, freqs, device, tblock=1):
     update_materials (H2D of the FP64 maps) -> run() (D2H of every series) ->
     s_matrix() (D2H) -> DAS image (D2H)."""
     import torch
-    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200 import BatchedFDTD2D, BatchedFDTD3D
     from ceep_b200.spectral import das_image
-    solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
-                           frequencies=freqs, device=str(device), temporal_block=tblock)
+    three = w.get("dim", 2) == 3
+    if three:
+        solver = BatchedFDTD3D(w["nx"], w["ny"], w["nz"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
+                               frequencies=freqs, device=str(device))
+    else:
+        solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
+                               frequencies=freqs, device=str(device), temporal_block=tblock)
+    half = 0.07 if three else 0.09
     phantoms = [None if ph is None else _HostMaps(ph) for ph in phantoms]
     if phantoms[0] is not None:
         solver.set_phantom(phantoms[0])
@@ -368,25 +377,44 @@ def run_e2e(w, phantoms, pos, freqs, device, tblock=1):
         out = solver.run()
         S = solver.s_matrix()
         img = das_image(torch.as_tensor(S, dtype=torch.complex64, device=device), freqs,
-                        np.asarray(pos, float) * w["dx"], w["das"], w["das"], w["nx"] // 2 * w["dx"] - 0.09,
-                        w["ny"] // 2 * w["dx"] - 0.09, 0.18 / w["das"], 299_792_458.0).cpu().numpy()
+                        np.asarray([p[:2] for p in pos], float) * w["dx"], w["das"], w["das"],
+                        w["nx"] // 2 * w["dx"] - half, w["ny"] // 2 * w["dx"] - half, 2 * half / w["das"],
+                        299_792_458.0).cpu().numpy()
         times.append(time.perf_counter() - t0)
-        # FP64 (nx, ny) maps: eps_r, sigma and 2 per Debye / 3 per Lorentz pole; S for the image
-        h2d = w["nx"] * w["ny"] * 8 * (2 + 2 * len(solver._debye) + 3 * len(solver._lorentz)) + S.size * 8
+        # FP64 maps: eps_r, sigma and 2 per Debye / 3 per Lorentz pole; S for the image
+        h2d = _cells(w) * 8 * (2 + 2 * len(solver._debye) + 3 * len(solver._lorentz)) + S.size * 8
         d2h = solver.probe_data.numel() * 4 + S.size * 8 + img.size * 4
-    cell_steps = w["nx"] * w["ny"] * w["steps"] * w["ntx"]
+    cell_steps = _cells(w) * w["steps"] * w["ntx"]
+    name = "BatchedFDTD3D" if three else "BatchedFDTD2D"
     return {"value": round(len(times) * cell_steps / sum(times) / 1e9, 3), "unit": "GCell-steps/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "path": "BatchedFDTD2D.set_phantom/run/s_matrix + DAS, host arrays in and out"}
+            "path": f"{name}.set_phantom/run/s_matrix + DAS, host arrays in and out"}
 
 
 def _oracle_worker_init(w, tx_list, seed):
+    """One oracle over the TX in ``tx_list`` of workload ``w``: the 2D disk
+    (config 1), the 2D Debye head (config 2, or a config-3 pack case when
+    ``w`` names its phantom), or the 3D Debye head (config 5)."""
     global _ORACLE
+    from ceep_b200.phantoms import HeadPhantom2D, HeadPhantom3D, ring_positions
+    if w.get("dim", 2) == 3:
+        from oracle.fdtd3d import Fdtd3DOracle
+        pos = [(x, y, w["nz"] // 2) for x, y in ring_positions(w["ntx"], (w["nx"] // 2, w["ny"] // 2), w["ring"])]
+        sc = min(w["nx"], w["ny"], w["nz"]) / 192.0
+        ph = HeadPhantom3D(w["nx"], w["ny"], w["nz"], w["dx"], seed=seed,
+                           semi_axes=(0.070 * sc, 0.056 * sc, 0.060 * sc))
+        eps, sig = ph.get_eps_map_3d()
+        _ORACLE = Fdtd3DOracle(w["nx"], w["ny"], w["nz"], w["dx"], w["steps"], w["cpml"], [pos[i] for i in tx_list],
+                               pos, 2e9, eps_r=eps, sigma_e=sig, dispersion=ph.get_dispersion())
+        return
     from oracle.fdtd2d import Fdtd2DOracle
-    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
     pos = ring_positions(w["ntx"], (w["nx"] // 2, w["ny"] // 2), w["ring"])
     src = [pos[i] for i in tx_list]
-    if w["debye"]:
+    if "phantom" in w:
+        ph = _case_phantom(w)
+        eps, sig = ph.get_eps_map()
+        disp = ph.get_dispersion()
+    elif w["debye"]:
         ph = HeadPhantom2D(w["nx"], w["ny"], w["dx"], seed=seed)
         eps, sig = ph.get_eps_map()
         disp = ph.get_dispersion()
@@ -412,53 +440,156 @@ def cpu_baseline(w, sample_steps=12):
     bounded number of time steps of the same workload."""
     _oracle_worker_init(w, list(range(w["ntx"])), 1000)
     dt = _oracle_worker_run(sample_steps)
-    v = w["nx"] * w["ny"] * w["ntx"] * sample_steps / dt / 1e9
+    v = _cells(w) * w["ntx"] * sample_steps / dt / 1e9
     return {"value": round(v, 6), "unit": "GCell-steps/s", "cores": 1, "kind": "port",
             "sample": f"{sample_steps} of {w['steps']} time steps, all {w['ntx']} TX, FP64 NumPy oracle, "
                       f"{dt:.1f} s"}
 
 
-def run_reference(args, w):
-    """Reference arm: the oracle port on all host cores (TX spread over spawn workers)."""
+def _cells(w):
+    return w["nx"] * w["ny"] * w.get("nz", 1)
+
+
+def _time_oracle_pools(cases, ncpu, warmup, steps, per_step):
+    """Spread the TX of every case in ``cases`` (workload dicts) over spawn
+    workers, one oracle per worker; time ``steps`` bench steps of ``per_step``
+    time steps each after ``warmup`` one-step rounds.  Returns (seconds per
+    bench step, worker count)."""
     import multiprocessing as mp
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    if rank != 0:
-        return
-    ncpu = os.cpu_count() or 1
-    nproc = max(1, min(ncpu, w["ntx"]))
-    groups = [list(range(w["ntx"]))[i::nproc] for i in range(nproc)]
     ctx = mp.get_context("spawn")
-    per_step_steps = args.cpu_steps
-    pools = [ctx.Pool(1, initializer=_oracle_worker_init, initargs=(w, g, 1000)) for g in groups]
+    share = max(1, ncpu // len(cases))
+    jobs = []
+    for w in cases:
+        nproc = max(1, min(share, w["ntx"]))
+        jobs += [(w, list(range(w["ntx"]))[i::nproc]) for i in range(nproc)]
+    pools = [ctx.Pool(1, initializer=_oracle_worker_init, initargs=(w, g, w.get("seed", 1000))) for w, g in jobs]
     try:
-        for _ in range(args.warmup):
-            rs = [p.apply_async(_oracle_worker_run, (1,)) for p in pools]
-            [r.get() for r in rs]
+        for _ in range(warmup):
+            [r.get() for r in [p.apply_async(_oracle_worker_run, (1,)) for p in pools]]
         times = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             t0 = time.perf_counter()
-            rs = [p.apply_async(_oracle_worker_run, (per_step_steps,)) for p in pools]
-            [r.get() for r in rs]
+            [r.get() for r in [p.apply_async(_oracle_worker_run, (per_step,)) for p in pools]]
             times.append(time.perf_counter() - t0)
     finally:
         for p in pools:
             p.close()
             p.join()
-    cell_steps = w["nx"] * w["ny"] * w["ntx"] * per_step_steps
-    value = len(times) * cell_steps / sum(times) / 1e9
-    line = {"impl": "reference", "metric": "batched FDTD GCell-steps/s", "value": round(value, 6),
-            "unit": "GCell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantoms)",
-            "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "tx": w["ntx"],
-                       "time_steps_per_bench_step": per_step_steps},
-            "cpu_baseline": {"value": round(value, 6), "unit": "GCell-steps/s", "cores": nproc, "kind": "port",
-                             "sample": f"{per_step_steps} time steps x {w['ntx']} TX per bench step, "
-                                       f"{nproc} spawn workers over TX, {ncpu} host cores"},
+    return times, len(pools)
+
+
+def _reference_line(args, workload, value, ms, cores, sample, config, metric="batched FDTD GCell-steps/s",
+                    dtype="f64"):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    line = {"impl": "reference", "metric": metric, "value": round(value, 6), "unit": "GCell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded phantoms)", "config": dict(workload=workload, **config),
+            "cpu_baseline": {"value": round(value, 6), "unit": "GCell-steps/s", "cores": cores, "kind": "port",
+                             "sample": sample},
             "e2e": {"value": round(value, 6), "unit": "GCell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_reference(args, w):
+    """Reference arm: the oracle port on all host cores (TX spread over spawn
+    workers), a bounded number of time steps per bench step."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    ncpu = os.cpu_count() or 1
+    per_step = args.cpu_steps if w.get("dim", 2) == 2 else max(1, args.cpu_steps // 6)
+    times, nproc = _time_oracle_pools([w], ncpu, args.warmup, args.steps, per_step)
+    value = len(times) * _cells(w) * w["ntx"] * per_step / sum(times) / 1e9
+    cfg = {k: w[k] for k in ("nx", "ny", "nz") if k in w}
+    cfg.update(tx=w["ntx"], time_steps_per_bench_step=per_step)
+    _reference_line(args, args.workload, value, 1e3 * sum(times) / len(times), nproc,
+                    f"{per_step} time steps x {w['ntx']} TX per bench step, {nproc} spawn workers over TX, "
+                    f"{ncpu} host cores", cfg)
+
+
+def run_pack_reference(args):
+    """Reference arm of the packed uneven batch: the 2D oracle on a sample of
+    the config-3 phantoms (every TX of each, spread over spawn workers), a
+    bounded number of time steps per bench step."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    ncpu = os.cpu_count() or 1
+    cases = _pack_cases(args.pack_count)
+    sample = cases[:: max(1, len(cases) // 4)][:4]
+    per_step = args.cpu_steps
+    times, nproc = _time_oracle_pools(sample, ncpu, args.warmup, args.steps, per_step)
+    cs = sum(_cells(c) * c["ntx"] for c in sample) * per_step
+    value = len(times) * cs / sum(times) / 1e9
+    _reference_line(args, "pack256", value, 1e3 * sum(times) / len(times), nproc,
+                    f"{len(sample)} of {args.pack_count} phantoms ({', '.join(f'{c['nx']}x{c['ny']}' for c in sample)}),"
+                    f" all TX, {per_step} time steps each per bench step, {nproc} spawn workers",
+                    {"phantoms": args.pack_count, "sampled": len(sample), "time_steps_per_bench_step": per_step},
+                    metric="packed uneven batch GCell-steps/s")
+
+
+def _single_case(nx):
+    """The non-batched workload: TMz, nx x nx, 1 mm, CFS-CPML 20, a Gaussian Ez
+    source at the centre, eight probes on a circle, a lossy dielectric disk of
+    radius nx/5 (eps_r 4, sigma 0.2 S/m)."""
+    from ceep_b200 import fdtd2d as F
+    T, n = 1000, 20
+    cfg = F.SimulationConfig(grid=F.GridConfig(nx=nx, ny=nx, dx=1e-3, dy=1e-3), mode=F.SimulationMode.TMZ,
+                             total_steps=T)
+    src = [F.GaussianSource(x=nx // 2, y=nx // 2, frequency_max=20e9)]
+    prb = [(nx // 2 + int(0.3 * nx * np.cos(a)), nx // 2 + int(0.3 * nx * np.sin(a)))
+           for a in np.linspace(0, 2 * np.pi, 8, endpoint=False)]
+    return cfg, src, prb, n, T
+
+
+def _single_oracle(nx):
+    """The oracle of ``_single_case``: coefficients from the disk map in FP64
+    (the update coefficients of grid.py:157-195)."""
+    from oracle.fdtd2d_single import EPS_0, MU_0, Single2DOracle
+    cfg, src, prb, n, T = _single_case(nx)
+    dt = cfg.dt
+    x, y = np.meshgrid(np.arange(nx), np.arange(nx), indexing="ij")
+    m = (x - nx // 2) ** 2 + (y - nx // 2) ** 2 <= (nx // 5) ** 2
+    eps = np.where(m, 4.0, 1.0) * EPS_0
+    se = np.where(m, 0.2, 0.0) * dt / (2.0 * eps)
+    mu = MU_0
+    ca, cb = (1.0 - se) / (1.0 + se), (dt / eps) / (1.0 + se)
+    da, db = np.ones((nx, nx)), np.full((nx, nx), dt / mu)
+    wave = np.array([src[0].value_at(k, dt) for k in range(T)])
+    return Single2DOracle(nx, nx, 1e-3, 1e-3, dt, "TMZ", ca, cb, da, db, [(nx // 2, nx // 2, "Ez", wave)],
+                          [("cpml", n, 4, 2.0, 0.05, 1.0)], prb), T
+
+
+def run_single_reference(args):
+    """Reference arm of the non-batched solver: the oracle (one NumPy process,
+    as the reference's own NumPy backend runs) for a bounded number of time
+    steps per bench step."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    nx = 1024 if args.small else 4096
+    o, T = _single_oracle(nx)
+    per_step = 2
+    o.run(args.warmup)
+    times = []
+    for _ in range(args.steps):
+        if o.n + per_step > T:
+            o.n = 0
+        t0 = time.perf_counter()
+        o.run(per_step)
+        times.append(time.perf_counter() - t0)
+    value = len(times) * nx * nx * per_step / sum(times) / 1e9
+    _reference_line(args, "single4096" if not args.small else "single1024", value, 1e3 * sum(times) / len(times), 1,
+                    f"{per_step} of {T} time steps per bench step, FP64 NumPy oracle, one process",
+                    {"nx": nx, "ny": nx, "mode": "TMz", "cpml": 20, "time_steps_per_bench_step": per_step},
+                    metric="FDTD2D (non-batched) GCell-steps/s")
+
+
+def run_adjoint_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    print(json.dumps({"impl": "reference", "workload": args.workload,
+                      "unavailable": "the reference computes no gradient of its solvers (no adjoint path)"}),
+          flush=True)
 
 
 def run_adjoint_bench(args):
@@ -650,12 +781,7 @@ def run_single_bench(args):
     from ceep_b200 import fdtd2d as F
     dev = torch.device("cuda", 0)
     nx = ny = 1024 if args.small else 4096
-    T, n = 1000, 20
-    cfg = F.SimulationConfig(grid=F.GridConfig(nx=nx, ny=ny, dx=1e-3, dy=1e-3), mode=F.SimulationMode.TMZ,
-                             total_steps=T)
-    src = [F.GaussianSource(x=nx // 2, y=ny // 2, frequency_max=20e9)]
-    prb = [(nx // 2 + int(0.3 * nx * np.cos(a)), ny // 2 + int(0.3 * ny * np.sin(a)))
-           for a in np.linspace(0, 2 * np.pi, 8, endpoint=False)]
+    cfg, src, prb, n, T = _single_case(nx)
     s = F.FDTD2D(cfg, sources=src, boundaries=[F.CPML(thickness=n)], probe_points=prb)
     s.grid.set_material_circle(nx // 2, ny // 2, nx // 5, eps_r=4.0, sigma_e=0.2)
     stream = torch.cuda.current_stream(dev)
@@ -699,12 +825,7 @@ def run_single_bench(args):
     e2e_ms = t0.elapsed_time(t1)
     cpu = None
     if not args.no_cpu:
-        from oracle.fdtd2d_single import Single2DOracle
-        import time
-        g = s.grid
-        w = [np.array([src[0].value_at(k, cfg.dt) for k in range(T)])]
-        o = Single2DOracle(nx, ny, 1e-3, 1e-3, cfg.dt, "TMZ", g._ca, g._cb, g._da, g._db,
-                           [(nx // 2, ny // 2, "Ez", w[0])], [("cpml", n, 4, 2.0, 0.05, 1.0)], prb)
+        o, _ = _single_oracle(nx)
         k = 6
         t = time.perf_counter()
         o.run(k)
@@ -732,11 +853,10 @@ def run_single_bench(args):
     print(json.dumps(line), flush=True)
 
 
-def _pack_solvers(count, device, seed=2024):
-    """Config-3 phantoms: nx, ny in {256..768 step 32}, steps in [600, 1200],
-    8-16 TX, one third with a two-pole Lorentz model instead of Debye."""
-    from ceep_b200 import BatchedFDTD2D
-    from ceep_b200.phantoms import HeadPhantom2D, LorentzHeadPhantom2D, ring_positions
+def _pack_cases(count, seed=2024):
+    """Config-3 phantoms as host-side specs: nx, ny in {256..768 step 32},
+    steps in [600, 1200], 8-16 TX on a ring, one third with a two-pole
+    Lorentz model instead of Debye."""
     rng = np.random.default_rng(seed)
     sizes = np.arange(256, 769, 32)
     out = []
@@ -744,11 +864,26 @@ def _pack_solvers(count, device, seed=2024):
         nx, ny = int(rng.choice(sizes)), int(rng.choice(sizes))
         steps, ntx = int(rng.integers(600, 1201)), int(rng.integers(8, 17))
         scale = min(nx, ny) / 600.0
-        cls = LorentzHeadPhantom2D if k % 3 == 2 else HeadPhantom2D
-        ph = cls(nx=nx, ny=ny, dx=0.5e-3, seed=seed + k, semi_axes=(0.09 * scale, 0.07 * scale))
-        pos = ring_positions(ntx, (nx // 2, ny // 2), 0.36 * min(nx, ny))
-        s = BatchedFDTD2D(nx, ny, 0.5e-3, steps, 15, pos, pos, 2e9, device=str(device))
-        s.set_phantom(ph)
+        out.append(dict(nx=nx, ny=ny, dx=0.5e-3, steps=steps, cpml=15, ntx=ntx, ring=0.36 * min(nx, ny),
+                        debye=True, phantom="lorentz" if k % 3 == 2 else "head",
+                        semi_axes=(0.09 * scale, 0.07 * scale), seed=seed + k))
+    return out
+
+
+def _case_phantom(c):
+    from ceep_b200.phantoms import HeadPhantom2D, LorentzHeadPhantom2D
+    cls = LorentzHeadPhantom2D if c["phantom"] == "lorentz" else HeadPhantom2D
+    return cls(nx=c["nx"], ny=c["ny"], dx=c["dx"], seed=c["seed"], semi_axes=c["semi_axes"])
+
+
+def _pack_solvers(count, device, seed=2024):
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.phantoms import ring_positions
+    out = []
+    for c in _pack_cases(count, seed):
+        pos = ring_positions(c["ntx"], (c["nx"] // 2, c["ny"] // 2), c["ring"])
+        s = BatchedFDTD2D(c["nx"], c["ny"], c["dx"], c["steps"], c["cpml"], pos, pos, 2e9, device=str(device))
+        s.set_phantom(_case_phantom(c))
         out.append(s)
     return out
 
@@ -915,6 +1050,16 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.impl == "reference":
+        if args.workload in ("adjoint400", "adjoint192"):
+            run_adjoint_reference(args)
+        elif args.workload == "single4096":
+            run_single_reference(args)
+        elif args.workload == "pack256":
+            run_pack_reference(args)
+        else:
+            run_reference(args, WORKLOADS[args.workload])
+        return
     if args.workload == "adjoint400":
         if args.profile:
             run_profile_adjoint(args)
@@ -936,8 +1081,6 @@ def main():
     w = WORKLOADS[args.workload]
     if args.profile:
         run_profile(args, w)
-    elif args.impl == "reference":
-        run_reference(args, w)
     else:
         run_ours(args, w)
 
