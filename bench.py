@@ -639,11 +639,13 @@ def run_adjoint_bench(args):
         s2.reset()
         s2.advance(0, T, stream=stream)
     t_fwd = timed(fwd, 3)
-    ratios = {}
-    for K in (1, 25, 50, 100):
+    ratios, kept_ratios, kept_info = {}, {}, {}
+    keep_budget = 16 << 30
+    for K, keep in ((1, 0), (25, 0), (50, 0), (100, 0), (25, keep_budget), (50, keep_budget),
+                    (100, keep_budget)):
         sk = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, pos, pos, 2e9, device=str(dev))
         sk.set_phantom(no_disk)
-        adj = Adjoint2D(sk, checkpoint_every=K)
+        adj = Adjoint2D(sk, checkpoint_every=K, keep_bytes=keep)
         e, g = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True)
         d = f64(de).requires_grad_(True)
 
@@ -651,7 +653,16 @@ def run_adjoint_bench(args):
             e.grad = g.grad = d.grad = None
             loss, _ = s_parameter_loss(probes_with_grad(e, g, adj, d, f64(tau)).double(), sk.dt, freqs, target)
             loss.backward()
-        ratios[K] = timed(grad_step, 2) / t_fwd
+        r = timed(grad_step, 2) / t_fwd
+        if keep:
+            kept_ratios[K] = r
+            nseg = -(-T // K)
+            kept_info[K] = f"{adj.kept_segments(nseg)} of {nseg} segments kept, " \
+                           f"{adj.kept_segments(nseg) * adj.segment_bytes() / 2 ** 30:.2f} GiB"
+            del adj, sk
+            torch.cuda.empty_cache()
+            continue
+        ratios[K] = r
         if K == 1:
             # split of one gradient: the forward that saves Ez/J of every step,
             # and the backward (adjoint steps + chain rule)
@@ -668,7 +679,9 @@ def run_adjoint_bench(args):
                        "debye_poles": 1, "dft_freqs": 101, "loss": "sum |S - S*|^2",
                        "grad": "eps_r, sigma, debye delta_eps"},
             "forward_ms": round(t_fwd, 3), "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()},
-            "every_step_kept": {k: round(v, 3) for k, v in split.items()}}
+            "every_step_kept": {k: round(v, 3) for k, v in split.items()},
+            "ratio_with_keep_budget": {str(k): round(v, 3) for k, v in kept_ratios.items()},
+            "keep_budget": {"bytes": keep_budget, **{str(k): v for k, v in kept_info.items()}}}
     print(json.dumps(line), flush=True)
 
 

@@ -63,50 +63,56 @@ def coefficient_maps(eps_r, sigma, debye, dt):
     return (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s), dt / (eps_r * EPS_0), poles
 
 
-def run_segments_backward(starts, seg_ready, recompute, adjoint, device, overlap):
+def run_segments_backward(starts, kept, recompute, adjoint, device, overlap, nbuf):
     """Drive the segments of a checkpointed adjoint, last first.
 
-    ``recompute(a, buf)`` enqueues, on the current stream, the restore of
-    checkpoint ``a`` and the saving recompute of its segment into segment
+    ``starts`` are the segment starts in descending order; the i-th of them
+    uses segment buffer ``i % nbuf``.  ``kept`` is the set of starts whose
+    slots the forward pass already left in their buffers (the last segments:
+    indices 0 .. len(kept)-1, so ``nbuf >= len(kept)``); every other segment
+    is recomputed.  ``recompute(a, buf)`` enqueues, on the current stream, the
+    restore of checkpoint ``a`` and the saving recompute of its segment into
     buffer ``buf``; ``adjoint(a, buf)`` enqueues the transposed steps of that
-    segment reading buffer ``buf``.  ``seg_ready`` is the segment whose slots
-    the forward pass already left in buffer 0.  With ``overlap`` (two
-    buffers) the recompute of the next segment runs on a second stream while
-    the adjoint of the current one runs on a high-priority stream: the two
-    are independent (different state, different buffers), and neither
-    saturates the GPU alone at these sizes.  Events order each buffer's
-    reuse; the caller's stream waits for both at the end."""
-    main = torch.cuda.current_stream(device)
+    segment reading buffer ``buf``.  With ``overlap`` (``nbuf >= 2``) the
+    recompute of the next segment runs on a second stream while the adjoint
+    of the current one runs on a high-priority stream: the two are
+    independent (different state, different buffers), and neither saturates
+    the GPU alone at these sizes.  Events order each buffer's reuse; the
+    caller's stream waits for both at the end."""
+    assert nbuf >= max(1, len(kept)) and all(a in kept for a in starts[:len(kept)])
     if not overlap:
-        for a in starts:
-            if a != seg_ready:
-                recompute(a, 0)
-            adjoint(a, 0)
+        for i, a in enumerate(starts):
+            if a not in kept:
+                recompute(a, i % nbuf)
+            adjoint(a, i % nbuf)
         return
+    assert nbuf >= 2
+    main = torch.cuda.current_stream(device)
     adj_s = torch.cuda.Stream(device, priority=-1)
     rec_s = torch.cuda.Stream(device)
     adj_s.wait_stream(main)
     rec_s.wait_stream(main)
-    freed = [None, None]
+    freed = [None] * nbuf
     ready = {}
-    if starts[0] != seg_ready:
+
+    def issue(i):
+        buf = i % nbuf
+        if freed[buf] is not None:
+            rec_s.wait_event(freed[buf])
         with torch.cuda.stream(rec_s):
-            recompute(starts[0], 0)
-        ready[0] = rec_s.record_event()
+            recompute(starts[i], buf)
+        ready[i] = rec_s.record_event()
+
+    if starts[0] not in kept:
+        issue(0)
     for i, a in enumerate(starts):
-        buf = i % 2
-        if i + 1 < len(starts):
-            nb = (i + 1) % 2
-            if freed[nb] is not None:
-                rec_s.wait_event(freed[nb])
-            with torch.cuda.stream(rec_s):
-                recompute(starts[i + 1], nb)
-            ready[i + 1] = rec_s.record_event()
+        if i + 1 < len(starts) and starts[i + 1] not in kept:
+            issue(i + 1)
         if i in ready:
             adj_s.wait_event(ready[i])
         with torch.cuda.stream(adj_s):
-            adjoint(a, buf)
-        freed[buf] = adj_s.record_event()
+            adjoint(a, i % nbuf)
+        freed[i % nbuf] = adj_s.record_event()
     main.wait_stream(adj_s)
     main.wait_stream(rec_s)
 
@@ -120,14 +126,15 @@ class Adjoint2D:
     the Debye currents of every step (one field less to write and read)."""
 
     def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False,
-                 overlap: bool = True):
+                 overlap: bool = True, keep_bytes: int = 0):
         if solver._lorentz:
             raise ValueError("the adjoint supports Debye poles only")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
         self.grad_tau = bool(grad_tau)
         self.overlap = bool(overlap)
-        self._seg_ready = None
+        self.keep_bytes = max(0, int(keep_bytes))
+        self._kept = set()
         self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
         self._ckpt = {}
@@ -167,6 +174,20 @@ class Adjoint2D:
     def _seglen(self):
         return self.s.total_steps if self.K == 1 else min(self.K, self.s.total_steps)
 
+    def segment_bytes(self):
+        """Device bytes of one segment buffer (the Ez slots, plus the J slots
+        when tau gradients are asked for)."""
+        s = self.s
+        n = (self._seglen() + 1) * s._groups * s.ny * s.nx * s._gwidth
+        if s._j is not None and self.grad_tau:
+            n += (self._seglen() + 1) * s._j[0].numel()
+        return 4 * n
+
+    def kept_segments(self, nseg):
+        """How many trailing segments the forward pass keeps: the last one
+        always, more while their buffers fit in ``keep_bytes``."""
+        return max(1, min(nseg, self.keep_bytes // max(1, self.segment_bytes())))
+
     def _buffers(self, count):
         """`count` segment buffers (Ez slots, J slots or None), allocated once:
         the saving graphs are keyed on their addresses."""
@@ -184,23 +205,28 @@ class Adjoint2D:
 
     def forward(self) -> torch.Tensor:
         """Run all steps from a zero state, keeping checkpoints; returns the probe
-        series (ntx, nprobe, T) float32 on the device.  The last segment runs
-        with the save on, so the backward pass never recomputes it."""
+        series (ntx, nprobe, T) float32 on the device.  The last segments (the
+        last one, and more within ``keep_bytes``) run with the save on into
+        their own buffers, so the backward pass never recomputes them; the
+        others start from a checkpoint of the full state."""
         s = self.s
         s.reset()
         T, L = s.total_steps, self._seglen()
         self._ckpt = {}
-        self._buffers(1)
-        stream = torch.cuda.current_stream(s.device)
         starts = list(range(0, T, L))
-        for a in starts:
+        M = self.kept_segments(len(starts))
+        self._buffers(M)
+        stream = torch.cuda.current_stream(s.device)
+        self._starts, self._kept = starts, set()
+        for j, a in enumerate(starts):
             b = min(a + L, T)
-            self._ckpt[a] = {k: v.clone() for k, v in self._state().items()}
-            if a == starts[-1]:
-                self._run_save(a, b, 0)
+            i = len(starts) - 1 - j                 # index in the backward order
+            if i < M:
+                self._run_save(a, b, i)
+                self._kept.add(a)
             else:
+                self._ckpt[a] = {k: v.clone() for k, v in self._state().items()}
                 s.advance(a, b - a, stream=stream)
-        self._seg_ready = starts[-1]
         return s.probe_data[:, :len(s.probe_positions)].clone()
 
     def _restore(self, a):
@@ -249,9 +275,11 @@ class Adjoint2D:
             arr[0], arr[1] = _ptr(bufs[0]), _ptr(bufs[1])
         d.grad, d.probe_grad = grad.data_ptr(), gp.data_ptr()
         d.grad_tau = int(self.grad_tau)
-        starts = sorted(self._ckpt, reverse=True)
-        two = self.overlap and len(starts) > 1
-        self._buffers(2 if two else 1)
+        starts = sorted(self._starts, reverse=True)
+        M = len(self._kept)
+        two = self.overlap and len(starts) > M
+        nbuf = max(M, 2 if two else 1)
+        self._buffers(nbuf)
         h = C.c_void_p()
         check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
         self.launch_rows = lib().ceep2d_adjoint_rows(h)
@@ -266,9 +294,9 @@ class Adjoint2D:
             check(lib().ceep2d_adjoint_run(h, min(a + L, T), min(a + L, T) - a, seg_ez.data_ptr(), _ptr(seg_j), a,
                                            C.c_void_p(st.cuda_stream)), "ceep2d_adjoint_run")
         try:
-            run_segments_backward(starts, self._seg_ready, recompute, adjoint, dev, two)
+            run_segments_backward(starts, self._kept, recompute, adjoint, dev, two, nbuf)
         finally:
-            self._seg_ready = None
+            self._kept = set()
             lib().ceep2d_adjoint_destroy(h)
         # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
         return self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])

@@ -178,7 +178,8 @@ class Adjoint3D:
             check(lib().ceep3d_adjoint_run(h, b, b - a, self._segs[buf].data_ptr(), a, C.c_void_p(st.cuda_stream)),
                   "ceep3d_adjoint_run")
         try:
-            run_segments_backward(starts, self._seg_ready, recompute, adjoint, dev, two)
+            kept = set() if self._seg_ready is None else {self._seg_ready}
+            run_segments_backward(starts, kept, recompute, adjoint, dev, two, 2 if two else 1)
         finally:
             self._seg_ready = None
             lib().ceep3d_adjoint_destroy(h)

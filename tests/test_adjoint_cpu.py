@@ -70,3 +70,23 @@ def test_autograd_matches_central_differences():
         fd, ad = np.array(fd), np.array(ad)
         err = np.linalg.norm(fd - ad) / np.linalg.norm(fd)
         assert err < 1e-4, (name, err)
+
+
+def test_segment_schedule_serial():
+    """The serial backward schedule: kept segments are read from their own
+    buffers, every other segment is recomputed into its buffer just before
+    its adjoint reads it, last segment first."""
+    from ceep_b200.adjoint import run_segments_backward
+    starts = [88, 77, 66, 55, 44, 33]
+    for kept in ({88}, {88, 77}, {88, 77, 66}, set(starts)):
+        nbuf = max(1, len(kept))
+        log, holds = [], {}
+        rec = lambda a, b: (log.append(("r", a, b)), holds.__setitem__(b, a))
+        adj = lambda a, b: log.append(("a", a, b, holds.get(b)))
+        for i, a in enumerate(starts):       # the forward pass left the kept ones in buffer i
+            if a in kept:
+                holds[i] = a
+        run_segments_backward(starts, kept, rec, adj, "cpu", False, nbuf)
+        assert [e[1] for e in log if e[0] == "a"] == starts
+        assert all(e[3] == e[1] for e in log if e[0] == "a")       # each adjoint reads its own segment
+        assert sorted(e[1] for e in log if e[0] == "r") == sorted(set(starts) - kept)

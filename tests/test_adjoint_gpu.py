@@ -159,3 +159,27 @@ def test_overlapped_recompute_gives_the_same_gradient(cuda_device):
         (p.double() ** 2).sum().backward()
         res.append(e.grad.clone())
     assert torch.equal(res[0], res[1])
+
+
+def test_kept_segments_give_the_same_gradient(cuda_device):
+    """Keeping 1, 2, 3 or all trailing segments (``keep_bytes``), with and
+    without the two-stream backward, gives the same bits."""
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    eps, sig, de, tau, m, ring = _case(72, 64, 6, 8)
+    res = []
+    for keep in (0, 2, 3, 99):
+        for overlap in (False, True):
+            s = BatchedFDTD2D(72, 64, 0.5e-3, 130, 6, ring[:3], ring, 2e9)
+            s.set_dispersion(debye=[(de, tau)])
+            adj = Adjoint2D(s, checkpoint_every=11, overlap=overlap)
+            s._build()
+            adj.keep_bytes = keep * adj.segment_bytes()
+            e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+            p = probes_with_grad(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                                 torch.tensor(tau, device="cuda"))
+            assert len(adj._ckpt) == 12 - min(12, max(1, keep))      # 12 segments of 11 steps
+            (p.double() ** 2).sum().backward()
+            res.append(e.grad.clone())
+    for r in res[1:]:
+        assert torch.equal(res[0], r)
