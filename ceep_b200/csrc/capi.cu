@@ -235,6 +235,7 @@ extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
 struct ceep3d_plan {
   ceep::Fdtd3dParams p;
   std::map<std::tuple<int64_t, int64_t, const void*, int64_t, int>, cudaGraphExec_t> graphs;
+  ceep::Fdtd3dSide side{nullptr, nullptr, nullptr};   // the H shell's stream
 };
 
 extern "C" int64_t ceep3d_desc_size(void) { return (int64_t)sizeof(ceep3d_desc); }
@@ -296,13 +297,25 @@ extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
   p.save_cs = p.groups * p.gs_field;
   p.save_base = 0;
   p.interior_only = 0;
+  // the H shell's stream at the highest priority, so that its blocks (few,
+  // long, register-heavy) start first and the box's fill the rest
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&pl->side.stream, cudaStreamNonBlocking, greatest);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->side.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->side.join, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    ceep3d_plan_destroy(pl);
+    return ceep::cuda_fail(e, "ceep3d_plan_create: side stream");
+  }
   *out = pl;
   return CEEP_OK;
 }
 
-static int run_steps3d(const ceep::Fdtd3dParams& q, int64_t step0, int64_t nsteps, cudaStream_t s) {
+static int run_steps3d(const ceep::Fdtd3dParams& q, int64_t step0, int64_t nsteps, cudaStream_t s,
+                       const ceep::Fdtd3dSide* side) {
   for (int64_t k = 0; k < nsteps; ++k) {
-    cudaError_t e = ceep::fdtd3d_launch_step(q, (int)(step0 + k), s);
+    cudaError_t e = ceep::fdtd3d_launch_step(q, (int)(step0 + k), s, side);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd3d step launch");
   }
   return CEEP_OK;
@@ -322,14 +335,15 @@ static int plan_run3d(ceep3d_plan* pl, int64_t step0, int64_t nsteps, void* stre
   q.save_base = save_e ? (int)save_base : 0;
   q.interior_only = interior_only && pl->p.n > 0 ? 1 : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!use_graph || s == nullptr) return run_steps3d(q, step0, nsteps, s);
+  const ceep::Fdtd3dSide* side = pl->side.stream ? &pl->side : nullptr;
+  if (!use_graph || s == nullptr) return run_steps3d(q, step0, nsteps, s, side);
   auto key = std::make_tuple(step0, nsteps, (const void*)save_e, (int64_t)q.save_base, q.interior_only);
   auto it = pl->graphs.find(key);
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps3d(q, step0, nsteps, s);
+    int rc = run_steps3d(q, step0, nsteps, s, side);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -356,6 +370,10 @@ extern "C" int ceep3d_plan_run_save(ceep3d_plan* pl, int64_t step0, int64_t nste
 extern "C" int ceep3d_plan_destroy(ceep3d_plan* pl) {
   if (!pl) return CEEP_OK;
   for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  if (pl->side.stream) cudaStreamSynchronize(pl->side.stream);
+  if (pl->side.join) cudaEventDestroy(pl->side.join);
+  if (pl->side.fork) cudaEventDestroy(pl->side.fork);
+  if (pl->side.stream) cudaStreamDestroy(pl->side.stream);
   delete pl;
   return CEEP_OK;
 }

@@ -135,29 +135,73 @@ __device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, 
   }
 }
 
+// The H half-step is two launches over disjoint cells.  The box
+// [n, N-m)^3 (m = max(n, 1)) lies inside all three interior boxes and on no
+// CPML face, so its cells take the lean path (no region tests, no face code,
+// fewer registers, more resident warps); the shell around it takes the
+// general path.  Both only read E, so their order does not matter.
 template <int L>
-__global__ void __launch_bounds__(kThreads3d, 6) fdtd3d_h_kernel(const Fdtd3dParams p) {
+__global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_h_box_kernel(const Fdtd3dParams p, int zsegs) {
   constexpr int CX = kThreads3d / L;
-  const int x0 = blockIdx.x * CX;
-  const int x = x0 + threadIdx.x / L;
+  const int n = p.n, m = n > 1 ? n : 1;
+  const int x = n + blockIdx.x * CX + threadIdx.x / L;
   const int lo = threadIdx.x % L;
-  const int y = blockIdx.y;
-  const int zseg = blockIdx.z % p.zsegs, g = blockIdx.z / p.zsegs;
-  const int z0 = zseg * p.zrows, z1 = min(z0 + p.zrows, p.nz);
-  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n;
-  if (x >= nx) return;
-  // every cell of the block in all three interior boxes and on no face:
-  // x in [n, nx-n), y in [n, ny-n), z in [n, nz-n) with n >= 1 (nx-n <= nx-1)
-  const int m = n > 1 ? n : 1;
-  const bool interior = x0 >= n && x0 + CX <= nx - m && y >= n && y < ny - m && z0 >= n && z1 <= nz - m;
-  if (interior) {
-    h_segment<L, false>(p, x, lo, y, g, z0, z1);
-  } else if (!p.interior_only) {
-    h_segment<L, true>(p, x, lo, y, g, z0, z1);
-  } else if (n > 0 && x >= n && x < nx - n && y >= n && y < ny - n) {
-    // the cells of [n, N-n)^3 take the same code path as in a full step
-    const int za = max(z0, n), zb = min(z1, nz - n);
-    if (za < zb) h_segment<L, true>(p, x, lo, y, g, za, zb);
+  const int y = n + blockIdx.y;
+  const int zseg = blockIdx.z % zsegs, g = blockIdx.z / zsegs;
+  const int z0 = n + zseg * p.zrows, z1 = min(z0 + p.zrows, p.nz - m);
+  if (x >= p.nx - m) return;
+  h_segment<L, false>(p, x, lo, y, g, z0, z1);
+}
+
+// The shell as a flat list of (column, z range) walks, L lanes per cell,
+// consecutive threads on consecutive lanes and x (coalesced):
+//   part 1: every (x, y) column, z in [0, zlo) and then [zhi, nz);
+//   part 2: the columns outside [n, nx-m) x [n, ny-m) -- the n + m full rows
+//           y < n, y >= ny-m, then the n + m face cells of each other row --
+//           for each of the zsegs z segments of [n, nz-m).
+// With a box (zlo = n, zhi = nz-m) the two parts are exactly the cells
+// outside it; a grid too small for a box runs part 1 alone with zlo = zhi =
+// nz (every cell, one walk per column) and zsegs = 0.
+template <int L>
+__global__ void __launch_bounds__(kThreads3d, 4) fdtd3d_h_shell_kernel(const Fdtd3dParams p, int zlo, int zhi,
+                                                                       int zsegs) {
+  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n, m = n > 1 ? n : 1;
+  const long long t = (long long)blockIdx.x * kThreads3d + threadIdx.x;
+  const int lo = (int)(t % L), g = blockIdx.y;
+  long long c = t / L;
+  const long long ncol1 = (long long)nx * ny;
+  int x, y, za0, za1, zb0 = nz, zb1 = nz;   // up to two z ranges per thread
+  if (c < ncol1) {
+    x = (int)(c % nx);
+    y = (int)(c / nx);
+    za0 = 0;
+    za1 = zlo;
+    zb0 = zhi;
+  } else {
+    c -= ncol1;
+    const long long rows_out = (long long)(n + m) * nx;
+    const long long ncol2 = rows_out + (long long)(ny - n - m) * (n + m);
+    const int zseg = (int)(c / ncol2);
+    if (zseg >= zsegs) return;
+    const long long col = c % ncol2;
+    if (col < rows_out) {
+      const int r = (int)(col / nx);
+      x = (int)(col % nx);
+      y = r < n ? r : ny - m + (r - n);
+    } else {
+      const long long k = col - rows_out;
+      const int r = (int)(k / (n + m)), f = (int)(k % (n + m));
+      y = n + r;
+      x = f < n ? f : nx - m + (f - n);
+    }
+    za0 = n + zseg * p.zrows;
+    za1 = min(za0 + p.zrows, nz - m);
+  }
+  // one call site: a single inlined copy of the general path
+#pragma unroll 1
+  for (int w = 0; w < 2; ++w) {
+    const int z0 = w ? zb0 : za0, z1 = w ? zb1 : za1;
+    if (z0 < z1) h_segment<L, true>(p, x, lo, y, g, z0, z1);
   }
 }
 
@@ -268,12 +312,39 @@ __global__ void fdtd3d_src_probe_kernel(const Fdtd3dParams p, int step) {
 
 // ---------------------------------------------------------------------------
 template <int L, int ND, int NL>
-static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s) {
+static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s, const Fdtd3dSide* side) {
   constexpr int CX = kThreads3d / L;
-  dim3 gh((p.nx + CX - 1) / CX, p.ny, p.zsegs * p.groups);
-  fdtd3d_h_kernel<L><<<gh, kThreads3d, 0, s>>>(p);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  const int n = p.n, m = n > 1 ? n : 1;
+  const int bx = p.nx - n - m, by = p.ny - n - m, bz = p.nz - n - m;   // the H box
+  const int zsb = bz > 0 ? (bz + p.zrows - 1) / p.zrows : 0;
+  const bool box = bx > 0 && by > 0 && bz > 0;
+  const bool shell = !p.interior_only || !box;
+  const bool fork = side != nullptr && box && shell;
+  cudaStream_t s2 = fork ? side->stream : s;
+  cudaError_t e;
+  if (fork) {
+    if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s2, side->fork, 0)) != cudaSuccess) return e;
+  }
+  if (shell) {
+    const long long ncol1 = (long long)p.nx * p.ny;
+    const long long ncol2 = box ? (long long)(n + m) * p.nx + (long long)by * (n + m) : 0;
+    const long long threads = L * (ncol1 + ncol2 * (box ? zsb : 0));
+    dim3 gs((unsigned)((threads + kThreads3d - 1) / kThreads3d), p.groups);
+    fdtd3d_h_shell_kernel<L><<<gs, kThreads3d, 0, s2>>>(p, box ? n : p.nz, box ? p.nz - m : p.nz, box ? zsb : 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (box) {
+    dim3 gb((bx + CX - 1) / CX, by, zsb * p.groups);
+    fdtd3d_h_box_kernel<L><<<gb, kThreads3d, 0, s>>>(p, zsb);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (fork) {
+    if ((e = cudaEventRecord(side->join, s2)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, side->join, 0)) != cudaSuccess) return e;
+  }
   const int ni = p.nx - 2 * p.n - 1, nj = p.ny - 2 * p.n - 1;
   if (ni > 0 && nj > 0 && p.zsegs_e > 0) {
     dim3 ge((ni + CX - 1) / CX, nj, p.zsegs_e * p.groups);
@@ -286,23 +357,23 @@ static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s) {
 }
 
 template <int ND, int NL>
-static cudaError_t step_ade(const Fdtd3dParams& p, int step, cudaStream_t s) {
+static cudaError_t step_ade(const Fdtd3dParams& p, int step, cudaStream_t s, const Fdtd3dSide* side) {
   switch (p.L) {
-    case 1: return step_l<1, ND, NL>(p, step, s);
-    case 2: return step_l<2, ND, NL>(p, step, s);
-    case 4: return step_l<4, ND, NL>(p, step, s);
-    default: return step_l<8, ND, NL>(p, step, s);
+    case 1: return step_l<1, ND, NL>(p, step, s, side);
+    case 2: return step_l<2, ND, NL>(p, step, s, side);
+    case 4: return step_l<4, ND, NL>(p, step, s, side);
+    default: return step_l<8, ND, NL>(p, step, s, side);
   }
 }
 
-cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s) {
+cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s, const Fdtd3dSide* side) {
   switch (p.n_debye * 3 + p.n_lorentz) {
-    case 0: return step_ade<0, 0>(p, step, s);
-    case 1: return step_ade<0, 1>(p, step, s);
-    case 2: return step_ade<0, 2>(p, step, s);
-    case 3: return step_ade<1, 0>(p, step, s);
-    case 4: return step_ade<1, 1>(p, step, s);
-    case 6: return step_ade<2, 0>(p, step, s);
+    case 0: return step_ade<0, 0>(p, step, s, side);
+    case 1: return step_ade<0, 1>(p, step, s, side);
+    case 2: return step_ade<0, 2>(p, step, s, side);
+    case 3: return step_ade<1, 0>(p, step, s, side);
+    case 4: return step_ade<1, 1>(p, step, s, side);
+    case 6: return step_ade<2, 0>(p, step, s, side);
     default: return cudaErrorInvalidValue;
   }
 }

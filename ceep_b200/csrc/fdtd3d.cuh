@@ -37,6 +37,15 @@ struct Fdtd3dParams {
   int interior_only;
 };
 
-cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s);
+// A second stream for the shell of the H half-step, with the events that
+// fork it from and join it back to the step's stream.
+struct Fdtd3dSide {
+  cudaStream_t stream;
+  cudaEvent_t fork, join;
+};
+
+// One step on stream s; with `side`, the H shell runs on side->stream beside
+// the H box (both only read E and write disjoint H cells and psi).
+cudaError_t fdtd3d_launch_step(const Fdtd3dParams& p, int step, cudaStream_t s, const Fdtd3dSide* side = nullptr);
 
 }  // namespace ceep

@@ -49,6 +49,7 @@ CASES = [
     (16, 19, 17, 0, 50, 5, 2, True),
     (21, 21, 21, 2, 70, 8, 3, False),
     (20, 17, 23, 3, 40, 17, 4, True),
+    (14, 15, 16, 6, 30, 3, 6, True),     # the smallest grid for n = 6: a 2 x 3 x 4 H box
 ]
 
 
