@@ -274,7 +274,7 @@ def run_ours(args, w):
     bytes_launch = bytes_step * steps_per_launch
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
     traffic = None
-    kname = "fdtd2d_step2" if tblock == 2 else "fdtd2d_step"
+    kname = "fdtd3d_kernels" if w.get("dim", 2) == 3 else ("fdtd2d_step2" if tblock == 2 else "fdtd2d_step")
     tpath = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}.md")
     if os.path.exists(tpath):
         for line in open(tpath):
@@ -311,7 +311,7 @@ def run_ours(args, w):
                      "frac": round(achieved / peak, 3), "traffic": traffic, "peak_source": peak_src,
                      "kernel": (("fdtd2d_step2_kernel (two steps per launch)" if tblock == 2 else
                                  "fdtd2d_step_kernel") if w.get("dim", 2) == 2 else
-                                "fdtd3d step: h + e + source/probe launches"),
+                                "fdtd3d step: h box + h shell (side stream) + e + source/probe launches"),
                      "steps_per_launch": steps_per_launch,
                      "launch_ms": round(launch_ms, 5),
                      "algorithmic_bytes_per_step": bytes_step,
