@@ -39,7 +39,7 @@ class Desc3D(C.Structure):
         ("ex", P), ("ey", P), ("ez", P), ("hx", P), ("hy", P), ("hz", P),
         ("psi_hxy", P), ("psi_hzy", P), ("psi_hyx", P), ("psi_hzx", P), ("psi_hxz", P), ("psi_hyz", P),
         ("j", P), ("j_prev", P), ("coef", P), ("ade_coef", P), ("cpml_b", P), ("cpml_c", P),
-        ("src_xyz", P), ("prb_xyz", P), ("waveform", P), ("probes", P), ("z_rows", I32),
+        ("src_xyz", P), ("prb_xyz", P), ("waveform", P), ("probes", P), ("z_rows", I32), ("shell_z_rows", I32),
     ]
 
 

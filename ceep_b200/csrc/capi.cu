@@ -272,6 +272,7 @@ extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
   p.nprobe = d->nprobe; p.nsteps = d->nsteps;
   p.n_debye = d->n_debye; p.n_lorentz = d->n_lorentz;
   p.zrows = d->z_rows > 0 ? d->z_rows : 16;
+  p.zrows_shell = d->shell_z_rows > 0 ? d->shell_z_rows : 4;
   p.zsegs = (d->nz + p.zrows - 1) / p.zrows;
   const int nzi = d->nz - 2 * n - 1;
   p.zsegs_e = nzi > 0 ? (nzi + p.zrows - 1) / p.zrows : 0;

@@ -37,7 +37,10 @@ constexpr int kThreads3d = 128;
 // ---------------------------------------------------------------------------
 // GEN = false for blocks whose cells all lie inside the three H interior
 // boxes and off every CPML face: the region tests and face code fold away.
-template <int L, bool GEN>
+// FACES (bits 1, 2, 4 = x, y, z) selects the CPML face code compiled in:
+// a cell outside the box lies on one face (a slab) or on several (an edge or
+// corner); the slabs' launches carry only their own face's code.
+template <int L, bool GEN, int FACES = 7>
 __device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, int y, int g, int z0, int z1) {
   const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n;
   const size_t gs = (size_t)g * p.gs_field;
@@ -81,7 +84,7 @@ __device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, 
       Hz = cf.x * Hz + cf.y * ((exyp - exc) * f4(inv) - (eyxp - eyc) * f4(inv));
     if (GEN && n > 0) {
       // x faces (:398-460)
-      if (xf >= 0) {
+      if ((FACES & 1) && xf >= 0) {
         const bool lof = x < n;
         const float4 ezn = lof ? ezxp : ld4(ez + at - sx);
         const float4 eyn = lof ? eyxp : ld4(ey + at - sx);
@@ -96,7 +99,7 @@ __device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, 
         if (y < ny - 1) Hz = cf.x * Hz + cf.y * pb;
       }
       // y faces (:462-523)
-      if (yf >= 0) {
+      if ((FACES & 2) && yf >= 0) {
         const bool lof = y < n;
         const float4 ezn = lof ? ezyp : ld4(ez + at - sy);
         const float4 exn = lof ? exyp : ld4(ex + at - sy);
@@ -112,7 +115,7 @@ __device__ __forceinline__ void h_segment(const Fdtd3dParams& p, int x, int lo, 
       }
       // z faces (:525-586)
       const int zf = z < n ? z : (z >= nz - n ? n + (z - (nz - n)) : -1);
-      if (zf >= 0) {
+      if ((FACES & 4) && zf >= 0) {
         const bool lof = z < n;
         const int zc = lof ? z : nz - 1 - z;
         const float4 dey = lof ? (eyu - eyc) * f4(inv) : (eyc - eym) * f4(inv);
@@ -153,56 +156,87 @@ __global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_h_box_kernel(const Fdtd3
   h_segment<L, false>(p, x, lo, y, g, z0, z1);
 }
 
-// The shell as a flat list of (column, z range) walks, L lanes per cell,
-// consecutive threads on consecutive lanes and x (coalesced):
-//   part 1: every (x, y) column, z in [0, zlo) and then [zhi, nz);
-//   part 2: the columns outside [n, nx-m) x [n, ny-m) -- the n + m full rows
-//           y < n, y >= ny-m, then the n + m face cells of each other row --
-//           for each of the zsegs z segments of [n, nz-m).
-// With a box (zlo = n, zhi = nz-m) the two parts are exactly the cells
-// outside it; a grid too small for a box runs part 1 alone with zlo = zhi =
-// nz (every cell, one walk per column) and zsegs = 0.
-template <int L>
-__global__ void __launch_bounds__(kThreads3d, 4) fdtd3d_h_shell_kernel(const Fdtd3dParams p, int zlo, int zhi,
-                                                                       int zsegs) {
-  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n, m = n > 1 ? n : 1;
+// The shell as lists of cell boxes [x0,x1) x [y0,y1) x [z0,z1), one launch
+// per kind of cell: the z slabs, x slabs and y slabs next to the box (cells
+// on that one CPML face: FACES = 4, 1, 2) and the edges and corners (every
+// face, FACES = 7).  A thread walks at most zr cells of one (x, y) column;
+// consecutive threads take consecutive lanes and x (coalesced).
+struct ShellBoxes {
+  int count;
+  int b[12][6];   // x0, x1, y0, y1, z0, z1
+};
+
+template <int L, int FACES>
+__global__ void __launch_bounds__(kThreads3d, FACES == 7 ? 4 : 6) fdtd3d_h_shell_kernel(const Fdtd3dParams p,
+                                                                                          const ShellBoxes sb, int zr) {
   const long long t = (long long)blockIdx.x * kThreads3d + threadIdx.x;
   const int lo = (int)(t % L), g = blockIdx.y;
   long long c = t / L;
-  const long long ncol1 = (long long)nx * ny;
-  int x, y, za0, za1, zb0 = nz, zb1 = nz;   // up to two z ranges per thread
-  if (c < ncol1) {
-    x = (int)(c % nx);
-    y = (int)(c / nx);
-    za0 = 0;
-    za1 = zlo;
-    zb0 = zhi;
-  } else {
-    c -= ncol1;
-    const long long rows_out = (long long)(n + m) * nx;
-    const long long ncol2 = rows_out + (long long)(ny - n - m) * (n + m);
-    const int zseg = (int)(c / ncol2);
-    if (zseg >= zsegs) return;
-    const long long col = c % ncol2;
-    if (col < rows_out) {
-      const int r = (int)(col / nx);
-      x = (int)(col % nx);
-      y = r < n ? r : ny - m + (r - n);
-    } else {
-      const long long k = col - rows_out;
-      const int r = (int)(k / (n + m)), f = (int)(k % (n + m));
-      y = n + r;
-      x = f < n ? f : nx - m + (f - n);
+  for (int i = 0; i < sb.count; ++i) {
+    const int* b = sb.b[i];
+    const int w = b[1] - b[0], cols = w * (b[3] - b[2]);
+    const long long items = (long long)cols * ((b[5] - b[4] + zr - 1) / zr);
+    if (c < items) {
+      const int seg = (int)(c / cols), col = (int)(c % cols);
+      const int z0 = b[4] + seg * zr;
+      h_segment<L, true, FACES>(p, b[0] + col % w, lo, b[2] + col / w, g, z0, min(z0 + zr, b[5]));
+      return;
     }
-    za0 = n + zseg * p.zrows;
-    za1 = min(za0 + p.zrows, nz - m);
+    c -= items;
   }
-  // one call site: a single inlined copy of the general path
-#pragma unroll 1
-  for (int w = 0; w < 2; ++w) {
-    const int z0 = w ? zb0 : za0, z1 = w ? zb1 : za1;
-    if (z0 < z1) h_segment<L, true>(p, x, lo, y, g, z0, z1);
+}
+
+static void add_box(ShellBoxes& sb, int x0, int x1, int y0, int y1, int z0, int z1) {
+  if (x0 < x1 && y0 < y1 && z0 < z1) {
+    int* b = sb.b[sb.count++];
+    b[0] = x0; b[1] = x1; b[2] = y0; b[3] = y1; b[4] = z0; b[5] = z1;
   }
+}
+
+static long long shell_items(const ShellBoxes& sb, int zr) {
+  long long n = 0;
+  for (int i = 0; i < sb.count; ++i) {
+    const int* b = sb.b[i];
+    n += (long long)(b[1] - b[0]) * (b[3] - b[2]) * ((b[5] - b[4] + zr - 1) / zr);
+  }
+  return n;
+}
+
+template <int L, int FACES>
+static cudaError_t launch_shell(const Fdtd3dParams& p, const ShellBoxes& sb, cudaStream_t s) {
+  const long long items = shell_items(sb, p.zrows_shell);
+  if (items == 0) return cudaSuccess;
+  dim3 gs((unsigned)((L * items + kThreads3d - 1) / kThreads3d), p.groups);
+  fdtd3d_h_shell_kernel<L, FACES><<<gs, kThreads3d, 0, s>>>(p, sb, p.zrows_shell);
+  return cudaGetLastError();
+}
+
+// The cells outside the box [n, nx-m) x [n, ny-m) x [n, nz-m) by kind; with
+// no box (a grid too small for one) every cell goes to the general list.
+template <int L>
+static cudaError_t launch_shells(const Fdtd3dParams& p, bool box, cudaStream_t s) {
+  const int nx = p.nx, ny = p.ny, nz = p.nz, n = p.n, m = n > 1 ? n : 1;
+  ShellBoxes fz{}, fx{}, fy{}, all{};
+  if (!box) {
+    add_box(all, 0, nx, 0, ny, 0, nz);
+    return launch_shell<L, 7>(p, all, s);
+  }
+  const int xs[2][2] = {{0, n}, {nx - m, nx}}, ys[2][2] = {{0, n}, {ny - m, ny}}, zs[2][2] = {{0, n}, {nz - m, nz}};
+  for (int k = 0; k < 2; ++k) {
+    add_box(fz, n, nx - m, n, ny - m, zs[k][0], zs[k][1]);          // z slabs
+    add_box(fx, xs[k][0], xs[k][1], n, ny - m, n, nz - m);          // x slabs
+    add_box(fy, n, nx - m, ys[k][0], ys[k][1], n, nz - m);          // y slabs
+    for (int q = 0; q < 2; ++q) add_box(all, xs[k][0], xs[k][1], ys[q][0], ys[q][1], n, nz - m);  // z edges
+    add_box(all, 0, nx, 0, n, zs[k][0], zs[k][1]);                    // the z slabs' rims
+    add_box(all, 0, nx, ny - m, ny, zs[k][0], zs[k][1]);
+    add_box(all, 0, n, n, ny - m, zs[k][0], zs[k][1]);
+    add_box(all, nx - m, nx, n, ny - m, zs[k][0], zs[k][1]);
+  }
+  cudaError_t e;
+  if ((e = launch_shell<L, 7>(p, all, s)) != cudaSuccess) return e;
+  if ((e = launch_shell<L, 4>(p, fz, s)) != cudaSuccess) return e;
+  if ((e = launch_shell<L, 1>(p, fx, s)) != cudaSuccess) return e;
+  return launch_shell<L, 2>(p, fy, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -326,15 +360,7 @@ static cudaError_t step_l(const Fdtd3dParams& p, int step, cudaStream_t s, const
     if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s2, side->fork, 0)) != cudaSuccess) return e;
   }
-  if (shell) {
-    const long long ncol1 = (long long)p.nx * p.ny;
-    const long long ncol2 = box ? (long long)(n + m) * p.nx + (long long)by * (n + m) : 0;
-    const long long threads = L * (ncol1 + ncol2 * (box ? zsb : 0));
-    dim3 gs((unsigned)((threads + kThreads3d - 1) / kThreads3d), p.groups);
-    fdtd3d_h_shell_kernel<L><<<gs, kThreads3d, 0, s2>>>(p, box ? n : p.nz, box ? p.nz - m : p.nz, box ? zsb : 0);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
+  if (shell && (e = launch_shells<L>(p, box, s2)) != cudaSuccess) return e;
   if (box) {
     dim3 gb((bx + CX - 1) / CX, by, zsb * p.groups);
     fdtd3d_h_box_kernel<L><<<gb, kThreads3d, 0, s>>>(p, zsb);

@@ -11,6 +11,7 @@ struct Fdtd3dParams {
   int nprobe, nsteps;
   int n_debye, n_lorentz;
   int zrows, zsegs, zsegs_e;   // z segment length; segments for the H and E grids
+  int zrows_shell;              // z walk length of the H shell launch
   float inv_dx, dt, inv_dt;
   long long gs_field, gs_px, gs_py, gs_pz, gs_j, gs_jp;  // per-group strides (float4)
   float4 *ex, *ey, *ez, *hx, *hy, *hz;

@@ -30,6 +30,7 @@ class BatchedFDTD3D:
                  source_positions: List[Tuple[int, int, int]], probe_positions: List[Tuple[int, int, int]],
                  frequency: float, delay_factor: float = 5.0, *, waveform: Optional[np.ndarray] = None,
                  frequencies: Optional[Sequence[float]] = None, device: str = "cuda", z_rows: int = 0,
+                 shell_z_rows: int = 0,
                  use_graph: bool = True):
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dx = self.dy = self.dz = float(dx)
@@ -52,6 +53,7 @@ class BatchedFDTD3D:
         self.frequencies = None if frequencies is None else np.asarray(frequencies, np.float64)
         self.device = torch.device(device)
         self.z_rows = int(z_rows)
+        self.shell_z_rows = int(shell_z_rows)
         self.use_graph = bool(use_graph)
         self._built = False
         self._plan = None
@@ -179,6 +181,7 @@ class BatchedFDTD3D:
         d.src_xyz, d.prb_xyz = _ptr(self._src), _ptr(self._prb)
         d.waveform, d.probes = _ptr(self.waveform), _ptr(self.probe_data)
         d.z_rows = self.z_rows
+        d.shell_z_rows = self.shell_z_rows
         self._desc = d
         plan = C.c_void_p()
         check(lib().ceep3d_plan_create(C.byref(d), C.byref(plan)), "ceep3d_plan_create")

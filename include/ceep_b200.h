@@ -207,8 +207,10 @@ int ceep2d_adjoint_rows(const ceep2d_adjoint* adj);
  * (_update_h_fields :753-818, _apply_h_cpml_x/y/z :398-586,
  *  _update_e_fields :820-884, low-face zeroing :936-944, source :949-951,
  *  probes :956-958), with optional Debye/Lorentz currents on each E component.
- * Three launches per step: H half-step, E half-step, source/probe epilogue;
- * all state is updated in place.
+ * Per step: the H half-step as two launches over disjoint cells (the box
+ * inside every interior box and off every CPML face, and the shell around it
+ * on a side stream of the plan), the E half-step, and the source/probe
+ * epilogue; all state is updated in place.
  * ---------------------------------------------------------------------- */
 typedef struct ceep3d_desc {
   int32_t nx, ny, nz;
@@ -233,6 +235,7 @@ typedef struct ceep3d_desc {
   const float* waveform;   /* (nsteps) */
   float* probes;           /* (ntx, nprobe, nsteps) */
   int32_t z_rows;          /* z segment per thread, 0 = default              */
+  int32_t shell_z_rows;    /* z walk of the H shell launch, 0 = default      */
 } ceep3d_desc;
 
 typedef struct ceep3d_plan ceep3d_plan;
