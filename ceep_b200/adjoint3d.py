@@ -42,6 +42,22 @@ class _AdjDesc3D(C.Structure):
     _fields_ = [("mu", P), ("nu", P), ("lj", P), ("grad", P), ("probe_grad", P)]
 
 
+def save_slot_shape(solver):
+    """One slot of a segment buffer: the three E components on the interior
+    box [n+1, N-n)^3, the only cells the E half-step updates,
+    (3, G, nzi, nyi, nxi, W)."""
+    G, nz, ny, nx, W = solver._f["ex"].shape
+    n = solver.cpml_thickness
+    return (3, G, nz - 2 * n - 1, ny - 2 * n - 1, nx - 2 * n - 1, W)
+
+
+def interior_e(solver, field):
+    """The interior-box view of one (G, nz, ny, nx, W) E component."""
+    n = solver.cpml_thickness
+    _, nz, ny, nx, _ = field.shape
+    return field[:, n + 1:nz - n, n + 1:ny - n, n + 1:nx - n]
+
+
 class Adjoint3D:
     """Gradient driver for one ``BatchedFDTD3D`` (Debye poles only, CPML >= 2)."""
 
@@ -95,8 +111,7 @@ class Adjoint3D:
                 t.copy_(c)
 
     def _segment_shape(self):
-        s = self.s
-        return (min(self.K, s.total_steps) + 1, 3) + tuple(s._f["ex"].shape)
+        return (min(self.K, self.s.total_steps) + 1,) + save_slot_shape(self.s)
 
     def _buffers(self, count):
         """`count` segment buffers, allocated once: the save graphs are keyed
@@ -110,7 +125,7 @@ class Adjoint3D:
         seg = self._segs[buf]
         stream = torch.cuda.current_stream(s.device)
         for c, k in enumerate(("ex", "ey", "ez")):
-            seg[0, c].copy_(s._f[k])
+            seg[0, c].copy_(interior_e(s, s._f[k]))
         check(lib().ceep3d_plan_run_save(s._plan, a, b - a, C.c_void_p(stream.cuda_stream), int(s.use_graph),
                                          seg.data_ptr(), a, int(interior_only)), "ceep3d_plan_run_save")
 

@@ -134,8 +134,8 @@ __global__ void __launch_bounds__(kAdj3dThreads, 4)
   const size_t goff = (size_t)g * p.gs_field;
   float4* mu = a.mu + goff;
   const float4* __restrict__ nu = a.nu + goff;
-  const float4* __restrict__ en = e_n + goff;
-  const float4* __restrict__ e1 = e_np1 + goff;
+  // the saved slots cover the interior box only: (3, G, nzi, nyi, nxi, L)
+  const size_t scs = (size_t)p.save_cs;
   float4* lj = a.lj + (size_t)g * p.gs_j;
   const float4* coef = reinterpret_cast<const float4*>(p.coef);
   const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
@@ -157,12 +157,16 @@ __global__ void __launch_bounds__(kAdj3dThreads, 4)
   }
   const int nxi = nx - 2 * n - 1, nyi = ny - 2 * n - 1;
   double* gw = a.g + (size_t)g * KS * a.icells + ((size_t)(z0 - n - 1) * nyi + (y - n - 1)) * nxi + (x - n - 1);
+  const size_t s_at0 = (size_t)g * a.icells * L + (((size_t)(z0 - n - 1) * nyi + (y - n - 1)) * nxi + (x - n - 1)) * L + lo;
+  const float4* __restrict__ en = e_n + s_at0;
+  const float4* __restrict__ e1 = e_np1 + s_at0;
+  const size_t s_sz = (size_t)nyi * nxi * L;
   size_t at = (size_t)z0 * sz + (size_t)y * sy + (size_t)x * sx + lo;
   size_t cc = (size_t)z0 * cz + (size_t)y * nx + x;
   // db nu of the plane below (x and y components)
   const float dbm = __ldg(coef + cc - cz).y;
   float4 nxm = dbm * ld4(nu + at - sz), nym = dbm * ld4(nu + cs + at - sz);
-  for (int z = z0; z < z1; ++z, at += sz, cc += cz, gw += (size_t)nyi * nxi) {
+  for (int z = z0; z < z1; ++z, at += sz, cc += cz, gw += (size_t)nyi * nxi, en += s_sz, e1 += s_sz) {
     const float4 cf = __ldg(coef + cc);
     const float4 Nx = cf.y * ld4(nu + at), Ny = cf.y * ld4(nu + cs + at), Nz = cf.y * ld4(nu + 2 * cs + at);
     const float dby = __ldg(coef + cc - nx).y;
@@ -181,8 +185,8 @@ __global__ void __launch_bounds__(kAdj3dThreads, 4)
     for (int c = 0; c < 3; ++c) {
       const size_t ac = c * cs + at;
       const float4 m = mu[ac];
-      float4 E0 = ld4(en + ac);
-      const float4 E1 = ld4(e1 + ac);
+      float4 E0 = ld4(en + c * scs);
+      const float4 E1 = ld4(e1 + c * scs);
       if (c == 2) {
 #pragma unroll
         for (int k = 0; k < 4; ++k)

@@ -295,7 +295,7 @@ extern "C" int ceep3d_plan_create(const ceep3d_desc* d, ceep3d_plan** out) {
   p.coef = d->coef; p.ade_coef = d->ade_coef; p.cpml_b = d->cpml_b; p.cpml_c = d->cpml_c;
   p.src_xyz = d->src_xyz; p.prb_xyz = d->prb_xyz; p.waveform = d->waveform; p.probes = d->probes;
   p.save_e = nullptr;
-  p.save_cs = p.groups * p.gs_field;
+  p.save_cs = p.groups * (long long)(d->nx - 2 * n - 1) * (d->ny - 2 * n - 1) * (d->nz - 2 * n - 1) * L;
   p.save_base = 0;
   p.interior_only = 0;
   // the H shell's stream at the highest priority, so that its blocks (few,
@@ -509,7 +509,7 @@ extern "C" int ceep3d_adjoint_run(ceep3d_adjoint* ad, int64_t step_hi, int64_t n
     return fail(CEEP_ERR_INVALID, "ceep3d_adjoint_run: steps [%lld, %lld) with segment base %lld",
                 (long long)(step_hi - nsteps), (long long)step_hi, (long long)seg_base);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t slot = 3 * (size_t)a.cs;
+  const size_t slot = 3 * (size_t)a.f.save_cs;   // interior E box per component
   const float4* E = reinterpret_cast<const float4*>(seg_e);
   for (int64_t n = step_hi - 1; n >= step_hi - nsteps; --n) {
     const size_t k = (size_t)(n - seg_base);

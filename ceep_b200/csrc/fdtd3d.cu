@@ -268,7 +268,13 @@ __global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dPar
   const float inv = p.inv_dx;
   size_t at = (size_t)z0 * sz + (size_t)y * sy + (size_t)x * sx + lo;
   float4 hxm = ld4(hx + at - sz), hym = ld4(hy + at - sz);
-  float4* save = p.save_e ? p.save_e + (size_t)(step + 1 - p.save_base) * 3 * p.save_cs + gs : nullptr;
+  // the save slot covers the interior box only: (G, nzi, nyi, nxi, L)
+  const int nxi = nx - 2 * n - 1, nyi = ny - 2 * n - 1, nzi = nz - 2 * n - 1;
+  float4* save = p.save_e ? p.save_e + (size_t)(step + 1 - p.save_base) * 3 * p.save_cs +
+                                (size_t)g * nzi * nyi * nxi * L +
+                                ((size_t)(z0 - n - 1) * nyi + (y - n - 1)) * nxi * L + (size_t)(x - n - 1) * L + lo
+                          : nullptr;
+  const size_t save_sz = (size_t)nyi * nxi * L;
   for (int z = z0; z < z1; ++z, at += sz) {
     const float4 Hx = ld4(hx + at), Hy = ld4(hy + at), Hz = ld4(hz + at);
     const float4 hzy = ld4(hz + at - sy), hzx = ld4(hz + at - sx);
@@ -312,8 +318,9 @@ __global__ void __launch_bounds__(kThreads3d, 8) fdtd3d_e_kernel(const Fdtd3dPar
         }
       }
       *E[c] = e;
-      if (save) save[c * p.save_cs + at] = e;
+      if (save) save[c * p.save_cs] = e;
     }
+    if (save) save += save_sz;
     hxm = Hx;
     hym = Hy;
   }

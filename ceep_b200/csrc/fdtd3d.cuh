@@ -29,7 +29,8 @@ struct Fdtd3dParams {
   float* probes;
   // optional: the E half-step also stores each updated component (before the
   // source) of step s into slot s + 1 - save_base of save_e, a
-  // (slots, 3, G, nz, ny, nx, L) array; save_cs = G * gs_field
+  // (slots, 3, G, nzi, nyi, nxi, L) array over the interior E box
+  // [n+1, N-n)^3 (the only cells it updates); save_cs = G * interior cells * L
   float4* save_e;
   long long save_cs;
   int save_base;

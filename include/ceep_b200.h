@@ -243,8 +243,9 @@ int ceep3d_plan_create(const ceep3d_desc* desc, ceep3d_plan** out);
 int ceep3d_plan_run(ceep3d_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
 /* As ceep3d_plan_run, and also store the three E components of every step n,
  * as the E half-step leaves them (before the source), into slot
- * n + 1 - save_base of save_e, a (slots, 3, G, nz, ny, nx, .) float array;
- * only the interior E box is written.  With interior_only the H half-step
+ * n + 1 - save_base of save_e, a (slots, 3, G, nzi, nyi, nxi, .) float array
+ * over the interior E box [n+1, N-n)^3 (nxi = nx - 2n - 1 and so on), the
+ * only cells the E half-step updates.  With interior_only the H half-step
  * skips the CPML shell (H outside [n, N-n)^3 and the psi arrays stay as they
  * were): E, the H box, the currents and the probes come out bit-identical,
  * since nothing in the shell reaches them, for a fraction of the traffic. */
@@ -330,7 +331,7 @@ typedef struct ceep3d_adjoint ceep3d_adjoint;
 int ceep3d_adjoint_create(const ceep3d_plan* plan, const ceep3d_adjoint_desc* desc, ceep3d_adjoint** out);
 /* Adjoint steps step_hi-1 down to step_hi-nsteps; seg_e holds the slots that
  * ceep3d_plan_run_save wrote with save_base = seg_base, slot 0 being a copy of
- * the E state at step seg_base (source included). */
+ * the interior E box at step seg_base (source included). */
 int ceep3d_adjoint_run(ceep3d_adjoint* adj, int64_t step_hi, int64_t nsteps, const float* seg_e,
                        int64_t seg_base, void* stream);
 int32_t ceep3d_adjoint_grad_slots(const ceep3d_adjoint* adj);

@@ -134,6 +134,7 @@ def test_interior_only_save_pass_is_bit_identical(cuda_device):
     import ctypes as C
     from ceep_b200 import BatchedFDTD3D
     from ceep_b200._lib import check, lib
+    from ceep_b200.adjoint3d import interior_e, save_slot_shape
     eps, sig, de, tau, m, ring = _case(30, 28, 26, 9)
     out = []
     for interior_only in (0, 1):
@@ -141,7 +142,7 @@ def test_interior_only_save_pass_is_bit_identical(cuda_device):
         s._eps_r[:], s._sigma_e[:] = eps, sig
         s.set_dispersion(debye=[(de, tau)])
         s.advance(0, 20)
-        seg = torch.zeros((41, 3) + tuple(s._f["ex"].shape), dtype=torch.float32, device="cuda")
+        seg = torch.zeros((41,) + save_slot_shape(s), dtype=torch.float32, device="cuda")
         st = torch.cuda.current_stream()
         check(lib().ceep3d_plan_run_save(s._plan, 20, 40, C.c_void_p(st.cuda_stream), 1, seg.data_ptr(), 20,
                                          interior_only), "ceep3d_plan_run_save")
@@ -155,6 +156,11 @@ def test_interior_only_save_pass_is_bit_identical(cuda_device):
         assert torch.equal(fa[k], fb[k])
     for k in ("hx", "hy", "hz"):
         assert torch.equal(fa[k][box], fb[k][box])
+    # the last slot is the interior E of the last step before its source: it
+    # differs from the final state at the three source cells only
+    for c, k in enumerate(("ex", "ey", "ez")):
+        d = (sa[40, c] != interior_e(s, fa[k])).sum().item()
+        assert d <= (3 if k == "ez" else 0), (k, d)
 
 
 def test_adjoint3d_overlapped_recompute_gives_the_same_gradient(cuda_device):
