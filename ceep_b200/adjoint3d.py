@@ -101,13 +101,27 @@ class Adjoint3D:
             ts.append(s._j)
         return ts
 
+    def _ckpt_views(self):
+        """What an interior-only recompute reads: E everywhere (its cells
+        outside the interior are read by the H box and may hold a source), H
+        on the box [n, N-n)^3 and the currents on the interior [n+1, N-n)^3;
+        not the psi arrays nor H in the shell, which it never touches."""
+        s = self.s
+        n = s.cpml_thickness
+        _, nz, ny, nx, _ = s._f["ex"].shape
+        box = (slice(None), slice(n, nz - n), slice(n, ny - n), slice(n, nx - n))
+        views = [s._f[k] for k in ("ex", "ey", "ez")] + [s._f[k][box] for k in ("hx", "hy", "hz")]
+        if s._j is not None:
+            views.append(s._j[:, :, :, n + 1:nz - n, n + 1:ny - n, n + 1:nx - n])
+        return views
+
     def _restore(self, a):
         ck = self._ckpt[a]
         if ck is None:                 # step 0: the zero state
             for t in self._state_tensors():
                 t.zero_()
         else:
-            for t, c in zip(self._state_tensors(), ck):
+            for t, c in zip(self._ckpt_views(), ck):
                 t.copy_(c)
 
     def _segment_shape(self):
@@ -141,7 +155,7 @@ class Adjoint3D:
         starts = list(range(0, T, K))
         for a in starts:
             b = min(a + K, T)
-            self._ckpt[a] = None if a == 0 else [t.clone() for t in self._state_tensors()]
+            self._ckpt[a] = None if a == 0 else [t.clone() for t in self._ckpt_views()]
             if a == starts[-1]:
                 self._run_save(a, b, 0, interior_only=False)
                 self._seg_ready = a
