@@ -994,15 +994,16 @@ def run_profile_adjoint(args):
 
 
 def run_profile_adjoint3d(args):
-    """One gradient of a 128^3, 8-TX Debye head over --profile steps (one
-    checkpoint segment, so no recompute), launched without graphs."""
+    """One gradient of a 192^3 (128^3 with --small), 8-TX Debye head over
+    --profile steps (one checkpoint segment, so no recompute), launched
+    without graphs."""
     import torch
     from ceep_b200 import BatchedFDTD3D
     from ceep_b200.adjoint3d import Adjoint3D, probes_with_grad_3d
     from ceep_b200.phantoms import HeadPhantom3D, ring_positions
     dev = torch.device("cuda", 0)
-    T, nx = args.profile, 128
-    pos = [(x, y, nx // 2) for x, y in ring_positions(8, (nx // 2, nx // 2), 50)]
+    T, nx = args.profile, (128 if args.small else 192)
+    pos = [(x, y, nx // 2) for x, y in ring_positions(8, (nx // 2, nx // 2), 50 if args.small else 75)]
     sc = nx / 192.0
     ph = HeadPhantom3D(nx=nx, ny=nx, nz=nx, dx=1e-3, seed=7, semi_axes=(0.070 * sc, 0.056 * sc, 0.060 * sc))
     s = BatchedFDTD3D(nx, nx, nx, 1e-3, T, 10, pos, pos, 2e9, device=str(dev), use_graph=False)
@@ -1052,7 +1053,8 @@ def main():
                     choices=list(WORKLOADS) + ["adjoint400", "adjoint192", "pack256", "single4096"])
     ap.add_argument("--pack-count", type=int, default=256)
     ap.add_argument("--pack-sample", type=int, default=32)
-    ap.add_argument("--small", action="store_true", help="with --profile: a smaller 3D grid")
+    ap.add_argument("--small", action="store_true", help="a smaller grid (--profile of the 3D gradient: 128^3; "
+                                                         "single4096: 1024^2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--temporal-block", type=int, default=2, choices=(1, 2),
                     help="2D steps per kernel launch (2 = temporal block of two)")
