@@ -409,6 +409,83 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
   }
 }
 
+// The TMz interior walk with two columns per lane: lane l holds columns
+// c, c+1 with c = j0 - 2 + 2l even, so every field row is read and written
+// as float2 and every coefficient pair as float4 (twice the bytes in flight
+// per warp of the one-column walk, half the load instructions).  Strips are
+// 62 columns wide (lanes 1..31 own them; lane 0 forms the H of column j0-1
+// for its neighbour's E update, and writes nothing).  Needs an even ny (the
+// float2 rows stay aligned) and a strip start j0 on an even column; the
+// cells it owns and their halo lie in the CPML- and edge-free interior, so
+// the region tests of the general walk fold away.  Same arithmetic, in the
+// same order, as the one-column walk.
+__global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tmz_pair_kernel(const Single2dParams p, int step,
+                                                                                 int r, int bx0, int by0) {
+  const int w = r ^ 1;
+  const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
+  const int j0 = 31 * bx0 + 62 * blockIdx.x;
+  const int c = j0 - 2 + 2 * lane;
+  constexpr int rows = kBlockRows / kWarpsInterior;
+  const int i0 = (by0 + blockIdx.y) * kBlockRows + threadIdx.y * rows;
+  if (i0 >= nx) return;  // whole warp
+  const int i1 = min(i0 + rows, nx);
+  const bool own = lane > 0;
+  const float* ez_r = p.f[0][r];
+  const float2* ez2 = reinterpret_cast<const float2*>(ez_r);
+  const float2* hx2 = reinterpret_cast<const float2*>(p.f[1][r]);
+  const float2* hy2 = reinterpret_cast<const float2*>(p.f[2][r]);
+  const float4* ch4 = reinterpret_cast<const float4*>(p.ch);  // (da, db) of c, then of c+1
+  const float4* ce4 = reinterpret_cast<const float4*>(p.ce);  // (ca, cb) of c, then of c+1
+  float2* ez_w = reinterpret_cast<float2*>(p.f[0][w]);
+  float2* hx_w = reinterpret_cast<float2*>(p.f[1][w]);
+  float2* hy_w = reinterpret_cast<float2*>(p.f[2][w]);
+  const size_t row2 = (size_t)ny / 2;
+  float2 hy_prev = make_float2(tmz_hy_at<false>(p, r, i0 - 1, c), tmz_hy_at<false>(p, r, i0 - 1, c + 1));
+  size_t k = ((size_t)i0 * ny + c) / 2;
+  float2 ez_c = __ldg(ez2 + k);
+  float2 ez_n = __ldg(ez2 + k + row2);
+  float2 hx_c = __ldg(hx2 + k), hy_c = __ldg(hy2 + k);
+  float4 d_c = __ldg(ch4 + k), e_c = __ldg(ce4 + k);
+  const float z2 = 0.f;
+  for (int i = i0; i < i1; ++i, k += row2) {
+    const bool more = i + 1 < i1;
+    const float2 ez_nn = more && i + 2 < nx ? __ldg(ez2 + k + 2 * row2) : make_float2(z2, z2);
+    const float2 hx_n = more ? __ldg(hx2 + k + row2) : make_float2(z2, z2);
+    const float2 hy_n = more ? __ldg(hy2 + k + row2) : make_float2(z2, z2);
+    const float4 d_n = more ? __ldg(ch4 + k + row2) : make_float4(z2, z2, z2, z2);
+    const float4 e_n = more ? __ldg(ce4 + k + row2) : make_float4(z2, z2, z2, z2);
+    float ez_rt = __shfl_down_sync(0xffffffffu, ez_c.x, 1);
+    if (lane == 31) ez_rt = __ldg(ez_r + (size_t)i * ny + c + 2);
+    float2 hx, hy;
+    hx.x = d_c.x * hx_c.x - (d_c.y * p.inv_dy) * (ez_c.y - ez_c.x);
+    hx.y = d_c.z * hx_c.y - (d_c.w * p.inv_dy) * (ez_rt - ez_c.y);
+    hy.x = d_c.x * hy_c.x + (d_c.y * p.inv_dx) * (ez_n.x - ez_c.x);
+    hy.y = d_c.z * hy_c.y + (d_c.w * p.inv_dx) * (ez_n.y - ez_c.y);
+    const float hx_l = __shfl_up_sync(0xffffffffu, hx.y, 1);
+    if (own) {
+      hx_w[k] = hx;
+      hy_w[k] = hy;
+      float2 e;
+      e.x = e_c.x * ez_c.x + e_c.y * ((hy.x - hy_prev.x) * p.inv_dx - (hx.x - hx_l) * p.inv_dy);
+      e.y = e_c.z * ez_c.y + e_c.w * ((hy.y - hy_prev.y) * p.inv_dx - (hx.y - hx.x) * p.inv_dy);
+      for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s) {  // fdtd_2d.py:245-260
+        if (__ldg(p.src + 3 * s + 2) != 0) continue;
+        const int sc = __ldg(p.src + 3 * s + 1);
+        if (sc == c) e.x += __ldg(p.waveform + (size_t)s * p.nsteps + step);
+        else if (sc == c + 1) e.y += __ldg(p.waveform + (size_t)s * p.nsteps + step);
+      }
+      ez_w[k] = e;
+    }
+    hy_prev = hy;
+    ez_c = ez_n;
+    ez_n = ez_nn;
+    hx_c = hx_n;
+    hy_c = hy_n;
+    d_c = d_n;
+    e_c = e_n;
+  }
+}
+
 // TEz Hz sources, in list order (fdtd_2d.py:253-254).
 __global__ void single2d_src_h_kernel(const Single2dParams p, int step, int cur) {
   if (threadIdx.x != 0) return;
@@ -480,6 +557,16 @@ template <int MODE, bool CPML>
 static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s, cudaStream_t s2,
                           cudaEvent_t fork, cudaEvent_t join) {
   BlockMap m = block_map(p);
+  // TMz with an even ny: the interior runs the two-column walk over pairs of
+  // 31-column blocks starting on an even block (an even column); a block
+  // left over at either end joins the frame
+  const bool pair = MODE == 0 && p.ny % 2 == 0;
+  if (pair && m.bx_hi > m.bx_lo) {
+    m.bx_lo += m.bx_lo & 1;
+    const int np = (m.bx_hi - m.bx_lo) / 2;
+    if (np > 0) m.bx_hi = m.bx_lo + 2 * np;
+    else m.bx_lo = m.bx_hi = m.by_lo = m.by_hi = 0;
+  }
   const int interior = (m.bx_hi - m.bx_lo) * (m.by_hi - m.by_lo);
   const int rest = m.gx * m.gy - interior;
   const bool two = interior > 0 && rest > 0;
@@ -495,8 +582,12 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (interior > 0) {
-    single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0, s>>>(
-        p, step, r, m);
+    if (pair)
+      single2d_tmz_pair_kernel<<<dim3((m.bx_hi - m.bx_lo) / 2, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0, s>>>(
+          p, step, r, m.bx_lo, m.by_lo);
+    else
+      single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0,
+                                          s>>>(p, step, r, m);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (two) {

@@ -131,3 +131,49 @@ def test_dft_monitor_matches_oracle_series(cuda_device):
     ref = (np.cos(ph) - 1j * np.sin(ph)) @ ser.T * float(g("dt"))         # (F, cells)
     got = np.concatenate([mon.get_complex_field().reshape(3, -1), pt.get_complex_field().reshape(3, 1)], 1)
     assert rel_l2(np.concatenate([got.real, got.imag]), np.concatenate([ref.real, ref.imag])) < TOL
+
+
+# Grids large enough for an interior rectangle of walk blocks (the golden
+# cases above are small enough that every block is a frame block): TMz with
+# an even ny runs the two-column interior walk, TMz with an odd ny and TEz the
+# one-column one.  Sources sit on even and odd columns, on a pair's first and
+# last owned columns (62 and 123) and in the frame.
+INTERIOR = [
+    ("tmz_pairs", "TMZ", 300, 262, 130, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
+     [("gauss", 150, 100, 20e9, 1.0, 6.0, "Ez"), ("gauss", 200, 131, 15e9, 0.8, 5.0, "Ez"),
+      ("gauss", 140, 62, 20e9, 0.5, 6.0, "Ez"), ("gauss", 180, 123, 20e9, 0.5, 6.0, "Ez"),
+      ("gauss", 20, 30, 20e9, 1.0, 6.0, "Ez")],
+     [(150, 100), (170, 140), (129, 61), (255, 200), (12, 250)], "Ez", 40,
+     [("circle", 150, 131, 40, 4.0, 1.0, 0.2, 0.0), ("region", 130, 170, 60, 70, 2.5, 1.0, 0.05, 0.0)]),
+    ("tmz_odd_ny", "TMZ", 290, 259, 120, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
+     [("gauss", 150, 100, 20e9, 1.0, 6.0, "Ez"), ("gauss", 190, 133, 20e9, 1.0, 6.0, "Ez")],
+     [(150, 100), (170, 140), (250, 251)], "Ez", 60,
+     [("circle", 145, 129, 35, 4.0, 1.0, 0.2, 0.0)]),
+    ("tez_interior", "TEZ", 280, 250, 120, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
+     [("gauss", 150, 100, 20e9, 1.0, 6.0, "Hz"), ("gauss", 180, 131, 15e9, 0.7, 5.0, "Ex"),
+      ("sin", 140, 90, 12e9, 0.3, "Ey")],
+     [(150, 100), (170, 140), (20, 20)], "Hz", 40,
+     [("circle", 140, 125, 35, 5.0, 1.0, 0.3, 0.0)]),
+]
+
+
+@pytest.mark.parametrize("case", INTERIOR, ids=[c[0] for c in INTERIOR])
+def test_interior_walks_match_oracle(cuda_device, case):
+    from oracle.fdtd2d_single import Single2DOracle
+    name, mode, nx, ny, steps, bcs, srcs, prbs, rec, interval, mats = case
+    s = build(case)
+    s.run()
+    g, dt = s.grid, s.config.dt
+    waves = [np.array([src.value_at(k, dt) for k in range(steps)]) for src in s.sources]
+    o = Single2DOracle(nx, ny, 1e-3, 0.8e-3, dt, mode, g._ca, g._cb, g._da, g._db,
+                       [(sp[1], sp[2], sp[-1], waves[k]) for k, sp in enumerate(srcs)], bcs, prbs, rec, interval)
+    o.run(steps)
+    got = np.array([s.probe_data[tuple(p)] for p in prbs])
+    ref = np.array([o.probe_data[tuple(p)] for p in prbs])
+    assert rel_l2(got, ref) < TOL, rel_l2(got, ref)
+    names = {"ez": "Ez", "hx": "Hx", "hy": "Hy", "hz": "Hz", "ex": "Ex", "ey": "Ey"}
+    for f in FIELDS[mode]:
+        e = rel_l2(getattr(s.grid, f).double().cpu().numpy(), o.f[names[f]])
+        assert e < TOL, (f, e)
+    assert len(s.field_snapshots) == len(o.snapshots)
+    assert rel_l2(np.array(s.field_snapshots), np.array(o.snapshots)) < TOL
