@@ -31,6 +31,7 @@ import torch
 
 from ._lib import check, lib
 from .constants import EPS_0
+from .physics import rdiv
 from .solvers import BatchedFDTD2D, _ptr
 
 
@@ -60,7 +61,7 @@ def coefficient_maps(eps_r, sigma, debye, dt):
         eps = eps + k2 / 2.0
         poles.append((k1, k2, g))
     s = sigma * dt / (2.0 * eps)
-    return (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s), dt / (eps_r * EPS_0), poles
+    return (1.0 - s) / (1.0 + s), rdiv(dt, eps) / (1.0 + s), rdiv(dt, eps_r * EPS_0), poles
 
 
 def run_segments_backward(starts, kept, recompute, adjoint, device, overlap, nbuf):

@@ -26,6 +26,7 @@
 // reads and writes each field and reads each coefficient pair once.  All
 // launches of a run are captured once into a CUDA graph and replayed.
 #include <map>
+#include <set>
 #include <tuple>
 
 #include "../../include/ceep_b200.h"
@@ -606,6 +607,7 @@ struct ceep2s_plan {
   cudaStream_t side = nullptr;  // the frame launch's stream
   cudaEvent_t fork = nullptr, join = nullptr;
   std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
+  std::set<std::tuple<int64_t, int64_t, int>> seen;  // step ranges run once without a graph
 };
 
 static int run_steps2s(const ceep2s_plan* pl, int64_t step0, int64_t nsteps, int cur, cudaStream_t s) {
@@ -727,6 +729,13 @@ extern "C" int ceep2s_plan_run(ceep2s_plan* pl, int64_t step0, int64_t nsteps, v
   }
   auto key = std::make_tuple(step0, nsteps, cur);
   auto it = pl->graphs.find(key);
+  if (it == pl->graphs.end() && pl->seen.insert(key).second) {
+    // first request of this range: launch directly (a one-off run does not
+    // pay for a capture); a second request captures it
+    const int rc = run_steps2s(pl, step0, nsteps, cur, s);
+    if (rc == CEEP_OK) pl->cur = cur_after;
+    return rc;
+  }
   if (it == pl->graphs.end()) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);

@@ -46,6 +46,7 @@ import torch
 
 from ._lib import check, lib
 from .constants import C_0, EPS_0, MU_0, cfl_timestep_2d, cfl_timestep_3d
+from .physics import rdiv
 
 TWO_PI = 2.0 * math.pi
 
@@ -313,15 +314,34 @@ class Grid2D:
         self._precompute_coefficients()
 
     def _precompute_coefficients(self) -> None:
-        """grid.py:157-195 in FP64 on the host."""
+        """grid.py:157-195 in FP64, formed on the device: the material maps as
+        they are now cross the host link once, and the four coefficient maps
+        are computed there with the host formulas' operations in the same
+        order (each one IEEE FP64 operation; the scalar divisions through
+        physics.rdiv), so they equal the host formulas bit for bit.  Later
+        edits of the maps take effect at the next call, as in the reference.
+        ``_ca``, ``_cb``, ``_da`` and ``_db`` copy them to the host when read."""
         dt = self.config.dt
-        eps = self.eps_inf * EPS_0
-        mu = self.mu_r * MU_0
-        se = self.sigma_e * dt / (2.0 * eps)
-        sm = self.sigma_m * dt / (2.0 * mu)
-        self._ca, self._cb = (1.0 - se) / (1.0 + se), (dt / eps) / (1.0 + se)
-        self._da, self._db = (1.0 - sm) / (1.0 + sm), (dt / mu) / (1.0 + sm)
+        dev = self._empty.device
+        f64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+        eps = f64(self.eps_inf) * EPS_0
+        mu = f64(self.mu_r) * MU_0
+        se = f64(self.sigma_e) * dt / (2.0 * eps)
+        sm = f64(self.sigma_m) * dt / (2.0 * mu)
+        self._coef_dev = ((1.0 - se) / (1.0 + se), rdiv(dt, eps) / (1.0 + se),
+                          (1.0 - sm) / (1.0 + sm), rdiv(dt, mu) / (1.0 + sm))
+        self._coef_host = None
         self._version += 1
+
+    def _host_coefficients(self):
+        if self._coef_host is None:
+            self._coef_host = tuple(t.cpu().numpy() for t in self._coef_dev)
+        return self._coef_host
+
+    _ca = property(lambda self: self._host_coefficients()[0])
+    _cb = property(lambda self: self._host_coefficients()[1])
+    _da = property(lambda self: self._host_coefficients()[2])
+    _db = property(lambda self: self._host_coefficients()[3])
 
     def set_material_region(self, x_start, x_end, y_start, y_end, eps_r=1.0, mu_r=1.0, sigma_e=0.0, sigma_m=0.0,
                             eps_inf=None, debye_poles=None) -> None:
@@ -556,10 +576,9 @@ class FDTD2D:
         g = self.grid
         if self._coef_version == g._version:
             return
-        e = np.stack([g._ca, g._cb], -1)
-        h = np.stack([g._da, g._db], -1)
-        self._coef_e.copy_(torch.as_tensor(e, dtype=torch.float32))
-        self._coef_h.copy_(torch.as_tensor(h, dtype=torch.float32))
+        ca, cb, da, db = g._coef_dev
+        self._coef_e.copy_(torch.stack([ca, cb], -1))      # FP64 -> FP32, rounded to nearest
+        self._coef_h.copy_(torch.stack([da, db], -1))
         self._coef_version = g._version
 
     def __del__(self):

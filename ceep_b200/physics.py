@@ -129,6 +129,15 @@ def ade_tensors(dt: float, debye=(), lorentz=(), shape=None, device=None):
     return eps_add, ade
 
 
+def rdiv(num: float, t):
+    """num / t elementwise with one correctly rounded division, as NumPy's
+    scalar / array.  torch evaluates float / Tensor as reciprocal(t) * num,
+    two roundings that differ from the quotient by an ulp in about a quarter
+    of FP64 elements."""
+    import torch
+    return torch.div(torch.tensor(num, dtype=t.dtype, device=t.device), t)
+
+
 def coefficient_tensors(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=None):
     """2D: ade_coefficients + update_coefficients on the device (see
     ade_tensors), in the kernel layout: coef (ny, nx, 4) float32 = (ca, cb,
@@ -141,8 +150,8 @@ def coefficient_tensors(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=
     if ade.shape[0]:
         eps = eps + eps_add
     s = torch.broadcast_to(_f64(sigma_e, eps_r.device), eps_r.shape) * dt / (2.0 * eps)
-    ca, cb = (1.0 - s) / (1.0 + s), (dt / eps) / (1.0 + s)
-    dteps = dt / (eps_r * EPS_0)
+    ca, cb = (1.0 - s) / (1.0 + s), rdiv(dt, eps) / (1.0 + s)
+    dteps = rdiv(dt, eps_r * EPS_0)
     coef = torch.stack([ca.t(), cb.t(), dteps.t(), torch.zeros_like(ca).t()], -1).float().contiguous()
     return coef, ade.transpose(1, 2).float().contiguous()
 
@@ -160,8 +169,8 @@ def coefficient_tensors_3d(eps_r, sigma_e, mu_r, sigma_m, dt: float, debye=(), l
     mu = bc(mu_r) * MU_0
     se = bc(sigma_e) * dt / (2.0 * eps)
     sm = bc(sigma_m) * dt / (2.0 * mu)
-    ca, cb = (1.0 - se) / (1.0 + se), (dt / eps) / (1.0 + se)
-    da, db = (1.0 - sm) / (1.0 + sm), (dt / mu) / (1.0 + sm)
+    ca, cb = (1.0 - se) / (1.0 + se), rdiv(dt, eps) / (1.0 + se)
+    da, db = (1.0 - sm) / (1.0 + sm), rdiv(dt, mu) / (1.0 + sm)
     coef = torch.stack([da, db, ca, cb], -1).permute(2, 1, 0, 3).float().contiguous()
     return coef, ade.permute(0, 3, 2, 1, 4).float().contiguous()
 

@@ -297,8 +297,10 @@ typedef struct ceep2s_desc {
 typedef struct ceep2s_plan ceep2s_plan;
 int ceep2s_plan_create(const ceep2s_desc* desc, ceep2s_plan** out);
 /* Steps step0 .. step0+nsteps-1 (the step index selects the waveform column,
- * the record column and the Mur state half); graph-captured per
- * (step0, nsteps) when use_graph and a stream are given. */
+ * the record column and the Mur state half).  With use_graph and a stream, a
+ * range is captured into a CUDA graph the second time it is asked for and
+ * replayed from then on; its first run launches directly, so a one-off run
+ * pays no capture. */
 int ceep2s_plan_run(ceep2s_plan* plan, int64_t step0, int64_t nsteps, void* stream, int use_graph);
 /* The half (0 or 1) of the ping-pong arrays that holds the current state;
  * each step flips it. */

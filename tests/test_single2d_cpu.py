@@ -5,6 +5,7 @@ import os
 import sys
 
 import numpy as np
+import torch
 import pytest
 
 from oracle.fdtd2d_single import Single2DOracle
@@ -90,6 +91,7 @@ def test_grid_coefficients_match_the_reference():
                                mode=getattr(SimulationMode, mode), total_steps=steps)
         g = Grid2D.__new__(Grid2D)
         g.config = cfg
+        g._empty = torch.empty(0)          # the coefficients are formed with torch on this device (CPU here)
         shp = (nx, ny)
         g.eps_r, g.eps_inf, g.mu_r = np.ones(shp), np.ones(shp), np.ones(shp)
         g.sigma_e, g.sigma_m = np.zeros(shp), np.zeros(shp)

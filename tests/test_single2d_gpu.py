@@ -76,6 +76,11 @@ def test_step_by_step_equals_run_and_graph_equals_stream(cuda_device):
     case = SINGLE2D[1]
     a = build(case)
     a.run()
+    first = {f: getattr(a.grid, f).clone() for f in FIELDS[case[1]]}
+    a.reset()
+    a.run()                # the same range again: captured and replayed as a graph
+    for f in FIELDS[case[1]]:
+        assert torch.equal(first[f], getattr(a.grid, f))
     b = build(case, use_graph=False)
     for _ in range(case[4]):
         b.step()
