@@ -857,8 +857,9 @@ def run_single_bench(args):
                          "kernel": "single2d_step_kernel interior + frame launches (+ record) per step",
                          "algorithmic_bytes_per_step": bytes_step, "step_ms": round(step_ms, 5)},
             "e2e": {"value": round(nx * ny * T / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GCell-steps/s",
-                    "h2d_bytes_per_step": 4 * 4 * nx * ny, "d2h_bytes_per_step": 4 * len(prb) * T,
-                    "path": "FDTD2D(...) + set materials + run(), probe lists back on the host"},
+                    "h2d_bytes_per_step": 8 * 4 * nx * ny, "d2h_bytes_per_step": 4 * len(prb) * T,
+                    "path": "FDTD2D(...) + set materials + run(), probe lists back on the host; the four FP64 "
+                            "material maps go up, the coefficients are formed on the device"},
             "gpu_launches": len(ms) * 3 * T,
             "clocks": clk.summary()}
     if cpu:

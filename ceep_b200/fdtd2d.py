@@ -311,7 +311,9 @@ class Grid2D:
         self.eps_r, self.eps_inf, self.mu_r = np.ones(shp), np.ones(shp), np.ones(shp)
         self.sigma_e, self.sigma_m = np.zeros(shp), np.zeros(shp)
         self._version = 0
-        self._precompute_coefficients()
+        # the maps start as ones and zeros: form those on the device directly
+        one = torch.ones(shp, dtype=torch.float64, device=dev)
+        self._form_coefficients(one, one, torch.zeros_like(one), torch.zeros_like(one))
 
     def _precompute_coefficients(self) -> None:
         """grid.py:157-195 in FP64, formed on the device: the material maps as
@@ -321,13 +323,16 @@ class Grid2D:
         physics.rdiv), so they equal the host formulas bit for bit.  Later
         edits of the maps take effect at the next call, as in the reference.
         ``_ca``, ``_cb``, ``_da`` and ``_db`` copy them to the host when read."""
-        dt = self.config.dt
         dev = self._empty.device
         f64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
-        eps = f64(self.eps_inf) * EPS_0
-        mu = f64(self.mu_r) * MU_0
-        se = f64(self.sigma_e) * dt / (2.0 * eps)
-        sm = f64(self.sigma_m) * dt / (2.0 * mu)
+        self._form_coefficients(f64(self.eps_inf), f64(self.mu_r), f64(self.sigma_e), f64(self.sigma_m))
+
+    def _form_coefficients(self, eps_inf, mu_r, sigma_e, sigma_m) -> None:
+        dt = self.config.dt
+        eps = eps_inf * EPS_0
+        mu = mu_r * MU_0
+        se = sigma_e * dt / (2.0 * eps)
+        sm = sigma_m * dt / (2.0 * mu)
         self._coef_dev = ((1.0 - se) / (1.0 + se), rdiv(dt, eps) / (1.0 + se),
                           (1.0 - sm) / (1.0 + sm), rdiv(dt, mu) / (1.0 + sm))
         self._coef_host = None
