@@ -23,8 +23,8 @@
 //   record     probe / monitor cells into (nrec, nsteps), and a copy of the
 //              snapshot field every snap_interval steps
 // Fields are (nx, ny) FP32 with y fastest, the reference's layout; a step
-// reads and writes each field and reads each coefficient pair once.  All
-// launches of a run are captured once into a CUDA graph and replayed.
+// reads and writes each field and reads each coefficient pair once.  A run
+// of steps asked for a second time is captured into a CUDA graph and replayed.
 #include <map>
 #include <set>
 #include <tuple>
@@ -229,32 +229,50 @@ CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
 // launch (few blocks, so shorter walks keep its duration down).
 constexpr int kBlockRows = 128, kWarpsInterior = 4, kWarpsFrame = 16;
 
-// Blocks (31 columns x kBlockRows rows) split into an interior rectangle,
-// whose cells and halo touch no CPML strip and no grid edge, and the frame
-// around it.  The interior launch runs the code without CPML (half the
-// registers, twice the resident warps); the frame launch maps its linear
-// block index onto the frame.
+// Blocks of 31 columns x up to kBlockRows rows, split into an interior
+// rectangle -- the column blocks [bx_lo, bx_hi) over the rows [row_lo,
+// row_hi), whose cells and halo touch no CPML strip and no grid edge -- and
+// the frame around it: a top band of rows [0, row_lo), a bottom band
+// [row_hi, nx), both full width, and the side blocks beside the rectangle.
+// The interior launch runs the code without CPML (half the registers, twice
+// the resident warps); the frame launch maps its linear block index onto the
+// bands and sides.  The interior rows are not rounded to whole blocks (its
+// last block may be short), so the frame holds only the strips themselves.
 struct BlockMap {
-  int gx, gy;                   // blocks along y (columns) and x (rows)
-  int bx_lo, bx_hi, by_lo, by_hi;  // interior rectangle [lo, hi)
+  int gx;                       // column blocks
+  int bx_lo, bx_hi;             // interior column blocks [lo, hi)
+  int row_lo, row_hi, nx;       // interior rows [lo, hi); grid rows
   int frame;                    // 0: interior launch (2D grid), 1: frame launch (1D grid)
 };
 
-CEEP_D void block_of(const BlockMap& m, int& bx, int& by) {
+// This block's column block and row range [rs, re).
+CEEP_D void block_of(const BlockMap& m, int& bx, int& rs, int& re) {
   if (!m.frame) {
     bx = m.bx_lo + blockIdx.x;
-    by = m.by_lo + blockIdx.y;
+    rs = m.row_lo + blockIdx.y * kBlockRows;
+    re = min(rs + kBlockRows, m.row_hi);
     return;
   }
   int f = blockIdx.x;
-  const int top = m.by_lo * m.gx;
-  if (f < top) { bx = f % m.gx; by = f / m.gx; return; }
+  const int top = (m.row_lo + kBlockRows - 1) / kBlockRows * m.gx;
+  if (f < top) {
+    bx = f % m.gx;
+    rs = f / m.gx * kBlockRows;
+    re = min(rs + kBlockRows, m.row_lo);
+    return;
+  }
   f -= top;
-  const int bottom = (m.gy - m.by_hi) * m.gx;
-  if (f < bottom) { bx = f % m.gx; by = m.by_hi + f / m.gx; return; }
+  const int bottom = (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx;
+  if (f < bottom) {
+    bx = f % m.gx;
+    rs = m.row_hi + f / m.gx * kBlockRows;
+    re = min(rs + kBlockRows, m.nx);
+    return;
+  }
   f -= bottom;
   const int side = m.bx_lo + (m.gx - m.bx_hi);
-  by = m.by_lo + f / side;
+  rs = m.row_lo + f / side * kBlockRows;
+  re = min(rs + kBlockRows, m.row_hi);
   const int q = f % side;
   bx = q < m.bx_lo ? q : m.bx_hi + (q - m.bx_lo);
 }
@@ -264,14 +282,14 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
                                                                            const BlockMap bm) {
   const int w = r ^ 1;
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
-  int bx, by;
-  block_of(bm, bx, by);
+  int bx, rs, re;
+  block_of(bm, bx, rs, re);
   const int j0 = bx * 31;
   const int c = j0 - 1 + lane;
   const int rows = kBlockRows / blockDim.y;
-  const int i0 = by * kBlockRows + threadIdx.y * rows;
-  if (i0 >= nx) return;  // whole warp
-  const int i1 = min(i0 + rows, nx);
+  const int i0 = rs + threadIdx.y * rows;
+  if (i0 >= re) return;  // whole warp
+  const int i1 = min(i0 + rows, re);
   const bool live = c >= 0 && c < ny;
   const bool own = live && lane > 0;
   const int cl = live ? c : max(min(c, ny - 1), 0);  // a valid column for the non-live lanes' loads
@@ -421,15 +439,16 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
 // the region tests of the general walk fold away.  Same arithmetic, in the
 // same order, as the one-column walk.
 __global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tmz_pair_kernel(const Single2dParams p, int step,
-                                                                                 int r, int bx0, int by0) {
+                                                                                 int r, int bx0, int row_lo,
+                                                                                 int row_hi) {
   const int w = r ^ 1;
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
   const int j0 = 31 * bx0 + 62 * blockIdx.x;
   const int c = j0 - 2 + 2 * lane;
   constexpr int rows = kBlockRows / kWarpsInterior;
-  const int i0 = (by0 + blockIdx.y) * kBlockRows + threadIdx.y * rows;
-  if (i0 >= nx) return;  // whole warp
-  const int i1 = min(i0 + rows, nx);
+  const int i0 = row_lo + blockIdx.y * kBlockRows + threadIdx.y * rows;
+  if (i0 >= row_hi) return;  // whole warp
+  const int i1 = min(i0 + rows, row_hi);
   const bool own = lane > 0;
   const float* ez_r = p.f[0][r];
   const float2* ez2 = reinterpret_cast<const float2*>(ez_r);
@@ -536,17 +555,17 @@ __global__ void single2d_record_kernel(const Single2dParams p, int step, int cur
 
 BlockMap block_map(const Single2dParams& p) {
   BlockMap m;
-  const int rows = kBlockRows;
   m.gx = (p.ny + 30) / 31;
-  m.gy = (p.nx + rows - 1) / rows;
-  // interior: columns bx*31-1 .. bx*31+30 and rows by*rows-1 .. by*rows+rows-1
-  // inside [e, n-e) with e = max(t, 1) (strips and edges excluded)
+  m.nx = p.nx;
+  // interior: owned columns bx*31 .. bx*31+30 with their halo bx*31-1 ..
+  // bx*31+31, and owned rows with the row below and above, inside [e, n-e)
+  // with e = max(t, 1) (strips and edges excluded)
   const int e = p.t > 1 ? p.t : 1;
   m.bx_lo = (e + 1 + 30) / 31;
   m.bx_hi = (p.ny - e - 31) >= 0 ? (p.ny - e - 31) / 31 + 1 : 0;
-  m.by_lo = (e + 1 + rows - 1) / rows;
-  m.by_hi = (p.nx - e - rows) >= 0 ? (p.nx - e - rows) / rows + 1 : 0;
-  if (m.bx_hi <= m.bx_lo || m.by_hi <= m.by_lo) m.bx_lo = m.bx_hi = m.by_lo = m.by_hi = 0;
+  m.row_lo = e + 1;
+  m.row_hi = p.nx - e;
+  if (m.bx_hi <= m.bx_lo || m.row_hi <= m.row_lo) m.bx_lo = m.bx_hi = m.row_lo = m.row_hi = 0;
   m.frame = 0;
   return m;
 }
@@ -566,10 +585,12 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
     m.bx_lo += m.bx_lo & 1;
     const int np = (m.bx_hi - m.bx_lo) / 2;
     if (np > 0) m.bx_hi = m.bx_lo + 2 * np;
-    else m.bx_lo = m.bx_hi = m.by_lo = m.by_hi = 0;
+    else m.bx_lo = m.bx_hi = m.row_lo = m.row_hi = 0;
   }
-  const int interior = (m.bx_hi - m.bx_lo) * (m.by_hi - m.by_lo);
-  const int rest = m.gx * m.gy - interior;
+  const int iby = (m.row_hi - m.row_lo + kBlockRows - 1) / kBlockRows;   // interior block rows
+  const int interior = (m.bx_hi - m.bx_lo) * iby;
+  const int rest = (m.row_lo + kBlockRows - 1) / kBlockRows * m.gx +
+                   (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx + iby * (m.bx_lo + m.gx - m.bx_hi);
   const bool two = interior > 0 && rest > 0;
   cudaError_t e;
   if (two) {
@@ -584,11 +605,11 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
   }
   if (interior > 0) {
     if (pair)
-      single2d_tmz_pair_kernel<<<dim3((m.bx_hi - m.bx_lo) / 2, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0, s>>>(
-          p, step, r, m.bx_lo, m.by_lo);
+      single2d_tmz_pair_kernel<<<dim3((m.bx_hi - m.bx_lo) / 2, iby), dim3(32, kWarpsInterior), 0, s>>>(
+          p, step, r, m.bx_lo, m.row_lo, m.row_hi);
     else
-      single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, m.by_hi - m.by_lo), dim3(32, kWarpsInterior), 0,
-                                          s>>>(p, step, r, m);
+      single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step,
+                                                                                                       r, m);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (two) {
