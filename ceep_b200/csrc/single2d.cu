@@ -230,33 +230,40 @@ CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
 constexpr int kBlockRows = 128, kWarpsInterior = 4, kWarpsFrame = 16;
 
 // Blocks of 31 columns x up to kBlockRows rows, split into an interior
-// rectangle -- the column blocks [bx_lo, bx_hi) over the rows [row_lo,
-// row_hi), whose cells and halo touch no CPML strip and no grid edge -- and
-// the frame around it: a top band of rows [0, row_lo), a bottom band
-// [row_hi, nx), both full width, and the side blocks beside the rectangle.
-// The interior launch runs the code without CPML (half the registers, twice
-// the resident warps); the frame launch maps its linear block index onto the
-// bands and sides.  The interior rows are not rounded to whole blocks (its
-// last block may be short), so the frame holds only the strips themselves.
+// rectangle -- columns [col_lo, col_hi) over rows [row_lo, row_hi), whose
+// cells and halo touch no CPML strip and no grid edge -- and the frame around
+// it: a top band of rows [0, row_lo), a bottom band [row_hi, nx), both full
+// width, and side blocks on the columns [0, col_lo) and [col_hi, ny) of the
+// interior rows.  The interior launch runs the code without CPML (half the
+// registers, twice the resident warps); the frame launch maps its linear
+// block index onto the bands and sides.  Neither the rows nor the columns of
+// the rectangle are rounded to whole blocks, so the frame holds little more
+// than the strips themselves.
 struct BlockMap {
-  int gx;                       // column blocks
-  int bx_lo, bx_hi;             // interior column blocks [lo, hi)
+  int gx;                       // column blocks of the bands
+  int col_lo, col_hi, ny;       // interior columns [lo, hi); grid columns
   int row_lo, row_hi, nx;       // interior rows [lo, hi); grid rows
   int frame;                    // 0: interior launch (2D grid), 1: frame launch (1D grid)
 };
 
-// This block's column block and row range [rs, re).
-CEEP_D void block_of(const BlockMap& m, int& bx, int& rs, int& re) {
+__host__ __device__ inline int side_blocks(int cols) { return (cols + 30) / 31; }
+
+// This block's first owned column j0, the end ce of the columns it owns (a
+// side block may reach into the interior and owns only up to it), and its
+// row range [rs, re).
+CEEP_D void block_of(const BlockMap& m, int& j0, int& ce, int& rs, int& re) {
   if (!m.frame) {
-    bx = m.bx_lo + blockIdx.x;
+    j0 = m.col_lo + blockIdx.x * 31;
+    ce = m.col_hi;
     rs = m.row_lo + blockIdx.y * kBlockRows;
     re = min(rs + kBlockRows, m.row_hi);
     return;
   }
+  ce = m.ny;
   int f = blockIdx.x;
   const int top = (m.row_lo + kBlockRows - 1) / kBlockRows * m.gx;
   if (f < top) {
-    bx = f % m.gx;
+    j0 = f % m.gx * 31;
     rs = f / m.gx * kBlockRows;
     re = min(rs + kBlockRows, m.row_lo);
     return;
@@ -264,17 +271,22 @@ CEEP_D void block_of(const BlockMap& m, int& bx, int& rs, int& re) {
   f -= top;
   const int bottom = (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx;
   if (f < bottom) {
-    bx = f % m.gx;
+    j0 = f % m.gx * 31;
     rs = m.row_hi + f / m.gx * kBlockRows;
     re = min(rs + kBlockRows, m.nx);
     return;
   }
   f -= bottom;
-  const int side = m.bx_lo + (m.gx - m.bx_hi);
+  const int nl = side_blocks(m.col_lo), side = nl + side_blocks(m.ny - m.col_hi);
   rs = m.row_lo + f / side * kBlockRows;
   re = min(rs + kBlockRows, m.row_hi);
   const int q = f % side;
-  bx = q < m.bx_lo ? q : m.bx_hi + (q - m.bx_lo);
+  if (q < nl) {
+    j0 = q * 31;
+    ce = m.col_lo;
+  } else {
+    j0 = m.col_hi + (q - nl) * 31;
+  }
 }
 
 template <int MODE, bool CPML>
@@ -282,16 +294,15 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
                                                                            const BlockMap bm) {
   const int w = r ^ 1;
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
-  int bx, rs, re;
-  block_of(bm, bx, rs, re);
-  const int j0 = bx * 31;
+  int j0, ce, rs, re;
+  block_of(bm, j0, ce, rs, re);
   const int c = j0 - 1 + lane;
   const int rows = kBlockRows / blockDim.y;
   const int i0 = rs + threadIdx.y * rows;
   if (i0 >= re) return;  // whole warp
   const int i1 = min(i0 + rows, re);
   const bool live = c >= 0 && c < ny;
-  const bool own = live && lane > 0;
+  const bool own = live && lane > 0 && c < ce;
   const int cl = live ? c : max(min(c, ny - 1), 0);  // a valid column for the non-live lanes' loads
   if (MODE == 0) {
     const float* ez_r = p.f[0][r];
@@ -434,16 +445,16 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
 // per warp of the one-column walk, half the load instructions).  Strips are
 // 62 columns wide (lanes 1..31 own them; lane 0 forms the H of column j0-1
 // for its neighbour's E update, and writes nothing).  Needs an even ny (the
-// float2 rows stay aligned) and a strip start j0 on an even column; the
+// float2 rows stay aligned) and strip starts j0 on even columns; the
 // cells it owns and their halo lie in the CPML- and edge-free interior, so
 // the region tests of the general walk fold away.  Same arithmetic, in the
 // same order, as the one-column walk.
 __global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tmz_pair_kernel(const Single2dParams p, int step,
-                                                                                 int r, int bx0, int row_lo,
+                                                                                 int r, int col_lo, int row_lo,
                                                                                  int row_hi) {
   const int w = r ^ 1;
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
-  const int j0 = 31 * bx0 + 62 * blockIdx.x;
+  const int j0 = col_lo + 62 * blockIdx.x;
   const int c = j0 - 2 + 2 * lane;
   constexpr int rows = kBlockRows / kWarpsInterior;
   const int i0 = row_lo + blockIdx.y * kBlockRows + threadIdx.y * rows;
@@ -553,19 +564,23 @@ __global__ void single2d_record_kernel(const Single2dParams p, int step, int cur
   p.rec_out[(size_t)r * p.nsteps + step] = p.f[p.rec[2 * r + 1]][cur][p.rec[2 * r]];
 }
 
-BlockMap block_map(const Single2dParams& p) {
+// The interior rectangle for a walk of `width`-column strips (31, or 62 for
+// the two-column walk, whose strips start on even columns): owned columns
+// and rows with their halo (the column and row on each side) inside
+// [e, n-e) with e = max(t, 1), i.e. clear of the CPML strips and the edges.
+BlockMap block_map(const Single2dParams& p, int width) {
   BlockMap m;
   m.gx = (p.ny + 30) / 31;
   m.nx = p.nx;
-  // interior: owned columns bx*31 .. bx*31+30 with their halo bx*31-1 ..
-  // bx*31+31, and owned rows with the row below and above, inside [e, n-e)
-  // with e = max(t, 1) (strips and edges excluded)
+  m.ny = p.ny;
   const int e = p.t > 1 ? p.t : 1;
-  m.bx_lo = (e + 1 + 30) / 31;
-  m.bx_hi = (p.ny - e - 31) >= 0 ? (p.ny - e - 31) / 31 + 1 : 0;
+  m.col_lo = e + 1;
+  if (width == 62) m.col_lo += m.col_lo & 1;
+  const int strips_n = p.ny - e - m.col_lo >= 0 ? (p.ny - e - m.col_lo) / width : 0;
+  m.col_hi = m.col_lo + strips_n * width;
   m.row_lo = e + 1;
   m.row_hi = p.nx - e;
-  if (m.bx_hi <= m.bx_lo || m.row_hi <= m.row_lo) m.bx_lo = m.bx_hi = m.row_lo = m.row_hi = 0;
+  if (strips_n <= 0 || m.row_hi <= m.row_lo) m.col_lo = m.col_hi = m.row_lo = m.row_hi = 0;
   m.frame = 0;
   return m;
 }
@@ -576,21 +591,17 @@ BlockMap block_map(const Single2dParams& p) {
 template <int MODE, bool CPML>
 static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s, cudaStream_t s2,
                           cudaEvent_t fork, cudaEvent_t join) {
-  BlockMap m = block_map(p);
-  // TMz with an even ny: the interior runs the two-column walk over pairs of
-  // 31-column blocks starting on an even block (an even column); a block
-  // left over at either end joins the frame
+  // TMz with an even ny: the interior runs the two-column walk (62-column
+  // strips starting on an even column)
   const bool pair = MODE == 0 && p.ny % 2 == 0;
-  if (pair && m.bx_hi > m.bx_lo) {
-    m.bx_lo += m.bx_lo & 1;
-    const int np = (m.bx_hi - m.bx_lo) / 2;
-    if (np > 0) m.bx_hi = m.bx_lo + 2 * np;
-    else m.bx_lo = m.bx_hi = m.row_lo = m.row_hi = 0;
-  }
+  const int width = pair ? 62 : 31;
+  BlockMap m = block_map(p, width);
+  const int ibx = (m.col_hi - m.col_lo) / width;                            // interior strips
   const int iby = (m.row_hi - m.row_lo + kBlockRows - 1) / kBlockRows;   // interior block rows
-  const int interior = (m.bx_hi - m.bx_lo) * iby;
+  const int interior = ibx * iby;
   const int rest = (m.row_lo + kBlockRows - 1) / kBlockRows * m.gx +
-                   (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx + iby * (m.bx_lo + m.gx - m.bx_hi);
+                   (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx +
+                   iby * (side_blocks(m.col_lo) + side_blocks(m.ny - m.col_hi));
   const bool two = interior > 0 && rest > 0;
   cudaError_t e;
   if (two) {
@@ -605,11 +616,10 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
   }
   if (interior > 0) {
     if (pair)
-      single2d_tmz_pair_kernel<<<dim3((m.bx_hi - m.bx_lo) / 2, iby), dim3(32, kWarpsInterior), 0, s>>>(
-          p, step, r, m.bx_lo, m.row_lo, m.row_hi);
+      single2d_tmz_pair_kernel<<<dim3(ibx, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step, r, m.col_lo, m.row_lo,
+                                                                                    m.row_hi);
     else
-      single2d_step_kernel<MODE, false><<<dim3(m.bx_hi - m.bx_lo, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step,
-                                                                                                       r, m);
+      single2d_step_kernel<MODE, false><<<dim3(ibx, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step, r, m);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (two) {

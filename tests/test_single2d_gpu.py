@@ -142,13 +142,15 @@ def test_dft_monitor_matches_oracle_series(cuda_device):
 # cases above are small enough that every block is a frame block): TMz with
 # an even ny runs the two-column interior walk, TMz with an odd ny and TEz the
 # one-column one.  Sources sit on even and odd columns, on a pair's first and
-# last owned columns (62 and 123) and in the frame.
+# last owned columns (74 and 135: the rectangle starts at column 12 for
+# CPML 10) and in the frame; probes sit beside the rectangle and on a pair
+# boundary.
 INTERIOR = [
     ("tmz_pairs", "TMZ", 300, 262, 130, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
      [("gauss", 150, 100, 20e9, 1.0, 6.0, "Ez"), ("gauss", 200, 131, 15e9, 0.8, 5.0, "Ez"),
-      ("gauss", 140, 62, 20e9, 0.5, 6.0, "Ez"), ("gauss", 180, 123, 20e9, 0.5, 6.0, "Ez"),
+      ("gauss", 140, 74, 20e9, 0.5, 6.0, "Ez"), ("gauss", 180, 135, 20e9, 0.5, 6.0, "Ez"),
       ("gauss", 20, 30, 20e9, 1.0, 6.0, "Ez")],
-     [(150, 100), (170, 140), (129, 61), (255, 200), (12, 250)], "Ez", 40,
+     [(150, 100), (170, 140), (129, 11), (129, 73), (255, 200), (12, 250), (289, 130)], "Ez", 40,
      [("circle", 150, 131, 40, 4.0, 1.0, 0.2, 0.0), ("region", 130, 170, 60, 70, 2.5, 1.0, 0.05, 0.0)]),
     ("tmz_odd_ny", "TMZ", 290, 259, 120, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
      [("gauss", 150, 100, 20e9, 1.0, 6.0, "Ez"), ("gauss", 190, 133, 20e9, 1.0, 6.0, "Ez")],
