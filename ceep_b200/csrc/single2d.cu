@@ -517,6 +517,83 @@ __global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tmz_pair_kernel(
   }
 }
 
+// The TEz interior walk with two columns per lane, as the TMz one above:
+// Hz from the Ex / Ey differences, then Ex and Ey from Hz of the left lane
+// and of the row below.  Same arithmetic, in the same order, as the
+// one-column walk.
+__global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tez_pair_kernel(const Single2dParams p, int step,
+                                                                                 int r, int col_lo, int row_lo,
+                                                                                 int row_hi) {
+  const int w = r ^ 1;
+  const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
+  const int j0 = col_lo + 62 * blockIdx.x;
+  const int c = j0 - 2 + 2 * lane;
+  constexpr int rows = kBlockRows / kWarpsInterior;
+  const int i0 = row_lo + blockIdx.y * kBlockRows + threadIdx.y * rows;
+  if (i0 >= row_hi) return;  // whole warp
+  const int i1 = min(i0 + rows, row_hi);
+  const bool own = lane > 0;
+  const float* ex_r = p.f[1][r];
+  const float2* hz2 = reinterpret_cast<const float2*>(p.f[0][r]);
+  const float2* ex2 = reinterpret_cast<const float2*>(ex_r);
+  const float2* ey2 = reinterpret_cast<const float2*>(p.f[2][r]);
+  const float4* ch4 = reinterpret_cast<const float4*>(p.ch);  // (da, db) of c, then of c+1
+  const float4* ce4 = reinterpret_cast<const float4*>(p.ce);  // (ca, cb) of c, then of c+1
+  float2* hz_w = reinterpret_cast<float2*>(p.f[0][w]);
+  float2* ex_w = reinterpret_cast<float2*>(p.f[1][w]);
+  float2* ey_w = reinterpret_cast<float2*>(p.f[2][w]);
+  const size_t row2 = (size_t)ny / 2;
+  float2 hz_prev = make_float2(tez_hz_at<false>(p, r, i0 - 1, c), tez_hz_at<false>(p, r, i0 - 1, c + 1));
+  size_t k = ((size_t)i0 * ny + c) / 2;
+  float2 ey_c = __ldg(ey2 + k);
+  float2 ey_n = __ldg(ey2 + k + row2);
+  float2 ex_c = __ldg(ex2 + k), hz_c = __ldg(hz2 + k);
+  float4 d_c = __ldg(ch4 + k), e_c = __ldg(ce4 + k);
+  const float z2 = 0.f;
+  for (int i = i0; i < i1; ++i, k += row2) {
+    const bool more = i + 1 < i1;
+    const float2 ey_nn = more && i + 2 < nx ? __ldg(ey2 + k + 2 * row2) : make_float2(z2, z2);
+    const float2 ex_n = more ? __ldg(ex2 + k + row2) : make_float2(z2, z2);
+    const float2 hz_n = more ? __ldg(hz2 + k + row2) : make_float2(z2, z2);
+    const float4 d_n = more ? __ldg(ch4 + k + row2) : make_float4(z2, z2, z2, z2);
+    const float4 e_n = more ? __ldg(ce4 + k + row2) : make_float4(z2, z2, z2, z2);
+    float ex_rt = __shfl_down_sync(0xffffffffu, ex_c.x, 1);
+    if (lane == 31) ex_rt = __ldg(ex_r + (size_t)i * ny + c + 2);
+    float2 hz;
+    hz.x = d_c.x * hz_c.x + d_c.y * ((ex_c.y - ex_c.x) * p.inv_dy - (ey_n.x - ey_c.x) * p.inv_dx);
+    hz.y = d_c.z * hz_c.y + d_c.w * ((ex_rt - ex_c.y) * p.inv_dy - (ey_n.y - ey_c.y) * p.inv_dx);
+    const float hz_l = __shfl_up_sync(0xffffffffu, hz.y, 1);
+    if (own) {
+      hz_w[k] = hz;
+      float2 vx, vy;
+      vx.x = e_c.x * ex_c.x + (e_c.y * p.inv_dy) * (hz.x - hz_l);
+      vx.y = e_c.z * ex_c.y + (e_c.w * p.inv_dy) * (hz.y - hz.x);
+      vy.x = e_c.x * ey_c.x - (e_c.y * p.inv_dx) * (hz.x - hz_prev.x);
+      vy.y = e_c.z * ey_c.y - (e_c.w * p.inv_dx) * (hz.y - hz_prev.y);
+      for (int s = __ldg(p.src_row + i); s < __ldg(p.src_row + i + 1); ++s) {  // fdtd_2d.py:245-260
+        const int sc = __ldg(p.src + 3 * s + 1);
+        if (sc != c && sc != c + 1) continue;
+        const int fld = __ldg(p.src + 3 * s + 2);
+        const float wv = __ldg(p.waveform + (size_t)s * p.nsteps + step);
+        float2& v = fld == 1 ? vx : vy;
+        if (fld == 1 || fld == 2) {
+          if (sc == c) v.x += wv;
+          else v.y += wv;
+        }
+      }
+      ex_w[k] = vx;
+      ey_w[k] = vy;
+    }
+    hz_prev = hz;
+    ey_c = ey_n;
+    ey_n = ey_nn;
+    ex_c = ex_n;
+    hz_c = hz_n;
+    d_c = d_n;
+    e_c = e_n;
+  }
+}
+
 // TEz Hz sources, in list order (fdtd_2d.py:253-254).
 __global__ void single2d_src_h_kernel(const Single2dParams p, int step, int cur) {
   if (threadIdx.x != 0) return;
@@ -591,9 +668,9 @@ BlockMap block_map(const Single2dParams& p, int width) {
 template <int MODE, bool CPML>
 static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t s, cudaStream_t s2,
                           cudaEvent_t fork, cudaEvent_t join) {
-  // TMz with an even ny: the interior runs the two-column walk (62-column
-  // strips starting on an even column)
-  const bool pair = MODE == 0 && p.ny % 2 == 0;
+  // an even ny: the interior runs the two-column walk (62-column strips
+  // starting on an even column)
+  const bool pair = p.ny % 2 == 0;
   const int width = pair ? 62 : 31;
   BlockMap m = block_map(p, width);
   const int ibx = (m.col_hi - m.col_lo) / width;                            // interior strips
@@ -615,8 +692,11 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (interior > 0) {
-    if (pair)
+    if (pair && MODE == 0)
       single2d_tmz_pair_kernel<<<dim3(ibx, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step, r, m.col_lo, m.row_lo,
+                                                                                    m.row_hi);
+    else if (pair)
+      single2d_tez_pair_kernel<<<dim3(ibx, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step, r, m.col_lo, m.row_lo,
                                                                                     m.row_hi);
     else
       single2d_step_kernel<MODE, false><<<dim3(ibx, iby), dim3(32, kWarpsInterior), 0, s>>>(p, step, r, m);

@@ -139,8 +139,8 @@ def test_dft_monitor_matches_oracle_series(cuda_device):
 
 
 # Grids large enough for an interior rectangle of walk blocks (the golden
-# cases above are small enough that every block is a frame block): TMz with
-# an even ny runs the two-column interior walk, TMz with an odd ny and TEz the
+# cases above are small enough that every block is a frame block): an even
+# ny runs the two-column interior walk (TMz and TEz), an odd ny the
 # one-column one.  Sources sit on even and odd columns, on a pair's first and
 # last owned columns (74 and 135: the rectangle starts at column 12 for
 # CPML 10) and in the frame; probes sit beside the rectangle and on a pair
@@ -161,6 +161,10 @@ INTERIOR = [
       ("sin", 140, 90, 12e9, 0.3, "Ey")],
      [(150, 100), (170, 140), (20, 20)], "Hz", 40,
      [("circle", 140, 125, 35, 5.0, 1.0, 0.3, 0.0)]),
+    ("tez_odd_ny", "TEZ", 270, 251, 100, [("cpml", 10, 3, 1.0, 0.05, 1.0)],
+     [("gauss", 140, 101, 20e9, 1.0, 6.0, "Hz"), ("gauss", 170, 130, 15e9, 0.7, 5.0, "Ey")],
+     [(140, 101), (160, 140), (260, 240)], "Ex", 50,
+     [("circle", 135, 125, 30, 5.0, 1.0, 0.3, 0.0)]),
 ]
 
 
