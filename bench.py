@@ -2,7 +2,7 @@
 """Throughput of the batched multistatic FDTD path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload head600|disk200|head192]
+                    [--workload head600|disk200|head192|pack256|adjoint400|adjoint192|single4096]
 
 A bench "step" is one complete head-imaging sample: the 800-step fused FDTD
 time loop for 16 transmit events with a one-pole Debye phantom, the DFT of
