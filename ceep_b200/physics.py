@@ -133,9 +133,10 @@ def rdiv(num: float, t):
     """num / t elementwise with one correctly rounded division, as NumPy's
     scalar / array.  torch evaluates float / Tensor as reciprocal(t) * num,
     two roundings that differ from the quotient by an ulp in about a quarter
-    of FP64 elements."""
+    of FP64 elements.  The numerator is a 0-d tensor filled on t's device (no
+    host-to-device copy, so no wait for the stream)."""
     import torch
-    return torch.div(torch.tensor(num, dtype=t.dtype, device=t.device), t)
+    return torch.div(t.new_full((), num), t)
 
 
 def coefficient_tensors(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=None):
