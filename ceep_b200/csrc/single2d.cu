@@ -228,6 +228,7 @@ CEEP_D float cpml_e_y(const Single2dParams& p, int i, int c, float diff) {
 // 4 warps of 32 rows in the interior launch, 16 warps of 8 rows in the frame
 // launch (few blocks, so shorter walks keep its duration down).
 constexpr int kBlockRows = 128, kWarpsInterior = 4, kWarpsFrame = 16;
+constexpr int kInteriorRows = 128;  // rows of one interior block (kWarpsInterior walks)
 
 // Blocks of 31 columns x up to kBlockRows rows, split into an interior
 // rectangle -- columns [col_lo, col_hi) over rows [row_lo, row_hi), whose
@@ -255,8 +256,8 @@ CEEP_D void block_of(const BlockMap& m, int& j0, int& ce, int& rs, int& re) {
   if (!m.frame) {
     j0 = m.col_lo + blockIdx.x * 31;
     ce = m.col_hi;
-    rs = m.row_lo + blockIdx.y * kBlockRows;
-    re = min(rs + kBlockRows, m.row_hi);
+    rs = m.row_lo + blockIdx.y * kInteriorRows;
+    re = min(rs + kInteriorRows, m.row_hi);
     return;
   }
   ce = m.ny;
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(32 * kWarpsFrame) single2d_step_kernel(const S
   int j0, ce, rs, re;
   block_of(bm, j0, ce, rs, re);
   const int c = j0 - 1 + lane;
-  const int rows = kBlockRows / blockDim.y;
+  const int rows = (bm.frame ? kBlockRows : kInteriorRows) / blockDim.y;
   const int i0 = rs + threadIdx.y * rows;
   if (i0 >= re) return;  // whole warp
   const int i1 = min(i0 + rows, re);
@@ -456,8 +457,8 @@ __global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tmz_pair_kernel(
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
   const int j0 = col_lo + 62 * blockIdx.x;
   const int c = j0 - 2 + 2 * lane;
-  constexpr int rows = kBlockRows / kWarpsInterior;
-  const int i0 = row_lo + blockIdx.y * kBlockRows + threadIdx.y * rows;
+  constexpr int rows = kInteriorRows / kWarpsInterior;
+  const int i0 = row_lo + blockIdx.y * kInteriorRows + threadIdx.y * rows;
   if (i0 >= row_hi) return;  // whole warp
   const int i1 = min(i0 + rows, row_hi);
   const bool own = lane > 0;
@@ -528,8 +529,8 @@ __global__ void __launch_bounds__(32 * kWarpsInterior) single2d_tez_pair_kernel(
   const int lane = threadIdx.x, nx = p.nx, ny = p.ny;
   const int j0 = col_lo + 62 * blockIdx.x;
   const int c = j0 - 2 + 2 * lane;
-  constexpr int rows = kBlockRows / kWarpsInterior;
-  const int i0 = row_lo + blockIdx.y * kBlockRows + threadIdx.y * rows;
+  constexpr int rows = kInteriorRows / kWarpsInterior;
+  const int i0 = row_lo + blockIdx.y * kInteriorRows + threadIdx.y * rows;
   if (i0 >= row_hi) return;  // whole warp
   const int i1 = min(i0 + rows, row_hi);
   const bool own = lane > 0;
@@ -674,11 +675,12 @@ static cudaError_t step_t(const Single2dParams& p, int step, int r, cudaStream_t
   const int width = pair ? 62 : 31;
   BlockMap m = block_map(p, width);
   const int ibx = (m.col_hi - m.col_lo) / width;                            // interior strips
-  const int iby = (m.row_hi - m.row_lo + kBlockRows - 1) / kBlockRows;   // interior block rows
+  const int iby = (m.row_hi - m.row_lo + kInteriorRows - 1) / kInteriorRows;   // interior block rows
   const int interior = ibx * iby;
+  const int fby = (m.row_hi - m.row_lo + kBlockRows - 1) / kBlockRows;      // frame side block rows
   const int rest = (m.row_lo + kBlockRows - 1) / kBlockRows * m.gx +
                    (m.nx - m.row_hi + kBlockRows - 1) / kBlockRows * m.gx +
-                   iby * (side_blocks(m.col_lo) + side_blocks(m.ny - m.col_hi));
+                   fby * (side_blocks(m.col_lo) + side_blocks(m.ny - m.col_hi));
   const bool two = interior > 0 && rest > 0;
   cudaError_t e;
   if (two) {
