@@ -741,11 +741,13 @@ def run_adjoint3d_bench(args):
     del s2
     torch.cuda.empty_cache()
     ratios, mem, split = {}, {}, {}
-    for K in (25, 50, 100):
+    kept_ratios, kept_info = {}, {}
+    keep_budget = 64 << 30
+    for K, keep in ((25, 0), (50, 0), (100, 0), (25, keep_budget), (50, keep_budget)):
         torch.cuda.reset_peak_memory_stats(dev)
         sk = mk()
         sk.set_phantom(guess)
-        adj = Adjoint3D(sk, checkpoint_every=K)
+        adj = Adjoint3D(sk, checkpoint_every=K, keep_bytes=keep)
         e, g, d = f64(eps).requires_grad_(True), f64(sig).requires_grad_(True), f64(de).requires_grad_(True)
 
         def grad_step():
@@ -753,7 +755,16 @@ def run_adjoint3d_bench(args):
             p = probes_with_grad_3d(e, g, adj, d, f64(tau))
             loss, _ = s_parameter_loss(p.double(), sk.dt, freqs, target)
             loss.backward()
-        ratios[K] = timed(grad_step, 1) / t_fwd
+        r = timed(grad_step, 1) / t_fwd
+        if keep:
+            nseg = -(-T // K)
+            kept_ratios[K] = r
+            kept_info[K] = (f"{adj.kept_segments(nseg)} of {nseg} segments kept, peak "
+                            f"{torch.cuda.max_memory_allocated(dev) / 2 ** 30:.1f} GiB")
+            del adj, sk, e, g, d
+            torch.cuda.empty_cache()
+            continue
+        ratios[K] = r
         mem[K] = torch.cuda.max_memory_allocated(dev) / 2 ** 30
         if K == 50:
             gprobe = torch.randn((len(pos), len(pos), T), dtype=torch.float32, device=dev)
@@ -771,7 +782,9 @@ def run_adjoint3d_bench(args):
             "forward_ms": round(t_fwd, 3),
             "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()},
             "peak_device_gib_by_checkpoint_interval": {str(k): round(v, 1) for k, v in mem.items()},
-            "checkpoint50_split_ms": {k: round(v, 3) for k, v in split.items()}}
+            "checkpoint50_split_ms": {k: round(v, 3) for k, v in split.items()},
+            "ratio_with_keep_budget": {str(k): round(v, 3) for k, v in kept_ratios.items()},
+            "keep_budget": {"bytes": keep_budget, **{str(k): v for k, v in kept_info.items()}}}
     print(json.dumps(line), flush=True)
 
 

@@ -61,7 +61,7 @@ def interior_e(solver, field):
 class Adjoint3D:
     """Gradient driver for one ``BatchedFDTD3D`` (Debye poles only, CPML >= 2)."""
 
-    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50, overlap=None):
+    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50, overlap=None, keep_bytes: int = 0):
         if solver._lorentz:
             raise ValueError("the 3D adjoint supports Debye poles only")
         if solver.cpml_thickness < 1:
@@ -69,10 +69,14 @@ class Adjoint3D:
         self.s = solver
         self.K = max(1, int(checkpoint_every))
         self.overlap = overlap          # None: when a second segment buffer fits in free memory
+        # device bytes the forward pass may spend on keeping trailing segments
+        # (each saves its recompute in the backward pass); the last one is
+        # always kept
+        self.keep_bytes = max(0, int(keep_bytes))
+        self._kept, self._starts = set(), []
         self._params = None
         self._ckpt = {}
         self._segs = []
-        self._seg_ready = None          # segment start whose E slots the forward already stored
 
     # -- parameters -------------------------------------------------------------
     def set_parameters(self, eps_r, sigma, deps=None, tau=None) -> None:
@@ -127,6 +131,15 @@ class Adjoint3D:
     def _segment_shape(self):
         return (min(self.K, self.s.total_steps) + 1,) + save_slot_shape(self.s)
 
+    def segment_bytes(self):
+        """Device bytes of one segment buffer (interior E slots of K + 1 steps)."""
+        return 4 * int(np.prod(self._segment_shape()))
+
+    def kept_segments(self, nseg):
+        """How many trailing segments the forward pass keeps: the last one
+        always, more while their buffers fit in ``keep_bytes``."""
+        return max(1, min(nseg, self.keep_bytes // max(1, self.segment_bytes())))
+
     def _buffers(self, count):
         """`count` segment buffers, allocated once: the save graphs are keyed
         on their addresses."""
@@ -149,17 +162,20 @@ class Adjoint3D:
         s = self.s
         s.reset()
         T, K = s.total_steps, self.K
-        self._ckpt, self._seg_ready = {}, None
-        self._buffers(1)
-        stream = torch.cuda.current_stream(s.device)
+        self._ckpt = {}
         starts = list(range(0, T, K))
-        for a in starts:
+        M = self.kept_segments(len(starts))
+        self._buffers(M)
+        stream = torch.cuda.current_stream(s.device)
+        self._starts, self._kept = starts, set()
+        for j, a in enumerate(starts):
             b = min(a + K, T)
-            self._ckpt[a] = None if a == 0 else [t.clone() for t in self._ckpt_views()]
-            if a == starts[-1]:
-                self._run_save(a, b, 0, interior_only=False)
-                self._seg_ready = a
+            i = len(starts) - 1 - j                 # index in the backward order
+            if i < M:                               # kept: its slots stay in buffer i
+                self._run_save(a, b, i, interior_only=False)
+                self._kept.add(a)
             else:
+                self._ckpt[a] = None if a == 0 else [t.clone() for t in self._ckpt_views()]
                 s.advance(a, b - a, stream=stream)
         return s.probe_data[:, :len(s.probe_positions)].clone()
 
@@ -188,13 +204,14 @@ class Adjoint3D:
             gp.data_ptr()
         h = C.c_void_p()
         check(lib().ceep3d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep3d_adjoint_create")
-        starts = sorted(self._ckpt, reverse=True)
+        starts = sorted(self._starts, reverse=True)
+        M = len(self._kept)
         overlap = self.overlap
         if overlap is None:
-            seg_bytes = 4 * int(np.prod(self._segment_shape()))
-            overlap = len(self._segs) >= 2 or torch.cuda.mem_get_info(dev)[0] > 2 * seg_bytes
-        two = bool(overlap) and len(starts) > 1
-        self._buffers(2 if two else 1)
+            overlap = len(self._segs) >= 2 or torch.cuda.mem_get_info(dev)[0] > 2 * self.segment_bytes()
+        two = bool(overlap) and len(starts) > M
+        nbuf = max(M, 2 if two else 1)
+        self._buffers(nbuf)
 
         def recompute(a, buf):
             self._restore(a)
@@ -207,10 +224,9 @@ class Adjoint3D:
             check(lib().ceep3d_adjoint_run(h, b, b - a, self._segs[buf].data_ptr(), a, C.c_void_p(st.cuda_stream)),
                   "ceep3d_adjoint_run")
         try:
-            kept = set() if self._seg_ready is None else {self._seg_ready}
-            run_segments_backward(starts, kept, recompute, adjoint, dev, two, 2 if two else 1)
+            run_segments_backward(starts, self._kept, recompute, adjoint, dev, two, nbuf)
         finally:
-            self._seg_ready = None
+            self._kept = set()
             lib().ceep3d_adjoint_destroy(h)
         full = torch.zeros((ks, s.nz, s.ny, s.nx), dtype=torch.float64, device=dev)
         full[:, n + 1:s.nz - n, n + 1:s.ny - n, n + 1:s.nx - n] = grad.sum(0)

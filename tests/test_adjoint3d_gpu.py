@@ -178,3 +178,27 @@ def test_adjoint3d_overlapped_recompute_gives_the_same_gradient(cuda_device):
         (p.double() ** 2).sum().backward()
         res.append(e.grad.clone())
     assert torch.equal(res[0], res[1])
+
+
+def test_adjoint3d_kept_segments_give_the_same_gradient(cuda_device):
+    """Keeping 1, 3 or all trailing segments (``keep_bytes``), with and
+    without the two-stream backward, gives the same bits."""
+    from ceep_b200 import BatchedFDTD3D
+    from ceep_b200.adjoint3d import Adjoint3D, probes_with_grad_3d
+    eps, sig, de, tau, m, ring = _case(30, 28, 26, 10)
+    res = []
+    for keep in (0, 3, 99):
+        for overlap in (False, True):
+            s = BatchedFDTD3D(30, 28, 26, 1e-3, 75, 3, ring[:3], ring, 2e9)
+            s.set_dispersion(debye=[(de, tau)])
+            s._build()
+            adj = Adjoint3D(s, checkpoint_every=9, overlap=overlap)
+            adj.keep_bytes = keep * adj.segment_bytes()
+            e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+            p = probes_with_grad_3d(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                                    torch.tensor(tau, device="cuda"))
+            assert len(adj._ckpt) == 9 - min(9, max(1, keep))     # 9 segments of 9 steps (the last 3)
+            (p.double() ** 2).sum().backward()
+            res.append(e.grad.clone())
+    for r in res[1:]:
+        assert torch.equal(res[0], r)
