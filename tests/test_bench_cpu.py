@@ -58,3 +58,9 @@ def test_pack_cases_match_their_draws():
         assert c["phantom"] == ("lorentz" if k % 3 == 2 else "head")
     assert bench._pack_cases(12) == cases                      # seeded
     assert np.isclose(cases[0]["ring"], 0.36 * min(cases[0]["nx"], cases[0]["ny"]))
+
+
+def test_reference_arm_pack():
+    d = _bench("--workload", "pack256", "--pack-count", "6", "--steps", "1", "--warmup", "1", "--cpu-steps", "1")
+    _check_line(d, "packed uneven batch GCell-steps/s")
+    assert d["config"]["phantoms"] == 6 and d["config"]["sampled"] >= 1
