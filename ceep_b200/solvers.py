@@ -140,14 +140,20 @@ class BatchedFDTD2D:
         shp = (self.nx, self.ny)
         deb = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in debye]
         lor = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in lorentz]
+        # the cells outside the interior E region [n+1, nx-n) x [n+1, ny-n):
+        # two full-width row bands and two column bands between them
         n = self.cpml_n
-        inner = np.zeros(shp, bool)
-        inner[n + 1:self.nx - n, n + 1:self.ny - n] = True
+        a0, a1, b0, b1 = n + 1, max(self.nx - n, n + 1), n + 1, max(self.ny - n, n + 1)
+        outside = [(slice(0, a0), slice(None)), (slice(a1, None), slice(None)),
+                   (slice(a0, a1), slice(0, b0)), (slice(a0, a1), slice(b1, None))]
+
+        def present_outside(pole):
+            return any(np.any((pole[1][r] > 0) & (pole[0][r] != 0)) for r in outside)
         for p in deb:
-            if np.any((p[1] > 0) & (p[0] != 0) & ~inner):
+            if present_outside(p):
                 raise ValueError("Debye pole present outside the interior E region")
         for p in lor:
-            if np.any((p[1] > 0) & (p[0] != 0) & ~inner):
+            if present_outside(p):
                 raise ValueError("Lorentz pole present outside the interior E region")
         self._debye, self._lorentz = deb, lor
 
