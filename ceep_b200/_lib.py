@@ -54,6 +54,9 @@ _SIGS = {
     "ceep2d_plan_set_temporal_block": (C.c_int, [P, C.c_int]),
     "ceep2d_plan_temporal_block": (C.c_int, [P]),
     "ceep2d_plan_launches": (I64, [P, I64]),
+    "ceep2d_plan_set_sentinel": (C.c_int, [P, I32]),
+    "ceep2d_plan_set_wait_limit": (C.c_int, [P, C.c_uint64]),
+    "ceep2d_plan_inject_copy_fault": (C.c_int, [P, I32]),
     "ceep2d_plan_current_buffer": (C.c_int, [P]),
     "ceep2d_plan_reset": (C.c_int, [P]),
     "ceep2d_desc_size": (I64, []),

@@ -31,6 +31,7 @@ import torch
 
 from ._lib import check, lib
 from .constants import EPS_0
+from .distributed import allreduce_gradient
 from .physics import rdiv
 from .solvers import BatchedFDTD2D, _ptr
 
@@ -127,7 +128,11 @@ class Adjoint2D:
     the Debye currents of every step (one field less to write and read)."""
 
     def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False,
-                 overlap: bool = True, keep_bytes: int = 0):
+                 overlap: bool = True, keep_bytes: int = 0, reduce_ranks: bool = False):
+        """``reduce_ranks``: the solver holds this rank's transmit events only
+        (``distributed.split_sources``) and the loss covers those; the
+        gradient maps are summed over ranks (one all_reduce each), so every
+        rank returns the gradient of the whole loss."""
         if solver._lorentz:
             raise ValueError("the adjoint supports Debye poles only")
         self.s = solver
@@ -135,6 +140,7 @@ class Adjoint2D:
         self.grad_tau = bool(grad_tau)
         self.overlap = bool(overlap)
         self.keep_bytes = max(0, int(keep_bytes))
+        self.reduce_ranks = bool(reduce_ranks)
         self._kept = set()
         self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
@@ -300,7 +306,8 @@ class Adjoint2D:
             self._kept = set()
             lib().ceep2d_adjoint_destroy(h)
         # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
-        return self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])
+        res = self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])
+        return allreduce_gradient(res) if self.reduce_ranks else res
 
     def _chain(self, grad):
         """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""

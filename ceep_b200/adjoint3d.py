@@ -33,6 +33,7 @@ import torch
 from . import physics
 from ._lib import check, lib
 from .adjoint import coefficient_maps, run_segments_backward
+from .distributed import allreduce_gradient
 from .solvers import _ptr
 from .solvers3d import BatchedFDTD3D
 
@@ -61,7 +62,10 @@ def interior_e(solver, field):
 class Adjoint3D:
     """Gradient driver for one ``BatchedFDTD3D`` (Debye poles only, CPML >= 2)."""
 
-    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50, overlap=None, keep_bytes: int = 0):
+    def __init__(self, solver: BatchedFDTD3D, checkpoint_every: int = 50, overlap=None, keep_bytes: int = 0,
+                 reduce_ranks: bool = False):
+        """``reduce_ranks``: as for ``Adjoint2D`` (this rank's transmit events
+        only; gradient maps summed over ranks)."""
         if solver._lorentz:
             raise ValueError("the 3D adjoint supports Debye poles only")
         if solver.cpml_thickness < 1:
@@ -73,6 +77,7 @@ class Adjoint3D:
         # (each saves its recompute in the backward pass); the last one is
         # always kept
         self.keep_bytes = max(0, int(keep_bytes))
+        self.reduce_ranks = bool(reduce_ranks)
         self._kept, self._starts = set(), []
         self._params = None
         self._ckpt = {}
@@ -230,7 +235,8 @@ class Adjoint3D:
             lib().ceep3d_adjoint_destroy(h)
         full = torch.zeros((ks, s.nz, s.ny, s.nx), dtype=torch.float64, device=dev)
         full[:, n + 1:s.nz - n, n + 1:s.ny - n, n + 1:s.nx - n] = grad.sum(0)
-        return self._chain(full.permute(0, 3, 2, 1))          # (ks, nx, ny, nz)
+        res = self._chain(full.permute(0, 3, 2, 1))           # (ks, nx, ny, nz)
+        return allreduce_gradient(res) if self.reduce_ranks else res
 
     def _chain(self, grad):
         """Coefficient gradients -> parameter gradients, all (nx, ny, nz)."""

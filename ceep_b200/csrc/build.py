@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -48,12 +49,18 @@ def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) 
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
     if ptxas_info:
         flags += ["-Xptxas", "-v"]
-    for src in SOURCES:
+    def compile_one(src):
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
         cmd = [nvcc()] + flags + ["-c", os.path.join(HERE, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per source, in parallel (the translation units are independent)
+    workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as pool:
+        results = list(pool.map(compile_one, SOURCES))
+    for src, obj, r in results:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
         if ptxas_info:

@@ -41,6 +41,7 @@ struct ceep2d_plan {
   ceep::Fdtd2dParams p;
   int cur = 0;       // ping-pong buffer holding the current state
   int tblock = 1;    // steps per launch (1, or 2 with the temporal-block kernel)
+  int sentinel = 0;  // NaN/Inf check every this many steps (0: only at the end of each run range)
   // captured step loops keyed by (step0, nsteps, starting buffer, save buffers, save base, steps per launch)
   std::map<std::tuple<int64_t, int64_t, int, const void*, const void*, int64_t, int>, cudaGraphExec_t> graphs;
 };
@@ -111,6 +112,8 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   p.src_xy = d->src_xy; p.prb_xy = d->prb_xy; p.row_flags = d->row_flags;
   p.waveform = d->waveform; p.probes = d->probes;
   p.status = d->status;
+  p.fault_row = -1;
+  p.wait_ns = 1000000000ull;
   cudaError_t ce = ceep::fdtd2d_configure(p);
   if (ce != cudaSuccess) {
     delete pl;
@@ -125,8 +128,12 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
 // and writes the other.
 static int64_t launch_count(int64_t nsteps, int tblock) { return tblock == 2 ? (nsteps + 1) / 2 : nsteps; }
 
-static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, int tblock,
+// With a status word, the NaN/Inf sentinel scans the current Ez and the probe
+// samples recorded since its previous scan after every `sentinel` steps (0:
+// none in between) and after the range's last step.
+static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, int tblock, int sentinel,
                      cudaStream_t s) {
+  int64_t checked = step0;
   for (int64_t k = 0; k < nsteps;) {
     const bool two = tblock == 2 && k + 1 < nsteps;
     cudaError_t e = two ? ceep::fdtd2d_launch_step2(p, (int)(step0 + k), cur, s)
@@ -134,8 +141,22 @@ static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps,
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd2d step launch");
     k += two ? 2 : 1;
     cur ^= 1;
+    const int64_t done = step0 + k;
+    if (p.status && (k == nsteps || (sentinel > 0 && done / sentinel != checked / sentinel))) {
+      e = ceep::finite_check_launch(p.ez[cur], p.groups * p.gs_field, p.probes, p.ntx, p.nprobe, p.nsteps,
+                                    (int)checked, (int)done, p.status, s);
+      if (e != cudaSuccess) return ceep::cuda_fail(e, "finite_check_kernel launch");
+      checked = done;
+    }
   }
   return CEEP_OK;
+}
+
+// Captured step loops hold the kernel parameters of their capture: drop them
+// when a setting that the launches carry changes.
+static void drop_graphs(ceep2d_plan* pl) {
+  for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  pl->graphs.clear();
 }
 
 static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream, int use_graph, float* save_ez,
@@ -154,7 +175,7 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
   const int cur = pl->cur;
   const int cur_after = cur ^ (int)(launch_count(nsteps, pl->tblock) & 1);
   if (!use_graph || s == nullptr) {
-    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, s);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s);
     if (rc == CEEP_OK) pl->cur = cur_after;
     return rc;
   }
@@ -164,7 +185,7 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, s);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -222,6 +243,28 @@ extern "C" int ceep2d_plan_set_temporal_block(ceep2d_plan* pl, int steps) {
 }
 
 extern "C" int ceep2d_plan_temporal_block(const ceep2d_plan* pl) { return pl ? pl->tblock : 0; }
+
+extern "C" int ceep2d_plan_set_sentinel(ceep2d_plan* pl, int32_t interval) {
+  if (!pl || interval < 0) return fail(CEEP_ERR_INVALID, "ceep2d_plan_set_sentinel: bad plan or interval %d", interval);
+  if (interval != pl->sentinel) drop_graphs(pl);
+  pl->sentinel = interval;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_set_wait_limit(ceep2d_plan* pl, uint64_t ns) {
+  if (!pl || ns == 0) return fail(CEEP_ERR_INVALID, "ceep2d_plan_set_wait_limit: bad plan or zero limit");
+  if (ns != pl->p.wait_ns) drop_graphs(pl);
+  pl->p.wait_ns = ns;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_inject_copy_fault(ceep2d_plan* pl, int32_t row) {
+  if (!pl || row < -1 || row >= pl->p.ny)
+    return fail(CEEP_ERR_INVALID, "ceep2d_plan_inject_copy_fault: bad plan or row %d", row);
+  if (row != pl->p.fault_row) drop_graphs(pl);
+  pl->p.fault_row = row;
+  return CEEP_OK;
+}
 
 extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
   return (!pl || nsteps < 0) ? 0 : launch_count(nsteps, pl->tblock);

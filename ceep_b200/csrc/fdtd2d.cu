@@ -61,7 +61,9 @@ constexpr int kConsumers = 128;
 #endif
 constexpr int kStages = CEEP_STAGES;
 constexpr int kMaxRows = 64;                        // rows per block (row masks are 64-bit)
-constexpr uint64_t kWaitLimitNs = 1000000000ull;    // 1 s
+constexpr uint64_t kWaitLimitNs = 1000000000ull;    // default bound of a wait: 1 s
+
+CEEP_D uint64_t wait_limit(const Fdtd2dParams& p) { return p.wait_ns ? p.wait_ns : kWaitLimitNs; }
 
 template <int L, int NP, int NL>
 struct Stage2d {
@@ -300,11 +302,15 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   int issued = 0;
   for (int k = 0; k < nslots; ++k) {
     const int s = k % NS, u = k / NS;
-    if (u > 0 && !mbar_wait_bounded(&empty[s], (u - 1) & 1, kWaitLimitNs)) {
+    if (u > 0 && !mbar_wait_bounded(&empty[s], (u - 1) & 1, wait_limit(p))) {
       record_status(p.status, CEEP_ERR_TIMEOUT);
       break;
     }
     const int r = rs + k;
+    if (r == p.fault_row) {  // injected fault: this slot never fills
+      issued = k + 1;
+      continue;
+    }
     const bool pro = r < y0, tail = r >= y1, body = !pro && !tail;
     const int shy = sp.hy_row(r), sey = sp.ey_row(r);
     Stage2d<L, NP, NL>& S = st[s];
@@ -347,7 +353,7 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   // Let every copy this thread issued land before it leaves (only matters on
   // the timeout path: otherwise the consumers have waited on all of them).
   for (int k = issued > NS ? issued - NS : 0; k < issued; ++k)
-    mbar_wait_bounded(&full[k % NS], (k / NS) & 1, kWaitLimitNs);
+    mbar_wait_bounded(&full[k % NS], (k / NS) & 1, wait_limit(p));
 }
 
 // ------------------------------------------------------------------------
@@ -390,7 +396,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
 
   // Warp-uniform bounded wait: if any lane gives up, the whole warp leaves.
   auto wait = [&](int k) {
-    const bool ok = mbar_wait_bounded(&full[k % kStages], (k / kStages) & 1, kWaitLimitNs);
+    const bool ok = mbar_wait_bounded(&full[k % kStages], (k / kStages) & 1, wait_limit(p));
     if (__any_sync(0xffffffffu, !ok)) {
       if (lane_warp == 0) record_status(p.status, CEEP_ERR_TIMEOUT);
       return false;
@@ -613,7 +619,7 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
   bool aborted = false;
   auto wait = [&](int k) {
     if (aborted) return;
-    const bool ok = mbar_wait_bounded(&full[k % kStages2], (k / kStages2) & 1, kWaitLimitNs);
+    const bool ok = mbar_wait_bounded(&full[k % kStages2], (k / kStages2) & 1, wait_limit(p));
     if (__any_sync(0xffffffffu, !ok)) {
       if (lane_warp == 0) {
         record_status(p.status, CEEP_ERR_TIMEOUT);
@@ -1014,6 +1020,36 @@ cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTi
 }
 
 int fdtd2d_cells_per_block(int L) { return kConsumers / L; }
+
+// NaN/Inf sentinel: grid-stride scans of Ez and of the probe samples of steps
+// [s0, s1); x != x is true only for NaN, and |x| > FLT_MAX only for Inf.
+__global__ void __launch_bounds__(256) finite_check_kernel(const float4* __restrict__ ez, long long nf4,
+                                                           const float* __restrict__ probes, int ntx, int nprobe,
+                                                           int nsteps, int s0, int s1, int* status) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false;
+  for (long long i = t0; i < nf4; i += stride) {
+    const float4 v = ez[i];
+    const float m = fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+    bad |= !(m <= 3.4028235e38f);  // false for NaN and Inf
+  }
+  const int w = s1 - s0;
+  const long long np = (long long)ntx * nprobe * (w > 0 ? w : 0);
+  for (long long i = t0; i < np; i += stride) {
+    const long long row = i / w;
+    const float v = probes[row * nsteps + s0 + i % w];
+    bad |= !(fabsf(v) <= 3.4028235e38f);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) record_status(status, CEEP_ERR_NONFINITE);
+}
+
+cudaError_t finite_check_launch(const float4* ez, long long nf4, const float* probes, int ntx, int nprobe,
+                                int nsteps, int s0, int s1, int* status, cudaStream_t s) {
+  if (!status) return cudaSuccess;
+  finite_check_kernel<<<2 * 148, 256, 0, s>>>(ez, nf4, probes, ntx, nprobe, nsteps, s0, s1, status);
+  return cudaGetLastError();
+}
 
 // what: 0 = configure, 1 = one step, 2 = two steps
 template <int L, int ND, int NL>

@@ -43,7 +43,18 @@ struct Fdtd2dParams {
   float4* save_ez;
   float4* save_j;
   int save_base;
+  // Failure injection for tests of the bounded waits: the producer of every
+  // block issues no copies (and no arrival) for this row, so the waits on it
+  // expire.  -1 = none (the default).
+  int fault_row;
+  // Bound of every mbarrier wait, in ns of the global timer (0 = 1 s).
+  unsigned long long wait_ns;
 };
+
+// Scan Ez (nf4 float4) and probes[tx][q][steps s0..s1) for NaN/Inf; on a hit
+// record CEEP_ERR_NONFINITE in *status (first error wins).
+cudaError_t finite_check_launch(const float4* ez, long long nf4, const float* probes, int ntx, int nprobe,
+                                int nsteps, int s0, int s1, int* status, cudaStream_t s);
 
 // One tile of a packed multi-phantom launch.
 struct PackTile {

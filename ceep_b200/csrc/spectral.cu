@@ -69,10 +69,21 @@ __global__ void __launch_bounds__(256) dft_kernel(const float* __restrict__ seri
 // --------------------------------------------------------------------------
 constexpr int kDasThreads = 128;
 constexpr int kDasMaxAnt = 32;
+// Largest image (pixels) the image kernels take: pixel indices are int, and
+// the last block's thread indices must stay below INT_MAX too.
+constexpr int64_t kMaxPixels = int64_t(1) << 30;
 
-static int das_chunks(int npix, int nfreq) {
-  const int pixblocks = (npix + kDasThreads - 1) / kDasThreads;
-  int chunks = (2 * 148 + pixblocks - 1) / pixblocks;
+// Pixel count of an nx x ny image formed in 64 bits; -1 when either side is
+// below 1 or the count exceeds kMaxPixels.
+static int64_t pixel_count(int32_t nx, int32_t ny) {
+  if (nx < 1 || ny < 1) return -1;
+  const int64_t n = (int64_t)nx * (int64_t)ny;
+  return n > kMaxPixels ? -1 : n;
+}
+
+static int das_chunks(int64_t npix, int nfreq) {
+  const int64_t pixblocks = (npix + kDasThreads - 1) / kDasThreads;
+  int chunks = (int)((2 * 148 + pixblocks - 1) / pixblocks);
   if (chunks > nfreq) chunks = nfreq;
   if (chunks < 1) chunks = 1;
   return chunks;
@@ -316,8 +327,8 @@ extern "C" int ceep_dft(const float* series, const float* twiddle, float* s_out,
 }
 
 extern "C" int64_t ceep_das_workspace_bytes(int32_t nx_pix, int32_t ny_pix, int32_t nfreq) {
-  if (nx_pix < 1 || ny_pix < 1 || nfreq < 1) return 0;
-  const int npix = nx_pix * ny_pix;
+  const int64_t npix = ceep::pixel_count(nx_pix, ny_pix);
+  if (npix < 0 || nfreq < 1) return 0;
   return (int64_t)ceep::das_chunks(npix, nfreq) * npix * (int64_t)sizeof(float2);
 }
 
@@ -329,6 +340,9 @@ extern "C" int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
     return fail(CEEP_ERR_INVALID, "ceep_das: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix, ny_pix);
   if (nant > ceep::kDasMaxAnt)
     return fail(CEEP_ERR_UNSUPPORTED, "ceep_das: %d antennas (at most %d)", nant, ceep::kDasMaxAnt);
+  if (ceep::pixel_count(nx_pix, ny_pix) < 0)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_das: image %dx%d exceeds %lld pixels", nx_pix, ny_pix,
+                (long long)ceep::kMaxPixels);
   const int npix = nx_pix * ny_pix;
   const int chunks = ceep::das_chunks(npix, nfreq);
   const int fpc = (nfreq + chunks - 1) / chunks;
@@ -363,7 +377,8 @@ extern "C" int ceep_das(const float* s, const float* kfreq, const float* ant_xy,
 }
 
 extern "C" int64_t ceep_dmas_workspace_bytes(int32_t nx_pix, int32_t ny_pix) {
-  return nx_pix > 0 && ny_pix > 0 ? (int64_t)nx_pix * ny_pix * (int64_t)sizeof(float2) : 0;
+  const int64_t npix = ceep::pixel_count(nx_pix, ny_pix);
+  return npix > 0 ? npix * (int64_t)sizeof(float2) : 0;
 }
 
 extern "C" int ceep_dmas(const float* s, const float* kfreq, const float* ant_xy, int32_t nfreq, int32_t nant,
@@ -374,6 +389,9 @@ extern "C" int ceep_dmas(const float* s, const float* kfreq, const float* ant_xy
     return fail(CEEP_ERR_INVALID, "ceep_dmas: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix, ny_pix);
   if (nant > ceep::kDmasMaxAnt)
     return fail(CEEP_ERR_UNSUPPORTED, "ceep_dmas: %d antennas (at most %d)", nant, ceep::kDmasMaxAnt);
+  if (ceep::pixel_count(nx_pix, ny_pix) < 0)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_dmas: image %dx%d exceeds %lld pixels", nx_pix, ny_pix,
+                (long long)ceep::kMaxPixels);
   const int npix = nx_pix * ny_pix;
   const int K = nant * nant;
   const int threads = ((K + 31) / 32) * 32;
@@ -394,6 +412,9 @@ extern "C" int ceep_das_time(const float* s, const double* ant_xy, int32_t nant,
   if (!s || !ant_xy || !image) return fail(CEEP_ERR_INVALID, "ceep_das_time: null pointer");
   if (nant < 1 || ntime < 1 || grid < 1 || !(frequency > 0))
     return fail(CEEP_ERR_INVALID, "ceep_das_time: sizes nant=%d ntime=%d grid=%d", nant, ntime, grid);
+  if (ceep::pixel_count(grid, grid) < 0)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_das_time: image %dx%d exceeds %lld pixels", grid, grid,
+                (long long)ceep::kMaxPixels);
   const double dt = 1.0 / (4.0 * frequency);
   const int npix = grid * grid;
   ceep::das_time_kernel<<<(npix + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
@@ -421,6 +442,12 @@ extern "C" int ceep_das_time(const float* s, const double* ant_xy, int32_t nant,
 //    address is looked up with cudaGetSymbolAddress on the first call made
 //    on each device (with that device current) and cached.  That first call
 //    therefore does set-up work and should be made before any stream capture.
+//    With lazy module loading (the CUDA 12.2+ default) the array is made
+//    resident by that first call too, so a host that reserves all of its GPU
+//    memory up front makes one call first (or sets CUDA_MODULE_LOADING=EAGER).
+//  * A call that fails with a CUDA error drops the cached address, so the
+//    next call looks it up again (after a device reset the module, and with
+//    it the array, can move).
 //  * Every call on a device shares the one array.  Two calls whose kernels
 //    overlap on the GPU (different streams, no ordering between them) race
 //    on it and give wrong images; order them on one stream or serialise them.
@@ -450,6 +477,9 @@ extern "C" int ceep_das_noalloc(const float* s, const float* kfreq, const float*
   if (nfreq < 1 || nant < 1 || nx_pix < 1 || ny_pix < 1)
     return fail(CEEP_ERR_INVALID, "ceep_das_noalloc: sizes nfreq=%d nant=%d image %dx%d", nfreq, nant, nx_pix,
                 ny_pix);
+  if (ceep::pixel_count(nx_pix, ny_pix) < 0)
+    return fail(CEEP_ERR_UNSUPPORTED, "ceep_das_noalloc: image %dx%d exceeds %lld pixels", nx_pix, ny_pix,
+                (long long)ceep::kMaxPixels);
   const int64_t need = ceep_das_workspace_bytes(nx_pix, ny_pix, nfreq) / (int64_t)sizeof(float2);
   if (need > ceep::kDasNoAllocScratch)
     return fail(CEEP_ERR_UNSUPPORTED,
@@ -471,5 +501,11 @@ extern "C" int ceep_das_noalloc(const float* s, const float* kfreq, const float*
     }
     scratch = g_das_scratch_ptr[dev];
   }
-  return ceep_das(s, kfreq, ant_xy, nfreq, nant, nx_pix, ny_pix, px0, py0, pix, normalize, scratch, image, stream);
+  const int rc = ceep_das(s, kfreq, ant_xy, nfreq, nant, nx_pix, ny_pix, px0, py0, pix, normalize, scratch, image,
+                          stream);
+  if (rc == CEEP_ERR_CUDA) {
+    std::lock_guard<std::mutex> lock(g_das_scratch_mu);
+    g_das_scratch_ptr[dev] = nullptr;
+  }
+  return rc;
 }

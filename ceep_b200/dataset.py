@@ -41,6 +41,7 @@ import torch
 
 from . import physics
 from ._lib import check, lib
+from .distributed import gather_objects, shard, world
 from .packed import PackedBatch2D
 from .phantoms import ring_positions
 from .solvers import BatchedFDTD2D
@@ -163,21 +164,29 @@ def generate_dataset(n_samples: int = 100, output_dir: str = "dataset_corrected"
                      total_steps: Optional[int] = None, seed: int = 0, batch: int = 128, device="cuda",
                      write: bool = True) -> dict:
     """Generate the dataset in batches of `batch` packed samples; returns the
-    dataset metadata (also written as dataset_metadata.json)."""
+    dataset metadata (also written as dataset_metadata.json).
+
+    Under torch.distributed (one process per GPU) every rank draws the same
+    sample specs and simulates and writes its contiguous share of them
+    (``distributed.shard``); the per-sample magnitudes and the slowest rank's
+    time are gathered, so every rank returns the whole dataset's metadata and
+    rank 0 writes it.  Samples never cross ranks: no collective touches the
+    simulation."""
+    rank, size = world()
     out = Path(output_dir)
     if write:
         for sub in ("s_matrix", "eps_map", "hem_mask", "metadata"):
             (out / sub).mkdir(parents=True, exist_ok=True)
-    specs = draw_samples(n_samples, hemorrhage_ratio, seed)
+    specs = shard(draw_samples(n_samples, hemorrhage_ratio, seed), rank, size)
     mags, t0 = [], time.perf_counter()
     T = None
-    for b0 in range(0, n_samples, batch):
+    for b0 in range(0, len(specs), batch):
         chunk = specs[b0:b0 + batch]
         eps, sig, mask, series, T = simulate_batch(chunk, nx, ny, dx, frequency, n_ant, total_steps,
                                                    device=device)
         series_h, eps_h, mask_h = series.cpu().numpy(), eps.cpu().numpy(), mask.cpu().numpy()
         for k, spec in enumerate(chunk):
-            mags.append(float(np.abs(series_h[k]).max()))
+            mags.append((spec.sample_id, float(np.abs(series_h[k]).max())))
             if write:
                 name = f"sample_{spec.sample_id:06d}"
                 np.save(out / "s_matrix" / f"{name}.npy", series_h[k])
@@ -186,7 +195,11 @@ def generate_dataset(n_samples: int = 100, output_dir: str = "dataset_corrected"
                 with open(out / "metadata" / f"{name}.json", "w") as f:
                     json.dump(sample_metadata(spec, nx, ny, dx, frequency, n_ant, T), f, indent=2)
     elapsed = time.perf_counter() - t0
-    m = np.array(mags)
+    gathered = gather_objects((mags, T, elapsed))
+    mags = sorted(m for part, _, _ in gathered for m in part)
+    T = next((t for _, t, _ in gathered if t is not None), T)
+    elapsed = max(e for _, _, e in gathered)
+    m = np.array([v for _, v in mags])
     expected = 3.368  # the MEEP-validated magnitude the reference checks against (:262-266)
     meta = {
         "n_samples": n_samples,
@@ -203,7 +216,9 @@ def generate_dataset(n_samples: int = 100, output_dir: str = "dataset_corrected"
         "generation_seconds": elapsed,
         "samples_per_second": n_samples / elapsed if elapsed > 0 else None,
     }
-    if write:
+    if size > 1:
+        meta["ranks"] = size
+    if write and rank == 0:
         with open(out / "dataset_metadata.json", "w") as f:
             json.dump(meta, f, indent=2)
     return meta

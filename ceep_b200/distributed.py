@@ -8,9 +8,18 @@ over NCCL on NVLink for the few collectives it needs):
 * ``gather_tx_split``     reassemble S[f, rx, tx] (or probe series) of a phantom
                           whose transmit events were split across ranks;
 * ``allreduce_gradient``  sum per-rank gradient maps of a TX-split adjoint;
-* ``max_time_ms``         the slowest rank's device time, for throughput.
+* ``max_time_ms``         the slowest rank's device time, for throughput;
+* ``split_sources`` / ``local_columns``  this rank's transmit events of a
+                          solver and the matching columns of a full S target;
+* ``sum_over_ranks`` / ``gather_objects``  reduce a loss value, collect
+                          per-rank host results (dataset statistics).
 
-None of these touches the data path inside a time step.
+The product uses them in three places: ``Adjoint2D`` / ``Adjoint3D`` with
+``reduce_ranks=True`` (a TX-split gradient: each rank's loss covers its own
+transmit events, one all_reduce of the gradient maps), ``generate_dataset``
+(samples sharded over ranks, statistics gathered) and ``bench.py --gpus N``
+(phantoms sharded over ranks).  None of these touches the data path inside a
+time step.
 """
 from __future__ import annotations
 
@@ -90,3 +99,43 @@ def max_time_ms(ms: float, device=None) -> float:
     t = torch.tensor([ms], dtype=torch.float64, device=device or "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def split_sources(positions: Sequence, rank: int = None, size: int = None):
+    """This rank's contiguous block of transmit events: (positions, tx range).
+    A solver built with these sources and every probe gives this rank's
+    columns S[:, :, tx_range] of the full multistatic matrix."""
+    if rank is None or size is None:
+        rank, size = world()
+    r = tx_range(len(positions), rank, size)
+    return [positions[i] for i in r], r
+
+
+def local_columns(target: torch.Tensor, ntx: int, axis: int = -1, rank: int = None, size: int = None):
+    """The slice of a full per-TX array (S target, probe series) along `axis`
+    that belongs to this rank's transmit events."""
+    if rank is None or size is None:
+        rank, size = world()
+    r = tx_range(ntx, rank, size)
+    idx = [slice(None)] * target.dim()
+    idx[axis] = slice(r.start, r.stop)
+    return target[tuple(idx)]
+
+
+def sum_over_ranks(value: torch.Tensor) -> torch.Tensor:
+    """Sum of a tensor over ranks (a copy; the input is not modified)."""
+    rank, size = world()
+    out = value.detach().clone()
+    if size > 1:
+        dist.all_reduce(out, op=dist.ReduceOp.SUM)
+    return out
+
+
+def gather_objects(obj) -> List:
+    """Every rank's `obj` (picklable), in rank order, on every rank."""
+    rank, size = world()
+    if size == 1:
+        return [obj]
+    out = [None] * size
+    dist.all_gather_object(out, obj)
+    return out

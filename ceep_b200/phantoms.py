@@ -120,10 +120,30 @@ class LorentzHeadPhantom2D(HeadPhantom2D):
 
 
 def ring_positions(n_ant: int, center: tuple, radius: float):
-    """Antenna grid positions on a circle with int() truncation, as
-    scripts/generate_corrected_dataset.py:121-129 and arrays.py:114-124 do."""
+    """Antenna grid positions of the dataset generator's circle
+    (scripts/generate_corrected_dataset.py:121-129): angles from
+    np.linspace(0, 2 pi, n, endpoint=False), radius in cells, int()
+    truncation."""
     ang = np.linspace(0, 2 * np.pi, n_ant, endpoint=False)
     return [(int(center[0] + radius * np.cos(a)), int(center[1] + radius * np.sin(a))) for a in ang]
+
+
+def circular_array_positions(num_antennas: int, radius_mm: float, center: tuple, dx: float):
+    """Antenna grid positions of ``CircularArray`` (src/ceep/antennas/arrays.py:
+    110-143): angle 2 pi i / n, offset radius_m cos(angle) / dx (radius in
+    metres), int() truncation; a third centre coordinate is carried through.
+    The angle and the division by dx are formed as there, so the truncation
+    lands on the same cell (ring_positions can differ by one cell where
+    r cos(angle) is within an ulp of an integer)."""
+    radius = radius_mm * 1e-3
+    out = []
+    for i in range(num_antennas):
+        angle = 2 * np.pi * i / num_antennas
+        x_off = radius * np.cos(angle) / dx
+        y_off = radius * np.sin(angle) / dx
+        pos = (int(center[0] + x_off), int(center[1] + y_off))
+        out.append(pos + ((int(center[2]),) if len(center) == 3 else ()))
+    return out
 
 
 @dataclass

@@ -41,6 +41,17 @@ def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
     return None if t is None else t.data_ptr()
 
 
+class FDTDStatusError(RuntimeError):
+    """A device status word reported a failure: CEEP_ERR_TIMEOUT (4, a bounded
+    wait ran out) or CEEP_ERR_NONFINITE (5, the sentinel found NaN/Inf)."""
+    TIMEOUT, NONFINITE = 4, 5
+
+    def __init__(self, code: int):
+        what = {4: "a bounded device wait expired", 5: "a NaN/Inf value was found by the sentinel"}
+        super().__init__(f"fused step reported status {code} ({what.get(code, 'unknown')})")
+        self.code = code
+
+
 class BatchedFDTD2D:
     """Batched 2D TMz FDTD, one transmit event per batch element, shared materials.
 
@@ -75,6 +86,8 @@ class BatchedFDTD2D:
         self.rows_per_block = int(rows_per_block)
         self.use_graph = bool(use_graph)
         self.temporal_block = int(temporal_block)   # steps per kernel launch (1 or 2)
+        self.sentinel_interval = 0                   # NaN/Inf scans between run-range ends (0: none)
+        self.wait_limit_ns = 1_000_000_000           # bound of every device wait
         self._built = False
         self._plan = None
         self._validate()
@@ -225,8 +238,14 @@ class BatchedFDTD2D:
         plan = C.c_void_p()
         check(lib().ceep2d_plan_create(C.byref(d), C.byref(plan)), "ceep2d_plan_create")
         self._plan = plan
-        check(lib().ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
+        self._apply_plan_settings()
         self._built = True
+
+    def _apply_plan_settings(self):
+        h, plan = lib(), self._plan
+        check(h.ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
+        check(h.ceep2d_plan_set_sentinel(plan, self.sentinel_interval), "ceep2d_plan_set_sentinel")
+        check(h.ceep2d_plan_set_wait_limit(plan, self.wait_limit_ns), "ceep2d_plan_set_wait_limit")
 
     def __del__(self):
         if getattr(self, "_plan", None) is not None:
@@ -248,7 +267,7 @@ class BatchedFDTD2D:
         plan = C.c_void_p()
         check(lib().ceep2d_plan_create(C.byref(self._desc), C.byref(plan)), "ceep2d_plan_create")
         self._plan = plan
-        check(lib().ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
+        self._apply_plan_settings()
         self.reset()
 
     def set_temporal_block(self, steps: int) -> None:
@@ -260,6 +279,32 @@ class BatchedFDTD2D:
         if self._built:
             check(lib().ceep2d_plan_set_temporal_block(self._plan, self.temporal_block),
                   "ceep2d_plan_set_temporal_block")
+
+    def set_sentinel(self, interval: int) -> None:
+        """NaN/Inf sentinel: scan Ez and the new probe samples every
+        `interval` steps as well as after every run range (0, the default:
+        only after every run range).  A hit makes ``run()`` raise."""
+        if interval < 0:
+            raise ValueError("sentinel interval must be >= 0")
+        self.sentinel_interval = int(interval)
+        if self._built:
+            check(lib().ceep2d_plan_set_sentinel(self._plan, self.sentinel_interval), "ceep2d_plan_set_sentinel")
+
+    def set_wait_limit(self, ns: int) -> None:
+        """Bound of the step kernels' device waits in ns (default 1 s)."""
+        if ns <= 0:
+            raise ValueError("wait limit must be positive")
+        self.wait_limit_ns = int(ns)
+        if self._built:
+            check(lib().ceep2d_plan_set_wait_limit(self._plan, self.wait_limit_ns), "ceep2d_plan_set_wait_limit")
+
+    def inject_copy_fault(self, row: int) -> None:
+        """Failure injection for tests: the step kernels copy nothing for grid
+        row `row`, so their bounded waits run out (-1 turns it off).  The
+        state afterwards is not a simulation state; use a fresh solver."""
+        if not self._built:
+            self._build()
+        check(lib().ceep2d_plan_inject_copy_fault(self._plan, int(row)), "ceep2d_plan_inject_copy_fault")
 
     def launches(self, nsteps: Optional[int] = None) -> int:
         """Kernel launches that advancing `nsteps` steps (default: all) issues."""
@@ -339,12 +384,13 @@ class BatchedFDTD2D:
         return self._ref_view(self._hy[self._cur()]) if self._built else None
 
     def check_status(self) -> None:
-        """Raise if a bounded device wait gave up during an earlier launch."""
+        """Raise if a bounded device wait gave up, or the NaN/Inf sentinel
+        found a non-finite value, during an earlier launch."""
         if self._built:
             code = int(self._status.item())
             if code:
                 self._status.zero_()
-                raise RuntimeError(f"fused step reported status {code} (bounded wait expired)")
+                raise FDTDStatusError(code)
 
     def reset(self) -> None:
         """Zero every field, psi and ADE state (not in the reference: lets one

@@ -107,8 +107,28 @@ int ceep2d_launches_per_step(const ceep2d_plan* plan);
  * A new plan uses 1; the Python solver sets 2. */
 int ceep2d_plan_set_temporal_block(ceep2d_plan* plan, int steps);
 int ceep2d_plan_temporal_block(const ceep2d_plan* plan);
-/* Kernel launches a ceep2d_plan_run of `nsteps` steps issues. */
+/* Kernel launches a ceep2d_plan_run of `nsteps` steps issues (step kernels
+ * only; the NaN/Inf sentinel's scans are not counted). */
 int64_t ceep2d_plan_launches(const ceep2d_plan* plan, int64_t nsteps);
+/* NaN/Inf sentinel.  Replaces the reference's after-the-fact check
+ * `np.all(np.isfinite(signal))` (tests/test_fdtd_3d_batched.py:240-244)
+ * with a device scan: when the plan has a status word, a small kernel scans
+ * the current Ez and the probe samples recorded since its last scan, after
+ * every `interval` steps and after the last step of every run range
+ * (interval 0, the default: only the latter), and records
+ * CEEP_ERR_NONFINITE in the status word on a NaN or Inf. */
+int ceep2d_plan_set_sentinel(ceep2d_plan* plan, int32_t interval);
+/* Bound of every mbarrier wait of the step kernels, in ns (default 1 s).  A
+ * wait that runs out records CEEP_ERR_TIMEOUT in the status word and the
+ * block leaves after its copies in flight have landed (no counterpart in
+ * the reference, whose CuPy kernels have no device waits). */
+int ceep2d_plan_set_wait_limit(ceep2d_plan* plan, uint64_t ns);
+/* Failure injection for tests of the bounded waits (no counterpart in the
+ * reference): the producer of every block issues no copies for grid row
+ * `row`, so the consumers' waits on that row run out after the wait limit
+ * and the launch reports CEEP_ERR_TIMEOUT.  The state it leaves is not a
+ * valid simulation state.  -1 (the default) turns it off. */
+int ceep2d_plan_inject_copy_fault(ceep2d_plan* plan, int32_t row);
 /* Which ping-pong buffer (0 or 1) holds the current state; reset sets it to 0
  * (the caller zeroes the state buffers). */
 int ceep2d_plan_current_buffer(const ceep2d_plan* plan);
@@ -396,8 +416,13 @@ int ceep_dmas(const float* s, const float* kfreq, const float* ant_xy,
  * library (ceep_das_noalloc_capacity() complex entries) that every GPU which
  * loads the library keeps until exit.  Larger problems are rejected with
  * CEEP_ERR_UNSUPPORTED.  The first call on a device looks up the array's
- * device address (make it before any stream capture); calls that overlap on
- * the GPU share the array and race.  Calls no allocating routine.
+ * device address (make it before any stream capture).  With lazy module
+ * loading (the CUDA 12.2+ default) the array becomes resident only at that
+ * first call, so make it before the host reserves its memory pool, or set
+ * CUDA_MODULE_LOADING=EAGER.  Calls that overlap on the GPU share the array
+ * and race.  The cached address is dropped when a call fails with a CUDA
+ * error; no call may follow a device reset without such a failure first.
+ * Calls no allocating routine.
  * ---------------------------------------------------------------------- */
 int64_t ceep_das_noalloc_capacity(void);
 int ceep_das_noalloc(const float* s, const float* kfreq, const float* ant_xy,

@@ -34,6 +34,15 @@ brain_phantom     BrainPhantom2D.get_eps_map (fixed tissue table) for a
                   head-sized 400x380 grid with and without hemorrhage, and
                   the 64x64 dataset-generator grid; hemorrhage masks as
                   scripts/generate_corrected_dataset.py builds them
+head600_ref_*     BatchedFDTD2D.run() at 600x600, 16 TX, 800 steps, CPML 15
+                  on the seeded head phantom's non-dispersive maps, FP32
+                  and FP64 (about 7 minutes each on one core)
+head600_oracle    the oracle (FP64) on the same phantom with its Debye poles:
+                  probes, S at 301 frequencies, 64x64 DAS image
+head192_oracle    the 3D oracle (FP64) at 192^3, 1000 steps, CPML 10, Debye
+                  shells with an inclusion; 4 of the 8 TX (spawn workers)
+positions         antenna positions of CircularArray and of the dataset
+                  generator's circle
 """
 from __future__ import annotations
 
@@ -382,7 +391,156 @@ def gen_single2d():
     _save("single2d", **out)
 
 
+# Full-size cases at the benchmarked configurations.  Their inputs are the
+# seeded synthetic phantoms of ceep_b200.phantoms (pure NumPy); the SHA-256 of
+# every input map is stored with the outputs, so a test can tell a changed
+# phantom generator from a changed solver.
+HEAD600 = dict(nx=600, ny=600, dx=0.5e-3, total_steps=800, cpml_thickness=15, frequency=2e9)
+HEAD600_SEED = 1000
+HEAD600_FREQS = (0.5e9, 3.5e9, 301)
+HEAD600_DAS = dict(npix=64, half=0.09)        # 64x64 pixels over +/-9 cm around the centre
+HEAD192 = dict(nx=192, ny=192, nz=192, dx=1e-3, total_steps=1000, cpml_thickness=10, frequency=2e9)
+HEAD192_SEED = 1000
+HEAD192_TX = (0, 3, 5, 6)                     # both float4 lanes of the 8-TX layout
+
+
+def _sha(*arrays):
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(np.asarray(a, np.float64)).tobytes())
+    return h.hexdigest()
+
+
+def _head600_inputs():
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from ceep_b200.phantoms import HeadPhantom2D, ring_positions
+    c = HEAD600["nx"] // 2
+    pos = ring_positions(16, (c, c), 200)
+    ph = HeadPhantom2D(HEAD600["nx"], HEAD600["ny"], HEAD600["dx"], seed=HEAD600_SEED)
+    eps, sig = ph.get_eps_map()
+    (de, tau), = ph.get_dispersion()["debye"]
+    return pos, eps, sig, de, tau
+
+
+def gen_head600_ref(dtype):
+    """The reference's own BatchedFDTD2D.run() at the head-imaging size (600^2,
+    16 TX on a ring of radius 200 cells, 800 steps, CPML 15) on the seeded head
+    phantom's non-dispersive maps (eps_inf, sigma written to _eps_r/_sigma_e,
+    as the reference's callers do): the batched reference has no ADE."""
+    pos, eps, sig, _, _ = _head600_inputs()
+    import_reference(dtype)
+    from ceep.solvers.fdtd_2d_batched import BatchedFDTD2D
+    s = BatchedFDTD2D(source_positions=pos, probe_positions=pos, **HEAD600)
+    s._eps_r[:] = eps
+    s._sigma_e[:] = sig
+    out = s.run()
+    _save("head600_ref_" + np.dtype(dtype).name, probes=_probes(out, 16, 16).astype(dtype),
+          positions=np.array(pos), dt=np.float64(s.dt), inputs_sha=np.array(_sha(eps, sig)))
+
+
+def gen_head600_oracle():
+    """Config 2 proper from the oracle (FP64): the same phantom with its Debye
+    pole per layer; probe series, S at 301 frequencies and the 64x64 DAS image."""
+    pos, eps, sig, de, tau = _head600_inputs()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.fdtd2d import Fdtd2DOracle
+    from oracle.spectral import das_frequency, running_dft
+    o = Fdtd2DOracle(HEAD600["nx"], HEAD600["ny"], HEAD600["dx"], HEAD600["total_steps"],
+                     HEAD600["cpml_thickness"], pos, pos, HEAD600["frequency"], eps_r=eps, sigma_e=sig,
+                     dispersion={"debye": [(de, tau)]})
+    probes = o.run()
+    freqs = np.linspace(*HEAD600_FREQS)
+    S = running_dft(probes, o.dt, freqs)
+    npix, half, dx = HEAD600_DAS["npix"], HEAD600_DAS["half"], HEAD600["dx"]
+    pitch = 2 * half / npix
+    x0 = ((HEAD600["nx"] // 2) * dx - half) / pitch
+    y0 = ((HEAD600["ny"] // 2) * dx - half) / pitch
+    ant = np.asarray(pos, np.float64) * dx / pitch   # grid index -> pitch units
+    img = das_frequency(S, freqs, ant, (x0, x0 + npix), (y0, y0 + npix), pitch)
+    _save("head600_oracle", probes=probes, S=S, das=img, positions=np.array(pos), dt=np.float64(o.dt),
+          inputs_sha=np.array(_sha(eps, sig, de, tau)))
+
+
+def _head192_inputs():
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from ceep_b200.phantoms import HeadPhantom3D, ring_positions
+    c = HEAD192["nx"] // 2
+    pos = [(x, y, HEAD192["nz"] // 2) for x, y in ring_positions(8, (c, c), 75)]
+    ph = HeadPhantom3D(HEAD192["nx"], HEAD192["ny"], HEAD192["nz"], HEAD192["dx"], seed=HEAD192_SEED)
+    eps, sig = ph.get_eps_map_3d()
+    (de, tau), = ph.get_dispersion()["debye"]
+    return pos, eps, sig, de, tau
+
+
+def _head192_one_tx(tx):
+    pos, eps, sig, de, tau = _head192_inputs()
+    from oracle.fdtd3d import Fdtd3DOracle
+    o = Fdtd3DOracle(HEAD192["nx"], HEAD192["ny"], HEAD192["nz"], HEAD192["dx"], HEAD192["total_steps"],
+                     HEAD192["cpml_thickness"], [pos[tx]], pos, HEAD192["frequency"], eps_r=eps, sigma_e=sig,
+                     dispersion={"debye": [(de, tau)]})
+    return o.run()[0]
+
+
+def gen_head192_oracle():
+    """Config 5's forward from the 3D oracle (FP64): 192^3, 1 mm, 1000 steps,
+    CPML 10, 8 Ez dipoles on a mid-plane ring, seeded Debye ellipsoid shells
+    with an inclusion.  The transmit events are independent, so four of the
+    eight (both float4 lanes) run in parallel worker processes."""
+    import multiprocessing as mp
+    pos, eps, sig, de, tau = _head192_inputs()
+    with mp.get_context("spawn").Pool(len(HEAD192_TX)) as pool:
+        rows = pool.map(_head192_one_tx, HEAD192_TX)
+    from oracle.fdtd3d import reference_dt_3d
+    _save("head192_oracle", probes=np.stack(rows), tx=np.array(HEAD192_TX), positions=np.array(pos),
+          dt=np.float64(reference_dt_3d(HEAD192["dx"])), inputs_sha=np.array(_sha(eps, sig, de, tau)))
+
+
+# CircularArray cases: (num_antennas, radius_mm, center, dx)
+CIRCULAR = [(8, 35.0, (100, 100), 0.5e-3), (16, 100.0, (300, 300), 0.5e-3), (12, 70.0, (100, 100), 1e-3),
+            (24, 120.0, (200, 200), 1e-3), (16, 75.0, (96, 96, 96), 1e-3), (8, 75.0, (96, 96, 96), 1e-3)]
+DATASET_GRIDS = [(64, 8), (64, 16), (128, 16), (256, 12), (600, 16)]   # (nx = ny, n_ant)
+
+
+def gen_positions():
+    """Antenna grid positions from the reference's CircularArray
+    (src/ceep/antennas/arrays.py:110-143) and from its dataset generator's
+    circle (scripts/generate_corrected_dataset.py:121-129), the latter read off
+    the source positions generate_sample() hands the solver (a stand-in
+    solver class records them and stops the sample)."""
+    import_reference(np.float64)
+    from ceep.antennas.arrays import CircularArray
+    out = {}
+    for k, (n, rmm, c, dx) in enumerate(CIRCULAR):
+        out[f"circular_{k}"] = np.array([e.position for e in CircularArray(n, rmm, c, dx).elements])
+        out[f"circular_case_{k}"] = np.array([n, rmm, dx] + list(c) + ([0] if len(c) == 2 else []), np.float64)
+    sys.path.insert(0, os.path.join(REFERENCE_ROOT, "scripts"))
+    import generate_corrected_dataset as gcd
+
+    class _Stop(Exception):
+        pass
+
+    class _Recorder:
+        def __init__(self, **kw):
+            raise _Stop(kw["source_positions"])
+
+    gcd.BatchedFDTD2D = _Recorder
+    for k, (nx, n_ant) in enumerate(DATASET_GRIDS):
+        try:
+            with contextlib.redirect_stdout(io.StringIO()):
+                gcd.generate_sample(0, include_hemorrhage=False, nx=nx, ny=nx, n_ant=n_ant)
+        except _Stop as e:
+            out[f"dataset_{k}"] = np.array(e.args[0])
+        out[f"dataset_case_{k}"] = np.array([nx, n_ant])
+    _save("positions", **out)
+
+
 JOBS = {
+    "positions": gen_positions,
+    "head600_ref32": lambda: gen_head600_ref(np.float32),
+    "head600_ref64": lambda: gen_head600_ref(np.float64),
+    "head600_oracle": gen_head600_oracle,
+    "head192_oracle": gen_head192_oracle,
     "single2d": gen_single2d,
     "ceep_results": gen_ceep_results,
     "brain_phantom": gen_brain_phantom,
@@ -397,5 +555,6 @@ JOBS = {
 }
 
 if __name__ == "__main__":
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))  # oracle/ for the spawn workers
     for job in (sys.argv[1:] or list(JOBS)):
         JOBS[job]()

@@ -66,6 +66,25 @@ def test_spectral_entry_points_validate():
     assert h.ceep_das_workspace_bytes(64, 64, 301) > 0
 
 
+@pytest.mark.parametrize("side", [65536, 65537, 46341])
+def test_image_entry_points_reject_pixel_counts_past_int(side):
+    """Pixel counts are formed in 64 bits: 65536^2 (a multiple of 2^32),
+    65537^2 (wraps to a small count in 32 bits) and 46341^2 (wraps negative)
+    are refused before any launch, with no device touched."""
+    from ceep_b200 import _lib
+    h = _lib.lib()
+    fake = C.c_void_p(256)  # never dereferenced: the size check comes first
+    assert h.ceep_das_workspace_bytes(side, side, 301) == 0
+    assert h.ceep_dmas_workspace_bytes(side, side) == 0
+    args = (fake, fake, fake, 301, 16, side, side, 0.0, 0.0, 1e-3, 1)
+    assert h.ceep_das(*args, fake, fake, None) == 3
+    assert b"exceeds" in h.ceep_last_error()
+    assert h.ceep_dmas(*args, fake, fake, None) == 3
+    assert h.ceep_das_noalloc(*args, fake, None) == 3
+    assert b"exceeds" in h.ceep_last_error()
+    assert h.ceep_das_time(fake, fake, 4, 16, side, 1e-3, 2e9, fake, None) == 3
+
+
 def test_solver_validates_positions_without_gpu():
     from ceep_b200 import BatchedFDTD2D
     with pytest.raises(ValueError):
