@@ -43,6 +43,11 @@
 namespace ceep {
 
 constexpr int kAdjConsumers = 128;
+// Resident blocks per SM the registers are budgeted for, and the ring depth
+// (stages are shrunk from 4 to 3 when 4 would not fit that many blocks).
+#ifndef CEEP_ADJ_MIN_BLOCKS
+#define CEEP_ADJ_MIN_BLOCKS 3
+#endif
 constexpr int kAdjMaxRows = 62;                  // rows + the two neighbour rows fit a 64-bit row mask
 constexpr uint64_t kAdjWaitNs = 1000000000ull;   // 1 s
 
@@ -83,10 +88,10 @@ struct AdjStage {
   float4 lhy[(CX + 1) * L];  // adjoint Hy (left-halo'd)
 };
 
-// Four stages where three blocks of them fit an SM, else three.
+// Four stages where CEEP_ADJ_MIN_BLOCKS blocks of them fit an SM, else three.
 template <int L, int ND>
 __host__ __device__ constexpr int adj_stages() {
-  return 4 * sizeof(AdjStage<L, ND>) <= 74 * 1024 ? 4 : 3;
+  return 4 * sizeof(AdjStage<L, ND>) <= (222 / CEEP_ADJ_MIN_BLOCKS) * 1024 ? 4 : 3;
 }
 template <int L, int ND>
 __host__ __device__ constexpr size_t adj_smem_bytes() {
@@ -483,7 +488,7 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
 }
 
 template <int L, int ND>
-__global__ void __launch_bounds__(kAdjConsumers + 32, 3)
+__global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
     adjoint2d_step_kernel(const Adjoint2dParams a, int step, int par, const float4* __restrict__ ez_n,
                           const float4* __restrict__ ez_np1, const float4* __restrict__ j_n) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

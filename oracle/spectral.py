@@ -54,8 +54,10 @@ def das_frequency(s_matrix, frequencies, antenna_positions, x_range, y_range, dx
     f = freqs[mask]
     S = s_matrix[mask]                      # (F, rx, tx)
     v = C_0 / np.sqrt(background_permittivity)
-    nx = x_range[1] - x_range[0]
-    ny = y_range[1] - y_range[0]
+    # ranges are grid indices in the reference (ImagingRegion); a fractional
+    # start (an image whose pitch does not divide its origin) is allowed here
+    nx = int(round(x_range[1] - x_range[0]))
+    ny = int(round(y_range[1] - y_range[0]))
     px = (x_range[0] + np.arange(nx)) * dx
     py = (y_range[0] + np.arange(ny)) * dx
     PX, PY = np.meshgrid(px, py, indexing="ij")
