@@ -82,6 +82,38 @@ def algorithmic_bytes_per_step_2d(w, n_debye, n_lorentz=0):
     return b
 
 
+# CUDA sources a kernel's DRAM traffic depends on (their hash is recorded in
+# the profile summary the traffic figure comes from)
+KERNEL_SOURCES = {2: ("fdtd2d.cu", "fdtd2d.cuh", "common.cuh", "tma.cuh"),
+                  3: ("fdtd3d.cu", "fdtd3d.cuh", "common.cuh")}
+
+
+def kernel_source_sha(dim):
+    import hashlib
+    h = hashlib.sha256()
+    for f in KERNEL_SOURCES[dim]:
+        with open(os.path.join(ROOT, "ceep_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def profile_traffic(name, dim):
+    """(DRAM bytes per launch, provenance) from the committed ncu summary
+    profiles/<name>: the `dram_bytes_per_launch = N` line, and whether its
+    `source_sha256 = ...` line matches the kernel sources built now."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None, None
+    traffic, sha = None, None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch"):
+            traffic = int(line.split("=")[1])
+        elif line.startswith("source_sha256"):
+            sha = line.split("=")[1].strip()
+    return traffic, {"file": "profiles/" + name, "source_sha256": sha,
+                     "matches_current_source": sha == kernel_source_sha(dim) if sha else None}
+
+
 def hbm_peak():
     """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json, else
     the pool's earlier measurement (6650 GB/s)."""
@@ -273,13 +305,8 @@ def run_ours(args, w):
     steps_per_launch = tblock if w.get("dim", 2) == 2 else 1
     bytes_launch = bytes_step * steps_per_launch
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
-    traffic = None
     kname = "fdtd3d_kernels" if w.get("dim", 2) == 3 else ("fdtd2d_step2" if tblock == 2 else "fdtd2d_step")
-    tpath = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}.md")
-    if os.path.exists(tpath):
-        for line in open(tpath):
-            if line.startswith("dram_bytes_per_launch"):
-                traffic = int(line.split("=")[1])
+    traffic, traffic_src = profile_traffic(f"{kname}_{args.workload}.md", w.get("dim", 2))
 
     # -- end to end through the public API with host buffers
     e2e = None
@@ -308,7 +335,8 @@ def run_ours(args, w):
                    "l2": "flushed (256 MB write) before every sample; per-step working set > L2",
                    "sample": "fused time loop + DFT->S + DAS image"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 3), "traffic": traffic, "peak_source": peak_src,
+                     "frac": round(achieved / peak, 3), "traffic": traffic, "traffic_source": traffic_src,
+                     "peak_source": peak_src,
                      "kernel": (("fdtd2d_step2_kernel (two steps per launch)" if tblock == 2 else
                                  "fdtd2d_step_kernel") if w.get("dim", 2) == 2 else
                                 "fdtd3d step: h box + h shell (side stream) + e + source/probe launches"),
@@ -982,7 +1010,8 @@ def run_pack_bench(args):
                        "cell_steps": pk.cell_steps},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 3), "peak_source": peak_src,
-                         "algorithmic_bytes": int(alg), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block},
+                         "algorithmic_bytes": int(alg), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block,
+                         "packing": ("concurrent class chains" if pk.packing else "interleaved") + f" ({pk.classes} classes)"},
             "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
             "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
             "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),

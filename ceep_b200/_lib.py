@@ -75,6 +75,8 @@ _SIGS = {
     "ceep2d_pack_tiles": (C.c_int, [P, I32]),
     "ceep2d_pack_set_temporal_block": (C.c_int, [P, C.c_int]),
     "ceep2d_pack_temporal_block": (C.c_int, [P]),
+    "ceep2d_pack_set_packing": (C.c_int, [P, C.c_int]),
+    "ceep2d_pack_packing": (C.c_int, [P]),
     "ceep2d_pack_destroy": (C.c_int, [P]),
     "ceep3d_plan_create": (C.c_int, [C.POINTER(Desc3D), C.POINTER(P)]),
     "ceep3d_plan_run": (C.c_int, [P, I64, I64, P, C.c_int]),

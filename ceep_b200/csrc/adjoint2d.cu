@@ -245,9 +245,10 @@ CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
       if (body) {
         cp(S.en, ez_n + gf + (rowc + x0) * L, (xe - x0) * cb);
         cp(S.e1, ez_np1 + gf + (rowc + x0) * L, (xe - x0) * cb);
+        if (a.grad_tau) {
 #pragma unroll
-        if (a.grad_tau)
           for (int q = 0; q < ND; ++q) cp(S.jn + q * CX * L, j_n + gj + (q * plane + rowc + x0) * L, (xe - x0) * cb);
+        }
         cp(S.lhy + ha * L, a.hy[par] + gf + (rowc + xa) * L, (xe - xa) * cb);
       }
       if (!pass) mbar_arrive_expect_tx(&full[s], bytes);
@@ -487,6 +488,159 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
   if (k < nslots) release(k);  // the row above the segment
 }
 
+// ------------------------------------------------------------------------
+// Consumer of interior tiles: every own cell, the halo columns x0-1 and
+// x0+CX and the rows y0-1 and y1 lie in the interior E region, off the edges
+// and outside every CPML strip, so the transposed step has no region tests
+// and reduces to
+//   mu = adj(E') + sum_q (k2_q/dt) adj(J_q')          (pointwise)
+//   nu = cb/dx mu
+//   adj(Hy) = adj(Hy') + nu(x) - nu(x+1),  adj(Hx) = adj(Hx') - nu(y) + nu(y+1)
+//   adj(E)  = ca mu - sum_q (k2_q/dt) adj(J_q')
+//             + db/dx (adj(Hy)(x-1) - adj(Hy)(x) + adj(Hx)(y) - adj(Hx)(y-1))
+//   adj(J_q) = k1_q adj(J_q') - cb gamma_q mu
+// with the operations of adj_consume in the same order.  Per row y a thread
+// forms mu of its own cell in row y+1 (carried into the next row with nu),
+// nu of the two neighbour cells in row y from the halo'd slices (no
+// shuffles, no divergent edge lanes), the three H adjoints it needs (adj(Hx)
+// of the row below is carried), and the new E adjoint, currents and
+// gradients of its cell.
+// ------------------------------------------------------------------------
+template <int L, int ND>
+CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty,
+                             int step, int par, int x0, int y0, int y1, int rs, int nslots, int g) {
+  using St = AdjStage<L, ND>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
+  constexpr int KG = 2 + 3 * ND, KP = adjoint2d_grad_width(ND);
+  const Fdtd2dParams& p = a.f;
+  const int nx = p.nx;
+  const int cx = threadIdx.x / L, lo = threadIdx.x % L;
+  const int x = x0 + cx;
+  const int lw = threadIdx.x & 31;
+  const int lane_g = g * L + lo;
+  const float inv = p.inv_dx, idt = p.inv_dt, dbdx = p.db_dx;
+  const size_t plane = (size_t)nx * p.ny, gf = (size_t)g * p.gs_field;
+  const int me = cx * L + lo;        // this cell in the plain slices
+  const int mh = (cx + 1) * L + lo;  // this cell in the halo'd slices
+  float4* ez_out = a.ez[par ^ 1] + gf;
+  float4* hx_out = a.hx[par ^ 1] + gf;
+  float4* hy_out = a.hy[par ^ 1] + gf;
+  float4* j_out = a.j[par ^ 1] + (size_t)g * p.gs_j;
+
+  // probe rows of the columns x-1, x, x+1 and this lane's source rows among
+  // the slots' rows rs .. rs + nslots - 1 (<= 64), as bit masks
+  uint64_t prb_l = 0, prb_c = 0, prb_r = 0, src_own = 0;
+  for (int q = 0; q < p.nprobe; ++q) {
+    const int px = __ldg(p.prb_xy + 2 * q), py = __ldg(p.prb_xy + 2 * q + 1) - rs;
+    if (py >= 0 && py < nslots) {
+      if (px == x - 1) prb_l |= 1ull << py;
+      if (px == x) prb_c |= 1ull << py;
+      if (px == x + 1) prb_r |= 1ull << py;
+    }
+  }
+  for (int s = 4 * lane_g; s < 4 * lane_g + 4 && s < p.ntx; ++s) {
+    const int sx = __ldg(p.src_xy + 2 * s), sy = __ldg(p.src_xy + 2 * s + 1) - rs;
+    if (sx == x && sy >= 0 && sy < nslots) src_own |= 1ull << sy;
+  }
+  auto wait = [&](int k) {
+    const bool ok = mbar_wait_bounded(&full[k % NS], (k / NS) & 1, kAdjWaitNs);
+    if (__any_sync(0xffffffffu, !ok)) {
+      if (lw == 0) adj_status(p.status, CEEP_ERR_TIMEOUT);
+      return false;
+    }
+    return true;
+  };
+  auto release = [&](int k) {
+    __syncwarp();
+    if (lw == 0) mbar_arrive(&empty[k % NS]);
+  };
+  // mu of halo'd cell i (cell xc) of row r, probe gradient included
+  auto mu_at = [&](const St& S, int i, int xc, int r, uint64_t mask) {
+    float4 E = S.le[i * L + lo];
+    if ((mask >> (r - rs)) & 1) inject_probes(a, E, xc, r, lane_g, step);
+    float4 js = f4(0.f);
+#pragma unroll
+    for (int q = 0; q < ND; ++q) js = fma4(S.ade[q * H + i].y * idt, S.lj[(q * H + i) * L + lo], js);
+    return E + js;
+  };
+  auto nu_of = [&](const St& S, int i, float4 mu) { return (S.coef[i].y * inv) * mu; };
+
+  // slot 0: row y0-1 (its adj(Hx) only), slot 1: row y0
+  if (!wait(0)) return;
+  if (!wait(1)) return;
+  float4 mu_c = mu_at(st[1], cx + 1, x, y0, prb_c);
+  float4 nu_c = nu_of(st[1], cx + 1, mu_c);
+  float4 d_u;  // -db/dx adj(Hx)(x, y-1)
+  {
+    const St& B = st[0];
+    const float4 nu_b = nu_of(B, cx + 1, mu_at(B, cx + 1, x, y0 - 1, prb_c));
+    d_u = (-dbdx) * (B.lhx[me] - nu_b + nu_c);
+  }
+  release(0);
+  int k = 1;
+  for (int y = y0; y < y1; ++y, ++k) {
+    if (!wait(k + 1)) return;  // row y+1 (row y1 < ny exists for an interior tile)
+    const St& A = st[k % NS];
+    const St& U = st[(k + 1) % NS];
+    const float4 mu_u = mu_at(U, cx + 1, x, y + 1, prb_c);
+    const float4 nu_u = nu_of(U, cx + 1, mu_u);
+    const float4 nu_l = nu_of(A, cx, mu_at(A, cx, x - 1, y, prb_l));
+    const float4 nu_r = nu_of(A, cx + 2, mu_at(A, cx + 2, x + 1, y, prb_r));
+    const float4 hyt = A.lhy[mh] + nu_c - nu_r;
+    const float4 hyt_l = A.lhy[mh - L] + nu_l - nu_c;
+    const float4 hxt = A.lhx[me] - nu_c + nu_u;
+    const size_t at = ((size_t)y * nx + x) * L + lo;
+    st4(hy_out + at, hyt);
+    st4(hx_out + at, hxt);
+
+    // pointwise part: E adjoint, currents, gradients of this cell
+    const float4 cf = A.coef[cx + 1];
+    float4 e1 = A.e1[me];
+    if ((src_own >> (y - rs)) & 1) {  // the forward added the source after E1
+      const float w = __ldg(p.waveform + step);
+      for (int s = 4 * lane_g; s < 4 * lane_g + 4 && s < p.ntx; ++s)
+        if (__ldg(p.src_xy + 2 * s) == x && __ldg(p.src_xy + 2 * s + 1) == y) add_comp(e1, s & 3, -w);
+    }
+    const float4 en = A.en[me];
+    const float4 dedt = (e1 - en) * f4(idt);
+    float gv[KG];
+#pragma unroll
+    for (int kk = 0; kk < KG; ++kk) gv[kk] = 0.f;
+    float4 elin = cf.x * mu_c;
+#pragma unroll
+    for (int q = 0; q < ND; ++q) {
+      const float4 kq = A.ade[q * H + cx + 1];
+      const float4 jin = A.lj[(q * H + cx + 1) * L + lo];
+      elin = fma4(-kq.y * idt, jin, elin);
+      st4(j_out + (q * plane + (size_t)y * nx + x) * L + lo, kq.x * jin - (cf.y * kq.z) * mu_c);
+      gv[3 + 3 * q] = dot4(jin, dedt);
+      if (a.grad_tau) {  // k1 and gamma depend on tau alone
+        const float4 jn = A.jn[q * CX * L + me];
+        gv[2 + 3 * q] = dot4(jin, jn);
+        gv[4 + 3 * q] = -cf.y * dot4(mu_c, jn);
+      }
+    }
+    gv[0] = dot4(mu_c, en);
+    gv[1] = __fdividef(dot4(mu_c, e1 - cf.x * en), cf.y);
+    float4 e = elin - dbdx * hyt - (-dbdx) * hxt + d_u;
+    e = e + dbdx * hyt_l;
+    st4(ez_out + at, e);
+    d_u = (-dbdx) * hxt;
+
+    double* gw = a.g + ((size_t)g * plane + (size_t)y * nx + x) * KP;
+#pragma unroll
+    for (int kk = 0; kk < KG; ++kk) {
+      if (kk >= 2 && (kk - 2) % 3 != 1 && !a.grad_tau) continue;  // k1, gamma slots: warp-uniform skip
+      const float v = lane_sum<L>(gv[kk]);
+      if ((kk % L) == lo) atomicAdd(gw + kk, (double)v);
+    }
+    mu_c = mu_u;
+    nu_c = nu_u;
+    release(k);
+  }
+  release(k);  // the row above the segment
+}
+
 template <int L, int ND>
 __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
     adjoint2d_step_kernel(const Adjoint2dParams a, int step, int par, const float4* __restrict__ ez_n,
@@ -528,7 +682,7 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
   const int m = n > 1 ? n : 1;
   const bool interior = x0 >= n + 2 && x0 + CX + 1 <= nx - m && y0 >= n + 2 && y1 + 1 <= ny - m;
   if (interior)
-    adj_consume<L, ND, false>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+    adj_consume_lean<L, ND>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
   else
     adj_consume<L, ND, true>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
 }

@@ -599,7 +599,14 @@ struct ceep2d_pack {
   std::vector<PackClass> classes;
   int max_steps = 0;
   int tblock = 1;  // steps per launch (1 or 2)
-  std::map<std::tuple<int64_t, int64_t, int>, cudaGraphExec_t> graphs;
+  // Packing of the classes in time: 0 = one stream, the classes' launches
+  // interleaved step by step (each launch waits for the previous class's);
+  // 1 = one stream per class, so the classes' launch chains (independent
+  // phantoms) run side by side, forked from and joined to the caller's stream.
+  int concurrent = 0;
+  std::vector<cudaStream_t> side;     // one per class beyond the first (concurrent packing)
+  std::vector<cudaEvent_t> events;    // fork + one join per side stream
+  std::map<std::tuple<int64_t, int64_t, int, int>, cudaGraphExec_t> graphs;
 };
 
 // Launches a phantom has taken after `steps` steps in the pack's mode; its
@@ -756,11 +763,13 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
   return CEEP_OK;
 }
 
-static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream_t s) {
+// Launch steps [step0, step0 + nsteps) of the classes [c0, c1) on stream s.
+static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream_t s, size_t c0, size_t c1) {
   if (pk->tblock == 2) {
     // pairs of steps: par is the pair index & 1 for every phantom still running
     for (int64_t t = step0 / 2; 2 * t < step0 + nsteps; ++t)
-      for (auto& c : pk->classes) {
+      for (size_t ci = c0; ci < c1; ++ci) {
+        auto& c = pk->classes[ci];
         const int a2 = c.active2_by_pair[t], lo = c.tail_lo_by_pair[t], hi = c.tail_hi_by_pair[t];
         cudaError_t e = cudaSuccess;
         if (a2 > 0)
@@ -774,7 +783,8 @@ static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream
     return CEEP_OK;
   }
   for (int64_t t = step0; t < step0 + nsteps; ++t)
-    for (auto& c : pk->classes) {
+    for (size_t ci = c0; ci < c1; ++ci) {
+      auto& c = pk->classes[ci];
       const int act = c.active_by_step[t];
       if (act == 0) continue;
       cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, act, pk->params, (int)t, (int)(t & 1),
@@ -783,6 +793,49 @@ static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream
     }
   return CEEP_OK;
 }
+
+// All classes: interleaved on s, or (concurrent packing) class 0 on s and
+// class c on side stream c-1, forked from and joined back to s.
+static int pack_all(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream_t s) {
+  const size_t nc = pk->classes.size();
+  if (!pk->concurrent || nc < 2) return pack_steps(pk, step0, nsteps, s, 0, nc);
+  cudaError_t e = cudaEventRecord(pk->events[0], s);
+  for (size_t c = 1; c < nc && e == cudaSuccess; ++c) e = cudaStreamWaitEvent(pk->side[c - 1], pk->events[0], 0);
+  if (e != cudaSuccess) return ceep::cuda_fail(e, "pack: fork");
+  int rc = pack_steps(pk, step0, nsteps, s, 0, 1);
+  for (size_t c = 1; c < nc; ++c) {
+    const int r = pack_steps(pk, step0, nsteps, pk->side[c - 1], c, c + 1);
+    if (rc == CEEP_OK) rc = r;
+    e = cudaEventRecord(pk->events[c], pk->side[c - 1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, pk->events[c], 0);
+    if (e != cudaSuccess && rc == CEEP_OK) rc = ceep::cuda_fail(e, "pack: join");
+  }
+  return rc;
+}
+
+extern "C" int ceep2d_pack_set_packing(ceep2d_pack* pk, int concurrent) {
+  if (!pk || (concurrent != 0 && concurrent != 1))
+    return fail(CEEP_ERR_INVALID, "pack: packing %d (0 or 1)", concurrent);
+  if (concurrent && pk->side.empty() && pk->classes.size() > 1) {
+    const size_t nc = pk->classes.size();
+    cudaError_t e = cudaSuccess;
+    for (size_t c = 0; c < nc && e == cudaSuccess; ++c) {
+      cudaEvent_t ev;
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess) pk->events.push_back(ev);
+    }
+    for (size_t c = 1; c < nc && e == cudaSuccess; ++c) {
+      cudaStream_t st;
+      e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+      if (e == cudaSuccess) pk->side.push_back(st);
+    }
+    if (e != cudaSuccess) return ceep::cuda_fail(e, "pack: side streams");
+  }
+  pk->concurrent = concurrent;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_pack_packing(const ceep2d_pack* pk) { return pk ? pk->concurrent : -1; }
 
 extern "C" int ceep2d_pack_set_temporal_block(ceep2d_pack* pk, int steps) {
   if (!pk || (steps != 1 && steps != 2)) return fail(CEEP_ERR_INVALID, "pack: temporal block %d (1 or 2)", steps);
@@ -806,15 +859,15 @@ extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, v
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = CEEP_OK;
   if (!use_graph || s == nullptr) {
-    rc = pack_steps(pk, step0, nsteps, s);
+    rc = pack_all(pk, step0, nsteps, s);
   } else {
-    auto key = std::make_tuple(step0, nsteps, pk->tblock);
+    auto key = std::make_tuple(step0, nsteps, pk->tblock, pk->concurrent);
     auto it = pk->graphs.find(key);
     if (it == pk->graphs.end()) {
       cudaGraph_t g;
       cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-      rc = pack_steps(pk, step0, nsteps, s);
+      rc = pack_all(pk, step0, nsteps, s);
       e = cudaStreamEndCapture(s, &g);
       if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
       if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -842,6 +895,8 @@ extern "C" int ceep2d_pack_tiles(const ceep2d_pack* pk, int32_t step) {
 extern "C" int ceep2d_pack_destroy(ceep2d_pack* pk) {
   if (!pk) return CEEP_OK;
   for (auto& kv : pk->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto st : pk->side) cudaStreamDestroy(st);
+  for (auto ev : pk->events) cudaEventDestroy(ev);
   delete pk;
   return CEEP_OK;
 }

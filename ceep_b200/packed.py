@@ -12,9 +12,11 @@ Each solver's ``probe_data``, ``ez`` ... hold its own results afterwards.
 
 ``temporal_block=2`` advances every running phantom two steps per launch with
 the temporal-block kernel (a phantom with an odd step count takes its last
-step alone).  ``autotune`` picks the temporal-block depth and the tile height
-(rows per block) by timing a short prefix of the packed run for each
-candidate pair.
+step alone).  ``packing`` places the classes in time: 0 interleaves their
+launches on one stream, 1 runs each class's launch chain on its own stream
+beside the others.  ``autotune`` picks the temporal-block depth, the tile
+height (rows per block) and the packing by timing a short prefix of the
+packed run for each candidate.
 """
 from __future__ import annotations
 
@@ -30,7 +32,7 @@ from .solvers import BatchedFDTD2D
 
 class PackedBatch2D:
     def __init__(self, solvers: Sequence[BatchedFDTD2D], rows: int = 16, use_graph: bool = True,
-                 temporal_block: int = 1):
+                 temporal_block: int = 1, packing: int = 0):
         if not solvers:
             raise ValueError("no solvers")
         self.solvers: List[BatchedFDTD2D] = list(solvers)
@@ -42,6 +44,9 @@ class PackedBatch2D:
         self.temporal_block = int(temporal_block)
         if self.temporal_block not in (1, 2):
             raise ValueError("temporal_block must be 1 or 2")
+        self.packing = int(packing)
+        if self.packing not in (0, 1):
+            raise ValueError("packing must be 0 (interleaved) or 1 (concurrent class chains)")
         for s in self.solvers:
             if s.device != self.device:
                 raise ValueError("all solvers must live on one device")
@@ -84,6 +89,12 @@ class PackedBatch2D:
         self._pack = h
         self.rows = rows
         check(lib().ceep2d_pack_set_temporal_block(h, self.temporal_block), "ceep2d_pack_set_temporal_block")
+        check(lib().ceep2d_pack_set_packing(h, self.packing), "ceep2d_pack_set_packing")
+
+    @property
+    def classes(self) -> int:
+        """Launch classes (lane width x ADE shape) of the packed solvers."""
+        return len({(s._gwidth, len(s._debye), len(s._lorentz)) for s in self.solvers})
 
     def reset(self):
         for s in self.solvers:
@@ -110,27 +121,32 @@ class PackedBatch2D:
         return lib().ceep2d_pack_tiles(self._pack, step)
 
     def autotune(self, candidates=(8, 12, 16, 20, 24, 32, 48), probe_steps: int = 40,
-                 temporal_blocks=(1, 2)) -> Dict[Tuple[int, int], float]:
+                 temporal_blocks=(1, 2), packings=(0, 1)) -> Dict[Tuple[int, int, int], float]:
         """Time ``probe_steps`` packed steps for each (temporal-block depth,
-        tile height) pair; keep the fastest.  Returns ms per step for each."""
+        tile height, packing); keep the fastest.  Returns ms per step for
+        each.  With a single class the packings coincide and only 0 is tried."""
         stream = torch.cuda.current_stream(self.device)
         timings = {}
         nst = min(probe_steps, self.max_steps)
         nst -= nst % 2 if nst < self.max_steps else 0    # even, unless the whole run
+        packings = tuple(packings) if self.classes > 1 else (0,)
         for tb in temporal_blocks:
             for rows in candidates:
                 self.temporal_block = tb
                 self._replan(rows)
-                self.advance(0, nst, stream)           # capture + warm
-                self.reset()
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                self.advance(0, nst, stream)
-                b.record(stream)
-                torch.cuda.synchronize(self.device)
-                timings[(tb, rows)] = a.elapsed_time(b) / nst
-                self.reset()
+                for pkg in packings:
+                    self.packing = pkg
+                    check(lib().ceep2d_pack_set_packing(self._pack, pkg), "ceep2d_pack_set_packing")
+                    self.advance(0, nst, stream)           # capture + warm
+                    self.reset()
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    self.advance(0, nst, stream)
+                    b.record(stream)
+                    torch.cuda.synchronize(self.device)
+                    timings[(tb, rows, pkg)] = a.elapsed_time(b) / nst
+                    self.reset()
         best = min(timings, key=timings.get)
-        self.temporal_block = best[0]
+        self.temporal_block, self.packing = best[0], best[2]
         self._replan(best[1])
         return timings

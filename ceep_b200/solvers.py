@@ -17,12 +17,13 @@ documented on the methods:
 from __future__ import annotations
 
 import ctypes as C
+import time
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
 
-from . import physics
+from . import physics, trace
 from ._lib import Desc2D, check, lib
 from .constants import C_0, EPS_0, MU_0
 
@@ -88,6 +89,8 @@ class BatchedFDTD2D:
         self.temporal_block = int(temporal_block)   # steps per kernel launch (1 or 2)
         self.sentinel_interval = 0                   # NaN/Inf scans between run-range ends (0: none)
         self.wait_limit_ns = 1_000_000_000           # bound of every device wait
+        self.run_record: Optional[dict] = None       # last run's record (ceep_b200.trace)
+        self.record_path: Optional[str] = None       # append each run's record as a JSON line
         self._built = False
         self._plan = None
         self._validate()
@@ -330,9 +333,15 @@ class BatchedFDTD2D:
     def run(self) -> Dict[int, Dict[int, np.ndarray]]:
         """All time steps; returns ``{tx: {rx: float64 series of total_steps}}``
         (fdtd_2d_batched.py:408-538).  As in the reference, fields persist, so
-        a second call continues the simulation and overwrites the series."""
-        self.advance(0, self.total_steps)
-        probe_np = self.probe_data.double().cpu().numpy()
+        a second call continues the simulation and overwrites the series.
+        Leaves ``run_record`` (see ``ceep_b200.trace``)."""
+        t0 = time.perf_counter()
+        with trace.phase("time_loop"):
+            self.advance(0, self.total_steps)
+            probe_np = self.probe_data.double().cpu().numpy()
+        code = int(self._status.item())
+        trace.emit(self, trace.make_record("BatchedFDTD2D", self.nx * self.ny, self.total_steps, self.batch,
+                                           time.perf_counter() - t0, code))
         self.check_status()
         P = len(self.probe_positions)
         return {tx: {rx: probe_np[tx, rx, :] for rx in range(P)} for tx in range(self.batch)}
@@ -358,7 +367,9 @@ class BatchedFDTD2D:
         if freqs is None:
             raise ValueError("no frequencies given")
         from .spectral import dft
-        return dft(self.probe_data[:, :len(self.probe_positions)], freqs, self.dt).cpu().numpy().astype(np.complex128)
+        with trace.phase("dft"):
+            return dft(self.probe_data[:, :len(self.probe_positions)], freqs,
+                       self.dt).cpu().numpy().astype(np.complex128)
 
     # -- state views in the reference layout (B, nx, ny) ----------------------
     def _cur(self) -> int:

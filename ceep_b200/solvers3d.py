@@ -17,7 +17,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from . import physics
+from . import physics, trace
 from ._lib import Desc3D, check, lib
 from .constants import EPS_0, MU_0, cfl_timestep_3d
 from .solvers import _pad_tx, _ptr
@@ -55,6 +55,8 @@ class BatchedFDTD3D:
         self.z_rows = int(z_rows)
         self.shell_z_rows = int(shell_z_rows)
         self.use_graph = bool(use_graph)
+        self.run_record: Optional[dict] = None       # last run's record (ceep_b200.trace)
+        self.record_path: Optional[str] = None       # append each run's record as a JSON line
         self._built = False
         self._plan = None
         n = self.cpml_thickness
@@ -208,8 +210,11 @@ class BatchedFDTD3D:
     def run(self, verbose: bool = False) -> Dict[int, Dict[int, np.ndarray]]:
         """fdtd_3d_batched.py:886-985; with ``verbose`` prints the throughput line."""
         t0 = time.perf_counter()
-        self.advance(0, self.total_steps)
-        probe_np = self.probe_data.double().cpu().numpy()
+        with trace.phase("time_loop"):
+            self.advance(0, self.total_steps)
+            probe_np = self.probe_data.double().cpu().numpy()
+        trace.emit(self, trace.make_record("BatchedFDTD3D", self.nx * self.ny * self.nz, self.total_steps,
+                                           self.batch, time.perf_counter() - t0))
         if verbose:
             el = time.perf_counter() - t0
             rate = self.batch * self.nx * self.ny * self.nz * self.total_steps / el / 1e9
@@ -223,7 +228,9 @@ class BatchedFDTD3D:
         if freqs is None:
             raise ValueError("no frequencies given")
         from .spectral import dft
-        return dft(self.probe_data[:, :len(self.probe_positions)], freqs, self.dt).cpu().numpy().astype(np.complex128)
+        with trace.phase("dft"):
+            return dft(self.probe_data[:, :len(self.probe_positions)], freqs,
+                       self.dt).cpu().numpy().astype(np.complex128)
 
     def _ref_view(self, t):
         G, nz, ny, nx, W = t.shape

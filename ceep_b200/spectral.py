@@ -16,7 +16,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from . import physics
+from . import physics, trace
 from ._lib import check, lib
 from .constants import C_0
 
@@ -139,11 +139,14 @@ def das_image(S: torch.Tensor, frequencies: Sequence[float], antenna_xy_m: np.nd
     k = torch.as_tensor((2.0 * np.pi * np.asarray(frequencies, np.float64) / velocity).astype(np.float32)).to(dev)
     ant = torch.as_tensor(np.asarray(antenna_xy_m, np.float32).reshape(N, 2)).to(dev)
     need = lib().ceep_das_workspace_bytes(nx_pix, ny_pix, F)
+    if need <= 0:
+        raise ValueError(f"DAS image {nx_pix}x{ny_pix} x {F} frequencies is not supported")
     if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = torch.empty(max(need, 8), dtype=torch.uint8, device=dev)
     img = torch.empty((nx_pix, ny_pix), dtype=torch.float32, device=dev)
-    check(lib().ceep_das(Sr.data_ptr(), k.data_ptr(), ant.data_ptr(), F, N, nx_pix, ny_pix, px0, py0, pix,
-                         int(normalize), workspace.data_ptr(), img.data_ptr(), _stream(dev)), "ceep_das")
+    with trace.phase("das"):
+        check(lib().ceep_das(Sr.data_ptr(), k.data_ptr(), ant.data_ptr(), F, N, nx_pix, ny_pix, px0, py0, pix,
+                             int(normalize), workspace.data_ptr(), img.data_ptr(), _stream(dev)), "ceep_das")
     return img
 
 

@@ -176,6 +176,15 @@ int ceep2d_pack_tiles(const ceep2d_pack* pack, int32_t step);
  * at an even step or the last one.  Set before the first run. */
 int ceep2d_pack_set_temporal_block(ceep2d_pack* pack, int steps);
 int ceep2d_pack_temporal_block(const ceep2d_pack* pack);
+/* Packing of the classes (lane width x ADE shape) in time, an autotuner
+ * choice with no counterpart in the reference (whose dataset generator runs
+ * one solver per phantom, scripts/generate_corrected_dataset.py:139-149):
+ * 0 (default) launches every class's step on the caller's stream in turn;
+ * 1 gives each class beyond the first its own stream (created here, owned by
+ * the pack), so the classes' launch chains, which touch disjoint phantoms,
+ * run side by side, forked from and joined back to the caller's stream. */
+int ceep2d_pack_set_packing(ceep2d_pack* pack, int concurrent);
+int ceep2d_pack_packing(const ceep2d_pack* pack);
 int ceep2d_pack_destroy(ceep2d_pack* pack);
 
 /* ------------------------------------------------------------------------

@@ -63,8 +63,9 @@ def test_packed_against_oracle_and_autotune(cuda_device):
     made = [_make(spec, 10 + k) for k, spec in enumerate(SPECS[:4])]
     pk = PackedBatch2D([m[0] for m in made])
     timings = pk.autotune(candidates=(8, 16, 24), probe_steps=20)
-    assert set(timings) == {(tb, r) for tb in (1, 2) for r in (8, 16, 24)}
-    assert (pk.temporal_block, pk.rows) in timings
+    pks = (0, 1) if pk.classes > 1 else (0,)
+    assert set(timings) == {(tb, r, c) for tb in (1, 2) for r in (8, 16, 24) for c in pks}
+    assert (pk.temporal_block, pk.rows, pk.packing) in timings
     results = pk.run()
     for (s, (eps, sig, disp)), res, spec in zip(made, results, SPECS):
         o = Fdtd2DOracle(s.nx, s.ny, 0.5e-3, s.total_steps, s.cpml_n, s.source_positions, s.probe_positions,
@@ -97,3 +98,25 @@ def test_packed_two_steps_per_launch_equals_individual_runs(cuda_device):
     pk.advance(40)
     for (pd, ez, hx), s in zip(solo, packed):
         assert torch.equal(pd, s.probe_data) and torch.equal(ez, s.ez)
+
+
+@pytest.mark.parametrize("tblock", [1, 2])
+def test_concurrent_class_chains_equal_individual_runs(cuda_device, tblock):
+    """packing=1: each class (lane width x ADE shape) runs its launch chain on
+    its own stream; probe series and fields equal each phantom's own run bit
+    for bit, with and without graph capture."""
+    from ceep_b200.packed import PackedBatch2D
+    solo = []
+    for k, spec in enumerate(SPECS):
+        s, _ = _make(spec, 30 + k)
+        s.set_rows_per_block(12)
+        s.set_temporal_block(tblock)
+        s.run()
+        solo.append((s.probe_data.clone(), s.ez.clone()))
+    for use_graph in (True, False):
+        packed = [_make(spec, 30 + k)[0] for k, spec in enumerate(SPECS)]
+        pk = PackedBatch2D(packed, rows=12, temporal_block=tblock, packing=1, use_graph=use_graph)
+        assert pk.classes > 1
+        pk.run()
+        for (pd, ez), s in zip(solo, packed):
+            assert torch.equal(pd, s.probe_data) and torch.equal(ez, s.ez)
