@@ -949,6 +949,47 @@ def _pack_solvers(count, device, seed=2024):
     return out
 
 
+def _pack_launch_count(solvers, tblock):
+    """Kernel launches of one packed run: per class (lane width x ADE shape)
+    one launch per step (tblock 1), or per step pair one two-step launch while
+    any phantom has two steps left plus one one-step launch where a phantom
+    takes its odd last step alone (tblock 2)."""
+    classes = {}
+    for s in solvers:
+        classes.setdefault((s._gwidth, len(s._debye), len(s._lorentz)), []).append(s.total_steps)
+    n = 0
+    for steps in classes.values():
+        top = max(steps)
+        if tblock == 1:
+            n += top
+        else:
+            for t in range((top + 1) // 2):
+                n += any(x >= 2 * t + 2 for x in steps) + any(x == 2 * t + 1 for x in steps)
+    return n
+
+
+def _graph_launch_gap_us(dev, stream, n=2000):
+    """Device time per launch of a CUDA graph of `n` launches of a one-element
+    kernel: an upper bound of what a graph of launches loses between kernels
+    (the cost a single persistent launch would save)."""
+    import torch
+    x = torch.zeros(1, device=dev)
+    x.add_(1.0)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(n):
+            x.add_(1.0)
+    g.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    g.replay()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) * 1e3 / n
+
+
 def run_pack_bench(args):
     """Config 3: aggregate GCell-steps/s of one packed, graph-replayed run of
     all phantoms against per-phantom run() calls of the single-grid kernel."""
@@ -994,6 +1035,8 @@ def run_pack_bench(args):
     for s in solvers:
         s.check_status()
     value = pk.cell_steps / float(np.median(times)) / 1e9
+    launches = _pack_launch_count(solvers, pk.temporal_block)
+    gap_us = _graph_launch_gap_us(dev, stream)
     # roofline of the whole packed run: compulsory bytes of every phantom's
     # steps (real TX counts, not the padded lanes) over the run's time
     alg = sum(algorithmic_bytes_per_step_2d({"nx": s.nx, "ny": s.ny, "cpml": s.cpml_n, "ntx": s.batch},
@@ -1013,6 +1056,8 @@ def run_pack_bench(args):
                          "algorithmic_bytes": int(alg), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block,
                          "packing": ("concurrent class chains" if pk.packing else "interleaved") + f" ({pk.classes} classes)"},
             "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
+            "graph_launches": launches, "graph_launch_gap_us": round(gap_us, 3),
+            "launch_gap_share": round(launches * gap_us * 1e-6 / float(np.median(times)), 5),
             "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
             "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),
             "baseline_sample": len(range(0, count, max(1, count // args.pack_sample)))}
