@@ -132,10 +132,11 @@ struct HAdj {
 };
 
 // Hy' = Hy + A (E(x+1) - E(x)) [+ db psi'],  psi' = b psi + c/dx (E(x+1) - E(x))
-// `psi_src` is this TX group's read half of the psi array, `lo` the lane.
+// `psi` is the adjoint psi of the cell (read by the caller ahead of the row's
+// stores; used by strip cells only).
 template <bool GEN>
 CEEP_D HAdj hy_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, float4 lhy, float4 cy_c, float4 cy_r,
-                   const float4* psi_src, int lo) {
+                   float4 psi) {
   HAdj r;
   r.tot = lhy + cy_c - cy_r;
   r.s = -1;
@@ -148,7 +149,6 @@ CEEP_D HAdj hy_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, fl
   r.s = rg.hx_col(x);
   if (r.s >= 0) {
     const int ci = x < p.n ? x : p.nx - 1 - x;
-    const float4 psi = __ldg(psi_src + ((size_t)y * 2 * p.n + r.s) * (p.L) + lo);
     const float4 pt = fma4(p.db, r.tot, psi);
     r.psi = p.cpml_b[ci] * pt;
     r.u = fma4(p.cpml_c[ci] * p.inv_dx, pt, r.u);
@@ -159,7 +159,7 @@ CEEP_D HAdj hy_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, fl
 // Hx' = Hx - A (E(y+1) - E(y)) [- db psi'],  psi' = b psi + c/dx (E(y+1) - E(y))
 template <bool GEN>
 CEEP_D HAdj hx_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, float4 lhx, float4 cx_c, float4 cx_u,
-                   const float4* psi_src, int lo) {
+                   float4 psi) {
   HAdj r;
   r.tot = lhx + cx_c - cx_u;
   r.s = -1;
@@ -172,7 +172,6 @@ CEEP_D HAdj hx_adj(const Fdtd2dParams& p, const AdjRegions& rg, int x, int y, fl
   r.s = rg.hy_row(y);
   if (r.s >= 0) {
     const int ci = y < p.n ? y : p.ny - 1 - y;
-    const float4 psi = __ldg(psi_src + ((size_t)r.s * p.nx + x) * (p.L) + lo);
     const float4 pt = fma4(-p.db, r.tot, psi);
     r.psi = p.cpml_b[ci] * pt;
     r.u = fma4(p.cpml_c[ci] * p.inv_dx, pt, r.u);
@@ -339,34 +338,64 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
     for (int q = 0; q < ND; ++q) s = fma4(S.ade[q * H + i].y * p.inv_dt, S.lj[(q * H + i) * L + lo], s);
     return s;
   };
-  // cy of halo'd cell i (cell xc) of row r
-  auto cy_at = [&](const St& S, int i, int xc, int r) {
+  // Adjoint psi of strip cells, read from the read halves of their pairs.  A
+  // row's values are all loaded at the top of its iteration, ahead of any
+  // store, so their latencies overlap each other and the shared-memory reads.
+  auto ld_pey = [&](int xc, int r) {  // E y strips (rows 1..n, ny-n..ny-1; x >= 1)
+    const int sy = rg.ey_row(r);
+    return (GEN && n > 0 && xc >= 1 && xc < nx && sy >= 0) ? __ldg(pey_r + ((size_t)sy * nx + xc) * L + lo) : f4(0.f);
+  };
+  auto ld_pex = [&](int xc, int r) {  // E x strips (columns 1..n, nx-n..nx-1; y >= 1)
+    const int sx = (xc >= 0 && xc < nx) ? rg.ex_col(xc) : -1;
+    return (GEN && n > 0 && r >= 1 && sx >= 0) ? __ldg(pex_r + ((size_t)r * 2 * n + sx) * L + lo) : f4(0.f);
+  };
+  auto ld_phy = [&](int xc, int y) {  // H x strips of Hy
+    const int sh = (xc >= 0 && xc < nx) ? rg.hx_col(xc) : -1;
+    return (GEN && sh >= 0) ? __ldg(phy_r + ((size_t)y * 2 * n + sh) * L + lo) : f4(0.f);
+  };
+  auto ld_phx = [&](int y) {  // H y strips of Hx, this column
+    const int sh = rg.hy_row(y);
+    return (GEN && active && sh >= 0) ? __ldg(phx_r + ((size_t)sh * nx + x) * L + lo) : f4(0.f);
+  };
+  // the column an edge lane recomputes cy for (its own otherwise)
+  const int x_nb = lw < L ? x - 1 : (lw >= 32 - L ? x + 1 : x);
+  // cy of halo'd cell i (cell xc) of row r; pex = that cell's adjoint E x-strip psi
+  auto cy_at = [&](const St& S, int i, int xc, int r, float4 pex) {
     const float4 E = e_adj(S, i, xc, r);
     const float4 cf = S.coef[i];
     if (!GEN || rg.f9(xc, r)) return (cf.y * inv) * (E + jsum(S, i));
     if (n > 0 && r >= 1) {
       const int sx = rg.ex_col(xc);
-      if (sx >= 0)
-        return (p.cpml_c[rg.ex_ci(xc)] * inv) * fma4(cf.z, E, __ldg(pex_r + ((size_t)r * 2 * n + sx) * L + lo));
+      if (sx >= 0) return (p.cpml_c[rg.ex_ci(xc)] * inv) * fma4(cf.z, E, pex);
     }
     return f4(0.f);
   };
-  // cx of this cell in a neighbour row (r = y0 - 1 or y1)
-  auto cx_row = [&](const St& S, int r) {
+  // cx of this cell in a neighbour row (r = y0 - 1 or y1); pey = its E y-strip psi
+  auto cx_row = [&](const St& S, int r, float4 pey) {
     if (!active) return f4(0.f);
     const float4 E = e_adj(S, cx + 1, x, r);
     const float4 cf = S.coef[cx + 1];
     if (!GEN || rg.f9(x, r)) return (-cf.y * inv) * (E + jsum(S, cx + 1));
     if (n > 0 && x >= 1) {
       const int sy = rg.ey_row(r);
-      if (sy >= 0)
-        return (p.cpml_c[rg.ey_ci(r)] * inv) * fma4(-cf.z, E, __ldg(pey_r + ((size_t)sy * nx + x) * L + lo));
+      if (sy >= 0) return (p.cpml_c[rg.ey_ci(r)] * inv) * fma4(-cf.z, E, pey);
     }
     return f4(0.f);
   };
+  // the E half's psi inputs of row r: this cell's y- and x-strip psi, and the
+  // x-strip psi of the neighbour an edge lane recomputes
+  struct EPsi {
+    float4 pey, pex, pex_nb;
+  };
+  auto ld_epsi = [&](int r) { return EPsi{ld_pey(x, r), ld_pex(x, r), ld_pex(x_nb, r)}; };
+  // the H half's psi inputs of row y: Hy at x and x-1, Hx at x
+  struct HPsi {
+    float4 phy, phy_l, phx;
+  };
+  auto ld_hpsi = [&](int y) { return HPsi{ld_phy(x, y), ld_phy(x - 1, y), ld_phx(y)}; };
   // E half of this cell in row r of the segment: writes the new adjoint J and
   // E psi, adds the gradients; every lane of the warp must call it.
-  auto e_half = [&](const St& S, int r) {
+  auto e_half = [&](const St& S, int r, const EPsi& ep) {
     AdjE o{f4(0.f), f4(0.f), f4(0.f), f4(0.f)};
     float gv[KG];
 #pragma unroll
@@ -413,14 +442,14 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
         const int sy = rg.ey_row(r);
         if (x >= 1 && sy >= 0) {
           const int ci = rg.ey_ci(r);
-          const float4 tot = fma4(-cf.z, E, __ldg(pey_r + ((size_t)sy * nx + x) * L + lo));
+          const float4 tot = fma4(-cf.z, E, ep.pey);
           st4(a.psi_ezy[par ^ 1] + (size_t)g * p.gs_psi_y + ((size_t)sy * nx + x) * L + lo, p.cpml_b[ci] * tot);
           o.cx = (p.cpml_c[ci] * inv) * tot;
         }
         const int sx = rg.ex_col(x);
         if (r >= 1 && sx >= 0) {
           const int ci = rg.ex_ci(x);
-          const float4 tot = fma4(cf.z, E, __ldg(pex_r + ((size_t)r * 2 * n + sx) * L + lo));
+          const float4 tot = fma4(cf.z, E, ep.pex);
           st4(a.psi_ezx[par ^ 1] + (size_t)g * p.gs_psi_x + ((size_t)r * 2 * n + sx) * L + lo, p.cpml_b[ci] * tot);
           o.cy = (p.cpml_c[ci] * inv) * tot;
         }
@@ -437,26 +466,26 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
     }
     if (lw < L || lw >= 32 - L) {
       const int dx = lw < L ? -1 : 1;
-      if (x + dx >= 0 && x + dx < nx) o.cye = cy_at(S, cx + 1 + dx, x + dx, r);
+      if (x + dx >= 0 && x + dx < nx) o.cye = cy_at(S, cx + 1 + dx, x + dx, r, ep.pex_nb);
     }
     return o;
   };
   // H half of this cell in row y; every lane of the warp must call it.
-  auto h_half = [&](const St& S, int y, const AdjE& c, float4 cx_up, float4& d_u) {
+  auto h_half = [&](const St& S, int y, const AdjE& c, float4 cx_up, float4& d_u, const HPsi& hp) {
     float4 cy_l = shfl_up4(c.cy, L), cy_r = shfl_down4(c.cy, L);
     if (lw < L) cy_l = c.cye;
     if (lw >= 32 - L) cy_r = c.cye;
     if (!active) return;
     const size_t at = ((size_t)y * nx + x) * L + lo;
-    const HAdj ry = hy_adj<GEN>(p, rg, x, y, S.lhy[mh], c.cy, cy_r, phy_r, lo);
-    const HAdj rx = hx_adj<GEN>(p, rg, x, y, S.lhx[me], c.cx, cx_up, phx_r, lo);
+    const HAdj ry = hy_adj<GEN>(p, rg, x, y, S.lhy[mh], c.cy, cy_r, hp.phy);
+    const HAdj rx = hx_adj<GEN>(p, rg, x, y, S.lhx[me], c.cx, cx_up, hp.phx);
     st4(a.hy[par ^ 1] + gf + at, ry.tot);
     st4(a.hx[par ^ 1] + gf + at, rx.tot);
     if (GEN && ry.s >= 0)
       st4(a.psi_hy[par ^ 1] + (size_t)g * p.gs_psi_x + ((size_t)y * 2 * n + ry.s) * L + lo, ry.psi);
     if (GEN && rx.s >= 0) st4(a.psi_hx[par ^ 1] + (size_t)g * p.gs_psi_y + ((size_t)rx.s * nx + x) * L + lo, rx.psi);
     float4 e = c.elin - ry.u - rx.u + d_u;
-    if (!GEN || x >= 1) e = e + hy_adj<GEN>(p, rg, x - 1, y, S.lhy[mh - L], cy_l, c.cy, phy_r, lo).u;
+    if (!GEN || x >= 1) e = e + hy_adj<GEN>(p, rg, x - 1, y, S.lhy[mh - L], cy_l, c.cy, hp.phy_l).u;
     st4(a.ez[par ^ 1] + gf + at, e);
     d_u = rx.u;
   };
@@ -466,22 +495,29 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
   AdjE c;
   float4 d_u = f4(0.f);  // adjoint of E(x, y) - E(x, y-1) from the Hx update of the row below
   if (y0 > 0) {          // slot 0 holds row y0-1
-    const float4 pcx = cx_row(st[0], y0 - 1);
+    const float4 pey_b = ld_pey(x, y0 - 1), phx_b = ld_phx(y0 - 1);
+    const EPsi ep0 = ld_epsi(y0);
+    const float4 pcx = cx_row(st[0], y0 - 1, pey_b);
     if (!wait(1)) return;
-    c = e_half(st[1 % NS], y0);
-    if (active) d_u = hx_adj<GEN>(p, rg, x, y0 - 1, st[0].lhx[me], pcx, c.cx, phx_r, lo).u;
+    c = e_half(st[1 % NS], y0, ep0);
+    if (active) d_u = hx_adj<GEN>(p, rg, x, y0 - 1, st[0].lhx[me], pcx, c.cx, phx_b).u;
     release(0);
     k = 1;
   } else {
-    c = e_half(st[0], y0);
+    c = e_half(st[0], y0, ld_epsi(y0));
   }
   for (int y = y0; y < y1; ++y, ++k) {
     const bool has_up = k + 1 < nslots;
+    // this iteration's psi inputs, issued before the wait and every store
+    const HPsi hp = ld_hpsi(y);
+    EPsi ep{f4(0.f), f4(0.f), f4(0.f)};
+    if (y + 1 < y1) ep = ld_epsi(y + 1);
+    else if (has_up) ep.pey = ld_pey(x, y + 1);
     if (has_up && !wait(k + 1)) return;
     AdjE up{f4(0.f), f4(0.f), f4(0.f), f4(0.f)};
-    if (y + 1 < y1) up = e_half(st[(k + 1) % NS], y + 1);
-    else if (has_up) up.cx = cx_row(st[(k + 1) % NS], y + 1);
-    h_half(st[k % NS], y, c, up.cx, d_u);
+    if (y + 1 < y1) up = e_half(st[(k + 1) % NS], y + 1, ep);
+    else if (has_up) up.cx = cx_row(st[(k + 1) % NS], y + 1, ep.pey);
+    h_half(st[k % NS], y, c, up.cx, d_u, hp);
     c = up;
     release(k);
   }

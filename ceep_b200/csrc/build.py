@@ -1,6 +1,7 @@
 """Build ``ceep_b200/_lib/libceep_b200.so`` from the CUDA sources in this folder.
 
     python -m ceep_b200.csrc.build            # or: python ceep_b200/csrc/build.py
+    python -m ceep_b200.csrc.build --incremental   # only the sources that changed
 
 Compiles for sm_100a only (B200), statically linking the CUDA runtime so the
 library does not depend on a particular libcudart on the loader path.  With
@@ -41,42 +42,59 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+OBJ_DIR = os.path.join(OUT_DIR, "obj")
+
+
+def _obj_stale(src: str, obj: str) -> bool:
+    """An object is rebuilt when it is missing or older than its source or
+    than any shared header."""
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    deps = [os.path.join(HERE, src)] + [os.path.join(HERE, h) for h in HEADERS] + \
+        [os.path.join(ROOT, "include", "ceep_b200.h")]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
 def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) -> str:
+    """Compile the sources that changed (every one with `force` or
+    `ptxas_info`), in parallel, and link the library.  Objects are kept in
+    _lib/obj so that a change to one source recompiles only that one."""
     if not force and not ptxas_info and not _stale():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
+    os.makedirs(OBJ_DIR, exist_ok=True)
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
     if ptxas_info:
         flags += ["-Xptxas", "-v"]
-    def compile_one(src):
-        obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
-        cmd = [nvcc()] + flags + ["-c", os.path.join(HERE, src), "-o", obj]
+    objs = [os.path.join(OBJ_DIR, src.replace(".cu", ".o")) for src in SOURCES]
+    todo = [(src, obj) for src, obj in zip(SOURCES, objs) if force or ptxas_info or _obj_stale(src, obj)]
+
+    def compile_one(job):
+        src, obj = job
+        cmd = [nvcc()] + flags + ["-c", os.path.join(HERE, src), "-o", obj + ".tmp"]
         if verbose:
             print(" ".join(cmd))
         return src, obj, subprocess.run(cmd, capture_output=True, text=True)
 
     # one nvcc per source, in parallel (the translation units are independent)
-    workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    workers = max(1, min(len(todo), os.cpu_count() or 1))
     with ThreadPoolExecutor(workers) as pool:
-        results = list(pool.map(compile_one, SOURCES))
+        results = list(pool.map(compile_one, todo))
     for src, obj, r in results:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
         if ptxas_info:
             sys.stdout.write(r.stderr)
-        objs.append(obj)
+        os.replace(obj + ".tmp", obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
-    for o in objs:
-        os.remove(o)
     return LIB
 
 
 if __name__ == "__main__":
     args = sys.argv[1:]
-    print(build(force=True, ptxas_info="--ptxas-info" in args, verbose="-v" in args))
+    print(build(force="--incremental" not in args, ptxas_info="--ptxas-info" in args, verbose="-v" in args))

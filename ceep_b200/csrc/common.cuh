@@ -81,6 +81,40 @@ CEEP_D void tile_costliest_first(int b, int gx, int gy, int& bx, int& by) {
   }
 }
 
+// Tile b of a gx x gy grid, frame tiles first: the fl leftmost and fr
+// rightmost tile columns (every row), then the ft top and fb bottom tile rows
+// of the other columns, then the interior tiles in row-major order (so that
+// neighbouring interior tiles, which share halo rows, still run close
+// together in time).  Frame tiles carry the CPML strips and edges and cost
+// several times an interior tile; started first, they no longer form the
+// launch's last wave.  A bijection of [0, gx*gy) for any fl + fr <= gx,
+// ft + fb <= gy.
+CEEP_D void tile_frame_first(int b, int gx, int gy, int fl, int fr, int ft, int fb, int& bx, int& by) {
+  const int fc = fl + fr, ic = gx - fc;
+  if (b < fc * gy) {
+    const int c = b % fc;
+    bx = c < fl ? c : gx - fr + (c - fl);
+    by = b / fc;
+    return;
+  }
+  int r = b - fc * gy;
+  if (ic <= 0) {  // every column is a frame column (handled above)
+    bx = 0;
+    by = 0;
+    return;
+  }
+  const int fw = ft + fb;
+  if (r < fw * ic) {
+    const int q = r / ic;
+    by = q < ft ? q : gy - fb + (q - ft);
+    bx = fl + r % ic;
+    return;
+  }
+  r -= fw * ic;
+  bx = fl + r % ic;
+  by = ft + r / ic;
+}
+
 // Streaming loads/stores.  Field state is read once and written once per
 // step, so the read-only path with an L1 hint is used for neighbours that
 // other threads of the same block also read.

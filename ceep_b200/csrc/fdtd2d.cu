@@ -536,7 +536,10 @@ template <int L, int ND, int NL>
 __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS) fdtd2d_step_kernel(const Fdtd2dParams p, int step, int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int CX = kConsumers / L;
-  step_block<L, ND, NL>(p, step, par, blockIdx.x * CX, blockIdx.y * p.rows, blockIdx.z, smem_raw);
+  int bx, by;
+  tile_frame_first(blockIdx.x, (p.nx + CX - 1) / CX, (p.ny + p.rows - 1) / p.rows, p.frame1[0], p.frame1[1],
+                   p.frame1[2], p.frame1[3], bx, by);
+  step_block<L, ND, NL>(p, step, par, bx * CX, by * p.rows, blockIdx.z, smem_raw);
 }
 
 // ------------------------------------------------------------------------
@@ -839,10 +842,13 @@ template <int L, int ND, int NL>
 __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step2_kernel(const Fdtd2dParams p, int step, int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int CX = kConsumers / L;
-  // row-major tile order: neighbouring tiles, which share halo rows and
-  // columns, run close together in time (their halos hit in L2)
-  step2_block<L, ND, NL>(p, step, par, (int)blockIdx.x * (CX - 2) - 1, (int)blockIdx.y * p.rows2, (int)blockIdx.z,
-                         smem_raw);
+  // frame tiles first, then the interior row-major: neighbouring interior
+  // tiles, which share halo rows and columns, run close together in time
+  // (their halos hit in L2)
+  int bx, by;
+  tile_frame_first(blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.frame2[0], p.frame2[1],
+                   p.frame2[2], p.frame2[3], bx, by);
+  step2_block<L, ND, NL>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
 }
 
 // Many phantoms, two steps per launch: block b runs two-step tile tiles[b]
@@ -881,6 +887,27 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
 // ------------------------------------------------------------------------
 // Host side: launch configuration and the rows-per-block choice.
 // ------------------------------------------------------------------------
+// Frame tile counts (left, right, top, bottom) of a tile grid whose column
+// bx starts at cell x0(bx) with `cw` thread columns and whose row by covers
+// `rows` cells (`halo`: the two-step kernel's step A rows reach one row
+// beyond each side), using the kernels' own interior tests.
+static void frame_counts(const Fdtd2dParams& p, int cw, int xstep, int xoff, int rows, bool halo, int out[4]) {
+  const int n = p.n, m = n > 1 ? n : 1;
+  const int gx = (p.nx + (halo ? cw - 3 : cw - 1)) / xstep, gy = (p.ny + rows - 1) / rows;
+  auto in_x = [&](int bx) { const int x0 = bx * xstep + xoff; return x0 >= n + 1 && x0 + cw <= p.nx - m; };
+  auto in_y = [&](int by) {
+    const int y0 = by * rows, y1 = y0 + rows < p.ny ? y0 + rows : p.ny;
+    const int a0 = halo ? (y0 > 0 ? y0 - 1 : 0) : y0, a1 = halo ? (y1 < p.ny ? y1 + 1 : p.ny) : y1;
+    return a0 >= n + 1 && a1 <= p.ny - m;
+  };
+  int fl = 0, fr = 0, ft = 0, fb = 0;
+  while (fl < gx && !in_x(fl)) ++fl;
+  while (fr < gx - fl && !in_x(gx - 1 - fr)) ++fr;
+  while (ft < gy && !in_y(ft)) ++ft;
+  while (fb < gy - ft && !in_y(gy - 1 - fb)) ++fb;
+  out[0] = fl; out[1] = fr; out[2] = ft; out[3] = fb;
+}
+
 template <int L, int ND, int NL>
 static cudaError_t configure_l(Fdtd2dParams& p) {
   constexpr size_t smem = stage_smem_bytes<L, ND + NL, NL>();
@@ -889,13 +916,15 @@ static cudaError_t configure_l(Fdtd2dParams& p) {
   if (e != cudaSuccess) return e;
   p.smem = (int)smem;
   if (p.rows > kMaxRows) p.rows = kMaxRows;
-  if (p.rows > 0) return cudaSuccess;
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConsumers + 32, smem);
-  if (e != cudaSuccess) return e;
-  p.rows = choose_rows(p.nx, p.ny, p.groups, kConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm), kMaxRows);
+  if (p.rows <= 0) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConsumers + 32, smem);
+    if (e != cudaSuccess) return e;
+    p.rows = choose_rows(p.nx, p.ny, p.groups, kConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm), kMaxRows);
+  }
+  frame_counts(p, kConsumers / L, kConsumers / L, 0, p.rows, false, p.frame1);
   return cudaSuccess;
 }
 
@@ -917,13 +946,14 @@ static cudaError_t configure2_l(Fdtd2dParams& p) {
   p.rows2 = p.rows_fixed > 0 ? (p.rows_fixed < 62 ? p.rows_fixed : 62)
                              : choose_rows(p.nx, p.ny, p.groups, kConsumers / L - 2,
                                            (long)sms * (per_sm < 1 ? 1 : per_sm), 62);
+  frame_counts(p, kConsumers / L, kConsumers / L - 2, -1, p.rows2, true, p.frame2);
   return cudaSuccess;
 }
 
 template <int L, int ND, int NL>
 static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
   constexpr int CX = kConsumers / L;
-  dim3 grid((p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.groups);
+  dim3 grid(((p.nx + CX - 3) / (CX - 2)) * ((p.ny + p.rows2 - 1) / p.rows2), 1, p.groups);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(kConsumers + 32);
@@ -954,7 +984,7 @@ int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int
 template <int L, int ND, int NL>
 static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
   constexpr int CX = kConsumers / L;
-  dim3 grid((p.nx + CX - 1) / CX, (p.ny + p.rows - 1) / p.rows, p.groups);
+  dim3 grid(((p.nx + CX - 1) / CX) * ((p.ny + p.rows - 1) / p.rows), 1, p.groups);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(kConsumers + 32);

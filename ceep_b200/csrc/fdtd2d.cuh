@@ -15,6 +15,8 @@ struct Fdtd2dParams {
   int rows;             // rows of the column segment one block walks
   int smem;             // dynamic shared memory per block
   int rows2, smem2;     // the same for the two-step kernel
+  int frame1[4];        // frame tile columns left/right and rows top/bottom, one-step geometry
+  int frame2[4];        // the same for the two-step geometry (launch order: frame tiles first)
   int rows_fixed;       // tile height the caller asked for (0 = chosen per kernel)
   float db, db_dx, inv_dx, dt, inv_dt;
   // per-group strides in float4
