@@ -689,7 +689,8 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
   uint64_t* empty = full + NS;
   const int nx = a.f.nx, ny = a.f.ny, n = a.f.n;
   int bx, by;
-  tile_costliest_first(blockIdx.x, (nx + CX - 1) / CX, (ny + a.rows - 1) / a.rows, bx, by);
+  tile_frame_first(blockIdx.x, (nx + CX - 1) / CX, (ny + a.rows - 1) / a.rows, a.frame[0], a.frame[1], a.frame[2],
+                   a.frame[3], bx, by);
   const int x0 = bx * CX, y0 = by * a.rows, g = blockIdx.y;
   const int y1 = min(y0 + a.rows, ny);
   const int rs = y0 > 0 ? y0 - 1 : 0;
@@ -727,7 +728,7 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
 // Host side
 // ------------------------------------------------------------------------
 // Tiles cost unequal time (CPML strips, probe rows), so a launch is cut into
-// about three waves of tiles, started costliest first, for the block
+// about three waves of tiles, frame tiles started first, for the block
 // scheduler to balance; segments stay >= 8 rows so the two neighbour rows
 // each one recomputes stay a small overhead.
 static int adjoint2d_rows(int nx, int ny, int groups, int cells_per_block, long slots) {
@@ -735,6 +736,25 @@ static int adjoint2d_rows(int nx, int ny, int groups, int cells_per_block, long 
   for (int rows = kAdjMaxRows; rows > 8; --rows)
     if (xb * ((ny + rows - 1) / rows) * groups >= 3 * slots) return rows;
   return 8;
+}
+
+// Frame tile counts (left, right, top, bottom) of the adjoint's tile grid,
+// by the kernel's own interior test: the leading and trailing columns and
+// rows of tiles that are not interior.
+static void adjoint_frame_counts(Adjoint2dParams& a, int cw) {
+  const int n = a.f.n, m = n > 1 ? n : 1, nx = a.f.nx, ny = a.f.ny;
+  const int gx = (nx + cw - 1) / cw, gy = (ny + a.rows - 1) / a.rows;
+  auto in_x = [&](int bx) { const int x0 = bx * cw; return x0 >= n + 2 && x0 + cw + 1 <= nx - m; };
+  auto in_y = [&](int by) {
+    const int y0 = by * a.rows, y1 = y0 + a.rows < ny ? y0 + a.rows : ny;
+    return y0 >= n + 2 && y1 + 1 <= ny - m;
+  };
+  int fl = 0, fr = 0, ft = 0, fb = 0;
+  while (fl < gx && !in_x(fl)) ++fl;
+  while (fr < gx - fl && !in_x(gx - 1 - fr)) ++fr;
+  while (ft < gy && !in_y(ft)) ++ft;
+  while (fb < gy - ft && !in_y(gy - 1 - fb)) ++fb;
+  a.frame[0] = fl; a.frame[1] = fr; a.frame[2] = ft; a.frame[3] = fb;
 }
 
 template <int L, int ND>
@@ -745,13 +765,15 @@ static cudaError_t configure_l(Adjoint2dParams& a) {
   if (e != cudaSuccess) return e;
   a.smem = (int)smem;
   if (a.rows > kAdjMaxRows) a.rows = kAdjMaxRows;
-  if (a.rows > 0) return cudaSuccess;
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kAdjConsumers + 32, smem);
-  if (e != cudaSuccess) return e;
-  a.rows = adjoint2d_rows(a.f.nx, a.f.ny, a.f.groups, kAdjConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm));
+  if (a.rows <= 0) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kAdjConsumers + 32, smem);
+    if (e != cudaSuccess) return e;
+    a.rows = adjoint2d_rows(a.f.nx, a.f.ny, a.f.groups, kAdjConsumers / L, (long)sms * (per_sm < 1 ? 1 : per_sm));
+  }
+  adjoint_frame_counts(a, kAdjConsumers / L);
   return cudaSuccess;
 }
 

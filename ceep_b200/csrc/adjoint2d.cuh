@@ -10,6 +10,7 @@ namespace ceep {
 struct Adjoint2dParams {
   Fdtd2dParams f;       // geometry, coefficients, CPML profile, sources, probes of the forward plan
   int rows;             // rows of the column segment one block walks
+  int frame[4];         // frame tile columns left/right and rows top/bottom (launch order: frame tiles first)
   int smem;             // dynamic shared memory per block
   // adjoint state, every array ping-pong (read [p], write [p ^ 1]) with the
   // layouts of the forward state

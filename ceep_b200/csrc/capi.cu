@@ -11,6 +11,7 @@
 #include "../../include/ceep_b200.h"
 #include "capi_internal.h"
 #include "fdtd2d.cuh"
+#include "common.cuh"
 
 namespace {
 thread_local char g_err[512] = "";
@@ -695,12 +696,17 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
     pc.nl = std::get<2>(keys[c]);
     std::vector<ceep::PackTile>& tl = host_tiles[c];
     std::vector<std::pair<int, size_t>> ends;  // (nsteps, tiles so far)
+    // each phantom's tiles in the single-grid launch order: frame tiles first
     for (auto& e : v) {
       const ceep::Fdtd2dParams& p = hp[e.second];
       const int cx = ceep::fdtd2d_cells_per_block(p.L);
+      const int gx = (p.nx + cx - 1) / cx, gy = (p.ny + p.rows - 1) / p.rows;
       for (int g = 0; g < p.groups; ++g)
-        for (int y0 = 0; y0 < p.ny; y0 += p.rows)
-          for (int x0 = 0; x0 < p.nx; x0 += cx) tl.push_back({e.second, x0, y0, g});
+        for (int b = 0; b < gx * gy; ++b) {
+          int bx, by;
+          ceep::tile_frame_first(b, gx, gy, p.frame1[0], p.frame1[1], p.frame1[2], p.frame1[3], bx, by);
+          tl.push_back({e.second, bx * cx, by * p.rows, g});
+        }
       ends.push_back({p.nsteps, tl.size()});
     }
     pc.active_by_step.assign(pk->max_steps, 0);
@@ -718,9 +724,13 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
     for (auto& e : v) {
       const ceep::Fdtd2dParams& p = hp[e.second];
       const int cx = ceep::fdtd2d_cells_per_block(p.L) - 2;
+      const int gx = (p.nx + cx - 1) / cx, gy = (p.ny + p.rows2 - 1) / p.rows2;
       for (int g = 0; g < p.groups; ++g)
-        for (int y0 = 0; y0 < p.ny; y0 += p.rows2)
-          for (int x = 0; x < p.nx; x += cx) t2.push_back({e.second, x - 1, y0, g});
+        for (int b = 0; b < gx * gy; ++b) {
+          int bx, by;
+          ceep::tile_frame_first(b, gx, gy, p.frame2[0], p.frame2[1], p.frame2[2], p.frame2[3], bx, by);
+          t2.push_back({e.second, bx * cx - 1, by * p.rows2, g});
+        }
       ends2.push_back({p.nsteps, t2.size()});
     }
     const int pairs = (pk->max_steps + 1) / 2;

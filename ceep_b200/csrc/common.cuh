@@ -51,36 +51,6 @@ CEEP_D void add_comp(float4& v, int i, float s) {
   if (i == 0) v.x += s; else if (i == 1) v.y += s; else if (i == 2) v.z += s; else v.w += s;
 }
 
-// Tile b of a gx x gy grid (columns x rows of tiles) in the order the block
-// scheduler should start them: the two edge columns (CPML x strips on every
-// row, the costliest tiles), then the first and last rows of tiles of the
-// other columns, then the rest.  A bijection of [0, gx*gy).
-CEEP_D void tile_costliest_first(int b, int gx, int gy, int& bx, int& by) {
-  if (gx <= 2) {
-    bx = b % gx;
-    by = b / gx;
-    return;
-  }
-  if (b < 2 * gy) {
-    bx = (b & 1) ? gx - 1 : 0;
-    by = b >> 1;
-    return;
-  }
-  int r = b - 2 * gy;
-  const int ic = gx - 2;
-  if (gy <= 2) {
-    bx = 1 + r % ic;
-    by = r / ic;
-  } else if (r < 2 * ic) {
-    bx = 1 + (r >> 1);
-    by = (r & 1) ? gy - 1 : 0;
-  } else {
-    r -= 2 * ic;
-    bx = 1 + r % ic;
-    by = 1 + r / ic;
-  }
-}
-
 // Tile b of a gx x gy grid, frame tiles first: the fl leftmost and fr
 // rightmost tile columns (every row), then the ft top and fb bottom tile rows
 // of the other columns, then the interior tiles in row-major order (so that
@@ -89,7 +59,8 @@ CEEP_D void tile_costliest_first(int b, int gx, int gy, int& bx, int& by) {
 // several times an interior tile; started first, they no longer form the
 // launch's last wave.  A bijection of [0, gx*gy) for any fl + fr <= gx,
 // ft + fb <= gy.
-CEEP_D void tile_frame_first(int b, int gx, int gy, int fl, int fr, int ft, int fb, int& bx, int& by) {
+__host__ __device__ __forceinline__ void tile_frame_first(int b, int gx, int gy, int fl, int fr, int ft, int fb,
+                                                          int& bx, int& by) {
   const int fc = fl + fr, ic = gx - fc;
   if (b < fc * gy) {
     const int c = b % fc;
