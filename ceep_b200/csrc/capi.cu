@@ -583,13 +583,20 @@ extern "C" int ceep2d_adjoint_rows(const ceep2d_adjoint* ad) { return ad ? ad->a
 namespace {
 struct PackClass {
   int L, nd, nl;
-  ceep::PackTile* tiles;            // device (inside the caller's workspace)
-  std::vector<int> active_by_step;  // tiles active at each step (a prefix)
-  // two steps per launch: tiles of the two-step geometry; at pair t (steps
-  // 2t, 2t+1) the phantoms with >= 2t+2 steps run two-step tiles (a prefix)
-  // and those with exactly 2t+1 steps run one-step tiles [tail_lo, tail_hi)
+  // One-step tiles: the frame tiles of every phantom (phantoms in order of
+  // decreasing step count), then their interior tiles, so that the running
+  // tiles of each part form a prefix and a launch starts every running
+  // phantom's frame tiles (several times an interior tile's cost) first.
+  ceep::PackTile* tiles;          // device (inside the caller's workspace)
+  int nf = 0;                     // frame tiles; the interior part starts at tiles + nf
+  std::vector<int> act_f, act_i;  // running frame / interior tiles at each step
+  // two steps per launch: tiles of the two-step geometry, laid out the same
+  // way; at pair t (steps 2t, 2t+1) the phantoms with >= 2t+2 steps run
+  // two-step tiles (a prefix of each part) and those with exactly 2t+1 steps
+  // run one-step tiles, a range of each part of the one-step table
   ceep::PackTile* tiles2;
-  std::vector<int> active2_by_pair, tail_lo_by_pair, tail_hi_by_pair;
+  int nf2 = 0;
+  std::vector<int> act2_f, act2_i, tail_f_lo, tail_f_hi, tail_i_lo, tail_i_hi;
 };
 size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 }  // namespace
@@ -694,61 +701,70 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
     pc.L = std::get<0>(keys[c]);
     pc.nd = std::get<1>(keys[c]);
     pc.nl = std::get<2>(keys[c]);
-    std::vector<ceep::PackTile>& tl = host_tiles[c];
-    std::vector<std::pair<int, size_t>> ends;  // (nsteps, tiles so far)
-    // each phantom's tiles in the single-grid launch order: frame tiles first
+    // frame test of tile (bx, by) of a gx x gy grid with frame counts fc
+    auto is_frame = [](int bx, int by, int gx, int gy, const int* fc) {
+      return bx < fc[0] || bx >= gx - fc[1] || by < fc[2] || by >= gy - fc[3];
+    };
+    std::vector<ceep::PackTile> tf, ti;
+    struct End { int steps; size_t f, i; };
+    std::vector<End> ends;  // per phantom: step count, frame and interior tiles so far
     for (auto& e : v) {
       const ceep::Fdtd2dParams& p = hp[e.second];
       const int cx = ceep::fdtd2d_cells_per_block(p.L);
       const int gx = (p.nx + cx - 1) / cx, gy = (p.ny + p.rows - 1) / p.rows;
       for (int g = 0; g < p.groups; ++g)
-        for (int b = 0; b < gx * gy; ++b) {
-          int bx, by;
-          ceep::tile_frame_first(b, gx, gy, p.frame1[0], p.frame1[1], p.frame1[2], p.frame1[3], bx, by);
-          tl.push_back({e.second, bx * cx, by * p.rows, g});
-        }
-      ends.push_back({p.nsteps, tl.size()});
+        for (int by = 0; by < gy; ++by)
+          for (int bx = 0; bx < gx; ++bx)
+            (is_frame(bx, by, gx, gy, p.frame1) ? tf : ti).push_back({e.second, bx * cx, by * p.rows, g});
+      ends.push_back({p.nsteps, tf.size(), ti.size()});
     }
-    pc.active_by_step.assign(pk->max_steps, 0);
-    for (int t = 0; t < pk->max_steps; ++t) {
-      size_t a = 0;
+    pc.nf = (int)tf.size();
+    std::vector<ceep::PackTile>& tl = host_tiles[c];
+    tl = tf;
+    tl.insert(tl.end(), ti.begin(), ti.end());
+    pc.act_f.assign(pk->max_steps, 0);
+    pc.act_i.assign(pk->max_steps, 0);
+    for (int t = 0; t < pk->max_steps; ++t)
       for (auto& en : ends)
-        if (en.first > t) a = en.second;
-      pc.active_by_step[t] = (int)a;
-    }
+        if (en.steps > t) {
+          pc.act_f[t] = (int)en.f;
+          pc.act_i[t] = (int)en.i;
+        }
     pc.tiles = reinterpret_cast<ceep::PackTile*>(ws + off);
     off += align16(tl.size() * sizeof(ceep::PackTile));
     // the two-step tables (same phantom order)
-    std::vector<ceep::PackTile>& t2 = host_tiles2[c];
-    std::vector<std::pair<int, size_t>> ends2;
+    std::vector<ceep::PackTile> t2f, t2i;
+    std::vector<End> ends2;
     for (auto& e : v) {
       const ceep::Fdtd2dParams& p = hp[e.second];
       const int cx = ceep::fdtd2d_cells_per_block(p.L) - 2;
       const int gx = (p.nx + cx - 1) / cx, gy = (p.ny + p.rows2 - 1) / p.rows2;
       for (int g = 0; g < p.groups; ++g)
-        for (int b = 0; b < gx * gy; ++b) {
-          int bx, by;
-          ceep::tile_frame_first(b, gx, gy, p.frame2[0], p.frame2[1], p.frame2[2], p.frame2[3], bx, by);
-          t2.push_back({e.second, bx * cx - 1, by * p.rows2, g});
-        }
-      ends2.push_back({p.nsteps, t2.size()});
+        for (int by = 0; by < gy; ++by)
+          for (int bx = 0; bx < gx; ++bx)
+            (is_frame(bx, by, gx, gy, p.frame2) ? t2f : t2i).push_back({e.second, bx * cx - 1, by * p.rows2, g});
+      ends2.push_back({p.nsteps, t2f.size(), t2i.size()});
     }
+    pc.nf2 = (int)t2f.size();
+    std::vector<ceep::PackTile>& t2 = host_tiles2[c];
+    t2 = t2f;
+    t2.insert(t2.end(), t2i.begin(), t2i.end());
     const int pairs = (pk->max_steps + 1) / 2;
-    pc.active2_by_pair.assign(pairs, 0);
-    pc.tail_lo_by_pair.assign(pairs, 0);
-    pc.tail_hi_by_pair.assign(pairs, 0);
+    for (auto* vec : {&pc.act2_f, &pc.act2_i, &pc.tail_f_lo, &pc.tail_f_hi, &pc.tail_i_lo, &pc.tail_i_hi})
+      vec->assign(pairs, 0);
     for (int t = 0; t < pairs; ++t) {
-      size_t a2 = 0, lo = 0, hi = 0;
       for (size_t k = 0; k < ends2.size(); ++k) {
-        if (ends2[k].first >= 2 * t + 2) {
-          a2 = ends2[k].second;
-          lo = ends[k].second;
+        if (ends2[k].steps >= 2 * t + 2) {
+          pc.act2_f[t] = (int)ends2[k].f;
+          pc.act2_i[t] = (int)ends2[k].i;
+          pc.tail_f_lo[t] = (int)ends[k].f;
+          pc.tail_i_lo[t] = (int)ends[k].i;
         }
-        if (ends2[k].first >= 2 * t + 1) hi = ends[k].second;
+        if (ends2[k].steps >= 2 * t + 1) {
+          pc.tail_f_hi[t] = (int)ends[k].f;
+          pc.tail_i_hi[t] = (int)ends[k].i;
+        }
       }
-      pc.active2_by_pair[t] = (int)a2;
-      pc.tail_lo_by_pair[t] = (int)lo;
-      pc.tail_hi_by_pair[t] = (int)hi;
     }
     pc.tiles2 = reinterpret_cast<ceep::PackTile*>(ws + off);
     off += align16(t2.size() * sizeof(ceep::PackTile));
@@ -780,14 +796,12 @@ static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream
     for (int64_t t = step0 / 2; 2 * t < step0 + nsteps; ++t)
       for (size_t ci = c0; ci < c1; ++ci) {
         auto& c = pk->classes[ci];
-        const int a2 = c.active2_by_pair[t], lo = c.tail_lo_by_pair[t], hi = c.tail_hi_by_pair[t];
-        cudaError_t e = cudaSuccess;
-        if (a2 > 0)
-          e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles2, a2, pk->params, (int)(2 * t), (int)(t & 1), true,
-                                         s);
-        if (e == cudaSuccess && hi > lo)
-          e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles + lo, hi - lo, pk->params, (int)(2 * t),
-                                         (int)(t & 1), false, s);
+        cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles2, c.act2_f[t], c.tiles2 + c.nf2,
+                                                   c.act2_i[t], pk->params, (int)(2 * t), (int)(t & 1), true, s);
+        if (e == cudaSuccess)
+          e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles + c.tail_f_lo[t], c.tail_f_hi[t] - c.tail_f_lo[t],
+                                         c.tiles + c.nf + c.tail_i_lo[t], c.tail_i_hi[t] - c.tail_i_lo[t],
+                                         pk->params, (int)(2 * t), (int)(t & 1), false, s);
         if (e != cudaSuccess) return ceep::cuda_fail(e, "packed step launch");
       }
     return CEEP_OK;
@@ -795,10 +809,8 @@ static int pack_steps(ceep2d_pack* pk, int64_t step0, int64_t nsteps, cudaStream
   for (int64_t t = step0; t < step0 + nsteps; ++t)
     for (size_t ci = c0; ci < c1; ++ci) {
       auto& c = pk->classes[ci];
-      const int act = c.active_by_step[t];
-      if (act == 0) continue;
-      cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, act, pk->params, (int)t, (int)(t & 1),
-                                                 false, s);
+      cudaError_t e = ceep::fdtd2d_launch_packed(c.L, c.nd, c.nl, c.tiles, c.act_f[t], c.tiles + c.nf, c.act_i[t],
+                                                 pk->params, (int)t, (int)(t & 1), false, s);
       if (e != cudaSuccess) return ceep::cuda_fail(e, "packed step launch");
     }
   return CEEP_OK;
@@ -898,7 +910,7 @@ extern "C" int ceep2d_pack_run(ceep2d_pack* pk, int64_t step0, int64_t nsteps, v
 extern "C" int ceep2d_pack_tiles(const ceep2d_pack* pk, int32_t step) {
   if (!pk || step < 0 || step >= pk->max_steps) return -1;
   int n = 0;
-  for (auto& c : pk->classes) n += c.active_by_step[step];
+  for (auto& c : pk->classes) n += c.act_f[step] + c.act_i[step];
   return n;
 }
 

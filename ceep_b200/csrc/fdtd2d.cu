@@ -851,15 +851,18 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   step2_block<L, ND, NL>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
 }
 
-// Many phantoms, two steps per launch: block b runs two-step tile tiles[b]
-// (x0 = its first thread column) of phantom tiles[b].phantom.
+// Many phantoms, two steps per launch: block b runs two-step tile
+// tiles_a[b] for b < na, else tiles_b[b - na] (the frame tiles of every
+// running phantom first, then their interior tiles; x0 = the tile's first
+// thread column) of phantom t.phantom.
 template <int L, int ND, int NL>
 __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
-    fdtd2d_packed2_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step,
-                          int par) {
+    fdtd2d_packed2_kernel(const PackTile* __restrict__ tiles_a, int na, const PackTile* __restrict__ tiles_b,
+                          const Fdtd2dParams* __restrict__ params, int step, int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(16) Fdtd2dParams sp;
-  const PackTile t = tiles[blockIdx.x];
+  const int b = (int)blockIdx.x;
+  const PackTile t = b < na ? tiles_a[b] : tiles_b[b - na];
   const int* src = reinterpret_cast<const int*>(params + t.phantom);
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
@@ -872,11 +875,12 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
 // (they are constant, so this happens before the dependency wait).
 template <int L, int ND, int NL>
 __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS)
-    fdtd2d_packed_kernel(const PackTile* __restrict__ tiles, const Fdtd2dParams* __restrict__ params, int step,
-                         int par) {
+    fdtd2d_packed_kernel(const PackTile* __restrict__ tiles_a, int na, const PackTile* __restrict__ tiles_b,
+                         const Fdtd2dParams* __restrict__ params, int step, int par) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(16) Fdtd2dParams sp;
-  const PackTile t = tiles[blockIdx.x];
+  const int b = (int)blockIdx.x;
+  const PackTile t = b < na ? tiles_a[b] : tiles_b[b - na];
   const int* src = reinterpret_cast<const int*>(params + t.phantom);
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
@@ -999,8 +1003,8 @@ static cudaError_t launch_l(const Fdtd2dParams& p, int step, int par, cudaStream
 }
 
 template <int L, int ND, int NL>
-static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step, int par,
-                                   bool two, cudaStream_t s) {
+static cudaError_t launch_packed_l(const PackTile* tiles_a, int na, const PackTile* tiles_b, int nb,
+                                   const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s) {
   const size_t smem = two ? step2_smem_bytes<L, ND, NL>() : stage_smem_bytes<L, ND + NL, NL>();
   static bool attr_set[2] = {false, false};
   if (!attr_set[two]) {
@@ -1012,7 +1016,7 @@ static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd
     attr_set[two] = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(ntiles);
+  cfg.gridDim = dim3(na + nb);
   cfg.blockDim = dim3(kConsumers + 32);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
@@ -1021,30 +1025,32 @@ static cudaError_t launch_packed_l(const PackTile* tiles, int ntiles, const Fdtd
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (two) return cudaLaunchKernelEx(&cfg, fdtd2d_packed2_kernel<L, ND, NL>, tiles, params, step, par);
-  return cudaLaunchKernelEx(&cfg, fdtd2d_packed_kernel<L, ND, NL>, tiles, params, step, par);
+  if (two) return cudaLaunchKernelEx(&cfg, fdtd2d_packed2_kernel<L, ND, NL>, tiles_a, na, tiles_b, params, step, par);
+  return cudaLaunchKernelEx(&cfg, fdtd2d_packed_kernel<L, ND, NL>, tiles_a, na, tiles_b, params, step, par);
 }
 
 template <int ND, int NL>
-static cudaError_t packed_l(int L, const PackTile* tiles, int ntiles, const Fdtd2dParams* params, int step, int par,
-                            bool two, cudaStream_t s) {
+static cudaError_t packed_l(int L, const PackTile* ta, int na, const PackTile* tb, int nb, const Fdtd2dParams* params,
+                            int step, int par, bool two, cudaStream_t s) {
   switch (L) {
-    case 1: return launch_packed_l<1, ND, NL>(tiles, ntiles, params, step, par, two, s);
-    case 2: return launch_packed_l<2, ND, NL>(tiles, ntiles, params, step, par, two, s);
-    case 4: return launch_packed_l<4, ND, NL>(tiles, ntiles, params, step, par, two, s);
-    default: return launch_packed_l<8, ND, NL>(tiles, ntiles, params, step, par, two, s);
+    case 1: return launch_packed_l<1, ND, NL>(ta, na, tb, nb, params, step, par, two, s);
+    case 2: return launch_packed_l<2, ND, NL>(ta, na, tb, nb, params, step, par, two, s);
+    case 4: return launch_packed_l<4, ND, NL>(ta, na, tb, nb, params, step, par, two, s);
+    default: return launch_packed_l<8, ND, NL>(ta, na, tb, nb, params, step, par, two, s);
   }
 }
 
-cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
-                                 const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s) {
+cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles_a, int na,
+                                 const PackTile* tiles_b, int nb, const Fdtd2dParams* params, int step, int par,
+                                 bool two, cudaStream_t s) {
+  if (na + nb <= 0) return cudaSuccess;
   switch (n_debye * 3 + n_lorentz) {
-    case 0: return packed_l<0, 0>(L, tiles, ntiles, params, step, par, two, s);
-    case 1: return packed_l<0, 1>(L, tiles, ntiles, params, step, par, two, s);
-    case 2: return packed_l<0, 2>(L, tiles, ntiles, params, step, par, two, s);
-    case 3: return packed_l<1, 0>(L, tiles, ntiles, params, step, par, two, s);
-    case 4: return packed_l<1, 1>(L, tiles, ntiles, params, step, par, two, s);
-    case 6: return packed_l<2, 0>(L, tiles, ntiles, params, step, par, two, s);
+    case 0: return packed_l<0, 0>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
+    case 1: return packed_l<0, 1>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
+    case 2: return packed_l<0, 2>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
+    case 3: return packed_l<1, 0>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
+    case 4: return packed_l<1, 1>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
+    case 6: return packed_l<2, 0>(L, tiles_a, na, tiles_b, nb, params, step, par, two, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -66,11 +66,14 @@ struct PackTile {
 };
 
 // Launch one step (two steps when `two`: tiles of the two-step geometry,
-// x0 = the first thread column) of every tile in `tiles` (all of one lane
-// width L and one ADE shape), each block reading its phantom's parameters
-// from `params`; `par` is the read half of every ping-pong array.
-cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles, int ntiles,
-                                 const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s);
+// x0 = the first thread column) of the tiles tiles_a[0, na) followed by
+// tiles_b[0, nb) (all of one lane width L and one ADE shape: the running
+// phantoms' frame tiles, then their interior tiles), each block reading its
+// phantom's parameters from `params`; `par` is the read half of every
+// ping-pong array.
+cudaError_t fdtd2d_launch_packed(int L, int n_debye, int n_lorentz, const PackTile* tiles_a, int na,
+                                 const PackTile* tiles_b, int nb, const Fdtd2dParams* params, int step, int par,
+                                 bool two, cudaStream_t s);
 int fdtd2d_cells_per_block(int L);
 // Rows per block for a column-strip x row-segment grid of `slots` resident blocks.
 int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int max_rows);

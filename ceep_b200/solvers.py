@@ -42,6 +42,29 @@ def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
     return None if t is None else t.data_ptr()
 
 
+class PinnedMaps:
+    """Page-locked host storage for the FP64 material maps of a solver that
+    runs on a CUDA device.  The maps are the one host-to-device transfer of a
+    material update (``update_materials``); from page-locked memory that copy
+    runs at the link's full rate instead of through the driver's staging
+    buffers.  ``hold`` returns a NumPy view of a page-locked buffer (kept per
+    key and reused while the shape stays) holding a copy of `arr`."""
+
+    def __init__(self):
+        self._bufs = {}
+
+    def hold(self, key, arr, shape=None) -> np.ndarray:
+        a = np.asarray(arr, np.float64)
+        shape = a.shape if shape is None else tuple(shape)
+        t = self._bufs.get(key)
+        if t is None or tuple(t.shape) != shape:
+            t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+            self._bufs[key] = t
+        out = t.numpy()
+        np.copyto(out, np.broadcast_to(a, shape))
+        return out
+
+
 class FDTDStatusError(RuntimeError):
     """A device status word reported a failure: CEEP_ERR_TIMEOUT (4, a bounded
     wait ran out) or CEEP_ERR_NONFINITE (5, the sentinel found NaN/Inf)."""
@@ -89,6 +112,7 @@ class BatchedFDTD2D:
         self.temporal_block = int(temporal_block)   # steps per kernel launch (1 or 2)
         self.sentinel_interval = 0                   # NaN/Inf scans between run-range ends (0: none)
         self.wait_limit_ns = 1_000_000_000           # bound of every device wait
+        self._pins: Optional[PinnedMaps] = None      # page-locked map storage once built on a GPU
         self.run_record: Optional[dict] = None       # last run's record (ceep_b200.trace)
         self.record_path: Optional[str] = None       # append each run's record as a JSON line
         self._built = False
@@ -154,8 +178,10 @@ class BatchedFDTD2D:
         if len(debye) + len(lorentz) > 2:
             raise ValueError("at most two ADE poles per cell are compiled in")
         shp = (self.nx, self.ny)
-        deb = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in debye]
-        lor = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in lorentz]
+        keep = ((lambda key, a: self._pins.hold(key, a, shp)) if self._pins is not None
+                else (lambda key, a: np.broadcast_to(np.asarray(a, np.float64), shp).copy()))
+        deb = [tuple(keep(("debye", i, j), a) for j, a in enumerate(p)) for i, p in enumerate(debye)]
+        lor = [tuple(keep(("lorentz", i, j), a) for j, a in enumerate(p)) for i, p in enumerate(lorentz)]
         # the cells outside the interior E region [n+1, nx-n) x [n+1, ny-n):
         # two full-width row bands and two column bands between them
         n = self.cpml_n
@@ -187,6 +213,14 @@ class BatchedFDTD2D:
         self._groups, self._gwidth = G, W
         dt = self.dt
         f32 = dict(dtype=torch.float32, device=dev)
+        # from here on the maps live in page-locked memory (update_materials copies them)
+        self._pins = PinnedMaps()
+        self._eps_r = self._pins.hold("eps_r", self._eps_r)
+        self._sigma_e = self._pins.hold("sigma_e", self._sigma_e)
+        self._debye = [tuple(self._pins.hold(("debye", i, j), a) for j, a in enumerate(p))
+                       for i, p in enumerate(self._debye)]
+        self._lorentz = [tuple(self._pins.hold(("lorentz", i, j), a) for j, a in enumerate(p))
+                         for i, p in enumerate(self._lorentz)]
         to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
         coef, ade = self._coef_tensors(self._eps_r, self._sigma_e, self._debye, self._lorentz)
         self._coef = coef

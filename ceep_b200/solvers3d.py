@@ -20,7 +20,7 @@ import torch
 from . import physics, trace
 from ._lib import Desc3D, check, lib
 from .constants import EPS_0, MU_0, cfl_timestep_3d
-from .solvers import _pad_tx, _ptr
+from .solvers import PinnedMaps, _pad_tx, _ptr
 
 
 class BatchedFDTD3D:
@@ -55,6 +55,7 @@ class BatchedFDTD3D:
         self.z_rows = int(z_rows)
         self.shell_z_rows = int(shell_z_rows)
         self.use_graph = bool(use_graph)
+        self._pins: Optional[PinnedMaps] = None      # page-locked map storage once built on a GPU
         self.run_record: Optional[dict] = None       # last run's record (ceep_b200.trace)
         self.record_path: Optional[str] = None       # append each run's record as a JSON line
         self._built = False
@@ -121,8 +122,10 @@ class BatchedFDTD3D:
         n = self.cpml_thickness
         inner = np.zeros(shp, bool)
         inner[n + 1:self.nx - n, n + 1:self.ny - n, n + 1:self.nz - n] = True
-        deb = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in debye]
-        lor = [tuple(np.broadcast_to(np.asarray(a, np.float64), shp).copy() for a in p) for p in lorentz]
+        keep = ((lambda key, a: self._pins.hold(key, a, shp)) if self._pins is not None
+                else (lambda key, a: np.broadcast_to(np.asarray(a, np.float64), shp).copy()))
+        deb = [tuple(keep(("debye", i, j), a) for j, a in enumerate(p)) for i, p in enumerate(debye)]
+        lor = [tuple(keep(("lorentz", i, j), a) for j, a in enumerate(p)) for i, p in enumerate(lorentz)]
         for p in deb + lor:
             if np.any((p[1] > 0) & (p[0] != 0) & ~inner):
                 raise ValueError("ADE pole present outside the interior E region")
@@ -148,6 +151,14 @@ class BatchedFDTD3D:
         self.ntx_pad, self._groups, self._gwidth = BP, G, W
         f32 = dict(dtype=torch.float32, device=dev)
         to_dev = lambda a, dt_=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt_).to(dev)
+        # from here on the maps live in page-locked memory (update_materials copies them)
+        self._pins = PinnedMaps()
+        for name in ("_eps_r", "_sigma_e", "_mu_r", "_sigma_m"):
+            setattr(self, name, self._pins.hold(name, getattr(self, name)))
+        self._debye = [tuple(self._pins.hold(("debye", i, j), a) for j, a in enumerate(p))
+                       for i, p in enumerate(self._debye)]
+        self._lorentz = [tuple(self._pins.hold(("lorentz", i, j), a) for j, a in enumerate(p))
+                         for i, p in enumerate(self._lorentz)]
         coef, ade = self._coef_maps()
         self._coef = coef
         self._ade_coef = ade if ade.shape[0] else None
