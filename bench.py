@@ -317,6 +317,15 @@ def run_ours(args, w):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w, sample_steps=args.cpu_steps if w.get("dim", 2) == 2 else 2)
 
+    # config 4's gradient cost (outside the timed region, one GPU only): the
+    # checkpointed adjoint at K = 50 and every step kept, against one forward
+    grad4 = None
+    if rank == 0 and world == 1 and args.workload == "head600" and not args.no_secondary:
+        t_fwd, ratios, _, _, _ = adjoint400_ratios(Ks=(1, 50), keep_budget=0, reps=2, split=False)
+        grad4 = {"workload": "adjoint400 (400^2, 1000 steps, 16 TX, Debye, S misfit)",
+                 "forward_ms": round(t_fwd, 3),
+                 "gradient_x_forward": {f"K={k}": round(v, 3) for k, v in ratios.items()}}
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -352,6 +361,8 @@ def run_ours(args, w):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    if grad4:
+        line["config4_gradient"] = grad4
     print(json.dumps(line), flush=True)
 
 
@@ -622,12 +633,15 @@ def run_adjoint_reference(args):
           flush=True)
 
 
-def run_adjoint_bench(args):
+def adjoint400_ratios(Ks=(1, 25, 50, 100), keep_budget=16 << 30, reps=2, split=True):
     """Config 4: cost of a full S-misfit gradient (forward with checkpoints +
-    segment recompute + adjoint) relative to one plain forward, for several
-    checkpoint intervals.  400x400, 0.5 mm, 1000 steps, CPML 15, 16 TX/RX,
-    101 frequencies, one-pole Debye head phantom (scaled to the grid); target
-    S from the phantom with its disk, parameters from the phantom without it."""
+    segment recompute + adjoint) relative to one plain forward, for the
+    checkpoint intervals `Ks` (and, with `keep_budget`, again with trailing
+    segments kept within that many bytes).  400x400, 0.5 mm, 1000 steps,
+    CPML 15, 16 TX/RX, 101 frequencies, one-pole Debye head phantom (scaled
+    to the grid); target S from the phantom with its disk, parameters from the
+    phantom without it.  Returns (forward ms, ratios, kept ratios, kept info,
+    the K = 1 split)."""
     import torch
     from ceep_b200 import BatchedFDTD2D
     from ceep_b200.adjoint import Adjoint2D, probes_with_grad, s_parameter_loss
@@ -669,10 +683,9 @@ def run_adjoint_bench(args):
         s2.reset()
         s2.advance(0, T, stream=stream)
     t_fwd = timed(fwd, 3)
-    ratios, kept_ratios, kept_info = {}, {}, {}
-    keep_budget = 16 << 30
-    for K, keep in ((1, 0), (25, 0), (50, 0), (100, 0), (25, keep_budget), (50, keep_budget),
-                    (100, keep_budget)):
+    ratios, kept_ratios, kept_info, split_ms = {}, {}, {}, None
+    cases = [(K, 0) for K in Ks] + ([(K, keep_budget) for K in Ks if K > 1] if keep_budget else [])
+    for K, keep in cases:
         sk = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, pos, pos, 2e9, device=str(dev))
         sk.set_phantom(no_disk)
         adj = Adjoint2D(sk, checkpoint_every=K, keep_bytes=keep)
@@ -683,7 +696,7 @@ def run_adjoint_bench(args):
             e.grad = g.grad = d.grad = None
             loss, _ = s_parameter_loss(probes_with_grad(e, g, adj, d, f64(tau)).double(), sk.dt, freqs, target)
             loss.backward()
-        r = timed(grad_step, 2) / t_fwd
+        r = timed(grad_step, reps) / t_fwd
         if keep:
             kept_ratios[K] = r
             nseg = -(-T // K)
@@ -693,19 +706,27 @@ def run_adjoint_bench(args):
             torch.cuda.empty_cache()
             continue
         ratios[K] = r
-        if K == 1:
+        if K == 1 and split:
             # split of one gradient: the forward that saves Ez/J of every step,
             # and the backward (adjoint steps + chain rule)
             adj.set_parameters(e.detach(), g.detach(), d.detach(), f64(tau))
             gprobe = torch.randn((len(pos), len(pos), T), dtype=torch.float32, device=dev)
             t_f = timed(adj.forward, 2)
             t_fb = timed(lambda: (adj.forward(), adj.backward(gprobe)), 2)
-            split = {"forward_save_ms": t_f, "backward_ms": t_fb - t_f}
+            split_ms = {"forward_save_ms": t_f, "backward_ms": t_fb - t_f}
         del adj, sk
         torch.cuda.empty_cache()
+    return t_fwd, ratios, kept_ratios, kept_info, split_ms
+
+
+def run_adjoint_bench(args):
+    """Config 4 on its own line: adjoint400_ratios at K = 1, 25, 50, 100 with
+    and without a 16 GiB keep budget."""
+    keep_budget = 16 << 30
+    t_fwd, ratios, kept_ratios, kept_info, split = adjoint400_ratios(keep_budget=keep_budget)
     line = {"metric": "adjoint gradient cost vs forward", "value": round(ratios[50], 3), "unit": "x forward",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded phantom)",
-            "config": {"workload": "adjoint400", "nx": nx, "ny": ny, "time_steps": T, "tx": 16, "cpml": n,
+            "config": {"workload": "adjoint400", "nx": 400, "ny": 400, "time_steps": 1000, "tx": 16, "cpml": 15,
                        "debye_poles": 1, "dft_freqs": 101, "loss": "sum |S - S*|^2",
                        "grad": "eps_r, sigma, debye delta_eps"},
             "forward_ms": round(t_fwd, 3), "ratio_by_checkpoint_interval": {str(k): round(v, 3) for k, v in ratios.items()},
@@ -1155,6 +1176,8 @@ def main():
     ap.add_argument("--temporal-block", type=int, default=2, choices=(1, 2),
                     help="2D steps per kernel launch (2 = temporal block of two)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="head600: skip the config-4 gradient-cost figure added to the line")
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N fused steps of one sample (for ncu), no timing, no JSON")

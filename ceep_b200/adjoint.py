@@ -39,17 +39,19 @@ from .solvers import BatchedFDTD2D, _ptr
 class _AdjDesc(C.Structure):
     P = C.c_void_p
     _fields_ = [("ez", P * 2), ("hx", P * 2), ("hy", P * 2), ("psi_hx", P * 2), ("psi_hy", P * 2),
-                ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("grad", P), ("probe_grad", P),
-                ("grad_tau", C.c_int32)]
+                ("psi_ezx", P * 2), ("psi_ezy", P * 2), ("j", P * 2), ("jp", P * 2), ("grad", P),
+                ("probe_grad", P), ("grad_tau", C.c_int32)]
 
 
-def grad_width(n_debye: int) -> int:
+def grad_width(poles: int) -> int:
     """Per-cell gradient slots of the adjoint: 2 + 3 per pole, rounded up to even."""
-    return (2 + 3 * n_debye + 1) // 2 * 2
+    return (2 + 3 * poles + 1) // 2 * 2
 
 
-def coefficient_maps(eps_r, sigma, debye, dt):
-    """Differentiable (ca, cb, dt/(eps_r eps0), [(k1, k2, gamma)]) from (nx, ny) FP64 maps."""
+def coefficient_maps(eps_r, sigma, debye, dt, lorentz=()):
+    """Differentiable (ca, cb, dt/(eps_r eps0), poles) from (nx, ny) FP64 maps;
+    poles: Debye (k1, k2, gamma), then Lorentz (k1, k2, k3)
+    (dispersive.py:253-261, :278-299)."""
     eps = eps_r * EPS_0
     poles = []
     for de, tau in debye:
@@ -61,6 +63,16 @@ def coefficient_maps(eps_r, sigma, debye, dt):
         g = torch.where(valid, (1.0 + k1) / 2.0, z)
         eps = eps + k2 / 2.0
         poles.append((k1, k2, g))
+    for de, w0, dl in lorentz:
+        valid = w0 > 0
+        w02, dt2 = w0 * w0, dt * dt
+        den = 4.0 + 2.0 * dl * dt + w02 * dt2
+        z = torch.zeros_like(w0)
+        k1 = torch.where(valid, (8.0 - 2.0 * w02 * dt2) / den, z)
+        k3 = torch.where(valid, -(4.0 - 2.0 * dl * dt + w02 * dt2) / den, z)
+        k2 = torch.where(valid, 2.0 * EPS_0 * de * w02 * dt2 / den, z)
+        eps = eps + k2 / 2.0
+        poles.append((k1, k2, k3))
     s = sigma * dt / (2.0 * eps)
     return (1.0 - s) / (1.0 + s), rdiv(dt, eps) / (1.0 + s), rdiv(dt, eps_r * EPS_0), poles
 
@@ -120,12 +132,15 @@ def run_segments_backward(starts, kept, recompute, adjoint, device, overlap, nbu
 
 
 class Adjoint2D:
-    """Gradient driver for one ``BatchedFDTD2D`` (Debye poles only).
+    """Gradient driver for one ``BatchedFDTD2D`` with at most one Debye pole
+    and any Lorentz poles (two poles in all).
 
-    ``grad_tau`` adds d(loss)/d(tau) for a dispersive solver.  Without it tau
-    is held fixed: the update coefficients k1 and gamma depend on tau alone,
-    so their gradients are never formed and the forward pass does not keep
-    the Debye currents of every step (one field less to write and read)."""
+    ``grad_tau`` adds d(loss)/d(tau) for a Debye pole.  Without it tau is held
+    fixed: the update coefficients k1 and gamma depend on tau alone, so their
+    gradients are never formed and the forward pass does not keep the Debye
+    currents of every step (one field less to write and read).  Lorentz poles
+    are differentiated in delta_eps; omega_0 and delta are held fixed (k1 and
+    k3 depend on them alone)."""
 
     def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False,
                  overlap: bool = True, keep_bytes: int = 0, reduce_ranks: bool = False):
@@ -133,8 +148,8 @@ class Adjoint2D:
         (``distributed.split_sources``) and the loss covers those; the
         gradient maps are summed over ranks (one all_reduce each), so every
         rank returns the gradient of the whole loss."""
-        if solver._lorentz:
-            raise ValueError("the adjoint supports Debye poles only")
+        if len(solver._debye) > 1:
+            raise ValueError("the adjoint supports one Debye pole (and Lorentz poles)")
         self.s = solver
         self.K = max(1, int(checkpoint_every))
         self.grad_tau = bool(grad_tau)
@@ -147,9 +162,12 @@ class Adjoint2D:
         self._ckpt = {}
 
     # -- parameters -------------------------------------------------------------
-    def set_parameters(self, eps_r: torch.Tensor, sigma: torch.Tensor, deps=None, tau=None) -> None:
+    def set_parameters(self, eps_r: torch.Tensor, sigma: torch.Tensor, deps=None, tau=None,
+                       lorentz_deps=()) -> None:
         """(nx, ny) maps in the reference's axis order; ``deps``/``tau`` are the
-        Debye maps of the solver's single pole when it has one."""
+        Debye maps of the solver's single Debye pole when it has one, and
+        ``lorentz_deps`` the delta_eps maps of its Lorentz poles (their
+        omega_0 and delta maps are the solver's own)."""
         s = self.s
         dev = s.device
         f64 = lambda t: torch.as_tensor(t, dtype=torch.float64).to(dev)
@@ -157,15 +175,18 @@ class Adjoint2D:
         debye = []
         if s._debye:
             debye = [(f64(deps), f64(tau))]
-        self._params = (eps_r, sigma, debye)
+        if len(lorentz_deps) != len(s._lorentz):
+            raise ValueError(f"{len(s._lorentz)} Lorentz delta_eps maps expected")
+        lorentz = [(f64(d), f64(w0), f64(dl)) for d, (_, w0, dl) in zip(lorentz_deps, s._lorentz)]
+        self._params = (eps_r, sigma, debye, lorentz)
         if not s._built:
             s._build()
-        ca, cb, dteps, poles = coefficient_maps(eps_r, sigma, debye, s.dt)
+        ca, cb, dteps, poles = coefficient_maps(eps_r, sigma, debye, s.dt, lorentz)
         coef = torch.stack([ca, cb, dteps, torch.zeros_like(ca)], -1).transpose(0, 1)   # (ny, nx, 4)
         s._coef.copy_(coef.to(torch.float32))
         if poles:
-            ade = torch.stack([torch.stack([k1, k2, g, torch.zeros_like(k1)], -1).transpose(0, 1)
-                               for k1, k2, g in poles])
+            ade = torch.stack([torch.stack([a, b, c, torch.zeros_like(a)], -1).transpose(0, 1)
+                               for a, b, c in poles])
             s._ade_coef.copy_(ade.to(torch.float32))
 
     # -- forward with checkpoints ---------------------------------------------------
@@ -176,6 +197,8 @@ class Adjoint2D:
               "psi_hx": s._psi_hx[cur], "psi_ezx": s._psi_ezx[cur], "psi_ezy": s._psi_ezy[cur]}
         if s._j is not None:
             st["j"] = s._j[cur]
+        if s._j_prev is not None:
+            st["j_prev"] = s._j_prev[cur]
         return st
 
     def _seglen(self):
@@ -244,6 +267,8 @@ class Adjoint2D:
         s._psi_ezx[0].copy_(ck["psi_ezx"]); s._psi_ezy[0].copy_(ck["psi_ezy"])
         if "j" in ck:
             s._j[0].copy_(ck["j"])
+        if "j_prev" in ck:
+            s._j_prev[0].copy_(ck["j_prev"])
         check(lib().ceep2d_plan_set_current_buffer(s._plan, 0), "ceep2d_plan_set_current_buffer")
 
     def _run_save(self, a, b, buf):
@@ -270,9 +295,10 @@ class Adjoint2D:
         pair = lambda t: [torch.zeros_like(t), torch.zeros_like(t)] if t is not None else [None, None]
         adj = {"ez": pair(s._ez[0]), "hx": pair(s._hx[0]), "hy": pair(s._hy[0]), "psi_hx": pair(s._psi_hx[0]),
                "psi_hy": pair(s._psi_hy[0]), "psi_ezx": pair(s._psi_ezx[0]), "psi_ezy": pair(s._psi_ezy[0]),
-               "j": pair(s._j[0] if s._j is not None else None)}
-        nd = len(s._debye)
-        kp = grad_width(nd)
+               "j": pair(s._j[0] if s._j is not None else None),
+               "jp": pair(s._j_prev[0] if s._j_prev is not None else None)}
+        nd, nl = len(s._debye), len(s._lorentz)
+        kp = grad_width(nd + nl)
         grad = torch.zeros((G, s.ny, s.nx, kp), dtype=torch.float64, device=dev)
         gp = torch.zeros((s.batch, max(len(s.probe_positions), 1), T), **f32)
         gp[:, :grad_probes.shape[1]] = grad_probes.to(torch.float32)
@@ -306,58 +332,72 @@ class Adjoint2D:
             self._kept = set()
             lib().ceep2d_adjoint_destroy(h)
         # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
-        res = self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * nd])
+        res = self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * (nd + nl)])
         return allreduce_gradient(res) if self.reduce_ranks else res
 
     def _chain(self, grad):
         """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""
-        eps_r, sigma, debye = self._params
+        eps_r, sigma, debye, lorentz = self._params
         inputs = [eps_r.detach().requires_grad_(True), sigma.detach().requires_grad_(True)]
         deb = [(de.detach().requires_grad_(True), tau.detach().requires_grad_(self.grad_tau)) for de, tau in debye]
+        lor = [(de.detach().requires_grad_(True), w0, dl) for de, w0, dl in lorentz]
         inputs += [de for de, _ in deb]
         if self.grad_tau:
             inputs += [tau for _, tau in deb]
+        inputs += [de for de, _, _ in lor]
         with torch.enable_grad():
-            ca, cb, _, poles = coefficient_maps(inputs[0], inputs[1], deb, self.s.dt)
+            ca, cb, _, poles = coefficient_maps(inputs[0], inputs[1], deb, self.s.dt, lor)
             outs = [ca, cb]
             gouts = [grad[0].t(), grad[1].t()]
-            for q, (k1, k2, g) in enumerate(poles):
-                outs += [k1, k2, g]
-                gouts += [grad[2 + 3 * q].t(), grad[3 + 3 * q].t(), grad[4 + 3 * q].t()]
+            for q, pole in enumerate(poles):
+                if q < len(deb):      # Debye: k1, k2, gamma
+                    outs += list(pole)
+                    gouts += [grad[2 + 3 * q].t(), grad[3 + 3 * q].t(), grad[4 + 3 * q].t()]
+                else:                 # Lorentz: only k2 depends on delta_eps
+                    outs.append(pole[1])
+                    gouts.append(grad[3 + 3 * q].t())
             # without grad_tau, k1 and gamma depend on fixed inputs only
             keep = [i for i, o in enumerate(outs) if o.requires_grad]
             grads = torch.autograd.grad([outs[i] for i in keep], inputs, [gouts[i] for i in keep],
                                         allow_unused=True)
         grads = [torch.zeros_like(x) if gr is None else gr for gr, x in zip(grads, inputs)]
         res = {"eps_r": grads[0], "sigma": grads[1]}
+        k = 2
         if deb:
             res["deps"] = grads[2]
+            k = 3
             if self.grad_tau:
                 res["tau"] = grads[3]
+                k = 4
+        if lor:
+            res["lorentz_deps"] = list(grads[k:k + len(lor)])
         return res
 
 
 class FDTD2DProbes(torch.autograd.Function):
-    """probes = FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint): the probe
-    series of an ``Adjoint2D``'s solver as a differentiable function of the
-    (nx, ny) maps; ``deps``/``tau`` may be None for a non-dispersive solver."""
+    """probes = FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint, *lorentz_deps):
+    the probe series of an ``Adjoint2D``'s solver as a differentiable function
+    of the (nx, ny) maps; ``deps``/``tau`` may be None for a solver without a
+    Debye pole, and ``lorentz_deps`` are the delta_eps maps of its Lorentz poles."""
 
     @staticmethod
-    def forward(ctx, eps_r, sigma, deps, tau, adjoint: Adjoint2D):
-        adjoint.set_parameters(eps_r, sigma, deps, tau)
+    def forward(ctx, eps_r, sigma, deps, tau, adjoint: Adjoint2D, *lorentz_deps):
+        adjoint.set_parameters(eps_r, sigma, deps, tau, lorentz_deps)
         ctx.adjoint = adjoint
         ctx.has_deps = deps is not None
+        ctx.n_lorentz = len(lorentz_deps)
         return adjoint.forward()
 
     @staticmethod
     def backward(ctx, grad_probes):
         g = ctx.adjoint.backward(grad_probes.contiguous())
+        lor = tuple(g.get("lorentz_deps", [None] * ctx.n_lorentz))
         return (g["eps_r"], g["sigma"], g.get("deps") if ctx.has_deps else None,
-                g.get("tau") if ctx.has_deps else None, None)
+                g.get("tau") if ctx.has_deps else None, None) + lor
 
 
-def probes_with_grad(eps_r, sigma, adjoint: Adjoint2D, deps=None, tau=None):
-    return FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint)
+def probes_with_grad(eps_r, sigma, adjoint: Adjoint2D, deps=None, tau=None, lorentz_deps=()):
+    return FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint, *lorentz_deps)
 
 
 def s_parameter_loss(probes: torch.Tensor, dt: float, frequencies, target: torch.Tensor):

@@ -72,30 +72,32 @@ CEEP_D float4 shfl_down4(float4 v, int d) {
 // The CPML psi slices are not staged: only strip cells read them, straight
 // from the read half of their ping-pong pair, which keeps a stage small
 // enough for three blocks per SM.
-template <int L, int ND>
+template <int L, int ND, int NL>
 struct AdjStage {
   static constexpr int CX = kAdjConsumers / L;
   static constexpr int H = CX + 2;
-  static constexpr int NQ = ND > 0 ? ND : 1;
-  float4 le[H * L];          // adjoint Ez (halo'd)
-  float4 lj[NQ * H * L];     // adjoint Debye currents (halo'd)
-  float4 coef[H];            // ca, cb, dt/(eps_r eps0), 0 (halo'd)
-  float4 ade[NQ * H];        // k1, k2, gamma, 0 (halo'd)
-  float4 en[CX * L];         // forward Ez^n
-  float4 e1[CX * L];         // forward Ez^{n+1}
-  float4 jn[NQ * CX * L];    // forward J^n
-  float4 lhx[CX * L];        // adjoint Hx
-  float4 lhy[(CX + 1) * L];  // adjoint Hy (left-halo'd)
+  static constexpr int NP = ND + NL;  // poles: the Debye ones first, then the Lorentz ones
+  static constexpr int NQ = NP > 0 ? NP : 1;
+  float4 le[H * L];                        // adjoint Ez (halo'd)
+  float4 lj[NQ * H * L];                   // adjoint currents of every pole (halo'd)
+  float4 coef[H];                          // ca, cb, dt/(eps_r eps0), 0 (halo'd)
+  float4 ade[NQ * H];                      // Debye (k1, k2, gamma, 0), Lorentz (k1, k2, k3, 0) (halo'd)
+  float4 en[CX * L];                       // forward Ez^n
+  float4 e1[CX * L];                       // forward Ez^{n+1}
+  float4 jn[ND > 0 ? ND * CX * L : 1];     // forward Debye J^n (tau gradients)
+  float4 ljp[NL > 0 ? NL * CX * L : 1];    // adjoint Lorentz J_prev
+  float4 lhx[CX * L];                      // adjoint Hx
+  float4 lhy[(CX + 1) * L];                // adjoint Hy (left-halo'd)
 };
 
 // Four stages where CEEP_ADJ_MIN_BLOCKS blocks of them fit an SM, else three.
-template <int L, int ND>
+template <int L, int ND, int NL>
 __host__ __device__ constexpr int adj_stages() {
-  return 4 * sizeof(AdjStage<L, ND>) <= (222 / CEEP_ADJ_MIN_BLOCKS) * 1024 ? 4 : 3;
+  return 4 * sizeof(AdjStage<L, ND, NL>) <= (222 / CEEP_ADJ_MIN_BLOCKS) * 1024 ? 4 : 3;
 }
-template <int L, int ND>
+template <int L, int ND, int NL>
 __host__ __device__ constexpr size_t adj_smem_bytes() {
-  return adj_stages<L, ND>() * sizeof(AdjStage<L, ND>) + 2 * adj_stages<L, ND>() * sizeof(uint64_t);
+  return adj_stages<L, ND, NL>() * sizeof(AdjStage<L, ND, NL>) + 2 * adj_stages<L, ND, NL>() * sizeof(uint64_t);
 }
 
 CEEP_D void adj_status(int* status, int code) {
@@ -198,18 +200,19 @@ CEEP_D void inject_probes(const Adjoint2dParams& a, float4& E, int x, int y, int
 // and the one below it: adjoint Hx.  Rows of the segment: forward Ez^n,
 // Ez^{n+1}, J^n and adjoint Hy.
 // ------------------------------------------------------------------------
-template <int L, int ND>
-CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty, int par,
+template <int L, int ND, int NL>
+CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND, NL>* st, uint64_t* full, uint64_t* empty, int par,
                         const float4* ez_n, const float4* ez_np1, const float4* j_n, int x0, int y0, int y1, int rs,
                         int nslots, int g) {
-  using St = AdjStage<L, ND>;
-  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
+  using St = AdjStage<L, ND, NL>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND, NL>();
   const Fdtd2dParams& p = a.f;
   const int nx = p.nx;
-  const size_t gf = (size_t)g * p.gs_field, gj = (size_t)g * p.gs_j;
+  const size_t gf = (size_t)g * p.gs_field, gj = (size_t)g * p.gs_j, gjp = (size_t)g * p.gs_jp;
   const size_t plane = (size_t)nx * p.ny;
   const float4* coef = reinterpret_cast<const float4*>(p.coef);
   const float4* ade = reinterpret_cast<const float4*>(p.ade_coef);
+  constexpr int NP = ND + NL;
   const int xa = x0 > 0 ? x0 - 1 : 0;                  // first halo'd cell
   const int xb = x0 + CX + 1 < nx ? x0 + CX + 1 : nx;  // end of the halo'd cells
   const int xe = x0 + CX < nx ? x0 + CX : nx;          // end of the owned cells
@@ -236,7 +239,7 @@ CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
       cp(S.le + ha * L, a.ez[par] + gf + (rowc + xa) * L, (xb - xa) * cb);
       cp(S.coef + ha, coef + rowc + xa, (xb - xa) * 16u);
 #pragma unroll
-      for (int q = 0; q < ND; ++q) {
+      for (int q = 0; q < NP; ++q) {
         cp(S.ade + q * H + ha, ade + q * plane + rowc + xa, (xb - xa) * 16u);
         cp(S.lj + (q * H + ha) * L, a.j[par] + gj + (q * plane + rowc + xa) * L, (xb - xa) * cb);
       }
@@ -249,6 +252,9 @@ CEEP_D void adj_produce(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
           for (int q = 0; q < ND; ++q) cp(S.jn + q * CX * L, j_n + gj + (q * plane + rowc + x0) * L, (xe - x0) * cb);
         }
         cp(S.lhy + ha * L, a.hy[par] + gf + (rowc + xa) * L, (xe - xa) * cb);
+#pragma unroll
+        for (int q = 0; q < NL; ++q)
+          cp(S.ljp + q * CX * L, a.jp[par] + gjp + (q * plane + rowc + x0) * L, (xe - x0) * cb);
       }
       if (!pass) mbar_arrive_expect_tx(&full[s], bytes);
     }
@@ -271,12 +277,12 @@ struct AdjE {
 // GEN = false for blocks whose cells, halo cells and neighbour rows all lie
 // in the plain interior of every region.
 // ------------------------------------------------------------------------
-template <int L, int ND, bool GEN>
-CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty, int step,
+template <int L, int ND, int NL, bool GEN>
+CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND, NL>* st, uint64_t* full, uint64_t* empty, int step,
                         int par, int x0, int y0, int y1, int rs, int nslots, int g) {
-  using St = AdjStage<L, ND>;
-  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
-  constexpr int KG = 2 + 3 * ND, KP = adjoint2d_grad_width(ND);
+  using St = AdjStage<L, ND, NL>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND, NL>();
+  constexpr int KG = 2 + 3 * (ND + NL), KP = adjoint2d_grad_width(ND + NL);
   const Fdtd2dParams& p = a.f;
   const int nx = p.nx, ny = p.ny, n = p.n;
   const AdjRegions rg{n, nx, ny};
@@ -335,7 +341,7 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
   auto jsum = [&](const St& S, int i) {
     float4 s = f4(0.f);
 #pragma unroll
-    for (int q = 0; q < ND; ++q) s = fma4(S.ade[q * H + i].y * p.inv_dt, S.lj[(q * H + i) * L + lo], s);
+    for (int q = 0; q < ND + NL; ++q) s = fma4(S.ade[q * H + i].y * p.inv_dt, S.lj[(q * H + i) * L + lo], s);
     return s;
   };
   // Adjoint psi of strip cells, read from the read halves of their pairs.  A
@@ -418,14 +424,20 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
         float4 elin = cf.x * e1tot;
         const float4 dedt = (e1 - en) * f4(p.inv_dt);
 #pragma unroll
-        for (int q = 0; q < ND; ++q) {
+        for (int q = 0; q < ND + NL; ++q) {
           const float4 kq = S.ade[q * H + cx + 1];
           const float4 jin = S.lj[(q * H + cx + 1) * L + lo];
           elin = fma4(-kq.y * p.inv_dt, jin, elin);
-          st4(a.j[par ^ 1] + (size_t)g * p.gs_j + (q * plane + (size_t)r * nx + x) * L + lo,
-              kq.x * jin - (cf.y * kq.z) * e1tot);
+          const size_t ja = (q * plane + (size_t)r * nx + x) * L + lo;
+          if (q < ND) {  // Debye: J' = k1 J + k2 dE/dt, E1 -= cb gamma J
+            st4(a.j[par ^ 1] + (size_t)g * p.gs_j + ja, kq.x * jin - (cf.y * kq.z) * e1tot);
+          } else {       // Lorentz: J' = k1 J + k3 Jp + k2 dE/dt, Jp' = J, E1 -= cb J
+            const size_t jpa = ((q - ND) * plane + (size_t)r * nx + x) * L + lo;
+            st4(a.j[par ^ 1] + (size_t)g * p.gs_j + ja, kq.x * jin + S.ljp[(q - ND) * CX * L + me] - cf.y * e1tot);
+            st4(a.jp[par ^ 1] + (size_t)g * p.gs_jp + jpa, kq.z * jin);
+          }
           gv[3 + 3 * q] = dot4(jin, dedt);
-          if (a.grad_tau) {  // k1 and gamma depend on tau alone
+          if (q < ND && a.grad_tau) {  // k1 and gamma depend on tau alone
             const float4 jn = S.jn[q * CX * L + me];
             gv[2 + 3 * q] = dot4(jin, jn);
             gv[4 + 3 * q] = -cf.y * dot4(e1tot, jn);
@@ -542,12 +554,12 @@ CEEP_D void adj_consume(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t*
 // of the row below is carried), and the new E adjoint, currents and
 // gradients of its cell.
 // ------------------------------------------------------------------------
-template <int L, int ND>
-CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint64_t* full, uint64_t* empty,
+template <int L, int ND, int NL>
+CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND, NL>* st, uint64_t* full, uint64_t* empty,
                              int step, int par, int x0, int y0, int y1, int rs, int nslots, int g) {
-  using St = AdjStage<L, ND>;
-  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND>();
-  constexpr int KG = 2 + 3 * ND, KP = adjoint2d_grad_width(ND);
+  using St = AdjStage<L, ND, NL>;
+  constexpr int CX = St::CX, H = St::H, NS = adj_stages<L, ND, NL>();
+  constexpr int KG = 2 + 3 * (ND + NL), KP = adjoint2d_grad_width(ND + NL);
   const Fdtd2dParams& p = a.f;
   const int nx = p.nx;
   const int cx = threadIdx.x / L, lo = threadIdx.x % L;
@@ -562,6 +574,7 @@ CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint
   float4* hx_out = a.hx[par ^ 1] + gf;
   float4* hy_out = a.hy[par ^ 1] + gf;
   float4* j_out = a.j[par ^ 1] + (size_t)g * p.gs_j;
+  float4* jp_out = a.jp[par ^ 1] + (size_t)g * p.gs_jp;
 
   // probe rows of the columns x-1, x, x+1 and this lane's source rows among
   // the slots' rows rs .. rs + nslots - 1 (<= 64), as bit masks
@@ -596,7 +609,7 @@ CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint
     if ((mask >> (r - rs)) & 1) inject_probes(a, E, xc, r, lane_g, step);
     float4 js = f4(0.f);
 #pragma unroll
-    for (int q = 0; q < ND; ++q) js = fma4(S.ade[q * H + i].y * idt, S.lj[(q * H + i) * L + lo], js);
+    for (int q = 0; q < ND + NL; ++q) js = fma4(S.ade[q * H + i].y * idt, S.lj[(q * H + i) * L + lo], js);
     return E + js;
   };
   auto nu_of = [&](const St& S, int i, float4 mu) { return (S.coef[i].y * inv) * mu; };
@@ -644,13 +657,19 @@ CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint
     for (int kk = 0; kk < KG; ++kk) gv[kk] = 0.f;
     float4 elin = cf.x * mu_c;
 #pragma unroll
-    for (int q = 0; q < ND; ++q) {
+    for (int q = 0; q < ND + NL; ++q) {
       const float4 kq = A.ade[q * H + cx + 1];
       const float4 jin = A.lj[(q * H + cx + 1) * L + lo];
       elin = fma4(-kq.y * idt, jin, elin);
-      st4(j_out + (q * plane + (size_t)y * nx + x) * L + lo, kq.x * jin - (cf.y * kq.z) * mu_c);
+      if (q < ND) {  // Debye
+        st4(j_out + (q * plane + (size_t)y * nx + x) * L + lo, kq.x * jin - (cf.y * kq.z) * mu_c);
+      } else {       // Lorentz (gamma = 1, second level J_prev)
+        st4(j_out + (q * plane + (size_t)y * nx + x) * L + lo,
+            kq.x * jin + A.ljp[(q - ND) * CX * L + me] - cf.y * mu_c);
+        st4(jp_out + ((q - ND) * plane + (size_t)y * nx + x) * L + lo, kq.z * jin);
+      }
       gv[3 + 3 * q] = dot4(jin, dedt);
-      if (a.grad_tau) {  // k1 and gamma depend on tau alone
+      if (q < ND && a.grad_tau) {  // k1 and gamma depend on tau alone
         const float4 jn = A.jn[q * CX * L + me];
         gv[2 + 3 * q] = dot4(jin, jn);
         gv[4 + 3 * q] = -cf.y * dot4(mu_c, jn);
@@ -677,13 +696,13 @@ CEEP_D void adj_consume_lean(const Adjoint2dParams& a, AdjStage<L, ND>* st, uint
   release(k);  // the row above the segment
 }
 
-template <int L, int ND>
+template <int L, int ND, int NL>
 __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
     adjoint2d_step_kernel(const Adjoint2dParams a, int step, int par, const float4* __restrict__ ez_n,
                           const float4* __restrict__ ez_np1, const float4* __restrict__ j_n) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  using St = AdjStage<L, ND>;
-  constexpr int NS = adj_stages<L, ND>(), CX = St::CX;
+  using St = AdjStage<L, ND, NL>;
+  constexpr int NS = adj_stages<L, ND, NL>(), CX = St::CX;
   St* st = reinterpret_cast<St*>(smem_raw);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * sizeof(St));
   uint64_t* empty = full + NS;
@@ -710,7 +729,7 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
   asm volatile("griddepcontrol.wait;" ::: "memory");
   if (threadIdx.x >= kAdjConsumers) {
     if (threadIdx.x == kAdjConsumers)
-      adj_produce<L, ND>(a, st, full, empty, par, ez_n, ez_np1, j_n, x0, y0, y1, rs, nslots, g);
+      adj_produce<L, ND, NL>(a, st, full, empty, par, ez_n, ez_np1, j_n, x0, y0, y1, rs, nslots, g);
     return;
   }
   // Block-uniform: own cells, the halo cells x0-1 and x0+CX and the rows
@@ -719,9 +738,9 @@ __global__ void __launch_bounds__(kAdjConsumers + 32, CEEP_ADJ_MIN_BLOCKS)
   const int m = n > 1 ? n : 1;
   const bool interior = x0 >= n + 2 && x0 + CX + 1 <= nx - m && y0 >= n + 2 && y1 + 1 <= ny - m;
   if (interior)
-    adj_consume_lean<L, ND>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+    adj_consume_lean<L, ND, NL>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
   else
-    adj_consume<L, ND, true>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+    adj_consume<L, ND, NL, true>(a, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
 }
 
 // ------------------------------------------------------------------------
@@ -757,10 +776,10 @@ static void adjoint_frame_counts(Adjoint2dParams& a, int cw) {
   a.frame[0] = fl; a.frame[1] = fr; a.frame[2] = ft; a.frame[3] = fb;
 }
 
-template <int L, int ND>
+template <int L, int ND, int NL>
 static cudaError_t configure_l(Adjoint2dParams& a) {
-  constexpr size_t smem = adj_smem_bytes<L, ND>();
-  auto kern = adjoint2d_step_kernel<L, ND>;
+  constexpr size_t smem = adj_smem_bytes<L, ND, NL>();
+  auto kern = adjoint2d_step_kernel<L, ND, NL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   a.smem = (int)smem;
@@ -777,7 +796,7 @@ static cudaError_t configure_l(Adjoint2dParams& a) {
   return cudaSuccess;
 }
 
-template <int L, int ND>
+template <int L, int ND, int NL>
 static cudaError_t launch_l(const Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
                             const float4* j_n, cudaStream_t s) {
   constexpr int CX = kAdjConsumers / L;
@@ -791,27 +810,29 @@ static cudaError_t launch_l(const Adjoint2dParams& a, int step, int par, const f
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, adjoint2d_step_kernel<L, ND>, a, step, par, ez_n, ez_np1, j_n);
+  return cudaLaunchKernelEx(&cfg, adjoint2d_step_kernel<L, ND, NL>, a, step, par, ez_n, ez_np1, j_n);
 }
 
-template <int ND>
+template <int ND, int NL>
 static cudaError_t dispatch_l(Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
                               const float4* j_n, cudaStream_t s, bool configure) {
   switch (a.f.L) {
-    case 1: return configure ? configure_l<1, ND>(a) : launch_l<1, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 2: return configure ? configure_l<2, ND>(a) : launch_l<2, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    case 4: return configure ? configure_l<4, ND>(a) : launch_l<4, ND>(a, step, par, ez_n, ez_np1, j_n, s);
-    default: return configure ? configure_l<8, ND>(a) : launch_l<8, ND>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 1: return configure ? configure_l<1, ND, NL>(a) : launch_l<1, ND, NL>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 2: return configure ? configure_l<2, ND, NL>(a) : launch_l<2, ND, NL>(a, step, par, ez_n, ez_np1, j_n, s);
+    case 4: return configure ? configure_l<4, ND, NL>(a) : launch_l<4, ND, NL>(a, step, par, ez_n, ez_np1, j_n, s);
+    default: return configure ? configure_l<8, ND, NL>(a) : launch_l<8, ND, NL>(a, step, par, ez_n, ez_np1, j_n, s);
   }
 }
 
 static cudaError_t dispatch(Adjoint2dParams& a, int step, int par, const float4* ez_n, const float4* ez_np1,
                             const float4* j_n, cudaStream_t s, bool configure) {
-  if (a.f.n_lorentz != 0) return cudaErrorInvalidValue;
-  switch (a.f.n_debye) {
-    case 0: return dispatch_l<0>(a, step, par, ez_n, ez_np1, j_n, s, configure);
-    case 1: return dispatch_l<1>(a, step, par, ez_n, ez_np1, j_n, s, configure);
-    case 2: return dispatch_l<2>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+  switch (a.f.n_debye * 3 + a.f.n_lorentz) {
+    case 0: return dispatch_l<0, 0>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 1: return dispatch_l<0, 1>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 2: return dispatch_l<0, 2>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 3: return dispatch_l<1, 0>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 4: return dispatch_l<1, 1>(a, step, par, ez_n, ez_np1, j_n, s, configure);
+    case 6: return dispatch_l<2, 0>(a, step, par, ez_n, ez_np1, j_n, s, configure);
     default: return cudaErrorInvalidValue;
   }
 }

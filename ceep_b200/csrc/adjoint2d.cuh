@@ -21,16 +21,18 @@ struct Adjoint2dParams {
   float4* psi_hy[2];    // x strips
   float4* psi_ezx[2];
   float4* psi_ezy[2];
-  float4* j[2];         // (G, poles, ny, nx, L)
+  float4* j[2];         // (G, poles, ny, nx, L), Debye poles first, then Lorentz
+  float4* jp[2];        // (G, n_lorentz, ny, nx, L): adjoint of the Lorentz J_prev
   // per-cell parameter gradients of each TX group, summed over steps:
   // (G, ny, nx, KP) with KP = 2 + 3*poles rounded up to even; per cell ca, cb,
-  // then per pole k1, k2, gamma (and a zero pad)
+  // then per Debye pole k1, k2, gamma and per Lorentz pole k1, k2, k3 (only
+  // k2 is formed for Lorentz poles), and a zero pad
   double* g;
   const float* probe_grad;  // (ntx, nprobe, nsteps) dLoss/dprobe
   int grad_tau;             // also d/dk1 and d/dgamma (reads the forward J^n); else those slots stay 0
 };
 
-__host__ __device__ constexpr int adjoint2d_grad_width(int n_debye) { return (2 + 3 * n_debye + 1) & ~1; }
+__host__ __device__ constexpr int adjoint2d_grad_width(int poles) { return (2 + 3 * poles + 1) & ~1; }
 
 // Kernel attributes and rows per block (when a.rows == 0).
 cudaError_t adjoint2d_configure(Adjoint2dParams& a);

@@ -436,13 +436,13 @@ struct ceep2d_adjoint {
 extern "C" int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoint_desc* d, ceep2d_adjoint** out) {
   if (!plan || !d || !out) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_create: null argument");
   *out = nullptr;
-  if (plan->p.n_lorentz) return fail(CEEP_ERR_UNSUPPORTED, "adjoint: Lorentz poles are not supported");
   for (int k = 0; k < 2; ++k) {
     if (!d->ez[k] || !d->hx[k] || !d->hy[k] || !d->grad)
       return fail(CEEP_ERR_INVALID, "adjoint: null state/gradient buffer");
     if (plan->p.n > 0 && (!d->psi_hx[k] || !d->psi_hy[k] || !d->psi_ezx[k] || !d->psi_ezy[k]))
       return fail(CEEP_ERR_INVALID, "adjoint: null psi buffer");
-    if (plan->p.n_debye && !d->j[k]) return fail(CEEP_ERR_INVALID, "adjoint: null current buffer");
+    if (plan->p.n_debye + plan->p.n_lorentz && !d->j[k]) return fail(CEEP_ERR_INVALID, "adjoint: null current buffer");
+    if (plan->p.n_lorentz && !d->jp[k]) return fail(CEEP_ERR_INVALID, "adjoint: null Lorentz J_prev buffer");
   }
   if (plan->p.nprobe && !d->probe_grad) return fail(CEEP_ERR_INVALID, "adjoint: null probe gradient");
   ceep2d_adjoint* ad = new (std::nothrow) ceep2d_adjoint();
@@ -460,6 +460,7 @@ extern "C" int ceep2d_adjoint_create(const ceep2d_plan* plan, const ceep2d_adjoi
     a.psi_ezx[k] = f4p(d->psi_ezx[k]);
     a.psi_ezy[k] = f4p(d->psi_ezy[k]);
     a.j[k] = f4p(d->j[k]);
+    a.jp[k] = f4p(d->jp[k]);
   }
   a.g = d->grad;
   a.probe_grad = d->probe_grad;

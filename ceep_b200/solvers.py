@@ -376,7 +376,7 @@ class BatchedFDTD2D:
         code = int(self._status.item())
         trace.emit(self, trace.make_record("BatchedFDTD2D", self.nx * self.ny, self.total_steps, self.batch,
                                            time.perf_counter() - t0, code))
-        self.check_status()
+        self.check_status(code)
         P = len(self.probe_positions)
         return {tx: {rx: probe_np[tx, rx, :] for rx in range(P)} for tx in range(self.batch)}
 
@@ -428,11 +428,12 @@ class BatchedFDTD2D:
     def hy(self):
         return self._ref_view(self._hy[self._cur()]) if self._built else None
 
-    def check_status(self) -> None:
+    def check_status(self, code: Optional[int] = None) -> None:
         """Raise if a bounded device wait gave up, or the NaN/Inf sentinel
-        found a non-finite value, during an earlier launch."""
+        found a non-finite value, during an earlier launch (`code`: the
+        status word when the caller has just read it)."""
         if self._built:
-            code = int(self._status.item())
+            code = int(self._status.item()) if code is None else int(code)
             if code:
                 self._status.zero_()
                 raise FDTDStatusError(code)

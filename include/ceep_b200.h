@@ -192,8 +192,9 @@ int ceep2d_pack_destroy(ceep2d_pack* pack);
  * (src/ceep/ai/__init__.py only announces a differentiable solver).  It is
  * the exact transpose of the fused step above, run backwards in time; per
  * cell it accumulates (over transmit events and steps) the gradients of the
- * loss with respect to ca, cb and the Debye k1, k2, gamma of each pole.
- * Debye poles only (Lorentz: CEEP_ERR_UNSUPPORTED).  One launch per step.
+ * loss with respect to ca, cb, the Debye k1, k2, gamma of each Debye pole
+ * and the k2 of each Lorentz pole (the transposed two-level Lorentz
+ * recurrence of dispersive.py:278-299 / :396-404).  One launch per step.
  * Every adjoint state array is a ping-pong pair shaped like the forward's
  * (both halves zeroed by the caller before the first run).
  * ---------------------------------------------------------------------- */
@@ -205,11 +206,17 @@ typedef struct ceep2d_adjoint_desc {
   float* psi_hy[2];
   float* psi_ezx[2];       /* adjoint E-CPML psi                             */
   float* psi_ezy[2];
-  float* j[2];             /* adjoint Debye currents                         */
-  double* grad;            /* (G, ny, nx, KP), KP = 2 + 3*n_debye rounded up
-                              to even: per TX group and cell d/dca, d/dcb,
-                              then per pole d/dk1, d/dk2, d/dgamma, then a
-                              zero pad; accumulated                          */
+  float* j[2];             /* adjoint currents of every pole (Debye first,
+                              then Lorentz; the forward J's shape)           */
+  float* jp[2];            /* adjoint Lorentz J_prev (the forward j_prev's
+                              shape); may be NULL without Lorentz poles      */
+  double* grad;            /* (G, ny, nx, KP), KP = 2 + 3*poles rounded up to
+                              even: per TX group and cell d/dca, d/dcb, then
+                              per Debye pole d/dk1, d/dk2, d/dgamma and per
+                              Lorentz pole d/dk1, d/dk2, d/dk3 (only d/dk2 is
+                              formed for Lorentz poles: k1 and k3 depend on
+                              omega_0 and delta alone), then a zero pad;
+                              accumulated                                    */
   const float* probe_grad; /* (ntx, nprobe, nsteps) dLoss/dprobe             */
   int32_t grad_tau;        /* nonzero: also d/dk1 and d/dgamma, which depend
                               on tau only and need the forward's saved J;

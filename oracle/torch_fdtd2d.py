@@ -19,8 +19,10 @@ import torch
 from .fdtd2d import EPS_0, MU_0, cpml_profile, gaussian_derivative_waveform, reference_dt_2d
 
 
-def coefficients(eps_r, sigma, debye, dt):
-    """ca, cb, dt/(eps_r eps0) and per-pole (k1, k2, gamma) as differentiable tensors."""
+def coefficients(eps_r, sigma, debye, dt, lorentz=()):
+    """ca, cb, dt/(eps_r eps0) and per-pole coefficients as differentiable
+    tensors: Debye (k1, k2, gamma), then Lorentz (k1, k2, k3)
+    (dispersive.py:253-261, :278-299)."""
     eps = eps_r * EPS_0
     poles = []
     for de, tau in debye:
@@ -31,6 +33,16 @@ def coefficients(eps_r, sigma, debye, dt):
         g = torch.where(valid, (1.0 + k1) / 2.0, torch.zeros_like(tau))
         eps = eps + k2 / 2.0
         poles.append((k1, k2, g))
+    for de, w0, dl in lorentz:
+        valid = w0 > 0
+        w02, dt2 = w0 * w0, dt * dt
+        den = 4.0 + 2.0 * dl * dt + w02 * dt2
+        z = torch.zeros_like(w0)
+        k1 = torch.where(valid, (8.0 - 2.0 * w02 * dt2) / den, z)
+        k3 = torch.where(valid, -(4.0 - 2.0 * dl * dt + w02 * dt2) / den, z)
+        k2 = torch.where(valid, 2.0 * EPS_0 * de * w02 * dt2 / den, z)
+        eps = eps + k2 / 2.0
+        poles.append((k1, k2, k3))
     s = sigma * dt / (2.0 * eps)
     ca = (1.0 - s) / (1.0 + s)
     cb = (dt / eps) / (1.0 + s)
@@ -83,16 +95,19 @@ class TorchFdtd2D:
             src[k, sx_, sy_] = 1.0
         self.srcmask = t(src)
 
-    def run(self, eps_r, sigma, debye=()):
-        """Probe series (B, P, T) as a differentiable function of the maps."""
+    def run(self, eps_r, sigma, debye=(), lorentz=()):
+        """Probe series (B, P, T) as a differentiable function of the maps
+        (Debye poles (delta_eps, tau), Lorentz poles (delta_eps, omega_0, delta))."""
         dt, inv = self.dt, 1.0 / self.dx
         db = dt / MU_0
         dbdx = db * inv
-        ca, cb, dteps, poles = coefficients(eps_r, sigma, debye, dt)
+        ca, cb, dteps, poles = coefficients(eps_r, sigma, debye, dt, lorentz)
+        nd = len(debye)
         B, nx, ny = self.B, self.nx, self.ny
         z = torch.zeros((B, nx, ny), dtype=torch.float64, device=self.device)
         E, X, Y, PHX, PHY, PEX, PEY = z, z, z, z, z, z, z
         J = [z for _ in poles]
+        Jp = [z for _ in poles[nd:]]
         px = torch.as_tensor([p[0] for p in self.prb], device=self.device)
         py = torch.as_tensor([p[1] for p in self.prb], device=self.device)
         out = []
@@ -109,10 +124,15 @@ class TorchFdtd2D:
             cX = X1 - torch.nn.functional.pad(X1[:, :, :-1], (1, 0))
             e1 = ca * E + cb * (cY * inv - cX * inv)
             if poles:
-                sgj = sum(g * j for (k1, k2, g), j in zip(poles, J))
+                # Debye J carries gamma, Lorentz J enters with gamma = 1
+                sgj = sum(c[2] * j if q < nd else j for q, (c, j) in enumerate(zip(poles, J)))
                 e1 = e1 - cb * sgj
                 dedt = (e1 - E) / dt
-                J = [torch.where(self.F9b, k1 * j + k2 * dedt, j) for (k1, k2, g), j in zip(poles, J)]
+                newJ = [torch.where(self.F9b, k1 * j + k2 * dedt, j) for (k1, k2, g), j in zip(poles[:nd], J[:nd])]
+                newJ += [torch.where(self.F9b, k1 * j + k3 * jp + k2 * dedt, j)
+                         for (k1, k2, k3), j, jp in zip(poles[nd:], J[nd:], Jp)]
+                Jp = [torch.where(self.F9b, j, jp) for j, jp in zip(J[nd:], Jp)]
+                J = newJ
             E1 = torch.where(self.F9b, e1, E)
             PEX = torch.where(self.SEx > 0, self.bex * PEX + self.cex * (cY * inv), PEX)
             E2 = E1 + self.SEx * dteps * PEX

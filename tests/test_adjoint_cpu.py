@@ -90,3 +90,59 @@ def test_segment_schedule_serial():
         assert [e[1] for e in log if e[0] == "a"] == starts
         assert all(e[3] == e[1] for e in log if e[0] == "a")       # each adjoint reads its own segment
         assert sorted(e[1] for e in log if e[0] == "r") == sorted(set(starts) - kept)
+
+
+def _lorentz_maps():
+    eps, sig, de, tau, m = _maps()
+    x, y = np.meshgrid(np.arange(NX), np.arange(NY), indexing="ij")
+    ml = (x - 16) ** 2 + (y - 15) ** 2 <= 5 ** 2
+    ldeps = np.where(ml, 4.0, 0.0)
+    lw0 = np.where(ml, 2 * np.pi * 6e9, 0.0)
+    ld = np.where(ml, 2 * np.pi * 0.5e9, 0.0)
+    return eps, sig, de, tau, (ldeps, lw0, ld), ml
+
+
+def _oracle_loss_lor(eps, sig, de, tau, lor, target):
+    o = Fdtd2DOracle(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9, eps_r=eps, sigma_e=sig,
+                     dispersion={"debye": [(de, tau)], "lorentz": [lor]})
+    o.run()
+    S = running_dft(o.probe_data, o.dt, FREQS)
+    return float(np.sum(np.abs(S - target) ** 2)), o
+
+
+def test_torch_restatement_with_a_lorentz_pole_equals_oracle():
+    eps, sig, de, tau, lor, _ = _lorentz_maps()
+    _, o = _oracle_loss_lor(eps, sig, de, tau, lor, 0.0)
+    t = TorchFdtd2D(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9)
+    tt = lambda a: torch.as_tensor(a, dtype=torch.float64)
+    p = t.run(tt(eps), tt(sig), [(tt(de), tt(tau))], [tuple(tt(a) for a in lor)]).numpy()
+    assert np.abs(p - o.probe_data).max() <= 1e-12 * np.abs(o.probe_data).max()
+
+
+def test_lorentz_delta_eps_gradient_matches_central_differences():
+    """d(S misfit)/d(Lorentz delta_eps) by autograd through the restatement
+    against central differences (h = 1e-3) of the FP64 oracle on 12 cells of
+    the Lorentz region (omega_0 and delta held fixed)."""
+    eps, sig, de, tau, (ldeps, lw0, ld), ml = _lorentz_maps()
+    eps_t = eps.copy(); eps_t[15:21, 13:19] = 12.0
+    _, ot = _oracle_loss_lor(eps_t, sig, de, tau, (ldeps, lw0, ld), 0.0)
+    target = running_dft(ot.probe_data, ot.dt, FREQS)
+    t = TorchFdtd2D(NX, NY, 0.5e-3, T, N, SRC, PRB, 2e9)
+    tt = lambda a: torch.as_tensor(a, dtype=torch.float64)
+    l_ = torch.tensor(ldeps, dtype=torch.float64, requires_grad=True)
+    probes = t.run(tt(eps), tt(sig), [(tt(de), tt(tau))], [(l_, tt(lw0), tt(ld))])
+    loss, _ = s_misfit_loss(probes, t.dt, FREQS, torch.as_tensor(target))
+    loss.backward()
+    rng = np.random.default_rng(5)
+    cells = [tuple(c) for c in np.argwhere(ml)[rng.choice(int(ml.sum()), 12, replace=False)]]
+    fd, ad = [], []
+    for c in cells:
+        vals = []
+        for sgn in (1, -1):
+            arr = ldeps.copy()
+            arr[c] += sgn * 1e-3
+            vals.append(_oracle_loss_lor(eps, sig, de, tau, (arr, lw0, ld), target)[0])
+        fd.append((vals[0] - vals[1]) / 2e-3)
+        ad.append(float(l_.grad[c]))
+    fd, ad = np.array(fd), np.array(ad)
+    assert np.linalg.norm(fd - ad) / np.linalg.norm(fd) < 1e-4

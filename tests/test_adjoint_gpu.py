@@ -183,3 +183,43 @@ def test_kept_segments_give_the_same_gradient(cuda_device):
             res.append(e.grad.clone())
     for r in res[1:]:
         assert torch.equal(res[0], r)
+
+
+@pytest.mark.parametrize("with_debye, K", [(True, 40), (False, 1)])
+def test_lorentz_pole_gradient_matches_autograd(with_debye, K):
+    """A Lorentz pole (with or without a Debye pole): the CUDA adjoint's
+    gradients of sum(probes * G) with respect to eps_r, sigma, the Debye
+    delta_eps and the Lorentz delta_eps against autograd through the FP64
+    restatement (dispersive.py:278-299 recurrence, two time levels)."""
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    dev = torch.device("cuda")
+    nx, ny, n, T, seed = 64, 60, 6, 150, 11   # sources outside the CPML strips
+    eps, sig, de, tau, m, ring = _case(nx, ny, n, seed, True, 4)
+    x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    ml = (x - nx // 2 - 2) ** 2 + (y - ny // 2 + 1) ** 2 <= 6 ** 2
+    lde = np.where(ml, 3.0 + np.random.default_rng(seed).random((nx, ny)), 0.0)
+    lw0, ldl = np.where(ml, 2 * np.pi * 5e9, 0.0), np.where(ml, 2 * np.pi * 0.6e9, 0.0)
+    src, prb = ring[:3], ring
+    f64 = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    G = torch.as_tensor(np.random.default_rng(seed + 100).standard_normal((3, len(prb), T)), device=dev)
+    t = TorchFdtd2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9, device=dev)
+    e_, s_, l_ = (f64(a).requires_grad_(True) for a in (eps, sig, lde))
+    d_ = f64(de).requires_grad_(True) if with_debye else None
+    deb = [(d_, f64(tau))] if with_debye else []
+    (t.run(e_, s_, deb, [(l_, f64(lw0), f64(ldl))]) * G).sum().backward()
+
+    s = BatchedFDTD2D(nx, ny, 0.5e-3, T, n, src, prb, 2e9)
+    s.set_dispersion(debye=[(de, tau)] if with_debye else [], lorentz=[(lde, lw0, ldl)])
+    adj = Adjoint2D(s, checkpoint_every=K)
+    e2, s2, l2 = (f64(a).requires_grad_(True) for a in (eps, sig, lde))
+    d2 = f64(de).requires_grad_(True) if with_debye else None
+    p = probes_with_grad(e2, s2, adj, d2, f64(tau) if with_debye else None, lorentz_deps=(l2,))
+    (p.double() * G).sum().backward()
+    pairs = [("eps_r", e2.grad, e_.grad), ("sigma", s2.grad, s_.grad), ("lorentz_deps", l2.grad, l_.grad)]
+    if with_debye:
+        pairs.append(("deps", d2.grad, d_.grad))
+    for name, got, want in pairs:
+        err = rel_l2(got.cpu().numpy(), want.cpu().numpy())
+        print(f"Lorentz adjoint (debye={with_debye}, K={K}) {name}: rel L2 {err:.2e}")
+        assert err < TOL, (name, err)
