@@ -249,6 +249,11 @@ def run_ours(args, w):
     if tblock != 1:
         solver.set_temporal_block(tblock)
     solver._build()
+    tile_rows = None
+    if w.get("dim", 2) == 2 and not args.no_autotune:
+        solver.load_material_tensors(mats[0])
+        solver.autotune()                  # tile height for this grid (results do not depend on it)
+        tile_rows = solver.rows_per_block
     stream = torch.cuda.current_stream(device)
     das_ws = torch.empty(1 << 20, dtype=torch.uint8, device=device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # > 126 MB L2
@@ -311,7 +316,7 @@ def run_ours(args, w):
     # -- end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(w, phantoms[:min(K, 5)], pos, freqs, device, tblock)
+        e2e = run_e2e(w, phantoms[:min(K, 5)], pos, freqs, device, tblock, rows=tile_rows or 0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -341,6 +346,7 @@ def run_ours(args, w):
                    "time_steps": w["steps"],
                    "tx": w["ntx"], "cpml": w["cpml"], "debye_poles": n_debye, "dft_freqs": w["nfreq"],
                    "das": f"{w['das']}x{w['das']}", "parallelism": f"replicas{world}",
+                   "tile_rows": tile_rows if tile_rows else "automatic",
                    "l2": "flushed (256 MB write) before every sample; per-step working set > L2",
                    "sample": "fused time loop + DFT->S + DAS image"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -384,7 +390,7 @@ class _HostMaps:
         return self.dispersion
 
 
-def run_e2e(w, phantoms, pos, freqs, device, tblock=1):
+def run_e2e(w, phantoms, pos, freqs, device, tblock=1, rows=0):
     """Public-API path per sample: host phantom maps -> set_phantom ->
     update_materials (H2D of the FP64 maps) -> run() (D2H of every series) ->
     s_matrix() (D2H) -> DAS image (D2H)."""
@@ -397,7 +403,8 @@ def run_e2e(w, phantoms, pos, freqs, device, tblock=1):
                                frequencies=freqs, device=str(device))
     else:
         solver = BatchedFDTD2D(w["nx"], w["ny"], w["dx"], w["steps"], w["cpml"], pos, pos, 2e9,
-                               frequencies=freqs, device=str(device), temporal_block=tblock)
+                               frequencies=freqs, device=str(device), temporal_block=tblock,
+                               rows_per_block=rows)   # the tile height the device-timed run tuned
     half = 0.07 if three else 0.09
     phantoms = [None if ph is None else _HostMaps(ph) for ph in phantoms]
     if phantoms[0] is not None:
@@ -1176,6 +1183,7 @@ def main():
     ap.add_argument("--temporal-block", type=int, default=2, choices=(1, 2),
                     help="2D steps per kernel launch (2 = temporal block of two)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="2D: keep the automatic tile height")
     ap.add_argument("--no-secondary", action="store_true",
                     help="head600: skip the config-4 gradient-cost figure added to the line")
     ap.add_argument("--cpu-steps", type=int, default=12)

@@ -307,6 +307,35 @@ class BatchedFDTD2D:
         self._apply_plan_settings()
         self.reset()
 
+    def autotune(self, candidates=(6, 8, 10, 12, 16), steps: int = 40) -> Dict[int, float]:
+        """Pick the tile height (rows per block) by timing `steps` graph-
+        replayed steps for each candidate on this solver's grid, and keep the
+        fastest; returns ms per step for each.  The results do not depend on
+        the tile height (the same cells, the same arithmetic); the state is
+        reset afterwards.  Not in the reference: a plan-time choice of this
+        framework's launch geometry."""
+        if not self._built:
+            self._build()
+        stream = torch.cuda.current_stream(self.device)
+        nst = min(int(steps), self.total_steps)
+        if self.temporal_block == 2 and nst > 1:
+            nst -= nst % 2
+        timings = {}
+        for rows in candidates:
+            self.set_rows_per_block(int(rows))
+            self.advance(0, nst, stream=stream)          # capture + warm
+            self.reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            self.advance(0, nst, stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize(self.device)
+            timings[int(rows)] = a.elapsed_time(b) / nst
+        best = min(timings, key=timings.get)
+        self.set_rows_per_block(best)
+        self.reset()
+        return timings
+
     def set_temporal_block(self, steps: int) -> None:
         """Steps per kernel launch: 1, or 2 (two steps per launch, each state
         word read and written once per pair; same arithmetic as 1)."""

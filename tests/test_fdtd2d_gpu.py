@@ -278,3 +278,24 @@ def test_ade_pole_mixes_against_oracle(cuda_device, kinds):
     s.set_dispersion(debye=deb, lorentz=lor)
     out = _probes(s.run(), B, len(prb))
     assert rel_l2(out, o.probe_data) < TOL
+
+
+def test_autotuned_tile_height_gives_the_same_bits():
+    """BatchedFDTD2D.autotune times each candidate tile height and keeps the
+    fastest; the probe series and fields equal a run at the automatic height."""
+    from ceep_b200 import BatchedFDTD2D
+    nx, ny, T = 120, 104, 90
+    src = [(30, 30), (90, 70), (60, 52), (40, 80), (85, 25)]
+    def mk():
+        s = BatchedFDTD2D(nx, ny, 0.5e-3, T, 10, src, src, 2e9)
+        x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+        m = (x - 60) ** 2 + (y - 52) ** 2 <= 20 ** 2
+        s._eps_r[m], s._sigma_e[m] = 12.0, 0.4
+        return s
+    a = mk()
+    a.run()
+    b = mk()
+    t = b.autotune(candidates=(6, 9, 14), steps=20)
+    assert set(t) == {6, 9, 14} and b.rows_per_block in t
+    b.run()
+    assert torch.equal(a.probe_data, b.probe_data) and torch.equal(a.ez, b.ez)
