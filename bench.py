@@ -1152,6 +1152,8 @@ def run_profile(args, w):
         w = dict(w, nx=128, ny=128, nz=128, ring=50)
     solver, pos, freqs, _, mats = build_inputs(w, 1, device)
     solver.use_graph = False
+    if args.rows and w.get("dim", 2) == 2:
+        solver.set_rows_per_block(args.rows)
     if w.get("dim", 2) == 2 and args.temporal_block != 1:
         solver.set_temporal_block(args.temporal_block)
     solver.load_material_tensors(mats[0])
@@ -1184,6 +1186,7 @@ def main():
                     help="2D steps per kernel launch (2 = temporal block of two)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="2D: keep the automatic tile height")
+    ap.add_argument("--rows", type=int, default=0, help="--profile of a 2D workload: this tile height")
     ap.add_argument("--no-secondary", action="store_true",
                     help="head600: skip the config-4 gradient-cost figure added to the line")
     ap.add_argument("--cpu-steps", type=int, default=12)

@@ -69,6 +69,7 @@ _SIGS = {
     "ceep2d_adjoint_destroy": (C.c_int, [P]),
     "ceep2d_adjoint_desc_size": (I64, []),
     "ceep2d_adjoint_rows": (C.c_int, [P]),
+    "ceep2d_adjoint_set_rows": (C.c_int, [P, I32]),
     "ceep2d_pack_workspace_bytes": (I64, [C.POINTER(P), I32]),
     "ceep2d_pack_create": (C.c_int, [C.POINTER(P), I32, P, I64, P, C.POINTER(P)]),
     "ceep2d_pack_run": (C.c_int, [P, I64, I64, P, C.c_int]),

@@ -143,7 +143,7 @@ class Adjoint2D:
     k3 depend on them alone)."""
 
     def __init__(self, solver: BatchedFDTD2D, checkpoint_every: int = 50, grad_tau: bool = False,
-                 overlap: bool = True, keep_bytes: int = 0, reduce_ranks: bool = False):
+                 overlap: bool = True, keep_bytes: int = 0, reduce_ranks: bool = False, rows: int = 0):
         """``reduce_ranks``: the solver holds this rank's transmit events only
         (``distributed.split_sources``) and the loss covers those; the
         gradient maps are summed over ranks (one all_reduce each), so every
@@ -156,6 +156,7 @@ class Adjoint2D:
         self.overlap = bool(overlap)
         self.keep_bytes = max(0, int(keep_bytes))
         self.reduce_ranks = bool(reduce_ranks)
+        self.rows = max(0, int(rows))   # tile height of the adjoint launch (0: automatic)
         self._kept = set()
         self.launch_rows = None         # tile rows of the adjoint launch (reported by the library)
         self._params = None
@@ -315,6 +316,8 @@ class Adjoint2D:
         self._buffers(nbuf)
         h = C.c_void_p()
         check(lib().ceep2d_adjoint_create(s._plan, C.addressof(d), C.byref(h)), "ceep2d_adjoint_create")
+        if self.rows:
+            check(lib().ceep2d_adjoint_set_rows(h, self.rows), "ceep2d_adjoint_set_rows")
         self.launch_rows = lib().ceep2d_adjoint_rows(h)
 
         def recompute(a, buf):

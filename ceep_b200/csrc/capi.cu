@@ -575,6 +575,13 @@ extern "C" int64_t ceep3d_adjoint_desc_size(void) { return (int64_t)sizeof(ceep3
 
 extern "C" int ceep2d_adjoint_rows(const ceep2d_adjoint* ad) { return ad ? ad->a.rows : 0; }
 
+extern "C" int ceep2d_adjoint_set_rows(ceep2d_adjoint* ad, int32_t rows) {
+  if (!ad || rows < 0) return fail(CEEP_ERR_INVALID, "ceep2d_adjoint_set_rows: bad adjoint or rows %d", rows);
+  ad->a.rows = rows;  // 0: the automatic choice
+  cudaError_t e = ceep::adjoint2d_configure(ad->a);
+  return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "adjoint2d configure");
+}
+
 // --------------------------------------------------------------------------
 // Packed multi-phantom 2D launch
 // --------------------------------------------------------------------------

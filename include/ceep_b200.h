@@ -236,6 +236,9 @@ int ceep2d_adjoint_destroy(ceep2d_adjoint* adj);
 int64_t ceep2d_adjoint_desc_size(void);
 /* Rows of the segment one block of the adjoint walks per step. */
 int ceep2d_adjoint_rows(const ceep2d_adjoint* adj);
+/* Tile height (rows per block) of the adjoint launch, 0 for the automatic
+ * choice (no reference counterpart: a launch-geometry setting). */
+int ceep2d_adjoint_set_rows(ceep2d_adjoint* adj, int32_t rows);
 
 /* ------------------------------------------------------------------------
  * 3D batched Yee FDTD.

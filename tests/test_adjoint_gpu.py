@@ -185,6 +185,31 @@ def test_kept_segments_give_the_same_gradient(cuda_device):
         assert torch.equal(res[0], r)
 
 
+def test_adjoint_tile_height_setting(cuda_device):
+    """``rows`` sets the adjoint launch's tile height; the gradient agrees
+    with the automatic choice to FP32 rounding: the interior-tile path adds
+    the adjoint curl terms in another order than the frame-tile path, so a
+    cell that moves between the two kinds of tile rounds differently."""
+    from ceep_b200 import BatchedFDTD2D
+    from ceep_b200.adjoint import Adjoint2D, probes_with_grad
+    eps, sig, de, tau, m, ring = _case(72, 64, 6, 8)
+    res = []
+    for rows in (0, 4, 12):
+        s = BatchedFDTD2D(72, 64, 0.5e-3, 130, 6, ring[:3], ring, 2e9)
+        s.set_dispersion(debye=[(de, tau)])
+        adj = Adjoint2D(s, checkpoint_every=11, rows=rows)
+        e = torch.tensor(eps, dtype=torch.float64, device="cuda", requires_grad=True)
+        p = probes_with_grad(e, torch.tensor(sig, device="cuda"), adj, torch.tensor(de, device="cuda"),
+                             torch.tensor(tau, device="cuda"))
+        (p.double() ** 2).sum().backward()
+        if rows:
+            assert adj.launch_rows == rows
+        res.append(e.grad.clone())
+    scale = res[0].abs().max()
+    for r in res[1:]:
+        assert float((r - res[0]).abs().max() / scale) < 1e-5
+
+
 @pytest.mark.parametrize("with_debye, K", [(True, 40), (False, 1)])
 def test_lorentz_pole_gradient_matches_autograd(with_debye, K):
     """A Lorentz pole (with or without a Debye pole): the CUDA adjoint's
