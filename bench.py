@@ -84,7 +84,7 @@ def algorithmic_bytes_per_step_2d(w, n_debye, n_lorentz=0):
 
 # CUDA sources a kernel's DRAM traffic depends on (their hash is recorded in
 # the profile summary the traffic figure comes from)
-KERNEL_SOURCES = {2: ("fdtd2d.cu", "fdtd2d.cuh", "common.cuh", "tma.cuh"),
+KERNEL_SOURCES = {2: ("fdtd2d.cu", "fdtd2d.cuh", "fdtd2d_kernels.cuh", "common.cuh", "tma.cuh"),
                   3: ("fdtd3d.cu", "fdtd3d.cuh", "common.cuh")}
 
 

@@ -1,6 +1,6 @@
 // Exact discrete adjoint of the fused 2D step (sm_100a): one launch per step.
 //
-// The forward step (fdtd2d.cu, after fdtd_2d_batched.py:454-526) is a chain
+// The forward step (fdtd2d_kernels.cuh, after fdtd_2d_batched.py:454-526) is a chain
 // of linear maps; the transposed step applies their transposes in reverse
 // order.  Per cell it has two halves:
 //
@@ -104,7 +104,7 @@ CEEP_D void adj_status(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
-// Region predicates of the forward step (fdtd2d.cu) for one cell.
+// Region predicates of the forward step (fdtd2d_kernels.cuh) for one cell.
 struct AdjRegions {
   int n, nx, ny;
   CEEP_D bool f9(int x, int y) const { return x >= n + 1 && x < nx - n && y >= n + 1 && y < ny - n; }

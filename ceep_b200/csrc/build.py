@@ -20,10 +20,13 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libceep_b200.so")
-SOURCES = ["capi.cu", "fdtd2d.cu", "fdtd3d.cu", "adjoint2d.cu", "adjoint3d.cu", "spectral.cu", "phantom.cu",
-           "single2d.cu"]
-HEADERS = ["common.cuh", "fdtd2d.cuh", "fdtd3d.cuh", "adjoint2d.cuh", "adjoint3d.cuh", "tma.cuh",
-           "capi_internal.h"]
+# the 2D forward kernels compile once per ADE shape (fdtd2d_d<ND>l<NL>.cu)
+FDTD2D_SHAPES = ["fdtd2d_d0l0.cu", "fdtd2d_d0l1.cu", "fdtd2d_d0l2.cu", "fdtd2d_d1l0.cu", "fdtd2d_d1l1.cu",
+                 "fdtd2d_d2l0.cu"]
+SOURCES = ["capi.cu", "fdtd2d.cu"] + FDTD2D_SHAPES + ["fdtd3d.cu", "adjoint2d.cu", "adjoint3d.cu", "spectral.cu",
+                                                      "phantom.cu", "single2d.cu"]
+HEADERS = ["common.cuh", "fdtd2d.cuh", "fdtd2d_kernels.cuh", "fdtd3d.cuh", "adjoint2d.cuh", "adjoint3d.cuh",
+           "tma.cuh", "capi_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -63,7 +66,9 @@ def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) 
     if not force and not ptxas_info and not _stale():
         return LIB
     os.makedirs(OBJ_DIR, exist_ok=True)
-    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
+    # -compress-all: the per-shape fatbins with line info are otherwise stored uncompressed (~3x larger)
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+                    "-Xfatbin", "-compress-all"]
     if ptxas_info:
         flags += ["-Xptxas", "-v"]
     objs = [os.path.join(OBJ_DIR, src.replace(".cu", ".o")) for src in SOURCES]

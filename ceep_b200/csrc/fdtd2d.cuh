@@ -5,6 +5,10 @@
 
 namespace ceep {
 
+// Consumer threads of a 2D step block (one float4 lane each); one producer
+// warp more makes the block.
+constexpr int kConsumers = 128;
+
 struct Fdtd2dParams {
   int nx, ny, n;
   int ntx;              // real transmit events
@@ -52,6 +56,11 @@ struct Fdtd2dParams {
   // Bound of every mbarrier wait, in ns of the global timer (0 = 1 s).
   unsigned long long wait_ns;
 };
+
+// Record an error code in the plan's status word; the first error wins.
+__device__ __forceinline__ void record_status(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
 
 // Scan Ez (nf4 float4) and probes[tx][q][steps s0..s1) for NaN/Inf; on a hit
 // record CEEP_ERR_NONFINITE in *status (first error wins).
