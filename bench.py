@@ -104,13 +104,15 @@ def profile_traffic(name, dim):
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None, None
-    traffic, sha = None, None
+    traffic, sha, rows = None, None, None
     for line in open(path):
         if line.startswith("dram_bytes_per_launch"):
             traffic = int(line.split("=")[1])
         elif line.startswith("source_sha256"):
             sha = line.split("=")[1].strip()
-    return traffic, {"file": "profiles/" + name, "source_sha256": sha,
+        elif line.startswith("tile_rows"):
+            rows = int(line.split("=")[1])
+    return traffic, {"file": "profiles/" + name, "source_sha256": sha, "tile_rows": rows,
                      "matches_current_source": sha == kernel_source_sha(dim) if sha else None}
 
 

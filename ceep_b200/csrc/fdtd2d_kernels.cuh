@@ -543,9 +543,22 @@ constexpr size_t step2_smem_bytes() {
   return kStages2 * sizeof(Stage2d<L, ND + NL, NL>) + 2 * kStages2 * sizeof(uint64_t) + 2 * sizeof(Exch2<L>) + 16;
 }
 
+// Slot index and phase parity of a position in an NS-slot mbarrier ring.
+template <int NS>
+struct RingPos {
+  int slot;
+  uint32_t phase;
+  CEEP_D void advance() {
+    if (++slot == NS) {
+      slot = 0;
+      phase ^= 1u;
+    }
+  }
+};
+
 CEEP_D void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
 
-template <int L, bool GEN, int ND, int NL>
+template <int L, bool GEN, int ND, int NL, bool PK>
 CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty,
                      Exch2<L>* xr, volatile int* abort_flag, int step, int par, int x0, int y0, int y1, int ya0,
                      int ya1, int rs, int nslots, int g) {
@@ -582,10 +595,12 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
   // A timed-out wait sets the block's abort flag; the warps then skip every
   // later wait and all arithmetic but keep taking the consumer barrier, so
   // all four reach it the same number of times.
+  // Ring positions advance by one slot per row (slot index and phase carried,
+  // no division by the ring depth).
   bool aborted = false;
-  auto wait = [&](int k) {
+  auto wait = [&](RingPos<kStages2> c) {
     if (aborted) return;
-    const bool ok = mbar_wait_bounded(&full[k % kStages2], (k / kStages2) & 1, wait_limit(p));
+    const bool ok = mbar_wait_bounded(&full[c.slot], c.phase, wait_limit(p));
     if (__any_sync(0xffffffffu, !ok)) {
       if (lane_warp == 0) {
         record_status(p.status, CEEP_ERR_TIMEOUT);
@@ -594,9 +609,9 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
       aborted = true;
     }
   };
-  auto release = [&](int k) {
+  auto release = [&](int slot) {
     __syncwarp();
-    if (lane_warp == 0) mbar_arrive(&empty[k % kStages2]);
+    if (lane_warp == 0) mbar_arrive(&empty[slot]);
   };
 
   // step A's results for this column's previous row, which step B uses next
@@ -610,7 +625,7 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
   float4 hxb_prev = f4(0.f);  // Hx^{n+3/2}(x, y-1)
 
   // Step B on own row y, given A's E^{n+1}(x, y+1) (zero above the grid).
-  auto b_row = [&](int y, float4 e1_up) {
+  auto b_row = [&](int y, float4 e1_up, bool src_row, bool prb_row) {
     const Exch2<L>& XB = xr[y & 1];
     const float4 e1_c = XB.e[t], e1_r = XB.e[t + L], e1_l = XB.e[t - L];
     float4 phy_c = XB.phy[t], phy_l = XB.phy[t - L];
@@ -648,29 +663,43 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
     }
     if (fl & kEX) st4(psi_ezx + ((size_t)y * 2 * n + ex_s) * L + lo, pex);
     if (fl & kEY) st4(psi_ezy + ((size_t)sp.ey_row(y) * nx + x) * L + lo, pey);
-    if ((src_rows >> (y - ya0)) & 1) add_sources(p, e2, x, y, lane_g, step + 1);
-    if ((prb_rows >> (y - ya0)) & 1) record_probes(p, e2, x, y, lane_g, step + 1);
+    if (PK ? (src_rows >> (y - ya0)) & 1 : src_row) add_sources(p, e2, x, y, lane_g, step + 1);
+    if (PK ? (prb_rows >> (y - ya0)) & 1 : prb_row) record_probes(p, e2, x, y, lane_g, step + 1);
     st4(ezw + at, e2);
     if (p.save_ez) st4(save_ez_slot(p, step + 2, g) + at, e2);
     hxb_prev = hxb;
   };
 
-  wait(0);
-  int k = 0;
+  // The ring position of row slice k+1 and the slot of slice k, k counting
+  // the slices from 0 (row rs).
+  RingPos<kStages2> up{0, 0u};
+  int cs = 0;
+  wait(up);
+  up.advance();
+  const int k0 = ya0 > 0 ? 1 : 0;  // slices before A's first row
   if (ya0 > 0) {  // slot 0 holds row ya0-1: A's Hx^{n+1/2}(x, ya0-1)
-    wait(1);
+    wait(up);
     if (valid && !aborted) {
       const Stage2d<L, NP, NL>& A = st[0];
       hxa_prev = hx_new<GEN>(p, A.phx[cx * L + lo], nullptr, x, ya0 - 1, A.hx[cx * L + lo],
-                             A.ez[(cx + 1) * L + lo], st[1 % kStages2].ez[(cx + 1) * L + lo]);
+                             A.ez[(cx + 1) * L + lo], st[up.slot].ez[(cx + 1) * L + lo]);
     }
-    release(0);
-    k = 1;
+    release(cs);
+    cs = up.slot;
+    up.advance();
   }
+  const int r_up = ya0 + nslots - 1 - k0;  // rows below r_up have the next slice in the ring
 
-  for (int r = ya0; r < ya1; ++r, ++k) {
-    const bool has_up = k + 1 < nslots;
-    if (has_up) wait(k + 1);
+  // Source/probe bits of A's row r and of B's row r-1.  The single-grid
+  // kernel shifts copies of the masks by one row per iteration; the packed
+  // kernel (its parameters held in shared memory leave fewer registers) tests
+  // bit r - ya0 of the masks in place.
+  uint64_t srcm = src_rows, prbm = prb_rows;
+  bool src_prev = false, prb_prev = false;
+
+  for (int r = ya0; r < ya1; ++r) {
+    const bool has_up = r < r_up;
+    if (has_up) wait(up);
     float4 a_e = f4(0.f), a_hy = f4(0.f), a_phy = f4(0.f);
     float4 c_hx = f4(0.f), c_cf = f4(0.f), c_phx = f4(0.f), c_pex = f4(0.f), c_pey = f4(0.f);
     float4 kq[NQ], jq[NQ], jm[NLQ];
@@ -678,12 +707,15 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
     for (int q = 0; q < NQ; ++q) kq[q] = jq[q] = f4(0.f);
 #pragma unroll
     for (int q = 0; q < NLQ; ++q) jm[q] = f4(0.f);
-    if (valid && !aborted) {
+    // Interior blocks compute step A unconditionally (every column is valid;
+    // after an abort the values are never stored), so the zero defaults
+    // above fold away on that path.
+    if (!GEN || (valid && !aborted)) {
       // step A on row r: the one-step consumer's arithmetic
-      const Stage2d<L, NP, NL>& A = st[k % kStages2];
+      const Stage2d<L, NP, NL>& A = st[cs];
       const int i0 = (cx + 1) * L + lo;
       const float4 ez_c = A.ez[i0];
-      const float4 ez_up = has_up ? st[(k + 1) % kStages2].ez[i0] : f4(0.f);
+      const float4 ez_up = has_up ? st[up.slot].ez[i0] : f4(0.f);
       bool sx, sy2, dummy;
       c_phx = A.phx[cx * L + lo];
       const float4 hxn = hx_step<GEN>(p, x, r, A.hx[cx * L + lo], ez_c, ez_up, c_phx, sx);
@@ -706,9 +738,9 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
       c_cf = A.coef[cx];
       uint32_t fl;
       a_e = e_step<GEN, ND, NL>(p, x, r, ez_c, hyn - hyl, hxn - hxa_prev, c_cf, kq, jq, jm, c_pex, c_pey, fl);
-      if ((src_rows >> (r - ya0)) & 1) add_sources(p, a_e, x, r, lane_g, step);
-      if (own && r >= y0 && r < y1) {
-        if ((prb_rows >> (r - ya0)) & 1) record_probes(p, a_e, x, r, lane_g, step);
+      if (PK ? (src_rows >> (r - ya0)) & 1 : srcm & 1) add_sources(p, a_e, x, r, lane_g, step);
+      if (own && !aborted && r >= y0 && r < y1) {
+        if (PK ? (prb_rows >> (r - ya0)) & 1 : prbm & 1) record_probes(p, a_e, x, r, lane_g, step);
         if (p.save_ez) {  // the adjoint's copy of step n+1 (own cells)
           const size_t at = ((size_t)r * nx + x) * L + lo;
           st4(save_ez_slot(p, step + 1, g) + at, a_e);
@@ -735,8 +767,14 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
         bool dummy;
         hxb_prev = hx_step<GEN>(p, x, y, pv_hx, xr[y & 1].e[t], a_e, ps, dummy);
       } else {
-        b_row(y, a_e);
+        b_row(y, a_e, src_prev, prb_prev);
       }
+    }
+    if (!PK) {
+      src_prev = srcm & 1;
+      prb_prev = prbm & 1;
+      srcm >>= 1;
+      prbm >>= 1;
     }
     pv_hx = c_hx;
     pv_cf = c_cf;
@@ -750,18 +788,20 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
     }
 #pragma unroll
     for (int q = 0; q < NLQ; ++q) pv_jm[q] = jm[q];
-    release(k);
+    release(cs);
+    cs = up.slot;
+    up.advance();
     consumer_barrier();
     if (*abort_flag) aborted = true;
   }
-  if (k < nslots) release(k);  // the Ez-only slot of row ya1
+  if (ya1 - ya0 + k0 < nslots) release(cs);  // the Ez-only slot of row ya1
   // the last own row when no A row lies above it (y1 == ny)
-  if (own && !aborted && ya1 == y1 && y1 - 1 >= y0) b_row(y1 - 1, f4(0.f));
+  if (own && !aborted && ya1 == y1 && y1 - 1 >= y0) b_row(y1 - 1, f4(0.f), src_prev, prb_prev);
 }
 
 // One block of the two-step kernel: thread columns x0 .. x0+CX-1 (outputs
 // x0+1 .. x0+CX-2), own rows y0 .. y0+rows2-1, TX group g.
-template <int L, int ND, int NL>
+template <int L, int ND, int NL, bool PK>
 CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
   using St = Stage2d<L, ND + NL, NL>;
   constexpr int CX = kConsumers / L;
@@ -796,9 +836,9 @@ CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0
   const int m = n > 1 ? n : 1;
   const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
   if (interior)
-    consume2<L, false, ND, NL>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
+    consume2<L, false, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
   else
-    consume2<L, true, ND, NL>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
+    consume2<L, true, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
 }
 
 template <int L, int ND, int NL>
@@ -811,7 +851,7 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   int bx, by;
   tile_frame_first(blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.frame2[0], p.frame2[1],
                    p.frame2[2], p.frame2[3], bx, by);
-  step2_block<L, ND, NL>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
+  step2_block<L, ND, NL, false>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
 }
 
 // Many phantoms, two steps per launch: block b runs two-step tile
@@ -830,7 +870,7 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  step2_block<L, ND, NL>(sp, step, par, t.x0, t.y0, t.g, smem_raw);
+  step2_block<L, ND, NL, true>(sp, step, par, t.x0, t.y0, t.g, smem_raw);
 }
 
 // Many phantoms in one launch: block b runs tile tiles[b] of phantom
