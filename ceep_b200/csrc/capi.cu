@@ -43,6 +43,7 @@ struct ceep2d_plan {
   int cur = 0;       // ping-pong buffer holding the current state
   int tblock = 1;    // steps per launch (1, or 2 with the temporal-block kernel)
   int sentinel = 0;  // NaN/Inf check every this many steps (0: only at the end of each run range)
+  ceep::Fdtd2dSide side{nullptr, nullptr, nullptr};  // the two-step frame tiles' stream
   // captured step loops keyed by (step0, nsteps, starting buffer, save buffers, save base, steps per launch)
   std::map<std::tuple<int64_t, int64_t, int, const void*, const void*, int64_t, int>, cudaGraphExec_t> graphs;
 };
@@ -115,10 +116,22 @@ extern "C" int ceep2d_plan_create(const ceep2d_desc* d, ceep2d_plan** out) {
   p.status = d->status;
   p.fault_row = -1;
   p.wait_ns = 1000000000ull;
+  p.split2 = 0;
   cudaError_t ce = ceep::fdtd2d_configure(p);
   if (ce != cudaSuccess) {
     delete pl;
     return ceep::cuda_fail(ce, "fdtd2d_configure");
+  }
+  // the frame tiles' stream at the highest priority, so that their blocks
+  // (few, long) start first and the interior kernel's fill the rest
+  int least = 0, greatest = 0;
+  ce = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&pl->side.stream, cudaStreamNonBlocking, greatest);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&pl->side.fork, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&pl->side.join, cudaEventDisableTiming);
+  if (ce != cudaSuccess) {
+    ceep2d_plan_destroy(pl);
+    return ceep::cuda_fail(ce, "ceep2d_plan_create: side stream");
   }
   *out = pl;
   return CEEP_OK;
@@ -133,11 +146,11 @@ static int64_t launch_count(int64_t nsteps, int tblock) { return tblock == 2 ? (
 // samples recorded since its previous scan after every `sentinel` steps (0:
 // none in between) and after the range's last step.
 static int run_steps(const ceep::Fdtd2dParams& p, int64_t step0, int64_t nsteps, int cur, int tblock, int sentinel,
-                     cudaStream_t s) {
+                     cudaStream_t s, const ceep::Fdtd2dSide* side) {
   int64_t checked = step0;
   for (int64_t k = 0; k < nsteps;) {
     const bool two = tblock == 2 && k + 1 < nsteps;
-    cudaError_t e = two ? ceep::fdtd2d_launch_step2(p, (int)(step0 + k), cur, s)
+    cudaError_t e = two ? ceep::fdtd2d_launch_step2(p, (int)(step0 + k), cur, s, side)
                         : ceep::fdtd2d_launch_step(p, (int)(step0 + k), cur, s);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "fdtd2d step launch");
     k += two ? 2 : 1;
@@ -175,8 +188,9 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int cur = pl->cur;
   const int cur_after = cur ^ (int)(launch_count(nsteps, pl->tblock) & 1);
+  const ceep::Fdtd2dSide* side = pl->side.stream ? &pl->side : nullptr;
   if (!use_graph || s == nullptr) {
-    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s, side);
     if (rc == CEEP_OK) pl->cur = cur_after;
     return rc;
   }
@@ -186,7 +200,7 @@ static int plan_run(ceep2d_plan* pl, int64_t step0, int64_t nsteps, void* stream
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamBeginCapture");
-    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s);
+    int rc = run_steps(q, step0, nsteps, cur, pl->tblock, pl->sentinel, s, side);
     e = cudaStreamEndCapture(s, &g);
     if (rc != CEEP_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return ceep::cuda_fail(e, "cudaStreamEndCapture");
@@ -230,7 +244,18 @@ extern "C" int ceep2d_plan_rows(const ceep2d_plan* pl) { return pl ? pl->p.rows 
 extern "C" int ceep2d_plan_destroy(ceep2d_plan* pl) {
   if (!pl) return CEEP_OK;
   for (auto& kv : pl->graphs) cudaGraphExecDestroy(kv.second);
+  if (pl->side.stream) cudaStreamSynchronize(pl->side.stream);
+  if (pl->side.join) cudaEventDestroy(pl->side.join);
+  if (pl->side.fork) cudaEventDestroy(pl->side.fork);
+  if (pl->side.stream) cudaStreamDestroy(pl->side.stream);
   delete pl;
+  return CEEP_OK;
+}
+
+extern "C" int ceep2d_plan_set_frame_split(ceep2d_plan* pl, int32_t on) {
+  if (!pl) return fail(CEEP_ERR_INVALID, "null plan");
+  if (pl->p.split2 != (on != 0)) drop_graphs(pl);
+  pl->p.split2 = on != 0;
   return CEEP_OK;
 }
 
@@ -268,7 +293,12 @@ extern "C" int ceep2d_plan_inject_copy_fault(ceep2d_plan* pl, int32_t row) {
 }
 
 extern "C" int64_t ceep2d_plan_launches(const ceep2d_plan* pl, int64_t nsteps) {
-  return (!pl || nsteps < 0) ? 0 : launch_count(nsteps, pl->tblock);
+  if (!pl || nsteps < 0) return 0;
+  // a split two-step launch is two kernels (frame tiles, interior tiles)
+  const ceep::Fdtd2dParams& p = pl->p;
+  const bool split = pl->side.stream && p.split2 && p.nframe2 > 0 && p.ntiles2 > p.nframe2;
+  const int64_t pairs = pl->tblock == 2 ? nsteps / 2 : 0;
+  return (nsteps - 2 * pairs) + pairs * (split ? 2 : 1);
 }
 
 // --------------------------------------------------------------------------

@@ -50,7 +50,8 @@ namespace ceep {
 // Configure (what = 0), one step (1) or two steps (2) of one ADE shape, and
 // the packed launch of one ADE shape; instantiated in fdtd2d_d<ND>l<NL>.cu.
 template <int ND, int NL>
-cudaError_t fdtd2d_dispatch_poles(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what);
+cudaError_t fdtd2d_dispatch_poles(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what,
+                                  const Fdtd2dSide* side);
 template <int ND, int NL>
 cudaError_t fdtd2d_packed_poles(int L, const PackTile* ta, int na, const PackTile* tb, int nb,
                                 const Fdtd2dParams* params, int step, int par, bool two, cudaStream_t s);
@@ -116,14 +117,15 @@ cudaError_t finite_check_launch(const float4* ez, long long nf4, const float* pr
   return cudaGetLastError();
 }
 
-static cudaError_t dispatch(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what) {
+static cudaError_t dispatch(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what,
+                            const Fdtd2dSide* side = nullptr) {
   switch (p.n_debye * 3 + p.n_lorentz) {
-    case 0: return fdtd2d_dispatch_poles<0, 0>(p, step, par, s, what);
-    case 1: return fdtd2d_dispatch_poles<0, 1>(p, step, par, s, what);
-    case 2: return fdtd2d_dispatch_poles<0, 2>(p, step, par, s, what);
-    case 3: return fdtd2d_dispatch_poles<1, 0>(p, step, par, s, what);
-    case 4: return fdtd2d_dispatch_poles<1, 1>(p, step, par, s, what);
-    case 6: return fdtd2d_dispatch_poles<2, 0>(p, step, par, s, what);
+    case 0: return fdtd2d_dispatch_poles<0, 0>(p, step, par, s, what, side);
+    case 1: return fdtd2d_dispatch_poles<0, 1>(p, step, par, s, what, side);
+    case 2: return fdtd2d_dispatch_poles<0, 2>(p, step, par, s, what, side);
+    case 3: return fdtd2d_dispatch_poles<1, 0>(p, step, par, s, what, side);
+    case 4: return fdtd2d_dispatch_poles<1, 1>(p, step, par, s, what, side);
+    case 6: return fdtd2d_dispatch_poles<2, 0>(p, step, par, s, what, side);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -135,9 +137,9 @@ cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStr
   return dispatch(q, step, par, s, 1);
 }
 
-cudaError_t fdtd2d_launch_step2(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
+cudaError_t fdtd2d_launch_step2(const Fdtd2dParams& p, int step, int par, cudaStream_t s, const Fdtd2dSide* side) {
   Fdtd2dParams q = p;
-  return dispatch(q, step, par, s, 2);
+  return dispatch(q, step, par, s, 2, side);
 }
 
 }  // namespace ceep

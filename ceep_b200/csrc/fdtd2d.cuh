@@ -22,6 +22,10 @@ struct Fdtd2dParams {
   int frame1[4];        // frame tile columns left/right and rows top/bottom, one-step geometry
   int frame2[4];        // the same for the two-step geometry (launch order: frame tiles first)
   int rows_fixed;       // tile height the caller asked for (0 = chosen per kernel)
+  int ntiles2;          // tiles of the two-step geometry per TX group
+  int nframe2;          // its frame tiles (the first nframe2 of the frame-first order)
+  int smem2i;           // dynamic shared memory of the interior-tile two-step kernel
+  int split2;           // run the two-step frame and interior tiles as two kernels (given a side stream; off by default)
   float db, db_dx, inv_dx, dt, inv_dt;
   // per-group strides in float4
   long long gs_field, gs_psi_x, gs_psi_y, gs_j, gs_jp;
@@ -62,6 +66,13 @@ __device__ __forceinline__ void record_status(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
+// The second stream of a split two-step launch (fdtd2d_launch_step2) and
+// the events that fork it from and join it back to the launching stream.
+struct Fdtd2dSide {
+  cudaStream_t stream;
+  cudaEvent_t fork, join;
+};
+
 // Scan Ez (nf4 float4) and probes[tx][q][steps s0..s1) for NaN/Inf; on a hit
 // record CEEP_ERR_NONFINITE in *status (first error wins).
 cudaError_t finite_check_launch(const float4* ez, long long nf4, const float* probes, int ntx, int nprobe,
@@ -91,9 +102,12 @@ int choose_rows(int nx, int ny, int groups, int cells_per_block, long slots, int
 cudaError_t fdtd2d_configure(Fdtd2dParams& p);
 // Launch one step reading buffer `par` and writing buffer `par ^ 1`.
 cudaError_t fdtd2d_launch_step(const Fdtd2dParams& p, int step, int par, cudaStream_t s);
-// Launch steps `step` and `step + 1` in one kernel (temporal block of two),
-// reading buffer `par` and writing buffer `par ^ 1` (and the adjoint's saved
-// Ez/J of both steps when the save pointers are set).
-cudaError_t fdtd2d_launch_step2(const Fdtd2dParams& p, int step, int par, cudaStream_t s);
+// Launch steps `step` and `step + 1` as one temporal block of two, reading
+// buffer `par` and writing buffer `par ^ 1` (and the adjoint's saved Ez/J of
+// both steps when the save pointers are set).  With `side` and p.split2 the
+// frame tiles run as one kernel on side->stream beside the interior tiles'
+// kernel on s (joined back to s before the call returns); otherwise one kernel.
+cudaError_t fdtd2d_launch_step2(const Fdtd2dParams& p, int step, int par, cudaStream_t s,
+                                const Fdtd2dSide* side = nullptr);
 
 }  // namespace ceep

@@ -32,17 +32,20 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;    // default bound of a wait: 
 
 CEEP_D uint64_t wait_limit(const Fdtd2dParams& p) { return p.wait_ns ? p.wait_ns : kWaitLimitNs; }
 
-template <int L, int NP, int NL>
+// One ring slot: the row slices of one row.  PSI = false is the slot of the
+// interior-tile kernel, whose blocks touch no CPML strip: its psi slices
+// shrink to one unused float4 each.
+template <int L, int NP, int NL, bool PSI = true>
 struct Stage2d {
   static constexpr int CX = kConsumers / L;
   float4 ez[(CX + 2) * L];   // cells x0-1 .. x0+CX
   float4 hx[CX * L];         // cells x0 .. x0+CX-1
   float4 hy[(CX + 1) * L];   // cells x0-1 .. x0+CX-1
   float4 coef[CX];           // ca, cb, dt/(eps_r eps0), 0
-  float4 phx[CX * L];        // H psi of the y strips (for Hx), cells x0..
-  float4 pey[CX * L];        // E psi of the y strips, cells x0..
-  float4 phy[(CX + 1) * L];  // H psi of the x strips (for Hy), cells x0-1..
-  float4 pex[CX * L];        // E psi of the x strips, cells x0..
+  float4 phx[PSI ? CX * L : 1];        // H psi of the y strips (for Hx), cells x0..
+  float4 pey[PSI ? CX * L : 1];        // E psi of the y strips, cells x0..
+  float4 phy[PSI ? (CX + 1) * L : 1];  // H psi of the x strips (for Hy), cells x0-1..
+  float4 pex[PSI ? CX * L : 1];        // E psi of the x strips, cells x0..
   float4 ade[NP > 0 ? NP * CX : 1];
   float4 j[NP > 0 ? NP * CX * L : 1];
   float4 jp[NL > 0 ? NL * CX * L : 1];
@@ -230,9 +233,9 @@ CEEP_D void record_probes(const Fdtd2dParams& p, float4 e, int x, int y, int lan
 // ------------------------------------------------------------------------
 // Producer: one thread, bulk copies of row slices into the stage ring.
 // ------------------------------------------------------------------------
-template <int L, int ND, int NL, int NS = kStages>
-CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty, int par,
-                    int x0, int y0, int y1, int rs, int nslots, int g) {
+template <int L, int ND, int NL, int NS = kStages, bool PSI = true>
+CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uint64_t* full, uint64_t* empty,
+                    int par, int x0, int y0, int y1, int rs, int nslots, int g) {
   constexpr int NP = ND + NL;
   constexpr int CX = kConsumers / L;
   const int nx = p.nx, ny = p.ny, n = p.n;
@@ -276,7 +279,7 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
     }
     const bool pro = r < y0, tail = r >= y1, body = !pro && !tail;
     const int shy = sp.hy_row(r), sey = sp.ey_row(r);
-    Stage2d<L, NP, NL>& S = st[s];
+    Stage2d<L, NP, NL, PSI>& S = st[s];
     const size_t rowc = (size_t)r * nx;
     const size_t rowp = (size_t)r * 2 * n;
     // Two passes over the same list: count the bytes, then issue the copies.
@@ -290,16 +293,16 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
       cp(S.ez + (xa - (x0 - 1)) * L, ez + (rowc + xa) * L, (xb - xa) * cb);
       if (!tail) {
         cp(S.hx + (xs - x0) * L, hx + (rowc + xs) * L, (xe - xs) * cb);
-        if (shy >= 0) cp(S.phx + (xs - x0) * L, psi_hx + ((size_t)shy * nx + xs) * L, (xe - xs) * cb);
+        if (PSI && shy >= 0) cp(S.phx + (xs - x0) * L, psi_hx + ((size_t)shy * nx + xs) * L, (xe - xs) * cb);
       }
       if (body) {
         cp(S.hy + (xa - (x0 - 1)) * L, hy + (rowc + xa) * L, (xe - xa) * cb);
         cp(S.coef + (xs - x0), coef + rowc + xs, (xe - xs) * 16u);
-        if (sey >= 0) cp(S.pey + (xs - x0) * L, psi_ezy + ((size_t)sey * nx + xs) * L, (xe - xs) * cb);
-        if (hl1 > hl0) cp(S.phy + (hl0 - (x0 - 1)) * L, psi_hy + (rowp + hl0) * L, (hl1 - hl0) * cb);
-        if (hr1 > hr0) cp(S.phy + (hr0 - (x0 - 1)) * L, psi_hy + (rowp + n + hr0 - (nx - n)) * L, (hr1 - hr0) * cb);
-        if (el1 > el0) cp(S.pex + (el0 - x0) * L, psi_ezx + (rowp + el0 - 1) * L, (el1 - el0) * cb);
-        if (er1 > er0) cp(S.pex + (er0 - x0) * L, psi_ezx + (rowp + n + er0 - (nx - n)) * L, (er1 - er0) * cb);
+        if (PSI && sey >= 0) cp(S.pey + (xs - x0) * L, psi_ezy + ((size_t)sey * nx + xs) * L, (xe - xs) * cb);
+        if (PSI && hl1 > hl0) cp(S.phy + (hl0 - (x0 - 1)) * L, psi_hy + (rowp + hl0) * L, (hl1 - hl0) * cb);
+        if (PSI && hr1 > hr0) cp(S.phy + (hr0 - (x0 - 1)) * L, psi_hy + (rowp + n + hr0 - (nx - n)) * L, (hr1 - hr0) * cb);
+        if (PSI && el1 > el0) cp(S.pex + (el0 - x0) * L, psi_ezx + (rowp + el0 - 1) * L, (el1 - el0) * cb);
+        if (PSI && er1 > er0) cp(S.pex + (er0 - x0) * L, psi_ezx + (rowp + n + er0 - (nx - n)) * L, (er1 - er0) * cb);
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
           cp(S.ade + q * CX + (xs - x0), ade + q * plane + rowc + xs, (xe - xs) * 16u);
@@ -527,6 +530,9 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS) fdtd2d_step_
 #define CEEP_STAGES2 3
 #endif
 constexpr int kStages2 = CEEP_STAGES2;
+#ifndef CEEP_MIN_BLOCKS2I
+#define CEEP_MIN_BLOCKS2I 4  // the interior-tile kernel (one or no ADE pole)
+#endif
 #ifndef CEEP_MIN_BLOCKS2
 #define CEEP_MIN_BLOCKS2 3
 #endif
@@ -538,9 +544,10 @@ struct Exch2 {
   float4 phy[kConsumers];  // x-strip psi of Hy after step A
 };
 
-template <int L, int ND, int NL>
+template <int L, int ND, int NL, bool PSI = true>
 constexpr size_t step2_smem_bytes() {
-  return kStages2 * sizeof(Stage2d<L, ND + NL, NL>) + 2 * kStages2 * sizeof(uint64_t) + 2 * sizeof(Exch2<L>) + 16;
+  return kStages2 * sizeof(Stage2d<L, ND + NL, NL, PSI>) + 2 * kStages2 * sizeof(uint64_t) + 2 * sizeof(Exch2<L>) +
+         16;
 }
 
 // Slot index and phase parity of a position in an NS-slot mbarrier ring.
@@ -558,10 +565,11 @@ struct RingPos {
 
 CEEP_D void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
 
-template <int L, bool GEN, int ND, int NL, bool PK>
-CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty,
+template <int L, bool GEN, int ND, int NL, bool PK, bool PSI = true>
+CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uint64_t* full, uint64_t* empty,
                      Exch2<L>* xr, volatile int* abort_flag, int step, int par, int x0, int y0, int y1, int ya0,
                      int ya1, int rs, int nslots, int g) {
+  static_assert(PSI || !GEN, "the general path reads the staged psi slices");
   constexpr int NP = ND + NL, NQ = NP > 0 ? NP : 1, NLQ = NL > 0 ? NL : 1;
   constexpr int CX = kConsumers / L;
   const int nx = p.nx, ny = p.ny, n = p.n;
@@ -680,8 +688,8 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
   if (ya0 > 0) {  // slot 0 holds row ya0-1: A's Hx^{n+1/2}(x, ya0-1)
     wait(up);
     if (valid && !aborted) {
-      const Stage2d<L, NP, NL>& A = st[0];
-      hxa_prev = hx_new<GEN>(p, A.phx[cx * L + lo], nullptr, x, ya0 - 1, A.hx[cx * L + lo],
+      const Stage2d<L, NP, NL, PSI>& A = st[0];
+      hxa_prev = hx_new<GEN>(p, GEN ? A.phx[cx * L + lo] : f4(0.f), nullptr, x, ya0 - 1, A.hx[cx * L + lo],
                              A.ez[(cx + 1) * L + lo], st[up.slot].ez[(cx + 1) * L + lo]);
     }
     release(cs);
@@ -712,18 +720,18 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
     // above fold away on that path.
     if (!GEN || (valid && !aborted)) {
       // step A on row r: the one-step consumer's arithmetic
-      const Stage2d<L, NP, NL>& A = st[cs];
+      const Stage2d<L, NP, NL, PSI>& A = st[cs];
       const int i0 = (cx + 1) * L + lo;
       const float4 ez_c = A.ez[i0];
       const float4 ez_up = has_up ? st[up.slot].ez[i0] : f4(0.f);
       bool sx, sy2, dummy;
-      c_phx = A.phx[cx * L + lo];
+      c_phx = GEN ? A.phx[cx * L + lo] : f4(0.f);  // psi slices: general path only
       const float4 hxn = hx_step<GEN>(p, x, r, A.hx[cx * L + lo], ez_c, ez_up, c_phx, sx);
-      a_phy = A.phy[i0];
+      a_phy = GEN ? A.phy[i0] : f4(0.f);
       const float4 hyn = hy_step<GEN>(p, x, r, A.hy[i0], ez_c, A.ez[i0 + L], a_phy, sy2);
       float4 hyl = f4(0.f);
       if (!GEN || x >= 1) {
-        float4 pl = A.phy[i0 - L];
+        float4 pl = GEN ? A.phy[i0 - L] : f4(0.f);
         hyl = hy_step<GEN>(p, x - 1, r, A.hy[i0 - L], A.ez[i0 - L], ez_c, pl, dummy);
       }
 #pragma unroll
@@ -733,8 +741,8 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
       }
 #pragma unroll
       for (int q = 0; q < NL; ++q) jm[q] = A.jp[(q * CX + cx) * L + lo];
-      c_pex = A.pex[cx * L + lo];
-      c_pey = A.pey[cx * L + lo];
+      c_pex = GEN ? A.pex[cx * L + lo] : f4(0.f);
+      c_pey = GEN ? A.pey[cx * L + lo] : f4(0.f);
       c_cf = A.coef[cx];
       uint32_t fl;
       a_e = e_step<GEN, ND, NL>(p, x, r, ez_c, hyn - hyl, hxn - hxa_prev, c_cf, kq, jq, jm, c_pex, c_pey, fl);
@@ -801,9 +809,11 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_
 
 // One block of the two-step kernel: thread columns x0 .. x0+CX-1 (outputs
 // x0+1 .. x0+CX-2), own rows y0 .. y0+rows2-1, TX group g.
-template <int L, int ND, int NL, bool PK>
+// INT: a block of the interior-tile kernel (a tile that touches no strip or
+// edge; slots without psi slices, interior code only).
+template <int L, int ND, int NL, bool PK, bool INT = false>
 CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
-  using St = Stage2d<L, ND + NL, NL>;
+  using St = Stage2d<L, ND + NL, NL, !INT>;
   constexpr int CX = kConsumers / L;
   St* st = reinterpret_cast<St*>(smem_raw);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages2 * sizeof(St));
@@ -830,15 +840,23 @@ CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0
   asm volatile("griddepcontrol.wait;" ::: "memory");
 
   if (threadIdx.x >= kConsumers) {
-    if (threadIdx.x == kConsumers) produce<L, ND, NL, kStages2>(p, st, full, empty, par, x0, ya0, ya1, rs, nslots, g);
+    if (threadIdx.x == kConsumers)
+      produce<L, ND, NL, kStages2, !INT>(p, st, full, empty, par, x0, ya0, ya1, rs, nslots, g);
     return;
   }
-  const int m = n > 1 ? n : 1;
-  const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
-  if (interior)
-    consume2<L, false, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
-  else
-    consume2<L, true, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots, g);
+  if constexpr (INT) {
+    consume2<L, false, ND, NL, PK, false>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs,
+                                          nslots, g);
+  } else {
+    const int m = n > 1 ? n : 1;
+    const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
+    if (interior)
+      consume2<L, false, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots,
+                                     g);
+    else
+      consume2<L, true, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots,
+                                    g);
+  }
 }
 
 template <int L, int ND, int NL>
@@ -852,6 +870,26 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   tile_frame_first(blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.frame2[0], p.frame2[1],
                    p.frame2[2], p.frame2[3], bx, by);
   step2_block<L, ND, NL, false>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
+}
+
+// The interior tiles of a split two-step launch (tiles nframe2 .. of the
+// frame-first order; fdtd2d_step2_kernel runs tiles 0 .. nframe2-1 beside it
+// on another stream).  Without the strip code and the psi slices a block
+// needs fewer registers and less shared memory, so four blocks share an SM
+// (three with two ADE poles) against three of the general kernel.  Not the
+// default: while the long frame blocks run, an SM holding one of them has
+// room for only two interior blocks, and the two kernels' step boundary is a
+// full join without programmatic dependent launch; on the 600^2 x 16 head
+// the split launch measured 31.5 us per step against 29.7 for one kernel.
+template <int L, int ND, int NL>
+__global__ void __launch_bounds__(kConsumers + 32, ND + NL >= 2 ? CEEP_MIN_BLOCKS2 : CEEP_MIN_BLOCKS2I)
+    fdtd2d_step2i_kernel(const Fdtd2dParams p, int step, int par) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int CX = kConsumers / L;
+  int bx, by;
+  tile_frame_first(p.nframe2 + (int)blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2,
+                   p.frame2[0], p.frame2[1], p.frame2[2], p.frame2[3], bx, by);
+  step2_block<L, ND, NL, false, true>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
 }
 
 // Many phantoms, two steps per launch: block b runs two-step tile
@@ -954,13 +992,48 @@ static cudaError_t configure2_l(Fdtd2dParams& p) {
                              : choose_rows(p.nx, p.ny, p.groups, kConsumers / L - 2,
                                            (long)sms * (per_sm < 1 ? 1 : per_sm), 62);
   frame_counts(p, kConsumers / L, kConsumers / L - 2, -1, p.rows2, true, p.frame2);
+  // the interior-tile kernel of a split launch, and the frame tile count
+  constexpr size_t smem_i = step2_smem_bytes<L, ND, NL, false>();
+  e = cudaFuncSetAttribute(fdtd2d_step2i_kernel<L, ND, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_i);
+  if (e != cudaSuccess) return e;
+  p.smem2i = (int)smem_i;
+  constexpr int CX = kConsumers / L;
+  const int gx = (p.nx + CX - 3) / (CX - 2), gy = (p.ny + p.rows2 - 1) / p.rows2;
+  const int ic = gx - p.frame2[0] - p.frame2[1], ir = gy - p.frame2[2] - p.frame2[3];
+  p.ntiles2 = gx * gy;
+  p.nframe2 = gx * gy - (ic > 0 && ir > 0 ? ic * ir : 0);
   return cudaSuccess;
 }
 
+// Two steps.  Split (a side stream given, p.split2 set, both kinds of tile
+// present): the frame tiles run as fdtd2d_step2_kernel on the side stream
+// (forked from and joined back to s) beside the interior tiles as
+// fdtd2d_step2i_kernel on s; both read the state of [par] and write disjoint
+// tiles of [par^1].  Otherwise one launch of every tile, with programmatic
+// dependent launch on the previous step.
 template <int L, int ND, int NL>
-static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s) {
+static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s, const Fdtd2dSide* side) {
   constexpr int CX = kConsumers / L;
-  dim3 grid(((p.nx + CX - 3) / (CX - 2)) * ((p.ny + p.rows2 - 1) / p.rows2), 1, p.groups);
+  const int ntiles = p.ntiles2, ninterior = ntiles - p.nframe2;
+  if (side && p.split2 && p.nframe2 > 0 && ninterior > 0) {
+    cudaError_t e;
+    if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(side->stream, side->fork, 0)) != cudaSuccess) return e;
+    cudaLaunchConfig_t cf = {};
+    cf.gridDim = dim3(p.nframe2, 1, p.groups);
+    cf.blockDim = dim3(kConsumers + 32);
+    cf.dynamicSmemBytes = p.smem2;
+    cf.stream = side->stream;
+    if ((e = cudaLaunchKernelEx(&cf, fdtd2d_step2_kernel<L, ND, NL>, p, step, par)) != cudaSuccess) return e;
+    cudaLaunchConfig_t ci = cf;
+    ci.gridDim = dim3(ninterior, 1, p.groups);
+    ci.dynamicSmemBytes = p.smem2i;
+    ci.stream = s;
+    if ((e = cudaLaunchKernelEx(&ci, fdtd2d_step2i_kernel<L, ND, NL>, p, step, par)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(side->join, side->stream)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(s, side->join, 0);
+  }
+  dim3 grid(ntiles, 1, p.groups);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(kConsumers + 32);
@@ -1031,21 +1104,22 @@ cudaError_t fdtd2d_packed_poles(int L, const PackTile* ta, int na, const PackTil
 
 // what: 0 = configure, 1 = one step, 2 = two steps
 template <int L, int ND, int NL>
-static cudaError_t act_l(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what) {
+static cudaError_t act_l(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what, const Fdtd2dSide* side) {
   if (what == 0) {
     cudaError_t e = configure_l<L, ND, NL>(p);
     return e != cudaSuccess ? e : configure2_l<L, ND, NL>(p);
   }
-  return what == 1 ? launch_l<L, ND, NL>(p, step, par, s) : launch2_l<L, ND, NL>(p, step, par, s);
+  return what == 1 ? launch_l<L, ND, NL>(p, step, par, s) : launch2_l<L, ND, NL>(p, step, par, s, side);
 }
 
 template <int ND, int NL>
-cudaError_t fdtd2d_dispatch_poles(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what) {
+cudaError_t fdtd2d_dispatch_poles(Fdtd2dParams& p, int step, int par, cudaStream_t s, int what,
+                                  const Fdtd2dSide* side) {
   switch (p.L) {
-    case 1: return act_l<1, ND, NL>(p, step, par, s, what);
-    case 2: return act_l<2, ND, NL>(p, step, par, s, what);
-    case 4: return act_l<4, ND, NL>(p, step, par, s, what);
-    default: return act_l<8, ND, NL>(p, step, par, s, what);
+    case 1: return act_l<1, ND, NL>(p, step, par, s, what, side);
+    case 2: return act_l<2, ND, NL>(p, step, par, s, what, side);
+    case 4: return act_l<4, ND, NL>(p, step, par, s, what, side);
+    default: return act_l<8, ND, NL>(p, step, par, s, what, side);
   }
 }
 
@@ -1055,7 +1129,8 @@ cudaError_t fdtd2d_dispatch_poles(Fdtd2dParams& p, int step, int par, cudaStream
 // (and through them every kernel of that shape).
 #define CEEP_FDTD2D_INSTANTIATE(ND, NL)                                                                        \
   namespace ceep {                                                                                           \
-  template cudaError_t fdtd2d_dispatch_poles<ND, NL>(Fdtd2dParams&, int, int, cudaStream_t, int);             \
+  template cudaError_t fdtd2d_dispatch_poles<ND, NL>(Fdtd2dParams&, int, int, cudaStream_t, int,             \
+                                                     const Fdtd2dSide*);                                     \
   template cudaError_t fdtd2d_packed_poles<ND, NL>(int, const PackTile*, int, const PackTile*, int,           \
                                                    const Fdtd2dParams*, int, int, bool, cudaStream_t);        \
   }

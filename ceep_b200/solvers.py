@@ -110,6 +110,7 @@ class BatchedFDTD2D:
         self.rows_per_block = int(rows_per_block)
         self.use_graph = bool(use_graph)
         self.temporal_block = int(temporal_block)   # steps per kernel launch (1 or 2)
+        self.frame_split = False                     # two-step frame and interior tiles as two kernels
         self.sentinel_interval = 0                   # NaN/Inf scans between run-range ends (0: none)
         self.wait_limit_ns = 1_000_000_000           # bound of every device wait
         self._pins: Optional[PinnedMaps] = None      # page-locked map storage once built on a GPU
@@ -281,6 +282,7 @@ class BatchedFDTD2D:
     def _apply_plan_settings(self):
         h, plan = lib(), self._plan
         check(h.ceep2d_plan_set_temporal_block(plan, self.temporal_block), "ceep2d_plan_set_temporal_block")
+        check(h.ceep2d_plan_set_frame_split(plan, int(self.frame_split)), "ceep2d_plan_set_frame_split")
         check(h.ceep2d_plan_set_sentinel(plan, self.sentinel_interval), "ceep2d_plan_set_sentinel")
         check(h.ceep2d_plan_set_wait_limit(plan, self.wait_limit_ns), "ceep2d_plan_set_wait_limit")
 
@@ -345,6 +347,16 @@ class BatchedFDTD2D:
         if self._built:
             check(lib().ceep2d_plan_set_temporal_block(self._plan, self.temporal_block),
                   "ceep2d_plan_set_temporal_block")
+
+    def set_frame_split(self, on: bool) -> None:
+        """Two steps per launch as two kernels: the frame tiles on a side
+        stream beside an interior-tile kernel that runs four blocks per SM
+        (False, the default: one kernel for every tile).  Bit-identical
+        results; faster only where the interior tiles form several waves
+        (768^2 x 16 at 12-row tiles: 43.1 against 44.5 us per step)."""
+        self.frame_split = bool(on)
+        if self._built:
+            check(lib().ceep2d_plan_set_frame_split(self._plan, int(self.frame_split)), "ceep2d_plan_set_frame_split")
 
     def set_sentinel(self, interval: int) -> None:
         """NaN/Inf sentinel: scan Ez and the new probe samples every

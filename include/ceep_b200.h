@@ -107,6 +107,12 @@ int ceep2d_launches_per_step(const ceep2d_plan* plan);
  * A new plan uses 1; the Python solver sets 2. */
 int ceep2d_plan_set_temporal_block(ceep2d_plan* plan, int steps);
 int ceep2d_plan_temporal_block(const ceep2d_plan* plan);
+/* Two-step launches as two kernels (1): the frame tiles (CPML strips, grid
+ * edges) on a high-priority stream of the plan beside a kernel of the
+ * interior tiles, which without the strip code and psi slices fits four
+ * blocks per SM; 0 (the default): one kernel for every tile.  Same
+ * arithmetic, bit-identical results.  No counterpart in the reference. */
+int ceep2d_plan_set_frame_split(ceep2d_plan* plan, int32_t on);
 /* Kernel launches a ceep2d_plan_run of `nsteps` steps issues (step kernels
  * only; the NaN/Inf sentinel's scans are not counted). */
 int64_t ceep2d_plan_launches(const ceep2d_plan* plan, int64_t nsteps);

@@ -299,3 +299,31 @@ def test_autotuned_tile_height_gives_the_same_bits():
     assert set(t) == {6, 9, 14} and b.rows_per_block in t
     b.run()
     assert torch.equal(a.probe_data, b.probe_data) and torch.equal(a.ez, b.ez)
+
+
+@pytest.mark.parametrize("poles, rows", [("debye", 0), ("lorentz", 6), ("none", 9)])
+def test_frame_split_gives_the_same_bits(poles, rows):
+    """Two steps per launch as a frame-tile kernel beside an interior-tile
+    kernel (the default) and as one kernel give the same probe series,
+    fields and currents, with and without ADE poles and for several tile
+    heights (an odd step count ends on a one-step launch)."""
+    from ceep_b200 import BatchedFDTD2D
+    nx, ny, T = 200, 176, 61
+    src = [(40, 40), (160, 130), (100, 88), (60, 140), (150, 30)]
+    x, y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    m = (x - 100) ** 2 + (y - 88) ** 2 <= 40 ** 2
+    runs = []
+    for split in (True, False):
+        s = BatchedFDTD2D(nx, ny, 0.5e-3, T, 12, src, src, 2e9, rows_per_block=rows)
+        s._eps_r[m], s._sigma_e[m] = 12.0, 0.4
+        if poles == "debye":
+            s.set_dispersion(debye=[(np.where(m, 20.0, 0.0), np.where(m, 8e-12, 0.0))])
+        elif poles == "lorentz":
+            s.set_dispersion(lorentz=[(np.where(m, 3.0, 0.0), np.where(m, 2 * np.pi * 3e9, 0.0),
+                                       np.where(m, 1e9, 0.0))])
+        s.set_frame_split(split)
+        s.run()
+        runs.append(s)
+    a, b = runs
+    assert torch.equal(a.probe_data, b.probe_data) and torch.equal(a.ez, b.ez)
+    assert torch.equal(a.hx, b.hx) and torch.equal(a.hy, b.hy)
