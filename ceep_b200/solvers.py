@@ -61,7 +61,10 @@ class PinnedMaps:
             t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
             self._bufs[key] = t
         out = t.numpy()
-        np.copyto(out, np.broadcast_to(a, shape))
+        if a.shape == shape and a.flags.c_contiguous:
+            t.copy_(torch.from_numpy(a))    # a full map: torch's copy runs on several host threads
+        else:
+            np.copyto(out, np.broadcast_to(a, shape))
         return out
 
 
