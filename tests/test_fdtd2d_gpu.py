@@ -327,3 +327,5 @@ def test_frame_split_gives_the_same_bits(poles, rows):
     a, b = runs
     assert torch.equal(a.probe_data, b.probe_data) and torch.equal(a.ez, b.ez)
     assert torch.equal(a.hx, b.hx) and torch.equal(a.hy, b.hy)
+    # kernel launches: two per two-step launch when split, plus the last single step
+    assert a.launches(T) == 2 * (T // 2) + T % 2 and b.launches(T) == T // 2 + T % 2
