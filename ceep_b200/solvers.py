@@ -68,6 +68,17 @@ class PinnedMaps:
         return out
 
 
+def fill_map(dst: np.ndarray, src) -> None:
+    """``dst[:] = src``; a full C-contiguous FP64 map of dst's shape goes
+    through torch's multithreaded host copy (a 600x600 map: 0.33 -> 0.10 ms)."""
+    a = np.asarray(src)
+    if (a.dtype == np.float64 and a.shape == dst.shape and a.flags.c_contiguous and dst.flags.c_contiguous
+            and dst.flags.writeable):
+        torch.from_numpy(dst).copy_(torch.from_numpy(a))
+    else:
+        dst[:] = a
+
+
 class FDTDStatusError(RuntimeError):
     """A device status word reported a failure: CEEP_ERR_TIMEOUT (4, a bounded
     wait ran out) or CEEP_ERR_NONFINITE (5, the sentinel found NaN/Inf)."""
@@ -155,8 +166,8 @@ class BatchedFDTD2D:
         sets the ADE poles as well."""
         if hasattr(phantom, "get_eps_map"):
             eps_r, sigma_e = phantom.get_eps_map(self.frequency)
-            self._eps_r[:] = eps_r
-            self._sigma_e[:] = sigma_e
+            fill_map(self._eps_r, eps_r)
+            fill_map(self._sigma_e, sigma_e)
         elif hasattr(phantom, "get_permittivity_map"):
             eps_real, eps_imag = phantom.get_permittivity_map(self.frequency)
             self._eps_r[:] = eps_real
