@@ -565,7 +565,9 @@ struct RingPos {
 
 CEEP_D void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
 
-template <int L, bool GEN, int ND, int NL, bool PK, bool PSI = true>
+// RR = false: a block none of whose rows holds a source or a probe, in a run
+// that saves nothing for the adjoint (the loop compiles without those paths).
+template <int L, bool GEN, int ND, int NL, bool PK, bool PSI = true, bool RR = true>
 CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uint64_t* full, uint64_t* empty,
                      Exch2<L>* xr, volatile int* abort_flag, int step, int par, int x0, int y0, int y1, int ya0,
                      int ya1, int rs, int nslots, int g) {
@@ -594,7 +596,7 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
 
   // source/probe rows among A's rows [ya0, ya1) (<= 64) as bit masks
   uint64_t src_rows = 0, prb_rows = 0;
-  for (int y = ya0; y < ya1; ++y) {
+  for (int y = ya0; RR && y < ya1; ++y) {
     const uint8_t f = __ldg(p.row_flags + y);
     if (f & 1) src_rows |= 1ull << (y - ya0);
     if (f & 2) prb_rows |= 1ull << (y - ya0);
@@ -664,17 +666,17 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
       for (int q = 0; q < NP; ++q) {
         const size_t ja = (q * plane + (size_t)y * nx + x) * L + lo;
         st4(J + ja, jq[q]);
-        if (q < ND && p.save_j) st4(save_j_slot(p, step + 2, g) + ja, jq[q]);
+        if (RR && q < ND && p.save_j) st4(save_j_slot(p, step + 2, g) + ja, jq[q]);
       }
 #pragma unroll
       for (int q = 0; q < NL; ++q) st4(Jp + (q * plane + (size_t)y * nx + x) * L + lo, jm[q]);
     }
     if (fl & kEX) st4(psi_ezx + ((size_t)y * 2 * n + ex_s) * L + lo, pex);
     if (fl & kEY) st4(psi_ezy + ((size_t)sp.ey_row(y) * nx + x) * L + lo, pey);
-    if (PK ? (src_rows >> (y - ya0)) & 1 : src_row) add_sources(p, e2, x, y, lane_g, step + 1);
-    if (PK ? (prb_rows >> (y - ya0)) & 1 : prb_row) record_probes(p, e2, x, y, lane_g, step + 1);
+    if (RR && (PK ? (src_rows >> (y - ya0)) & 1 : src_row)) add_sources(p, e2, x, y, lane_g, step + 1);
+    if (RR && (PK ? (prb_rows >> (y - ya0)) & 1 : prb_row)) record_probes(p, e2, x, y, lane_g, step + 1);
     st4(ezw + at, e2);
-    if (p.save_ez) st4(save_ez_slot(p, step + 2, g) + at, e2);
+    if (RR && p.save_ez) st4(save_ez_slot(p, step + 2, g) + at, e2);
     hxb_prev = hxb;
   };
 
@@ -746,10 +748,10 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
       c_cf = A.coef[cx];
       uint32_t fl;
       a_e = e_step<GEN, ND, NL>(p, x, r, ez_c, hyn - hyl, hxn - hxa_prev, c_cf, kq, jq, jm, c_pex, c_pey, fl);
-      if (PK ? (src_rows >> (r - ya0)) & 1 : srcm & 1) add_sources(p, a_e, x, r, lane_g, step);
+      if (RR && (PK ? (src_rows >> (r - ya0)) & 1 : srcm & 1)) add_sources(p, a_e, x, r, lane_g, step);
       if (own && !aborted && r >= y0 && r < y1) {
-        if (PK ? (prb_rows >> (r - ya0)) & 1 : prbm & 1) record_probes(p, a_e, x, r, lane_g, step);
-        if (p.save_ez) {  // the adjoint's copy of step n+1 (own cells)
+        if (RR && (PK ? (prb_rows >> (r - ya0)) & 1 : prbm & 1)) record_probes(p, a_e, x, r, lane_g, step);
+        if (RR && p.save_ez) {  // the adjoint's copy of step n+1 (own cells)
           const size_t at = ((size_t)r * nx + x) * L + lo;
           st4(save_ez_slot(p, step + 1, g) + at, a_e);
           if (NP > 0 && p.save_j && (fl & kF9)) {
@@ -850,7 +852,14 @@ CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0
   } else {
     const int m = n > 1 ? n : 1;
     const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
-    if (interior)
+    // an interior block of the single-grid kernel with no source/probe row and
+    // no adjoint save runs a loop without those paths (smaller code)
+    bool rare = PK || p.save_ez != nullptr;
+    for (int y = ya0; !rare && y < ya1; ++y) rare = (__ldg(p.row_flags + y) & 3) != 0;
+    if (interior && !rare)
+      consume2<L, false, ND, NL, PK, true, false>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1,
+                                                  rs, nslots, g);
+    else if (interior)
       consume2<L, false, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots,
                                      g);
     else
@@ -1013,7 +1022,6 @@ static cudaError_t configure2_l(Fdtd2dParams& p) {
 // dependent launch on the previous step.
 template <int L, int ND, int NL>
 static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStream_t s, const Fdtd2dSide* side) {
-  constexpr int CX = kConsumers / L;
   const int ntiles = p.ntiles2, ninterior = ntiles - p.nframe2;
   if (side && p.split2 && p.nframe2 > 0 && ninterior > 0) {
     cudaError_t e;
