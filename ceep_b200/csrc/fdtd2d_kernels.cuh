@@ -854,7 +854,7 @@ CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0
     const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
     // an interior block of the single-grid kernel with no source/probe row and
     // no adjoint save runs a loop without those paths (smaller code)
-    bool rare = PK || p.save_ez != nullptr;
+    bool rare = p.save_ez != nullptr;
     for (int y = ya0; !rare && y < ya1; ++y) rare = (__ldg(p.row_flags + y) & 3) != 0;
     if (interior && !rare)
       consume2<L, false, ND, NL, PK, true, false>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1,
