@@ -53,6 +53,7 @@ _SIGS = {
     "ceep2d_launches_per_step": (C.c_int, [P]),
     "ceep2d_plan_set_temporal_block": (C.c_int, [P, C.c_int]),
     "ceep2d_plan_set_frame_split": (C.c_int, [P, I32]),
+    "ceep2d_material_coefficients": (C.c_int, [P, P, P, I32, I32, I32, I32, C.c_double, C.c_double, P, P, P]),
     "ceep2d_plan_temporal_block": (C.c_int, [P]),
     "ceep2d_plan_launches": (I64, [P, I64]),
     "ceep2d_plan_set_sentinel": (C.c_int, [P, I32]),

@@ -24,7 +24,7 @@ LIB = os.path.join(OUT_DIR, "libceep_b200.so")
 FDTD2D_SHAPES = ["fdtd2d_d0l0.cu", "fdtd2d_d0l1.cu", "fdtd2d_d0l2.cu", "fdtd2d_d1l0.cu", "fdtd2d_d1l1.cu",
                  "fdtd2d_d2l0.cu"]
 SOURCES = ["capi.cu", "fdtd2d.cu"] + FDTD2D_SHAPES + ["fdtd3d.cu", "adjoint2d.cu", "adjoint3d.cu", "spectral.cu",
-                                                      "phantom.cu", "single2d.cu"]
+                                                      "phantom.cu", "single2d.cu", "materials.cu"]
 HEADERS = ["common.cuh", "fdtd2d.cuh", "fdtd2d_kernels.cuh", "fdtd3d.cuh", "adjoint2d.cuh", "adjoint3d.cuh",
            "tma.cuh", "capi_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -157,6 +157,32 @@ def coefficient_tensors(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=
     return coef, ade.transpose(1, 2).float().contiguous()
 
 
+def coefficient_tensors_kernel(eps_r, sigma_e, dt: float, debye=(), lorentz=(), device=None):
+    """The maps of coefficient_tensors from one library kernel
+    (``ceep2d_material_coefficients``: the same FP64 operations in the same
+    order, no contraction, so the same bits) instead of a chain of torch
+    element-wise launches; the solver's material update uses this one."""
+    import ctypes as C
+    import torch
+    from ._lib import check, lib
+    eps = _f64(eps_r, device)
+    dev, shape = eps.device, tuple(eps.shape)
+    full = lambda a: torch.broadcast_to(_f64(a, dev), shape).contiguous()
+    sig = full(sigma_e)
+    maps = [full(a) for p in debye for a in p] + [full(a) for p in lorentz for a in p]
+    nx, ny = shape
+    npoles = len(debye) + len(lorentz)
+    coef = torch.empty((ny, nx, 4), dtype=torch.float32, device=dev)
+    ade = torch.empty((npoles, ny, nx, 4), dtype=torch.float32, device=dev)
+    ptrs = (C.c_void_p * max(1, len(maps)))(*[m.data_ptr() for m in maps])
+    check(lib().ceep2d_material_coefficients(eps.contiguous().data_ptr(), sig.data_ptr(), ptrs, len(debye),
+                                             len(lorentz), nx, ny, float(dt), EPS_0, coef.data_ptr(),
+                                             ade.data_ptr() if npoles else None,
+                                             torch.cuda.current_stream(dev).cuda_stream),
+          "ceep2d_material_coefficients")
+    return coef, ade
+
+
 def coefficient_tensors_3d(eps_r, sigma_e, mu_r, sigma_m, dt: float, debye=(), lorentz=(), device=None):
     """3D (fdtd_3d_batched.py:281-296 with the ADE eps): coef (nz, ny, nx, 4)
     float32 = (da, db, ca, cb) and ade (poles, nz, ny, nx, 4) float32 from
@@ -185,5 +211,6 @@ def dft_twiddles(frequencies, nsteps: int, dt: float) -> np.ndarray:
 
 
 __all__ = ["gaussian_derivative", "modulated_gaussian", "cpml_profile", "ade_coefficients",
-           "update_coefficients", "ade_tensors", "coefficient_tensors", "coefficient_tensors_3d", "dft_twiddles",
+           "update_coefficients", "ade_tensors", "coefficient_tensors", "coefficient_tensors_kernel",
+           "coefficient_tensors_3d", "dft_twiddles",
            "C_0", "EPS_0", "MU_0"]

@@ -508,8 +508,9 @@ class BatchedFDTD2D:
         """(nx, ny) FP64 maps -> device (ny, nx, 4) float32 (ca, cb, dt/(eps_r eps0), 0)
         and (poles, ny, nx, 4) ADE coefficients, in the kernel's (y, x) order;
         FP64 arithmetic on the device, bit-identical to the host formulas
-        (fdtd_2d_batched.py:151-167, dispersive.py:240-339)."""
-        return physics.coefficient_tensors(eps_r, sigma_e, self.dt, debye, lorentz, self.device)
+        (fdtd_2d_batched.py:151-167, dispersive.py:240-339), in one library
+        kernel (physics.coefficient_tensors is the same formula as torch ops)."""
+        return physics.coefficient_tensors_kernel(eps_r, sigma_e, self.dt, debye, lorentz, self.device)
 
     def material_tensors(self, eps_r, sigma_e, debye=(), lorentz=()):
         """Device tensors (coef, ade_coef) for the given (nx, ny) maps in this

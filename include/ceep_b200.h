@@ -488,6 +488,27 @@ int ceep_brain_phantom_2d(int32_t batch, int32_t nx, int32_t ny, double dx, cons
                           const double* tissue, const double* hem, double* eps_out, double* sigma_out,
                           double* mask_out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * 2D update coefficients from the FP64 material maps, on the device.
+ * Replaces the host-side coefficient set-up of BatchedFDTD2D
+ * (src/ceep/solvers/fdtd_2d_batched.py:151-167, the ADE coefficients of
+ * src/ceep/materials/dispersive.py:240-339) with one kernel whose FP64
+ * operations follow the host formulas' order with no contraction, so the
+ * FP32 results equal the host formulas' bit for bit.
+ *   eps_r, sigma : device (nx, ny) FP64 maps (x-major, the reference layout)
+ *   poles        : host array of device (nx, ny) FP64 maps, per Debye pole
+ *                  (delta_eps, tau), then per Lorentz pole (delta_eps,
+ *                  omega_0, delta); n_debye + n_lorentz <= 2
+ *   eps0         : the vacuum permittivity the host formulas use
+ *   coef         : device (ny, nx, 4) FP32 out: (ca, cb, dt/(eps_r eps0), 0)
+ *   ade          : device (poles, ny, nx, 4) FP32 out: Debye (k1, k2,
+ *                  (1 + k1)/2, 0), Lorentz (k1, k2, k3, 0); zero where the
+ *                  pole's tau / omega_0 is not positive
+ * ---------------------------------------------------------------------- */
+int ceep2d_material_coefficients(const double* eps_r, const double* sigma, const double* const* poles,
+                                 int32_t n_debye, int32_t n_lorentz, int32_t nx, int32_t ny, double dt,
+                                 double eps0, float* coef, float* ade, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

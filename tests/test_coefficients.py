@@ -1,4 +1,4 @@
-"""Device-side coefficient maps (physics.coefficient_tensors*) against the host
+"""Device-side coefficient maps (physics.coefficient_tensors*, the library kernel) against the host
 NumPy formulas they restate (fdtd_2d_batched.py:151-167,
 fdtd_3d_batched.py:281-296, dispersive.py:240-339): bit-identical after the
 FP32 rounding, for Debye, two-pole Lorentz, scalar and pole-free inputs."""
@@ -64,3 +64,13 @@ def test_coefficient_tensors_cpu():
 @pytest.mark.gpu
 def test_coefficient_tensors_cuda(cuda_device):
     _check(cuda_device)
+
+
+@pytest.mark.gpu
+def test_coefficient_kernel_cuda(cuda_device):
+    """The library's one-pass coefficient kernel (the solver's material path)
+    gives the host formulas' FP32 bits as well."""
+    for e, s, deb, lor in _cases_2d():
+        c0, a0 = _host_2d(e, s, deb, lor)
+        c1, a1 = physics.coefficient_tensors_kernel(e, s, DT, deb, lor, cuda_device)
+        assert np.array_equal(c0, c1.cpu().numpy()) and np.array_equal(a0, a1.cpu().numpy())
