@@ -128,7 +128,7 @@ def simulate_batch(specs: Sequence[SampleSpec], nx: int = 64, ny: int = 64, dx: 
     for b in range(len(specs)):
         s = BatchedFDTD2D(nx, ny, dx, T, cpml, pos, pos, frequency, device=str(device))
         s._build()
-        coef, _ = physics.coefficient_tensors(eps[b], sig[b], s.dt, device=s.device)
+        coef, _ = physics.coefficient_tensors_kernel(eps[b], sig[b], s.dt, device=s.device)
         s.load_material_tensors((coef, None))
         solvers.append(s)
     pk = PackedBatch2D(solvers)
