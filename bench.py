@@ -327,12 +327,23 @@ def run_ours(args, w):
 
     # config 4's gradient cost (outside the timed region, one GPU only): the
     # checkpointed adjoint at K = 50 and every step kept, against one forward
-    grad4 = None
+    grad4 = pack3 = None
     if rank == 0 and world == 1 and args.workload == "head600" and not args.no_secondary:
         t_fwd, ratios, _, _, _ = adjoint400_ratios(Ks=(1, 50), keep_budget=0, reps=2, split=False)
         grad4 = {"workload": "adjoint400 (400^2, 1000 steps, 16 TX, Debye, S misfit)",
                  "forward_ms": round(t_fwd, 3),
                  "gradient_x_forward": {f"K={k}": round(v, 3) for k, v in ratios.items()}}
+        # config 3's packed uneven batch (256 seeded phantoms, one timed run)
+        del solver
+        torch.cuda.empty_cache()
+        m = pack_measure(256, 32, 1)
+        pack3 = {"workload": "pack256 (256 phantoms 256..768^2, 600..1200 steps, 8..16 TX, 1/3 Lorentz)",
+                 "value": round(m["value"], 3), "unit": "GCell-steps/s",
+                 "roofline_frac": round(m["achieved"] / m["peak"], 3),
+                 "speedup_vs_run": round(m["value"] / m["base_fresh"], 2),
+                 "speedup_vs_replay": round(m["value"] / m["base_replay"], 2),
+                 "tile_rows": m["pk"].rows, "temporal_block": m["pk"].temporal_block}
+        del m
 
     if world > 1:
         dist.barrier()
@@ -372,6 +383,8 @@ def run_ours(args, w):
         line["cpu_baseline"] = cpu
     if grad4:
         line["config4_gradient"] = grad4
+    if pack3:
+        line["config3_packed"] = pack3
     print(json.dumps(line), flush=True)
 
 
@@ -1023,16 +1036,16 @@ def _graph_launch_gap_us(dev, stream, n=2000):
     return a.elapsed_time(b) * 1e3 / n
 
 
-def run_pack_bench(args):
-    """Config 3: aggregate GCell-steps/s of one packed, graph-replayed run of
-    all phantoms against per-phantom run() calls of the single-grid kernel."""
+def pack_measure(count, pack_sample, steps):
+    """Config 3: one packed, graph-replayed run of `count` seeded phantoms
+    (autotuned), its per-phantom baselines on a sample, and its roofline.
+    Returns the figures run_pack_bench prints."""
     import torch
     from ceep_b200.packed import PackedBatch2D
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
-    count = args.pack_count
     # baseline: per-phantom run() on a sample (fresh solver = what a caller does)
-    sample = _pack_solvers(count, dev)[:: max(1, count // args.pack_sample)]
+    sample = _pack_solvers(count, dev)[:: max(1, count // pack_sample)]
     t_fresh = t_replay = cs_sample = 0.0
     for s in sample:
         torch.cuda.synchronize()
@@ -1057,7 +1070,7 @@ def run_pack_bench(args):
     pk.advance(0, pk.max_steps, stream)          # graph capture of the full run
     torch.cuda.synchronize()
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         pk.reset()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -1078,22 +1091,35 @@ def run_pack_bench(args):
     achieved = alg / float(np.median(times)) / 1e9
     base_fresh = cs_sample / t_fresh / 1e9
     base_replay = cs_sample / t_replay / 1e9
+    out = {"value": value, "pk": pk, "timings": timings, "alg": alg, "peak": peak, "peak_src": peak_src,
+           "achieved": achieved, "launches": launches, "gap_us": gap_us, "run_s": float(np.median(times)),
+           "base_fresh": base_fresh, "base_replay": base_replay,
+           "baseline_sample": len(range(0, count, max(1, count // pack_sample)))}
+    del solvers
+    return out
+
+
+def run_pack_bench(args):
+    """Config 3: aggregate GCell-steps/s of one packed, graph-replayed run of
+    all phantoms against per-phantom run() calls of the single-grid kernel."""
+    m = pack_measure(args.pack_count, args.pack_sample, args.steps)
+    pk, value, achieved, peak = m["pk"], m["value"], m["achieved"], m["peak"]
     line = {"metric": "packed uneven batch GCell-steps/s", "value": round(value, 3), "unit": "GCell-steps/s",
             "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded phantoms)",
-            "config": {"workload": "pack256", "phantoms": count, "sizes": "256..768 step 32", "time_steps": "600..1200",
-                       "tx": "8..16", "lorentz_fraction": "1/3", "cpml": 15, "tile_rows": pk.rows,
-                       "cell_steps": pk.cell_steps},
+            "config": {"workload": "pack256", "phantoms": args.pack_count, "sizes": "256..768 step 32",
+                       "time_steps": "600..1200", "tx": "8..16", "lorentz_fraction": "1/3", "cpml": 15,
+                       "tile_rows": pk.rows, "cell_steps": pk.cell_steps},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 3), "peak_source": peak_src,
-                         "algorithmic_bytes": int(alg), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block,
+                         "frac": round(achieved / peak, 3), "peak_source": m["peak_src"],
+                         "algorithmic_bytes": int(m["alg"]), "kernel": ("fdtd2d_packed2_kernel, two steps per launch" if pk.temporal_block == 2 else "fdtd2d_packed_kernel") + " (whole run)", "temporal_block": pk.temporal_block,
                          "packing": ("concurrent class chains" if pk.packing else "interleaved") + f" ({pk.classes} classes)"},
-            "autotune_ms_per_step": {str(k): round(v, 4) for k, v in timings.items()},
-            "graph_launches": launches, "graph_launch_gap_us": round(gap_us, 3),
-            "launch_gap_share": round(launches * gap_us * 1e-6 / float(np.median(times)), 5),
-            "per_phantom_run_gcells": round(base_fresh, 3), "per_phantom_replay_gcells": round(base_replay, 3),
-            "speedup_vs_run": round(value / base_fresh, 2), "speedup_vs_replay": round(value / base_replay, 2),
-            "baseline_sample": len(range(0, count, max(1, count // args.pack_sample)))}
+            "autotune_ms_per_step": {str(k): round(v, 4) for k, v in m["timings"].items()},
+            "graph_launches": m["launches"], "graph_launch_gap_us": round(m["gap_us"], 3),
+            "launch_gap_share": round(m["launches"] * m["gap_us"] * 1e-6 / m["run_s"], 5),
+            "per_phantom_run_gcells": round(m["base_fresh"], 3), "per_phantom_replay_gcells": round(m["base_replay"], 3),
+            "speedup_vs_run": round(value / m["base_fresh"], 2), "speedup_vs_replay": round(value / m["base_replay"], 2),
+            "baseline_sample": m["baseline_sample"]}
     print(json.dumps(line), flush=True)
 
 
@@ -1191,7 +1217,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="2D: keep the automatic tile height")
     ap.add_argument("--rows", type=int, default=0, help="--profile of a 2D workload: this tile height")
     ap.add_argument("--no-secondary", action="store_true",
-                    help="head600: skip the config-4 gradient-cost figure added to the line")
+                    help="head600: skip the config-3 packed-batch and config-4 gradient-cost figures added to the line")
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N fused steps of one sample (for ncu), no timing, no JSON")
