@@ -423,25 +423,30 @@ def run_e2e(w, phantoms, pos, freqs, device, tblock=1, rows=0):
                                rows_per_block=rows)   # the tile height the device-timed run tuned
     half = 0.07 if three else 0.09
     phantoms = [None if ph is None else _HostMaps(ph) for ph in phantoms]
-    if phantoms[0] is not None:
-        solver.set_phantom(phantoms[0])
-    solver.run()  # builds and captures the graph once
-    solver.s_matrix()
-    torch.cuda.synchronize()
-    h2d = d2h = 0
-    times = []
-    for ph in phantoms:
-        t0 = time.perf_counter()
+
+    def sample(ph):
         solver.reset()
         if ph is not None:
             solver.set_phantom(ph)
         solver.update_materials()
-        out = solver.run()
+        solver.run()
         S = solver.s_matrix()
         img = das_image(torch.as_tensor(S, dtype=torch.complex64, device=device), freqs,
                         np.asarray([p[:2] for p in pos], float) * w["dx"], w["das"], w["das"],
                         w["nx"] // 2 * w["dx"] - half, w["ny"] // 2 * w["dx"] - half, 2 * half / w["das"],
                         299_792_458.0).cpu().numpy()
+        return S, img
+
+    if phantoms[0] is not None:
+        solver.set_phantom(phantoms[0])
+    solver.run()  # builds and captures the graph once
+    sample(phantoms[0])  # one untimed pass of the whole path (first use of every kernel module)
+    torch.cuda.synchronize()
+    h2d = d2h = 0
+    times = []
+    for ph in phantoms:
+        t0 = time.perf_counter()
+        S, img = sample(ph)
         times.append(time.perf_counter() - t0)
         # FP64 maps: eps_r, sigma and 2 per Debye / 3 per Lorentz pole; S for the image
         h2d = _cells(w) * 8 * (2 + 2 * len(solver._debye) + 3 * len(solver._lorentz)) + S.size * 8
