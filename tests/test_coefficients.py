@@ -41,6 +41,12 @@ def _cases_2d():
         yield e, s, d["debye"], d["lorentz"]
     yield np.full((5, 7), 3.0), 0.2, [(10.0, 8e-12)], []
     yield np.full((5, 7), 3.0), np.zeros((5, 7)), [], []
+    # one Debye and one Lorentz pole per cell, poles absent in part of the grid
+    lph = LorentzHeadPhantom2D(64, 72, 0.5e-3, seed=6)
+    e, s = lph.get_eps_map()
+    lor = lph.get_dispersion()["lorentz"][:1]
+    de = np.where(lor[0][0] > 0, 12.0, 0.0)
+    yield e, s, [(de, np.where(de > 0, 7e-12, 0.0))], lor
 
 
 def _check(device):
