@@ -66,6 +66,21 @@ def test_spectral_entry_points_validate():
     assert h.ceep_das_workspace_bytes(64, 64, 301) > 0
 
 
+def test_material_and_plan_settings_validate():
+    """The coefficient kernel's entry point and the plan settings reject bad
+    arguments before any CUDA call."""
+    from ceep_b200 import _lib
+    h = _lib.lib()
+    assert h.ceep2d_material_coefficients(None, None, None, 0, 0, 4, 4, 1e-12, 8.85e-12, None, None, None) == 1
+    one = C.c_void_p(16)  # never dereferenced: the checks fail first
+    assert h.ceep2d_material_coefficients(one, one, None, 3, 0, 4, 4, 1e-12, 8.85e-12, one, one, None) == 1
+    assert h.ceep2d_material_coefficients(one, one, None, 1, 0, 4, 4, 1e-12, 8.85e-12, one, one, None) == 1
+    assert b"pole" in h.ceep_last_error()
+    assert h.ceep2d_material_coefficients(one, one, None, 0, 0, 0, 4, 1e-12, 8.85e-12, one, None, None) == 1
+    assert h.ceep2d_plan_set_frame_split(None, 1) == 1
+    assert h.ceep2d_adjoint_set_rows(None, 4) == 1
+
+
 @pytest.mark.parametrize("side", [65536, 65537, 46341])
 def test_image_entry_points_reject_pixel_counts_past_int(side):
     """Pixel counts are formed in 64 bits: 65536^2 (a multiple of 2^32),
