@@ -544,10 +544,27 @@ struct Exch2 {
   float4 phy[kConsumers];  // x-strip psi of Hy after step A
 };
 
+// Bytes of a two-step block's shared memory with NS ring slots of the given kind.
+template <int L, int ND, int NL, bool PSI, int NS>
+constexpr size_t step2_layout_bytes() {
+  return NS * sizeof(Stage2d<L, ND + NL, NL, PSI>) + 2 * NS * sizeof(uint64_t) + 2 * sizeof(Exch2<L>) + 16;
+}
+
+// Ring depth of interior blocks: their slots carry no psi slices, so the
+// shared memory of the general blocks' kStages2 full slots holds four of
+// theirs (one more row in flight ahead of the consumers).
+template <int L, int ND, int NL>
+constexpr int interior_stages2() {
+  return step2_layout_bytes<L, ND, NL, false, 4>() <= step2_layout_bytes<L, ND, NL, true, kStages2>() ? 4
+                                                                                                      : kStages2;
+}
+
+// Dynamic shared memory of the two-step kernel (PSI: any block may be a
+// frame block) and of the interior-tile kernel (PSI = false).
 template <int L, int ND, int NL, bool PSI = true>
 constexpr size_t step2_smem_bytes() {
-  return kStages2 * sizeof(Stage2d<L, ND + NL, NL, PSI>) + 2 * kStages2 * sizeof(uint64_t) + 2 * sizeof(Exch2<L>) +
-         16;
+  return PSI ? step2_layout_bytes<L, ND, NL, true, kStages2>()
+             : step2_layout_bytes<L, ND, NL, false, interior_stages2<L, ND, NL>()>();
 }
 
 // Slot index and phase parity of a position in an NS-slot mbarrier ring.
@@ -567,7 +584,7 @@ CEEP_D void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers
 
 // RR = false: a block none of whose rows holds a source or a probe, in a run
 // that saves nothing for the adjoint (the loop compiles without those paths).
-template <int L, bool GEN, int ND, int NL, bool PK, bool PSI = true, bool RR = true>
+template <int L, bool GEN, int ND, int NL, bool PK, bool PSI = true, bool RR = true, int NS = kStages2>
 CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uint64_t* full, uint64_t* empty,
                      Exch2<L>* xr, volatile int* abort_flag, int step, int par, int x0, int y0, int y1, int ya0,
                      int ya1, int rs, int nslots, int g) {
@@ -608,7 +625,7 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
   // Ring positions advance by one slot per row (slot index and phase carried,
   // no division by the ring depth).
   bool aborted = false;
-  auto wait = [&](RingPos<kStages2> c) {
+  auto wait = [&](RingPos<NS> c) {
     if (aborted) return;
     const bool ok = mbar_wait_bounded(&full[c.slot], c.phase, wait_limit(p));
     if (__any_sync(0xffffffffu, !ok)) {
@@ -682,7 +699,7 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
 
   // The ring position of row slice k+1 and the slot of slice k, k counting
   // the slices from 0 (row rs).
-  RingPos<kStages2> up{0, 0u};
+  RingPos<NS> up{0, 0u};
   int cs = 0;
   wait(up);
   up.advance();
@@ -809,28 +826,24 @@ CEEP_D void consume2(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, ui
   if (own && !aborted && ya1 == y1 && y1 - 1 >= y0) b_row(y1 - 1, f4(0.f), src_prev, prb_prev);
 }
 
-// One block of the two-step kernel: thread columns x0 .. x0+CX-1 (outputs
-// x0+1 .. x0+CX-2), own rows y0 .. y0+rows2-1, TX group g.
-// INT: a block of the interior-tile kernel (a tile that touches no strip or
-// edge; slots without psi slices, interior code only).
-template <int L, int ND, int NL, bool PK, bool INT = false>
-CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
-  using St = Stage2d<L, ND + NL, NL, !INT>;
-  constexpr int CX = kConsumers / L;
+// A two-step block with ring slots of one kind: PSI (a frame block: full
+// slots, kStages2 of them, the general code) or not (an interior block:
+// psi-less slots, NS of them, the interior code).
+template <int L, int ND, int NL, bool PK, bool PSI, int NS>
+CEEP_D void step2_run(const Fdtd2dParams& p, int step, int par, int x0, int y0, int y1, int ya0, int ya1,
+                      int g, unsigned char* smem_raw) {
+  using St = Stage2d<L, ND + NL, NL, PSI>;
   St* st = reinterpret_cast<St*>(smem_raw);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages2 * sizeof(St));
-  uint64_t* empty = full + kStages2;
-  Exch2<L>* xr = reinterpret_cast<Exch2<L>*>(empty + kStages2);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * sizeof(St));
+  uint64_t* empty = full + NS;
+  Exch2<L>* xr = reinterpret_cast<Exch2<L>*>(empty + NS);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(xr + 2);
-  const int ny = p.ny, n = p.n;
-  const int y1 = min(y0 + p.rows2, ny);
-  const int ya0 = y0 > 0 ? y0 - 1 : 0, ya1 = y1 < ny ? y1 + 1 : ny;  // step A's rows
   const int rs = ya0 > 0 ? ya0 - 1 : 0;
-  const int nslots = (ya1 - rs) + (ya1 < ny ? 1 : 0);
+  const int nslots = (ya1 - rs) + (ya1 < p.ny ? 1 : 0);
 
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int s = 0; s < kStages2; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kConsumers / 32);
     }
@@ -842,30 +855,48 @@ CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0
   asm volatile("griddepcontrol.wait;" ::: "memory");
 
   if (threadIdx.x >= kConsumers) {
-    if (threadIdx.x == kConsumers)
-      produce<L, ND, NL, kStages2, !INT>(p, st, full, empty, par, x0, ya0, ya1, rs, nslots, g);
+    if (threadIdx.x == kConsumers) produce<L, ND, NL, NS, PSI>(p, st, full, empty, par, x0, ya0, ya1, rs, nslots, g);
     return;
   }
-  if constexpr (INT) {
-    consume2<L, false, ND, NL, PK, false>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs,
-                                          nslots, g);
+  if constexpr (PSI) {
+    consume2<L, true, ND, NL, PK, true, true, NS>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0,
+                                                  ya1, rs, nslots, g);
   } else {
-    const int m = n > 1 ? n : 1;
-    const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m);
-    // an interior block of the single-grid kernel with no source/probe row and
-    // no adjoint save runs a loop without those paths (smaller code)
+    // a block with no source/probe row and no adjoint save runs a loop
+    // compiled without those paths (smaller code)
     bool rare = p.save_ez != nullptr;
     for (int y = ya0; !rare && y < ya1; ++y) rare = (__ldg(p.row_flags + y) & 3) != 0;
-    if (interior && !rare)
-      consume2<L, false, ND, NL, PK, true, false>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1,
-                                                  rs, nslots, g);
-    else if (interior)
-      consume2<L, false, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots,
-                                     g);
+    if (!rare)
+      consume2<L, false, ND, NL, PK, false, false, NS>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1,
+                                                       ya0, ya1, rs, nslots, g);
     else
-      consume2<L, true, ND, NL, PK>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1, ya0, ya1, rs, nslots,
-                                    g);
+      consume2<L, false, ND, NL, PK, false, true, NS>(p, st, full, empty, xr, abort_flag, step, par, x0, y0, y1,
+                                                      ya0, ya1, rs, nslots, g);
   }
+}
+
+// One block of the two-step kernel: thread columns x0 .. x0+CX-1 (outputs
+// x0+1 .. x0+CX-2), own rows y0 .. y0+rows2-1, TX group g.  Block-uniform:
+// a block whose every cell, recomputed halo H included, lies in the plain
+// interior of all regions (or any block of the interior-tile kernel, INT)
+// runs the interior code on a deeper ring of psi-less slots; the far
+// column/row is excluded too (Hy(nx-1), Hx(ny-1) are never updated and Ez
+// there is an edge).
+template <int L, int ND, int NL, bool PK, bool INT = false>
+CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
+  constexpr int CX = kConsumers / L;
+  const int ny = p.ny, n = p.n;
+  const int y1 = min(y0 + p.rows2, ny);
+  const int ya0 = y0 > 0 ? y0 - 1 : 0, ya1 = y1 < ny ? y1 + 1 : ny;  // step A's rows
+  const int m = n > 1 ? n : 1;
+  const bool interior = INT || ((x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m));
+  static_assert(step2_layout_bytes<L, ND, NL, false, interior_stages2<L, ND, NL>()>() <=
+                    step2_layout_bytes<L, ND, NL, true, kStages2>(),
+                "interior slots must fit the general blocks' shared memory");
+  if (interior)
+    step2_run<L, ND, NL, PK, false, interior_stages2<L, ND, NL>()>(p, step, par, x0, y0, y1, ya0, ya1, g, smem_raw);
+  else if constexpr (!INT)
+    step2_run<L, ND, NL, PK, true, kStages2>(p, step, par, x0, y0, y1, ya0, ya1, g, smem_raw);
 }
 
 template <int L, int ND, int NL>
