@@ -551,12 +551,14 @@ constexpr size_t step2_layout_bytes() {
 }
 
 // Ring depth of interior blocks: their slots carry no psi slices, so the
-// shared memory of the general blocks' kStages2 full slots holds four of
-// theirs (one more row in flight ahead of the consumers).
+// shared memory of the general blocks' kStages2 full slots holds four or
+// five of theirs (more rows in flight ahead of the consumers).
 template <int L, int ND, int NL>
 constexpr int interior_stages2() {
-  return step2_layout_bytes<L, ND, NL, false, 4>() <= step2_layout_bytes<L, ND, NL, true, kStages2>() ? 4
-                                                                                                      : kStages2;
+  constexpr size_t budget = step2_layout_bytes<L, ND, NL, true, kStages2>();
+  return step2_layout_bytes<L, ND, NL, false, 5>() <= budget   ? 5
+         : step2_layout_bytes<L, ND, NL, false, 4>() <= budget ? 4
+                                                               : kStages2;
 }
 
 // Dynamic shared memory of the two-step kernel (PSI: any block may be a
