@@ -24,6 +24,7 @@ struct Fdtd2dParams {
   int rows_fixed;       // tile height the caller asked for (0 = chosen per kernel)
   int ntiles2;          // tiles of the two-step geometry per TX group
   int nframe2;          // its frame tiles (the first nframe2 of the frame-first order)
+  int fpieces2;         // blocks (row pieces) per frame tile of the two-step kernel
   int smem2i;           // dynamic shared memory of the interior-tile two-step kernel
   int split2;           // run the two-step frame and interior tiles as two kernels (given a side stream; off by default)
   float db, db_dx, inv_dx, dt, inv_dt;

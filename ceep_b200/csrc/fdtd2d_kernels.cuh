@@ -885,10 +885,12 @@ CEEP_D void step2_run(const Fdtd2dParams& p, int step, int par, int x0, int y0, 
 // column/row is excluded too (Hy(nx-1), Hx(ny-1) are never updated and Ez
 // there is an edge).
 template <int L, int ND, int NL, bool PK, bool INT = false>
-CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
+CEEP_D void step2_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int rows, int g,
+                        unsigned char* smem_raw) {
   constexpr int CX = kConsumers / L;
   const int ny = p.ny, n = p.n;
-  const int y1 = min(y0 + p.rows2, ny);
+  const int y1 = min(y0 + rows, ny);
+  if (y0 >= y1) return;  // an empty piece of a short last tile row
   const int ya0 = y0 > 0 ? y0 - 1 : 0, ya1 = y1 < ny ? y1 + 1 : ny;  // step A's rows
   const int m = n > 1 ? n : 1;
   const bool interior = INT || ((x0 >= n + 1) && (x0 + CX <= p.nx - m) && (ya0 >= n + 1) && (ya1 <= ny - m));
@@ -908,10 +910,23 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2) fdtd2d_step
   // frame tiles first, then the interior row-major: neighbouring interior
   // tiles, which share halo rows and columns, run close together in time
   // (their halos hit in L2)
+  // Frame tiles run as p.fpieces2 blocks of about four rows each: a frame
+  // tile takes several times an interior tile's time, and shorter, more
+  // numerous frame blocks end sooner (the launch's last frame block sets its
+  // length on small grids).
+  const int fp = p.fpieces2;
+  const int b = (int)blockIdx.x, nfp = fp * p.nframe2;
+  const int tb = b < nfp ? b / fp : b - nfp + p.nframe2;
   int bx, by;
-  tile_frame_first(blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.frame2[0], p.frame2[1],
+  tile_frame_first(tb, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2, p.frame2[0], p.frame2[1],
                    p.frame2[2], p.frame2[3], bx, by);
-  step2_block<L, ND, NL, false>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
+  int y0 = by * p.rows2, rows = p.rows2;
+  if (b < nfp) {
+    const int piece = b % fp;
+    y0 += piece * p.rows2 / fp;
+    rows = (piece + 1) * p.rows2 / fp - piece * p.rows2 / fp;
+  }
+  step2_block<L, ND, NL, false>(p, step, par, bx * (CX - 2) - 1, y0, rows, (int)blockIdx.z, smem_raw);
 }
 
 // The interior tiles of a split two-step launch (tiles nframe2 .. of the
@@ -931,7 +946,8 @@ __global__ void __launch_bounds__(kConsumers + 32, ND + NL >= 2 ? CEEP_MIN_BLOCK
   int bx, by;
   tile_frame_first(p.nframe2 + (int)blockIdx.x, (p.nx + CX - 3) / (CX - 2), (p.ny + p.rows2 - 1) / p.rows2,
                    p.frame2[0], p.frame2[1], p.frame2[2], p.frame2[3], bx, by);
-  step2_block<L, ND, NL, false, true>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, (int)blockIdx.z, smem_raw);
+  step2_block<L, ND, NL, false, true>(p, step, par, bx * (CX - 2) - 1, by * p.rows2, p.rows2, (int)blockIdx.z,
+                                      smem_raw);
 }
 
 // Many phantoms, two steps per launch: block b runs two-step tile
@@ -950,7 +966,7 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  step2_block<L, ND, NL, true>(sp, step, par, t.x0, t.y0, t.g, smem_raw);
+  step2_block<L, ND, NL, true>(sp, step, par, t.x0, t.y0, sp.rows2, t.g, smem_raw);
 }
 
 // Many phantoms in one launch: block b runs tile tiles[b] of phantom
@@ -1043,6 +1059,9 @@ static cudaError_t configure2_l(Fdtd2dParams& p) {
   const int gx = (p.nx + CX - 3) / (CX - 2), gy = (p.ny + p.rows2 - 1) / p.rows2;
   const int ic = gx - p.frame2[0] - p.frame2[1], ir = gy - p.frame2[2] - p.frame2[3];
   p.ntiles2 = gx * gy;
+  // frame tiles as pieces of about four rows (measured at 600^2 x 16:
+  // 10-row tiles in 2 pieces, 12-row tiles in 3)
+  p.fpieces2 = p.rows2 >= 8 ? p.rows2 / 4 : 1;
   p.nframe2 = gx * gy - (ic > 0 && ir > 0 ? ic * ir : 0);
   return cudaSuccess;
 }
@@ -1061,7 +1080,7 @@ static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStrea
     if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(side->stream, side->fork, 0)) != cudaSuccess) return e;
     cudaLaunchConfig_t cf = {};
-    cf.gridDim = dim3(p.nframe2, 1, p.groups);
+    cf.gridDim = dim3(p.fpieces2 * p.nframe2, 1, p.groups);
     cf.blockDim = dim3(kConsumers + 32);
     cf.dynamicSmemBytes = p.smem2;
     cf.stream = side->stream;
@@ -1074,7 +1093,7 @@ static cudaError_t launch2_l(const Fdtd2dParams& p, int step, int par, cudaStrea
     if ((e = cudaEventRecord(side->join, side->stream)) != cudaSuccess) return e;
     return cudaStreamWaitEvent(s, side->join, 0);
   }
-  dim3 grid(ntiles, 1, p.groups);
+  dim3 grid(ntiles + (p.fpieces2 - 1) * p.nframe2, 1, p.groups);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(kConsumers + 32);

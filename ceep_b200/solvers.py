@@ -323,7 +323,7 @@ class BatchedFDTD2D:
         self._apply_plan_settings()
         self.reset()
 
-    def autotune(self, candidates=(6, 8, 10, 12, 14, 16), steps: int = 40) -> Dict[int, float]:
+    def autotune(self, candidates=(6, 8, 10, 12, 14, 16), steps: int = 100) -> Dict[int, float]:
         """Pick the tile height (rows per block) by timing `steps` graph-
         replayed steps for each candidate on this solver's grid, and keep the
         fastest; returns ms per step for each.  The results do not depend on
