@@ -325,8 +325,9 @@ class BatchedFDTD2D:
 
     def autotune(self, candidates=(6, 8, 10, 12, 14, 16), steps: int = 100) -> Dict[int, float]:
         """Pick the tile height (rows per block) by timing `steps` graph-
-        replayed steps for each candidate on this solver's grid, and keep the
-        fastest; returns ms per step for each.  The results do not depend on
+        replayed steps for each candidate on this solver's grid (two passes,
+        the faster of each), and keep the fastest; returns ms per step for
+        each.  The results do not depend on
         the tile height (the same cells, the same arithmetic); the state is
         reset afterwards.  Not in the reference: a plan-time choice of this
         framework's launch geometry."""
@@ -337,16 +338,18 @@ class BatchedFDTD2D:
         if self.temporal_block == 2 and nst > 1:
             nst -= nst % 2
         timings = {}
-        for rows in candidates:
-            self.set_rows_per_block(int(rows))
-            self.advance(0, nst, stream=stream)          # capture + warm
-            self.reset()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            self.advance(0, nst, stream=stream)
-            b.record(stream)
-            torch.cuda.synchronize(self.device)
-            timings[int(rows)] = a.elapsed_time(b) / nst
+        for _ in range(2):  # two passes over the candidates, the faster time of each kept
+            for rows in candidates:
+                self.set_rows_per_block(int(rows))
+                self.advance(0, nst, stream=stream)          # capture + warm
+                self.reset()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                self.advance(0, nst, stream=stream)
+                b.record(stream)
+                torch.cuda.synchronize(self.device)
+                ms = a.elapsed_time(b) / nst
+                timings[int(rows)] = min(ms, timings.get(int(rows), ms))
         best = min(timings, key=timings.get)
         self.set_rows_per_block(best)
         self.reset()
