@@ -612,6 +612,10 @@ extern "C" int ceep2d_adjoint_set_rows(ceep2d_adjoint* ad, int32_t rows) {
   return e == cudaSuccess ? CEEP_OK : ceep::cuda_fail(e, "adjoint2d configure");
 }
 
+#ifndef CEEP_PACK_FRAME_PIECES
+#define CEEP_PACK_FRAME_PIECES 1  // blocks per frame tile in the packed two-step tables
+#endif
+
 // --------------------------------------------------------------------------
 // Packed multi-phantom 2D launch
 // --------------------------------------------------------------------------
@@ -691,7 +695,8 @@ static int pack_layout(ceep2d_plan* const* plans, int32_t count, size_t* bytes,
       const ceep::Fdtd2dParams& p = plans[e.second]->p;
       const int cx = ceep::fdtd2d_cells_per_block(p.L) - 2;
       if (p.rows2 < 1) return fail(CEEP_ERR_INVALID, "pack: plan %d has no two-step tile height", e.second);
-      tiles2 += (size_t)((p.nx + cx - 1) / cx) * ((p.ny + p.rows2 - 1) / p.rows2) * p.groups;
+      tiles2 += ((size_t)((p.nx + cx - 1) / cx) * ((p.ny + p.rows2 - 1) / p.rows2) +
+                 (size_t)(CEEP_PACK_FRAME_PIECES - 1) * p.nframe2) * p.groups;
     }
     b += align16(tiles2 * sizeof(ceep::PackTile));
   }
@@ -753,7 +758,7 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
       for (int g = 0; g < p.groups; ++g)
         for (int by = 0; by < gy; ++by)
           for (int bx = 0; bx < gx; ++bx)
-            (is_frame(bx, by, gx, gy, p.frame1) ? tf : ti).push_back({e.second, bx * cx, by * p.rows, g});
+            (is_frame(bx, by, gx, gy, p.frame1) ? tf : ti).push_back({e.second, bx * cx, by * p.rows, g, p.rows});
       ends.push_back({p.nsteps, tf.size(), ti.size()});
     }
     pc.nf = (int)tf.size();
@@ -780,7 +785,14 @@ extern "C" int ceep2d_pack_create(ceep2d_plan* const* plans, int32_t count, void
       for (int g = 0; g < p.groups; ++g)
         for (int by = 0; by < gy; ++by)
           for (int bx = 0; bx < gx; ++bx)
-            (is_frame(bx, by, gx, gy, p.frame2) ? t2f : t2i).push_back({e.second, bx * cx - 1, by * p.rows2, g});
+            if (is_frame(bx, by, gx, gy, p.frame2)) {  // frame tiles as row pieces
+              const int fp = CEEP_PACK_FRAME_PIECES;
+              for (int k = 0; k < fp; ++k)
+                t2f.push_back({e.second, bx * cx - 1, by * p.rows2 + k * p.rows2 / fp, g,
+                               (k + 1) * p.rows2 / fp - k * p.rows2 / fp});
+            } else {
+              t2i.push_back({e.second, bx * cx - 1, by * p.rows2, g, p.rows2});
+            }
       ends2.push_back({p.nsteps, t2f.size(), t2i.size()});
     }
     pc.nf2 = (int)t2f.size();

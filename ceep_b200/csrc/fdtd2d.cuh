@@ -84,6 +84,7 @@ struct PackTile {
   int phantom;  // index into the parameter array
   int x0, y0;   // first cell column and row of the tile
   int g;        // TX group
+  int rows;     // rows of the tile (two-step tables: a frame tile's row piece)
 };
 
 // Launch one step (two steps when `two`: tiles of the two-step geometry,

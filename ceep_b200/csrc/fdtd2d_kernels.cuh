@@ -966,7 +966,7 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS2)
   int* dst = reinterpret_cast<int*>(&sp);
   for (int i = threadIdx.x; i < (int)(sizeof(Fdtd2dParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  step2_block<L, ND, NL, true>(sp, step, par, t.x0, t.y0, sp.rows2, t.g, smem_raw);
+  step2_block<L, ND, NL, true>(sp, step, par, t.x0, t.y0, t.rows, t.g, smem_raw);
 }
 
 // Many phantoms in one launch: block b runs tile tiles[b] of phantom
