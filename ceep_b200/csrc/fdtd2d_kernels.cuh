@@ -524,8 +524,10 @@ __global__ void __launch_bounds__(kConsumers + 32, CEEP_MIN_BLOCKS) fdtd2d_step_
 // before A overwrites that buffer with row r+1.  Each state word is read once
 // and written once per two steps.
 // ------------------------------------------------------------------------
-// The two-step consumer holds a row slot twice as long, so a shallower ring
-// keeps it fed and leaves shared memory for three blocks per SM.
+// Ring slots of the two-step kernel: a frame block has kStages2 full slots
+// (three leave shared memory for three blocks per SM); an interior block
+// lays the same shared memory out as interior_stages2() psi-less slots, so
+// more of its rows are in flight.
 #ifndef CEEP_STAGES2
 #define CEEP_STAGES2 3
 #endif
