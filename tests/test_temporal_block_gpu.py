@@ -16,6 +16,8 @@ CASES = [
     (200, 180, 30, 8, 10, "debye+lorentz"),  # interior tiles take the plain path
     (64, 64, 19, 12, 0, "debye"),          # no CPML
     (96, 72, 26, 4, 8, "lorentz"),
+    (300, 120, 24, 4, 8, "debye"),         # 1 float4 per cell with interior tiles (their deep ring)
+    (160, 140, 20, 40, 6, "debye"),        # 8 float4 per cell, two TX groups, interior tiles
 ]
 
 
