@@ -293,11 +293,7 @@ class Adjoint2D:
         T, L = s.total_steps, self._seglen()
         G, W = s._groups, s._gwidth
         f32 = dict(dtype=torch.float32, device=dev)
-        pair = lambda t: [torch.zeros_like(t), torch.zeros_like(t)] if t is not None else [None, None]
-        adj = {"ez": pair(s._ez[0]), "hx": pair(s._hx[0]), "hy": pair(s._hy[0]), "psi_hx": pair(s._psi_hx[0]),
-               "psi_hy": pair(s._psi_hy[0]), "psi_ezx": pair(s._psi_ezx[0]), "psi_ezy": pair(s._psi_ezy[0]),
-               "j": pair(s._j[0] if s._j is not None else None),
-               "jp": pair(s._j_prev[0] if s._j_prev is not None else None)}
+        adj = self._adjoint_state()
         nd, nl = len(s._debye), len(s._lorentz)
         kp = grad_width(nd + nl)
         grad = torch.zeros((G, s.ny, s.nx, kp), dtype=torch.float64, device=dev)
@@ -337,6 +333,32 @@ class Adjoint2D:
         # (G, ny, nx, KP) per TX group -> (2 + 3 poles, ny, nx)
         res = self._chain(grad.sum(0).permute(2, 0, 1)[:2 + 3 * (nd + nl)])
         return allreduce_gradient(res) if self.reduce_ranks else res
+
+    def _adjoint_state(self):
+        """The adjoint state, every array a ping-pong pair shaped like the
+        forward's: views of one flat buffer kept while the layout stays, zeroed
+        with one fill per backward."""
+        s = self.s
+        specs = [("ez", s._ez[0]), ("hx", s._hx[0]), ("hy", s._hy[0]), ("psi_hx", s._psi_hx[0]),
+                 ("psi_hy", s._psi_hy[0]), ("psi_ezx", s._psi_ezx[0]), ("psi_ezy", s._psi_ezy[0]),
+                 ("j", s._j[0] if s._j is not None else None),
+                 ("jp", s._j_prev[0] if s._j_prev is not None else None)]
+        key = tuple((name, None if t is None else (tuple(t.shape), t.dtype)) for name, t in specs)
+        if getattr(self, "_adj_key", None) != key:
+            total = sum(2 * t.numel() for _, t in specs if t is not None)
+            flat = torch.empty(max(total, 1), dtype=torch.float32, device=s.device)
+            bufs, off = {}, 0
+            for name, t in specs:
+                if t is None:
+                    bufs[name] = [None, None]
+                    continue
+                bufs[name] = []
+                for _ in range(2):  # every size is a multiple of 4 floats, so every view stays 16-byte aligned
+                    bufs[name].append(flat[off:off + t.numel()].view(t.shape))
+                    off += t.numel()
+            self._adj_flat, self._adj_bufs, self._adj_key = flat, bufs, key
+        self._adj_flat.zero_()
+        return self._adj_bufs
 
     def _chain(self, grad):
         """Coefficient gradients (ny, nx) -> parameter gradients (nx, ny)."""
@@ -403,13 +425,29 @@ def probes_with_grad(eps_r, sigma, adjoint: Adjoint2D, deps=None, tau=None, lore
     return FDTD2DProbes.apply(eps_r, sigma, deps, tau, adjoint, *lorentz_deps)
 
 
+_LOSS_TWIDDLES = {}  # (frequencies, T, dt, device) -> (F, T) complex128 DFT weights; a few entries
+
+
+def _loss_twiddles(frequencies, T: int, dt: float, device) -> torch.Tensor:
+    import math
+    import numpy as np
+    f = np.ascontiguousarray(np.asarray(frequencies, np.float64))
+    key = (f.tobytes(), int(T), float(dt), str(device))
+    tw = _LOSS_TWIDDLES.get(key)
+    if tw is None:
+        if len(_LOSS_TWIDDLES) >= 8:
+            _LOSS_TWIDDLES.pop(next(iter(_LOSS_TWIDDLES)))
+        w = 2.0 * math.pi * torch.as_tensor(f, dtype=torch.float64, device=device)
+        ph = w[:, None] * (torch.arange(T, dtype=torch.float64, device=device) * dt)[None, :]
+        tw = torch.complex(torch.cos(ph) * dt, -torch.sin(ph) * dt)
+        _LOSS_TWIDDLES[key] = tw
+    return tw
+
+
 def s_parameter_loss(probes: torch.Tensor, dt: float, frequencies, target: torch.Tensor):
     """L = sum |S - S*|^2 over S[f, rx, tx] = sum_n probe[tx, rx, n] e^{-j w n dt} dt
-    (the running DFT of src/ceep/solvers/dft.py:55-90); returns (L, S)."""
-    import math
-    T = probes.shape[-1]
-    w = 2.0 * math.pi * torch.as_tensor(frequencies, dtype=torch.float64, device=probes.device)
-    ph = w[:, None] * (torch.arange(T, dtype=torch.float64, device=probes.device) * dt)[None, :]
-    tw = torch.complex(torch.cos(ph) * dt, -torch.sin(ph) * dt)
+    (the running DFT of src/ceep/solvers/dft.py:55-90); returns (L, S).  The
+    DFT weights are built once per (frequencies, T, dt) and kept."""
+    tw = _loss_twiddles(frequencies, probes.shape[-1], dt, probes.device)
     S = torch.einsum("bpt,ft->fpb", probes.to(torch.complex128), tw)
     return (S - target).abs().pow(2).sum(), S
