@@ -327,7 +327,7 @@ def run_ours(args, w):
 
     # config 4's gradient cost (outside the timed region, one GPU only): the
     # checkpointed adjoint at K = 50 and every step kept, against one forward
-    grad4 = pack3 = None
+    grad4 = pack3 = fwd5 = None
     if rank == 0 and world == 1 and args.workload == "head600" and not args.no_secondary:
         t_fwd, ratios, _, _, _ = adjoint400_ratios(Ks=(1, 50), keep_budget=0, reps=2, split=False)
         grad4 = {"workload": "adjoint400 (400^2, 1000 steps, 16 TX, Debye, S misfit)",
@@ -344,6 +344,8 @@ def run_ours(args, w):
                  "speedup_vs_replay": round(m["value"] / m["base_replay"], 2),
                  "tile_rows": m["pk"].rows, "temporal_block": m["pk"].temporal_block}
         del m
+        torch.cuda.empty_cache()
+        fwd5 = head192_forward_figure()
 
     if world > 1:
         dist.barrier()
@@ -385,6 +387,8 @@ def run_ours(args, w):
         line["config4_gradient"] = grad4
     if pack3:
         line["config3_packed"] = pack3
+    if fwd5:
+        line["config5_forward"] = fwd5
     print(json.dumps(line), flush=True)
 
 
@@ -1041,6 +1045,40 @@ def _graph_launch_gap_us(dev, stream, n=2000):
     return a.elapsed_time(b) * 1e3 / n
 
 
+def head192_forward_figure():
+    """Config 5's forward on its own (the 3D Debye head, 192^3 x 8 TX x 1000
+    steps): one graph-replayed time loop, L2 flushed before it, against the
+    3D formula's compulsory bytes."""
+    import torch
+    dev = torch.device("cuda", 0)
+    w = WORKLOADS["head192"]
+    solver, _, _, phantoms, _ = build_inputs_3d(w, 1, dev)
+    stream = torch.cuda.current_stream(dev)
+    solver.advance(0, w["steps"], stream=stream)  # capture + warm
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    times = []
+    for _ in range(2):
+        flush.zero_()
+        solver.reset()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solver.advance(0, w["steps"], stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) * 1e-3)
+    t = float(min(times))
+    n_debye = len(phantoms[0].get_dispersion()["debye"])
+    peak, _ = hbm_peak()
+    bytes_step = algorithmic_bytes_per_step_3d(w, n_debye)
+    out = {"workload": "head192 forward (192^3, 1 mm, 1000 steps, 8 TX, Debye head)",
+           "value": round(w["nx"] * w["ny"] * w["nz"] * w["steps"] * w["ntx"] / t / 1e9, 3),
+           "unit": "GCell-steps/s", "ms_per_run": round(t * 1e3, 2),
+           "roofline_frac": round(bytes_step * w["steps"] / t / 1e9 / peak, 3)}
+    del solver, flush
+    torch.cuda.empty_cache()
+    return out
+
+
 def pack_measure(count, pack_sample, steps):
     """Config 3: one packed, graph-replayed run of `count` seeded phantoms
     (autotuned), its per-phantom baselines on a sample, and its roofline.
@@ -1222,7 +1260,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="2D: keep the automatic tile height")
     ap.add_argument("--rows", type=int, default=0, help="--profile of a 2D workload: this tile height")
     ap.add_argument("--no-secondary", action="store_true",
-                    help="head600: skip the config-3 packed-batch and config-4 gradient-cost figures added to the line")
+                    help="head600: skip the config-3, config-4 and config-5 figures added to the line")
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--profile", type=int, default=0,
                     help="run only N fused steps of one sample (for ncu), no timing, no JSON")
