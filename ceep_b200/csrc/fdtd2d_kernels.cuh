@@ -56,6 +56,28 @@ constexpr size_t stage_smem_bytes() {
   return kStages * sizeof(Stage2d<L, NP, NL>) + 2 * kStages * sizeof(uint64_t);
 }
 
+// Ring depth of the one-step kernel's interior blocks: their psi-less slots
+// in the shared memory of kStages full slots (more rows in flight).
+template <int L, int NP, int NL>
+constexpr int interior_stages1() {
+  constexpr size_t slot = sizeof(Stage2d<L, NP, NL, false>) + 2 * sizeof(uint64_t);
+  constexpr size_t budget = stage_smem_bytes<L, NP, NL>();
+  return 7 * slot <= budget ? 7 : 6 * slot <= budget ? 6 : 5 * slot <= budget ? 5 : kStages;
+}
+
+// Slot index and phase parity of a position in an NS-slot mbarrier ring.
+template <int NS>
+struct RingPos {
+  int slot;
+  uint32_t phase;
+  CEEP_D void advance() {
+    if (++slot == NS) {
+      slot = 0;
+      phase ^= 1u;
+    }
+  }
+};
+
 // Strip bookkeeping shared by producer and consumers.
 struct Strips {
   int n, nx, ny;
@@ -325,9 +347,10 @@ CEEP_D void produce(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uin
 // ------------------------------------------------------------------------
 // Consumer: one float4 (4 TX) of one cell per thread, walking the rows.
 // ------------------------------------------------------------------------
-template <int L, bool GEN, int ND, int NL>
-CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t* full, uint64_t* empty,
+template <int L, bool GEN, int ND, int NL, bool PSI = true, int NS = kStages>
+CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL, PSI>* st, uint64_t* full, uint64_t* empty,
                     int step, int par, int x0, int y0, int y1, int rs, int nslots, int g) {
+  static_assert(PSI || !GEN, "the general path reads the staged psi slices");
   constexpr int NP = ND + NL;
   constexpr int CX = kConsumers / L;
   const int nx = p.nx, ny = p.ny, n = p.n;
@@ -361,54 +384,60 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
   }
 
   // Warp-uniform bounded wait: if any lane gives up, the whole warp leaves.
-  auto wait = [&](int k) {
-    const bool ok = mbar_wait_bounded(&full[k % kStages], (k / kStages) & 1, wait_limit(p));
+  auto wait = [&](RingPos<NS> c) {
+    const bool ok = mbar_wait_bounded(&full[c.slot], c.phase, wait_limit(p));
     if (__any_sync(0xffffffffu, !ok)) {
       if (lane_warp == 0) record_status(p.status, CEEP_ERR_TIMEOUT);
       return false;
     }
     return true;
   };
-  auto release = [&](int k) {
+  auto release = [&](int slot) {
     __syncwarp();
-    if (lane_warp == 0) mbar_arrive(&empty[k % kStages]);
+    if (lane_warp == 0) mbar_arrive(&empty[slot]);
   };
 
-  if (!wait(0)) return;
+  // ring position of slice k+1 and the slot of slice k (k from 0 at row rs)
+  RingPos<NS> up{0, 0u};
+  int cs = 0;
+  if (!wait(up)) return;
+  up.advance();
   int k = 0;
   float4 hx_prev = f4(0.f);
   if (y0 > 0) {  // slot 0 holds row y0-1 (Ez, Hx, H psi): Hx^{n+1/2}(x, y0-1)
-    if (!wait(1)) return;
+    if (!wait(up)) return;
     if (active) {
-      const Stage2d<L, NP, NL>& A = st[0];
-      hx_prev = hx_new<GEN>(p, A.phx[cx * L + lo], nullptr, x, y0 - 1, A.hx[cx * L + lo], A.ez[(cx + 1) * L + lo],
-                            st[1 % kStages].ez[(cx + 1) * L + lo]);
+      const Stage2d<L, NP, NL, PSI>& A = st[0];
+      hx_prev = hx_new<GEN>(p, GEN ? A.phx[cx * L + lo] : f4(0.f), nullptr, x, y0 - 1, A.hx[cx * L + lo],
+                            A.ez[(cx + 1) * L + lo], st[up.slot].ez[(cx + 1) * L + lo]);
     }
-    release(0);
+    release(cs);
+    cs = up.slot;
+    up.advance();
     k = 1;
   }
 
   for (int y = y0; y < y1; ++y, ++k) {
     const bool has_up = k + 1 < nslots;
-    if (has_up && !wait(k + 1)) return;
-    const Stage2d<L, NP, NL>& A = st[k % kStages];
+    if (has_up && !wait(up)) return;
+    const Stage2d<L, NP, NL, PSI>& A = st[cs];
     if (active) {
       const int i0 = (cx + 1) * L + lo;  // this cell in the halo'd slices
       const float4 ez_c = A.ez[i0];
-      const float4 ez_up = has_up ? st[(k + 1) % kStages].ez[i0] : f4(0.f);
+      const float4 ez_up = has_up ? st[up.slot].ez[i0] : f4(0.f);
       const size_t at = ((size_t)y * nx + x) * L + lo;
       const int shy = GEN ? sp.hy_row(y) : -1;
       const int sey = GEN ? sp.ey_row(y) : -1;
 
       // H phase: this cell, plus the recomputed Hy of the left neighbour
-      const float4 hxn = hx_new<GEN>(p, A.phx[cx * L + lo],
+      const float4 hxn = hx_new<GEN>(p, GEN ? A.phx[cx * L + lo] : f4(0.f),
                                      shy >= 0 ? psi_hx_out + ((size_t)shy * nx + x) * L + lo : nullptr, x, y,
                                      A.hx[cx * L + lo], ez_c, ez_up);
-      const float4 hyn = hy_new<GEN>(p, A.phy[i0], hxs >= 0 ? psi_hy_out + ((size_t)y * 2 * n + hxs) * L + lo : nullptr,
+      const float4 hyn = hy_new<GEN>(p, GEN ? A.phy[i0] : f4(0.f), hxs >= 0 ? psi_hy_out + ((size_t)y * 2 * n + hxs) * L + lo : nullptr,
                                      x, y, A.hy[i0], ez_c, A.ez[i0 + L]);
       float4 hyl = f4(0.f);
       if (!GEN || x >= 1)
-        hyl = hy_new<GEN>(p, A.phy[i0 - L], nullptr, x - 1, y, A.hy[i0 - L], A.ez[i0 - L], ez_c);
+        hyl = hy_new<GEN>(p, GEN ? A.phy[i0 - L] : f4(0.f), nullptr, x - 1, y, A.hy[i0 - L], A.ez[i0 - L], ez_c);
       st4(hxw + at, hxn);
       st4(hyw + at, hyn);
 
@@ -422,7 +451,7 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
       }
 #pragma unroll
       for (int q = 0; q < NL; ++q) jm[q] = A.jp[(q * CX + cx) * L + lo];
-      float4 pex = A.pex[cx * L + lo], pey = A.pey[cx * L + lo];
+      float4 pex = GEN ? A.pex[cx * L + lo] : f4(0.f), pey = GEN ? A.pey[cx * L + lo] : f4(0.f);
       uint32_t fl;
       float4 e = e_step<GEN, ND, NL>(p, x, y, ez_c, hyn - hyl, hxn - hx_prev, A.coef[cx], kq, jq, jm, pex, pey, fl);
       if (NP > 0 && (fl & kF9)) {
@@ -446,28 +475,29 @@ CEEP_D void consume(const Fdtd2dParams& p, Stage2d<L, ND + NL, NL>* st, uint64_t
       if (p.save_ez) st4(p.save_ez + (size_t)(step + 1 - p.save_base) * p.groups * p.gs_field + gf + at, e);
       hx_prev = hxn;
     }
-    release(k);
+    release(cs);
+    cs = up.slot;
+    up.advance();
   }
-  if (k < nslots) release(k);  // the Ez-only slot of row y1
+  if (k < nslots) release(cs);  // the Ez-only slot of row y1
 }
 
-// One block's work for one time step: a column strip of CX cells starting at
-// x0, rows [y0, y0 + rows), TX group g.  Shared by the single-grid kernel and
-// the packed multi-phantom kernel.
-template <int L, int ND, int NL>
-CEEP_D void step_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
-  using St = Stage2d<L, ND + NL, NL>;
-  constexpr int CX = kConsumers / L;
+// One block's work for one time step with ring slots of one kind: PSI (a
+// frame block: kStages full slots, the general code) or not (an interior
+// block: NS psi-less slots in the same shared memory, the interior code).
+template <int L, int ND, int NL, bool PSI, int NS>
+CEEP_D void step_run(const Fdtd2dParams& p, int step, int par, int x0, int y0, int y1, int g,
+                     unsigned char* smem_raw) {
+  using St = Stage2d<L, ND + NL, NL, PSI>;
   St* st = reinterpret_cast<St*>(smem_raw);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * sizeof(St));
-  uint64_t* empty = full + kStages;
-  const int y1 = min(y0 + p.rows, p.ny);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * sizeof(St));
+  uint64_t* empty = full + NS;
   const int rs = y0 > 0 ? y0 - 1 : 0;
   const int nslots = (y1 - rs) + (y1 < p.ny ? 1 : 0);
 
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kConsumers / 32);
     }
@@ -483,19 +513,32 @@ CEEP_D void step_block(const Fdtd2dParams& p, int step, int par, int x0, int y0,
   asm volatile("griddepcontrol.wait;" ::: "memory");
 
   if (threadIdx.x >= kConsumers) {
-    if (threadIdx.x == kConsumers) produce<L, ND, NL>(p, st, full, empty, par, x0, y0, y1, rs, nslots, g);
+    if (threadIdx.x == kConsumers) produce<L, ND, NL, NS, PSI>(p, st, full, empty, par, x0, y0, y1, rs, nslots, g);
     return;
   }
-  const int n = p.n;
-  // Block-uniform: every owned cell (and every recomputed halo H) lies in the
-  // plain interior of all regions; the far column/row is excluded too
-  // (Hy(nx-1), Hx(ny-1) are never updated and Ez there is an edge).
-  const int m = n > 1 ? n : 1;
+  consume<L, PSI, ND, NL, PSI, NS>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+}
+
+// One block's work for one time step: a column strip of CX cells starting at
+// x0, rows [y0, y0 + rows), TX group g.  Shared by the single-grid kernel and
+// the packed multi-phantom kernel.  Block-uniform: every owned cell (and every
+// recomputed halo H) lies in the plain interior of all regions; the far
+// column/row is excluded too (Hy(nx-1), Hx(ny-1) are never updated and Ez
+// there is an edge).
+template <int L, int ND, int NL>
+CEEP_D void step_block(const Fdtd2dParams& p, int step, int par, int x0, int y0, int g, unsigned char* smem_raw) {
+  constexpr int CX = kConsumers / L;
+  const int y1 = min(y0 + p.rows, p.ny);
+  const int n = p.n, m = n > 1 ? n : 1;
   const bool interior = (x0 >= n + 1) && (x0 + CX <= p.nx - m) && (y0 >= n + 1) && (y1 <= p.ny - m);
+  constexpr int NSI = interior_stages1<L, ND + NL, NL>();
+  static_assert(NSI * (sizeof(Stage2d<L, ND + NL, NL, false>) + 2 * sizeof(uint64_t)) <=
+                    stage_smem_bytes<L, ND + NL, NL>(),
+                "interior slots must fit the general blocks' shared memory");
   if (interior)
-    consume<L, false, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+    step_run<L, ND, NL, false, NSI>(p, step, par, x0, y0, y1, g, smem_raw);
   else
-    consume<L, true, ND, NL>(p, st, full, empty, step, par, x0, y0, y1, rs, nslots, g);
+    step_run<L, ND, NL, true, kStages>(p, step, par, x0, y0, y1, g, smem_raw);
 }
 
 template <int L, int ND, int NL>
@@ -570,19 +613,6 @@ constexpr size_t step2_smem_bytes() {
   return PSI ? step2_layout_bytes<L, ND, NL, true, kStages2>()
              : step2_layout_bytes<L, ND, NL, false, interior_stages2<L, ND, NL>()>();
 }
-
-// Slot index and phase parity of a position in an NS-slot mbarrier ring.
-template <int NS>
-struct RingPos {
-  int slot;
-  uint32_t phase;
-  CEEP_D void advance() {
-    if (++slot == NS) {
-      slot = 0;
-      phase ^= 1u;
-    }
-  }
-};
 
 CEEP_D void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
 
