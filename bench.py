@@ -248,8 +248,8 @@ def run_ours(args, w):
     K, W = args.steps, args.warmup
     solver, pos, freqs, phantoms, mats = build_inputs(w, K + W, device, seed0=1000 + 97 * rank)
     tblock = args.temporal_block if w.get("dim", 2) == 2 else 1
-    if tblock != 1:
-        solver.set_temporal_block(tblock)
+    if w.get("dim", 2) == 2:
+        solver.set_temporal_block(tblock)   # the solver's own default is two steps per launch
     solver._build()
     tile_rows = None
     if w.get("dim", 2) == 2 and not args.no_autotune:
@@ -1226,7 +1226,7 @@ def run_profile(args, w):
     solver.use_graph = False
     if args.rows and w.get("dim", 2) == 2:
         solver.set_rows_per_block(args.rows)
-    if w.get("dim", 2) == 2 and args.temporal_block != 1:
+    if w.get("dim", 2) == 2:
         solver.set_temporal_block(args.temporal_block)
     solver.load_material_tensors(mats[0])
     stream = torch.cuda.current_stream(device)
