@@ -247,9 +247,7 @@ def run_ours(args, w):
     torch.cuda.set_device(device)
     K, W = args.steps, args.warmup
     solver, pos, freqs, phantoms, mats = build_inputs(w, K + W, device, seed0=1000 + 97 * rank)
-    tblock = args.temporal_block if w.get("dim", 2) == 2 else 1
-    if w.get("dim", 2) == 2:
-        solver.set_temporal_block(tblock)   # the solver's own default is two steps per launch
+    tblock = apply_temporal_block(solver, w, args.temporal_block)
     solver._build()
     tile_rows = None
     if w.get("dim", 2) == 2 and not args.no_autotune:
@@ -408,6 +406,16 @@ class _HostMaps:
 
     def get_dispersion(self):
         return self.dispersion
+
+
+def apply_temporal_block(solver, w, steps):
+    """Steps per launch for a 2D workload's solver, set explicitly whatever it
+    is (the solver's own default is two); 3D workloads run one step per
+    launch.  Returns the steps per launch in use."""
+    if w.get("dim", 2) != 2:
+        return 1
+    solver.set_temporal_block(steps)
+    return steps
 
 
 def run_e2e(w, phantoms, pos, freqs, device, tblock=1, rows=0):
@@ -1226,8 +1234,7 @@ def run_profile(args, w):
     solver.use_graph = False
     if args.rows and w.get("dim", 2) == 2:
         solver.set_rows_per_block(args.rows)
-    if w.get("dim", 2) == 2:
-        solver.set_temporal_block(args.temporal_block)
+    apply_temporal_block(solver, w, args.temporal_block)
     solver.load_material_tensors(mats[0])
     stream = torch.cuda.current_stream(device)
     solver.advance(0, min(args.profile, w["steps"]), stream=stream)

@@ -64,3 +64,24 @@ def test_reference_arm_pack():
     d = _bench("--workload", "pack256", "--pack-count", "6", "--steps", "1", "--warmup", "1", "--cpu-steps", "1")
     _check_line(d, "packed uneven batch GCell-steps/s")
     assert d["config"]["phantoms"] == 6 and d["config"]["sampled"] >= 1
+
+
+@pytest.mark.parametrize("steps", [1, 2])
+def test_temporal_block_is_always_applied(steps):
+    """`--temporal-block 1` must reach the solver even though the solver's own
+    default is two steps per launch; 3D workloads stay at one."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Solver:
+        calls = []
+
+        def set_temporal_block(self, n):
+            self.calls.append(n)
+
+    s = Solver()
+    assert bench.apply_temporal_block(s, bench.WORKLOADS["head600"], steps) == steps
+    assert s.calls == [steps]
+    s.calls.clear()
+    assert bench.apply_temporal_block(s, bench.WORKLOADS["head192"], steps) == 1
+    assert s.calls == []
